@@ -1,0 +1,196 @@
+"""ctypes binding of the CPU FP64 oracle (test infrastructure only).
+
+The oracle restates the reference's CPU algorithms for the scattering-rate
+path (see the header of each C++ file for the reference lines it follows).
+Only the tests, ``__graft_entry__.smoke`` and the CPU-baseline leg of
+``bench.py`` may import this package; the product library never uses it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+
+
+def build():
+    """Compile the oracle with its Makefile (gcc + OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_ws_reorder.restype = ctypes.c_int
+        L.orc_ws_reorder.argtypes = [ctypes.c_int, _D, _D, _I, _D, _I, _D, _D, _D]
+        L.orc_ph_diag.restype = ctypes.c_int
+        L.orc_ph_diag.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, _D,
+                                  ctypes.c_int, _D, _D]
+        L.orc_ph_velocities.restype = ctypes.c_int
+        L.orc_ph_velocities.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, ctypes.c_int,
+                                        _D, _D, _D]
+        L.orc_v3_create.restype = ctypes.c_void_p
+        L.orc_v3_create.argtypes = [ctypes.c_int] * 3 + [_D] * 5
+        L.orc_v3_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_v3_cache_d3.argtypes = [ctypes.c_void_p, _D]
+        L.orc_v3_couplings.argtypes = [ctypes.c_void_p, ctypes.c_int] + [_D] * 7
+        L.orc_symmetrize_coupling.argtypes = [_D, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D,
+                                              _D]
+        L.orc_ph_linewidths.restype = ctypes.c_int
+        L.orc_ph_linewidths.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _D, _D, _D, _D, _D,
+                                        ctypes.c_int, _D, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_int, _I, ctypes.c_int, _D]
+        L.orc_rta_kappa.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, ctypes.c_long,
+                                    ctypes.c_double, _D]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _p(a):
+    return a.ctypes.data_as(_D)
+
+
+def ws_reorder(crystal, fc):
+    """ASR "simple" + Wigner-Seitz reorder -> (R (nR,3), w (nR,), mat2R (nR,nb,nb))."""
+    L = lib()
+    nat = crystal.num_atoms
+    cell = _d(crystal.direct_cell)
+    pos = _d(crystal.positions)
+    grid = np.ascontiguousarray(fc.shape[2:5], dtype=np.int32)
+    fcc = _d(fc)
+    n = ctypes.c_int(0)
+    rc = L.orc_ws_reorder(nat, _p(cell), _p(pos), grid.ctypes.data_as(_I), _p(fcc),
+                          ctypes.byref(n), None, None, None)
+    if rc:
+        raise RuntimeError("orc_ws_reorder failed: %d" % rc)
+    nR = n.value
+    nb = 3 * nat
+    R = np.zeros((nR, 3))
+    w = np.zeros(nR)
+    M = np.zeros((nR, nb, nb))
+    rc = L.orc_ws_reorder(nat, _p(cell), _p(pos), grid.ctypes.data_as(_I), _p(fcc),
+                          ctypes.byref(n), _p(R), _p(w), _p(M))
+    if rc:
+        raise RuntimeError("orc_ws_reorder failed: %d" % rc)
+    return R, w, M
+
+
+class PhononH0:
+    """Oracle harmonic Hamiltonian (CPU path of PhononH0)."""
+
+    def __init__(self, crystal, fc):
+        self.crystal = crystal
+        self.R, self.w, self.mat2R = ws_reorder(crystal, fc)
+        self.nb = crystal.num_bands
+        self.masses = _d(np.repeat(crystal.atomic_masses, 3))
+
+    def diagonalize(self, q_cart, mass_scaling=True):
+        q = _d(np.atleast_2d(q_cart))
+        nq = q.shape[0]
+        E = np.zeros((nq, self.nb))
+        U = np.zeros((nq, self.nb, self.nb, 2))
+        rc = lib().orc_ph_diag(self.nb, len(self.w), _p(self.R), _p(self.w), _p(self.mat2R),
+                               _p(self.masses), nq, _p(q), int(mass_scaling), _p(E), _p(U))
+        if rc:
+            raise RuntimeError("oracle eigensolver failed")
+        return E, U[..., 0] + 1j * U[..., 1]
+
+    def velocities(self, q_cart, full=False):
+        q = _d(np.atleast_2d(q_cart))
+        nq = q.shape[0]
+        vg = np.zeros((nq, self.nb, 3))
+        vf = np.zeros((nq, self.nb, self.nb, 3, 2)) if full else None
+        rc = lib().orc_ph_velocities(self.nb, len(self.w), _p(self.R), _p(self.w),
+                                     _p(self.mat2R), _p(self.masses), nq, _p(q), _p(vg),
+                                     _p(vf) if full else None)
+        if rc:
+            raise RuntimeError("oracle eigensolver failed")
+        if full:
+            return vg, vf[..., 0] + 1j * vf[..., 1]
+        return vg
+
+
+def _c(a):
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    return a.view(np.float64)
+
+
+class Interaction3Ph:
+    """Oracle 3-phonon vertex (Interaction3Ph CPU restatement)."""
+
+    def __init__(self, crystal, fc3):
+        self.nat = crystal.num_atoms
+        self.nb = 3 * self.nat
+        self._keep = [_d(fc3.D3), _d(fc3.R2), _d(fc3.R3), _d(fc3.w2), _d(fc3.w3)]
+        nr3, nr2 = fc3.D3.shape[3], fc3.D3.shape[4]
+        self.h = lib().orc_v3_create(self.nat, nr2, nr3, *[_p(x) for x in self._keep])
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_v3_destroy(self.h)
+            self.h = None
+
+    def cache_d3(self, q2):
+        q = _d(q2)
+        lib().orc_v3_cache_d3(self.h, _p(q))
+
+    def couplings_squared(self, q1s, ev1s, ev2, ev3p, ev3m):
+        q1s = _d(np.atleast_2d(q1s))
+        nq1 = q1s.shape[0]
+        nb = self.nb
+        e1, e2, e3p, e3m = _c(ev1s), _c(ev2), _c(ev3p), _c(ev3m)
+        outP = np.zeros((nq1, nb, nb, nb))
+        outM = np.zeros((nq1, nb, nb, nb))
+        lib().orc_v3_couplings(self.h, nq1, _p(q1s), _p(e1), _p(e2), _p(e3p), _p(e3m), _p(outP),
+                               _p(outM))
+        return outP, outM
+
+    def linewidths(self, mesh, E, ev, vg, qcart, recip, temps_ry, smearing, sigma,
+                   q2_list=None, finalize=True, out=None):
+        nq, nb = E.shape
+        m = np.ascontiguousarray(mesh, dtype=np.int32)
+        T = _d(temps_ry)
+        nT = len(T)
+        if out is None:
+            out = np.zeros((nT, nq * nb))
+        Ed, evd, vgd, qd, rd = _d(E), _c(ev), _d(vg), _d(qcart), _d(recip)
+        if q2_list is None:
+            nq2, ql = nq, None
+        else:
+            ql_arr = np.ascontiguousarray(q2_list, dtype=np.int32)
+            nq2, ql = len(ql_arr), ql_arr.ctypes.data_as(_I)
+        rc = lib().orc_ph_linewidths(self.h, nq, m.ctypes.data_as(_I), _p(Ed), _p(evd), _p(vgd),
+                                     _p(qd), _p(rd), nT, _p(T), 0 if smearing == "gaussian" else 1,
+                                     float(sigma), nq2, ql, int(finalize), _p(out))
+        if rc:
+            raise RuntimeError("oracle linewidth builder failed: %d" % rc)
+        return out
+
+
+def symmetrize_coupling(c, e1, e2, e3):
+    c = _d(c).copy()
+    nb1, nb2, nb3 = c.shape
+    lib().orc_symmetrize_coupling(_p(c), nb1, nb2, nb3, _p(_d(e1)), _p(_d(e2)), _p(_d(e3)))
+    return c
+
+
+def rta_kappa(E, vg, Aout, temps_ry, nqmesh, volume):
+    ns = E.size
+    T = _d(temps_ry)
+    kappa = np.zeros((len(T), 3, 3))
+    lib().orc_rta_kappa(ns, len(T), _p(T), _p(_d(E)), _p(_d(vg)), _p(_d(Aout)), int(nqmesh),
+                        float(volume), _p(kappa))
+    return kappa

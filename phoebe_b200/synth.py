@@ -1,0 +1,322 @@
+"""Seeded synthetic force constants with the shapes of the benchmark workloads.
+
+No reference generator exists: the reference reads DFT force constants from
+files (QE ``.fc`` for FC2, src/parser/qe_input_parser.cpp:385-560; ShengBTE
+``FORCE_CONSTANTS_3RD`` for FC3, src/parser/ifc3_parser.cpp:648-840).  This
+module produces arrays in exactly those in-memory layouts:
+
+* FC2 as ``forceConstants(3,3,n1,n2,n3,nat,nat)`` in Ry/Bohr^2, element
+  (i,j,m,na,nb) = Phi_ij(atom na in cell R_m; atom nb in cell 0);
+* FC3 as the dense ``D3(nb,nb,nb,nr3,nr2)`` tensor in Ry/Bohr^3 with the list
+  of distinct second/third cell vectors (Bohr) and unit weights, as the
+  ShengBTE reader builds it.
+
+Randomness comes from a counter-based generator (splitmix64 -> uniform in
+(0,1] -> Box-Muller, FP64) so every consumer regenerates identical inputs.
+"""
+from dataclasses import dataclass
+import itertools
+
+import numpy as np
+
+from . import constants as C
+from .lattice import Crystal
+
+_M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
+SEED_BASE = 0x5048584B00000000
+
+
+def _splitmix64(x):
+    x = (x + np.uint64(0x9E3779B97F4A7C15)) & _M64
+    z = x
+    z = ((z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)) & _M64
+    z = ((z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)) & _M64
+    return z ^ (z >> np.uint64(31))
+
+
+class CounterRNG:
+    """Stateless counter-based RNG: value i of stream s depends only on (seed, s, i)."""
+
+    def __init__(self, seed):
+        self.seed = np.uint64(seed & 0xFFFFFFFFFFFFFFFF)
+
+    def uniform(self, stream, n):
+        with np.errstate(over="ignore"):
+            ctr = np.arange(n, dtype=np.uint64) + (np.uint64(stream) << np.uint64(40))
+            z = _splitmix64(self.seed ^ _splitmix64(ctr))
+        return ((z >> np.uint64(11)).astype(np.float64) + 1.0) * (2.0 ** -53)
+
+    def normal(self, stream, n):
+        u = self.uniform(stream, 2 * n)
+        u1, u2 = u[0::2], u[1::2]
+        return np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2)
+
+
+# ---------------------------------------------------------------------------
+# cells
+# ---------------------------------------------------------------------------
+
+def diamond_crystal(a_ang=5.43, mass_amu=28.0):
+    """Diamond-structure cell: FCC lattice, 2 atoms, a=5.43 A, 28 amu."""
+    a = a_ang / C.distanceBohrToAng
+    cell = 0.5 * a * np.array([[0.0, 1.0, 1.0], [1.0, 0.0, 1.0], [1.0, 1.0, 0.0]]).T
+    pos = np.array([[0.0, 0.0, 0.0], [0.25 * a, 0.25 * a, 0.25 * a]])
+    return Crystal(cell, pos, np.array([0, 0]), np.array([mass_amu * C.massAmuToRy]))
+
+
+def perovskite_crystal(a_ang=3.9, masses_amu=(137.0, 48.0, 16.0, 16.0, 16.0)):
+    """5-atom cubic perovskite-like cell ABO3 (A at corner, B at centre)."""
+    a = a_ang / C.distanceBohrToAng
+    cell = a * np.eye(3)
+    frac = np.array([[0.0, 0.0, 0.0], [0.5, 0.5, 0.5],
+                     [0.5, 0.5, 0.0], [0.5, 0.0, 0.5], [0.0, 0.5, 0.5]])
+    pos = frac @ cell.T
+    return Crystal(cell, pos, np.arange(5), np.array(masses_amu) * C.massAmuToRy)
+
+
+def twelve_atom_crystal(seed, a_ang=5.43):
+    """12-atom cubic cell (3x the diamond primitive basis along a cubic cell).
+
+    Atoms sit on the 8 diamond sites of the conventional cubic cell plus 4
+    octahedral interstitials; masses are drawn uniformly in [20, 80] amu.
+    """
+    a = a_ang / C.distanceBohrToAng
+    cell = a * np.eye(3)
+    fcc = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0]])
+    frac = np.vstack([fcc, fcc + 0.25, fcc + np.array([0.5, 0.0, 0.0])])
+    pos = frac @ cell.T
+    rng = CounterRNG(seed)
+    masses = 20.0 + 60.0 * rng.uniform(7, 12)
+    return Crystal(cell, pos, np.arange(12), masses * C.massAmuToRy)
+
+
+# ---------------------------------------------------------------------------
+# FC2: central springs on a coarse supercell grid
+# ---------------------------------------------------------------------------
+
+def spring_fc2(crystal, shells, grid=(4, 4, 4), tol=1e-6):
+    """Central-spring harmonic force constants in the QE ``.fc`` layout.
+
+    ``shells`` is a list of (radius_bohr, k_ry_per_bohr2, pair_filter) where
+    pair_filter(na, nb) selects which atom pairs the shell connects (None =
+    all).  Off-site blocks are -k * d d^T for every neighbour vector d; the
+    on-site block is fixed by the acoustic sum rule.
+    """
+    nat = crystal.num_atoms
+    g = np.array(grid)
+    fc = np.zeros((3, 3, g[0], g[1], g[2], nat, nat))
+    A = crystal.direct_cell
+    rmax = max(s[0] for s in shells) + tol
+    nmax = int(np.ceil(rmax / min(np.linalg.norm(A, axis=0)))) + 2
+    rng = range(-nmax, nmax + 1)
+    for na in range(nat):
+        for nb in range(nat):
+            for n1, n2, n3 in itertools.product(rng, rng, rng):
+                R = A @ np.array([n1, n2, n3], dtype=np.float64)
+                d = R + crystal.positions[na] - crystal.positions[nb]
+                r = np.linalg.norm(d)
+                if r < tol:
+                    continue
+                for radius, k, filt in shells:
+                    if abs(r - radius) < tol and (filt is None or filt(na, nb)):
+                        dd = d / r
+                        fc[:, :, n1 % g[0], n2 % g[1], n3 % g[2], na, nb] += -k * np.outer(dd, dd)
+    for na in range(nat):
+        s = fc[:, :, :, :, :, na, :].sum(axis=(2, 3, 4, 5))
+        fc[:, :, 0, 0, 0, na, na] -= s
+    return fc
+
+
+def _k_ry(k_ev_ang2):
+    return k_ev_ang2 * C.distanceBohrToAng ** 2 / C.energyRyToEv
+
+
+def diamond_fc2(crystal, k1=45.0, k2=5.0, grid=(4, 4, 4)):
+    a = np.linalg.norm(crystal.direct_cell[:, 0]) * np.sqrt(2.0)
+    shells = [(a * np.sqrt(3.0) / 4.0, _k_ry(k1), None), (a / np.sqrt(2.0), _k_ry(k2), None)]
+    return spring_fc2(crystal, shells, grid)
+
+
+def perovskite_fc2(crystal, grid=(4, 4, 4)):
+    a = crystal.direct_cell[0, 0]
+    shells = [(0.5 * a, _k_ry(12.0), None),                    # B-O
+              (a / np.sqrt(2.0), _k_ry(3.0), None),            # A-O and O-O
+              (a * np.sqrt(3.0) / 2.0, _k_ry(2.0), None),      # A-B
+              (a, _k_ry(1.5), None)]                           # A-A, B-B, O-O
+    return spring_fc2(crystal, shells, grid)
+
+
+def twelve_atom_fc2(crystal, grid=(2, 2, 2)):
+    a = crystal.direct_cell[0, 0]
+    shells = [(a * np.sqrt(3.0) / 4.0, _k_ry(40.0), None),
+              (0.5 * a, _k_ry(12.0), None),
+              (a / np.sqrt(2.0), _k_ry(5.0), None)]
+    return spring_fc2(crystal, shells, grid)
+
+
+# ---------------------------------------------------------------------------
+# FC3: (R2,R3) pairs closed under index permutations, symmetrised + ASR
+# ---------------------------------------------------------------------------
+
+def _orbit(p):
+    """Images of the cell pair (R2,R3) under the 6 permutations of the triple
+    (0, R2, R3), each translated so the first cell is 0, with the transpose
+    that maps the (i1,i2,i3) block onto the image block."""
+    R2, R3 = p
+    neg = lambda v: tuple(-x for x in v)
+    sub = lambda u, v: tuple(x - y for x, y in zip(u, v))
+    return [((R2, R3), (0, 1, 2)),
+            ((R3, R2), (0, 2, 1)),
+            ((neg(R2), sub(R3, R2)), (1, 0, 2)),
+            ((sub(R2, R3), neg(R3)), (2, 1, 0)),
+            ((sub(R3, R2), neg(R2)), (1, 2, 0)),
+            ((neg(R3), sub(R2, R3)), (2, 0, 1))]
+
+
+@dataclass
+class FC3:
+    D3: np.ndarray        # (nb,nb,nb,nr3,nr2) Ry/Bohr^3
+    R2: np.ndarray        # (nr2,3) Bohr
+    R3: np.ndarray        # (nr3,3) Bohr
+    w2: np.ndarray        # (nr2,nat,nat)
+    w3: np.ndarray        # (nr3,nat,nat)
+    num_pairs: int
+    iterations: int = 0
+    residual: float = 0.0
+
+
+def random_fc3(crystal, num_pairs, seed, amp_ev=3.0, decay_ang=4.0,
+               tol=1e-12, max_iter=500):
+    """FC3 on ``num_pairs`` (R2,R3) lattice-vector pairs.
+
+    Orbits of pairs under index permutation are added in order of increasing
+    largest |R| among R2, R3, R3-R2 (ties broken by the seeded RNG), skipping
+    an orbit that would overshoot, until exactly ``num_pairs`` pairs are in.
+    Entries start as N(0,1)*amp*exp(-(|R2|+|R3|)/decay) (eV/A^3, A) and are
+    then alternately permutation-symmetrised and projected onto the acoustic
+    sum rule sum_{R3,c} Phi(0a,R2b,R3c) = 0 until both residuals are below
+    tol relative to max|Phi| (at most max_iter rounds).
+    """
+    nat = crystal.num_atoms
+    nb = 3 * nat
+    A = crystal.direct_cell
+    rng = CounterRNG(seed)
+    nmax = 4
+    vecs = [v for v in itertools.product(range(-nmax, nmax + 1), repeat=3)]
+    length = {v: np.linalg.norm(A @ np.array(v, dtype=np.float64)) for v in vecs}
+    vecset = set(vecs)
+    # candidate orbits with all three vectors short
+    orbits = {}
+    lim = sorted(set(round(x, 6) for x in length.values()))[8]
+    short = [v for v in vecs if length[v] <= lim + 1e-9]
+    for R2 in short:
+        for R3 in short:
+            R32 = tuple(x - y for x, y in zip(R3, R2))
+            if R32 not in vecset or length[R32] > lim + 1e-9:
+                continue
+            imgs = frozenset(q for q, _ in _orbit((R2, R3)))
+            if imgs in orbits:
+                continue
+            orbits[imgs] = max(length[R2], length[R3], length[R32])
+    keys = list(orbits.keys())
+    tie = rng.uniform(1, len(keys))
+    order = sorted(range(len(keys)), key=lambda i: (round(orbits[keys[i]], 6), tie[i]))
+    pairs = []
+    for i in order:
+        orb = sorted(keys[i])
+        if len(pairs) + len(orb) <= num_pairs:
+            pairs.extend(orb)
+        if len(pairs) == num_pairs:
+            break
+    if len(pairs) != num_pairs:
+        raise RuntimeError("could not assemble %d permutation-closed pairs" % num_pairs)
+    pidx = {p: i for i, p in enumerate(pairs)}
+    # initial random blocks
+    scale = C.distanceBohrToAng ** 3 / C.energyRyToEv
+    z = rng.normal(2, num_pairs * nb ** 3).reshape(num_pairs, nb, nb, nb)
+    B = np.empty_like(z)
+    for p, i in pidx.items():
+        r2 = length[p[0]] * C.distanceBohrToAng
+        r3 = length[p[1]] * C.distanceBohrToAng
+        B[i] = z[i] * amp_ev * np.exp(-(r2 + r3) / decay_ang) * scale
+    # precompute permutation maps and ASR groups
+    perm_maps = [[(pidx[q], ax) for q, ax in _orbit(p)] for p in pairs]
+    R2s = sorted(set(p[0] for p in pairs))
+    groups = {R2: [pidx[p] for p in pairs if p[0] == R2] for R2 in R2s}
+
+    def symmetrise(B):
+        S = np.zeros_like(B)
+        for i, imgs in enumerate(perm_maps):
+            for j, ax in imgs:
+                S[j] += np.transpose(B[i], ax)
+        return S / 6.0
+
+    def asr_project(B):
+        out = B.copy()
+        for R2, idx in groups.items():
+            blk = B[idx].reshape(len(idx), nb, nb, nat, 3)
+            s = blk.sum(axis=(0, 3))  # (nb, nb, 3)
+            cnt = len(idx) * nat
+            out[idx] = (blk - s[None, :, :, None, :] / cnt).reshape(len(idx), nb, nb, nb)
+        return out
+
+    def asr_residual(B):
+        r = 0.0
+        for R2, idx in groups.items():
+            blk = B[idx].reshape(len(idx), nb, nb, nat, 3)
+            r = max(r, np.abs(blk.sum(axis=(0, 3))).max())
+        return r
+
+    for it in range(max_iter):
+        B = asr_project(symmetrise(B))
+        ref = np.abs(B).max()
+        res = max(np.abs(symmetrise(B) - B).max(), asr_residual(B)) / ref
+        if res < tol:
+            break
+    # dense ShengBTE-style layout
+    Rvecs = sorted(set(p[0] for p in pairs) | set(p[1] for p in pairs))
+    ridx = {v: i for i, v in enumerate(Rvecs)}
+    nr = len(Rvecs)
+    D3 = np.zeros((nb, nb, nb, nr, nr))
+    for p, i in pidx.items():
+        D3[:, :, :, ridx[p[1]], ridx[p[0]]] = B[i]
+    Rcart = np.array([A @ np.array(v, dtype=np.float64) for v in Rvecs])
+    w = np.ones((nr, nat, nat))
+    return FC3(D3, Rcart.copy(), Rcart.copy(), w, w.copy(), num_pairs, it + 1, res)
+
+
+# ---------------------------------------------------------------------------
+# benchmark workloads
+# ---------------------------------------------------------------------------
+
+@dataclass
+class Workload:
+    name: str
+    crystal: Crystal
+    fc2: np.ndarray
+    fc3: FC3
+    mesh: tuple
+    temperatures_k: tuple
+    smearing: str          # "gaussian" or "adaptive"
+    sigma_ry: float        # Gaussian width (Ry); ignored for adaptive
+
+
+def diamond_workload(mesh=(8, 8, 8), smearing="gaussian", temperatures_k=(300.0,),
+                     num_pairs=400):
+    """Diamond cell with spring FC2 and the seed-0 FC3 (shared by both diamond
+    workloads, which differ only in mesh, smearing and temperatures)."""
+    cr = diamond_crystal()
+    fc2 = diamond_fc2(cr)
+    fc3 = random_fc3(cr, num_pairs, SEED_BASE + 0)
+    return Workload("diamond-%dx%dx%d" % tuple(mesh), cr, fc2, fc3, tuple(mesh),
+                    tuple(temperatures_k), smearing, 0.3 / C.ryToTHz)
+
+
+def config0():
+    """Diamond, 8^3 mesh, Gaussian 0.3 THz, 300 K (CPU-runnable case)."""
+    return diamond_workload((8, 8, 8), "gaussian", (300.0,))
+
+
+def config1():
+    """Diamond, 20^3 mesh, adaptive smearing, 100/300/600 K (headline case)."""
+    return diamond_workload((20, 20, 20), "adaptive", (100.0, 300.0, 600.0))

@@ -1,0 +1,335 @@
+"""Benchmark: 3-phonon RTA linewidths on the 20x20x20 diamond mesh.
+
+Workload (one "step"): the whole PhScatteringMatrix builder in linewidth mode
+-- every (q1, q2) pair of the 8000-point Gamma-centred mesh (64,000,000
+pairs, both +/- processes, all 216 branch triplets, 3 temperatures
+100/300/600 K, adaptive smearing from group velocities) -- on synthetic
+force constants of the diamond cell (seeded generator, phoebe_b200.synth).
+
+metric: triplets/s, where a triplet is one (q1,q2) pair (q3 fixed by
+momentum); linewidths/s = Nq*nb*nT / step time is reported beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision fp64|split_bf16|split_tf32] [--mesh 20]
+
+Under torchrun each rank processes a contiguous slice of q2 and the
+per-rank partial A_out vectors are summed with one NCCL all-reduce
+(the reference's allReduceSum of the linewidths, ph_scattering.cpp:800).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+TEMPS_K = (100.0, 300.0, 600.0)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default=os.environ.get("PHX_BENCH_PRECISION", "fp64"),
+                    choices=["fp64", "split_bf16", "split_tf32"])
+    ap.add_argument("--mesh", type=int, default=20)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def workload(mesh):
+    from phoebe_b200 import synth
+    cr = synth.diamond_crystal()
+    fc2 = synth.diamond_fc2(cr)
+    fc3 = synth.random_fc3(cr, 400, synth.SEED_BASE)
+    return cr, fc2, fc3, (mesh, mesh, mesh)
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for i, n in enumerate(names):
+                if len(s) > 4 + i and s[4 + i].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+def flops_per_pair(nb, nr3):
+    """FLOPs the fused kernel executes per (q1,q2) pair (complex MAC = 8):
+    the '+' vertex R3 transform (nb^3 nr3 MACs) and the e1 / e3 contractions
+    (2 nb^4 MACs); the e2 contraction is folded per q2."""
+    return 8 * nb ** 3 * nr3 + 8 * 2 * nb ** 4
+
+
+def flops_per_pair_reference(nb, nr3):
+    """F_pair of the reference's formulation (both vertices, three contractions)."""
+    return 16 * nb ** 3 * nr3 + 16 * nb ** 4 + 16 * nb ** 4 + 8 * nb ** 4 * 2 + 3 * nb ** 3 * 2
+
+
+def cpu_baseline(cr, fc2, fc3, mesh, budget_s, q2_hint=None):
+    """Oracle (restatement of the reference CPU path) on a q2 sample."""
+    import oracle
+    from phoebe_b200 import constants as C
+    from phoebe_b200 import lattice
+    m = lattice.Mesh(cr, mesh)
+    q = m.cartesian_coords()
+    h0 = oracle.PhononH0(cr, fc2)
+    E, U = h0.diagonalize(q)
+    vg = h0.velocities(q)
+    v3 = oracle.Interaction3Ph(cr, fc3)
+    T = np.array([C.kelvin_to_ry(t) for t in TEMPS_K])
+    nq = m.num_points
+    rng = np.random.default_rng(0)
+    order = rng.permutation(nq)
+    t0 = time.perf_counter()
+    v3.linewidths(mesh, E, U, vg, q, cr.reciprocal_cell, T, "adaptive", 0.0,
+                  q2_list=order[:1], finalize=False)
+    t1 = time.perf_counter() - t0
+    n = max(1, min(nq - 1, int(budget_s / max(t1, 1e-3))))
+    if q2_hint:
+        n = q2_hint
+    t0 = time.perf_counter()
+    v3.linewidths(mesh, E, U, vg, q, cr.reciprocal_cell, T, "adaptive", 0.0,
+                  q2_list=order[1:1 + n], finalize=False)
+    dt = time.perf_counter() - t0
+    pairs = n * nq
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": pairs / dt, "unit": "triplets/s", "cores": threads, "kind": "port",
+            "sample": "%d q2 points x all %d q1 of the %s mesh (%d pairs, %.1f s), OpenMP oracle"
+                      % (n, nq, "x".join(map(str, mesh)), pairs, dt)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cr, fc2, fc3, mesh = workload(args.mesh)
+    import oracle
+    oracle.lib()
+    vals = []
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline(cr, fc2, fc3, mesh, max(2.0, args.cpu_seconds / 3), q2_hint=None)
+        if i >= args.warmup:
+            vals.append(b["value"])
+    v = float(np.median(vals))
+    nq = int(np.prod(mesh))
+    line = {"impl": "reference", "metric": "3ph triplets/s @20^3 mesh", "value": v,
+            "unit": "triplets/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * nq * nq / v, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "diamond 20x20x20, 400 FC3 pairs, adaptive smearing, "
+                                   "100/300/600 K (CPU sample per step)"},
+            "cpu_baseline": dict(b, value=v),
+            "e2e": {"value": v, "unit": "triplets/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from phoebe_b200 import _abi
+    from phoebe_b200 import constants as C
+    from phoebe_b200.core import Context, Interaction3Ph, PhononH0, PhScatteringMatrix
+    import ctypes
+
+    cr, fc2, fc3, mesh = workload(args.mesh)
+    nq = int(np.prod(mesh))
+    nb = cr.num_bands
+    nr3 = fc3.D3.shape[3]
+    T = np.array([C.kelvin_to_ry(t) for t in TEMPS_K])
+    nT = len(T)
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    h0 = PhononH0(ctx, cr, fc2)
+    bands = h0.populate(mesh, withVelocities=True)
+    v3 = Interaction3Ph(ctx, cr, fc3, precision=args.precision)
+    sm = PhScatteringMatrix(v3, bands, T, "adaptive")
+    q2b = rank * nq // world
+    q2e = (rank + 1) * nq // world
+    A = torch.zeros(nT * nq * nb, dtype=torch.float64, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    L = _abi.load()
+
+    def step():
+        p = sm._params(q2b, q2e, finalize=(world == 1))
+        st = _abi.LwStats()
+        _abi.check(L.phx_ph_linewidths_d(v3.h, bands.h, ctypes.byref(p),
+                                         ctypes.c_void_p(A.data_ptr()), ctypes.byref(st)), ctx.h)
+        return st
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+        flush.zero_()
+    barrier()
+    dev_ms = []
+    vertex_ms = []
+    launches = 0
+    with Clocks(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            st = step()
+            dev_ms.append(st.ms_total)
+            vertex_ms.append(st.ms_vertex)
+            launches += st.kernel_launches
+        barrier()
+        wall = time.perf_counter() - t0
+    total_ms = float(np.sum(dev_ms))
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_step = total_ms / args.steps
+    pairs_step = nq * nq
+    value = pairs_step / (ms_step / 1000.0)
+
+    # end to end through the public API with host buffers, every step:
+    # FC2/FC3 host->device, band structure, builder, A_out device->host
+    h2d = fc2.nbytes + fc3.D3.nbytes + fc3.R2.nbytes + fc3.R3.nbytes + fc3.w2.nbytes + \
+        fc3.w3.nbytes + T.nbytes
+    d2h = nT * nq * nb * 8
+    e2e_times = []
+    for i in range(1 + min(args.steps, 3)):
+        barrier()
+        t0 = time.perf_counter()
+        h0e = PhononH0(ctx, cr, fc2)
+        be = h0e.populate(mesh, withVelocities=True)
+        ve = Interaction3Ph(ctx, cr, fc3, precision=args.precision)
+        se = PhScatteringMatrix(ve, be, T, "adaptive")
+        Ae = se.setup(q2b, q2e, finalize=(world == 1))
+        if dist:
+            At = torch.from_numpy(Ae).cuda()
+            dist.all_reduce(At)
+            Ae = At.cpu().numpy()
+        ve.close()
+        be.close()
+        h0e.close()
+        dt = time.perf_counter() - t0
+        if i > 0:
+            e2e_times.append(dt)
+    e2e_value = pairs_step / float(np.median(e2e_times))
+
+    # roofline of the dominant kernel (fused pair kernel), device-timed
+    fl = flops_per_pair(nb, nr3)
+    achieved = fl * (q2e - q2b) * nq / (float(np.mean(vertex_ms)) / 1000.0) / 1e12
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    if args.precision == "fp64":
+        roof = {"bound": "fp64", "achieved": achieved, "peak": 37.0, "unit": "TFLOP/s",
+                "frac": achieved / 37.0, "traffic": None,
+                "note": "plain FP64 SIMT path; peak is the nominal B200 FP64 rate (no measured "
+                        "FP64 peak available)"}
+    else:
+        pk = peaks.get("bf16_tflops_sustained", 1394.6)
+        roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
+                "frac": achieved / pk, "traffic": None, "peak_source": "measured (sustained)"}
+    roof["flops_per_pair"] = fl
+    roof["flops_per_pair_reference_formulation"] = flops_per_pair_reference(nb, nr3)
+
+    out = None
+    if rank == 0:
+        cpu = cpu_baseline(cr, fc2, fc3, mesh, args.cpu_seconds)
+        out = {"metric": "3ph triplets/s @20^3 mesh", "value": value, "unit": "triplets/s",
+               "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
+               "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else
+               ("bf16x3->f32" if args.precision == "split_bf16" else "tf32x3->f32"),
+               "data": "synthetic",
+               "config": {"workload": "diamond 20x20x20 (8000 q, 64e6 pairs), 400 FC3 pairs "
+                                      "(nr3=%d), adaptive smearing, T=100/300/600 K" % nr3,
+                          "precision": args.precision, "l2": "flushed between steps (256 MB write)",
+                          "parallelism": "q2-sliced x%d" % world},
+               "linewidths_per_s": nq * nb * nT / (ms_step / 1000.0),
+               "branch_triplets_per_s": value * 2 * nb ** 3,
+               "wall_s_timed": wall,
+               "e2e": {"value": e2e_value, "unit": "triplets/s", "h2d_bytes_per_step": int(h2d),
+                       "d2h_bytes_per_step": int(d2h)},
+               "gpu_launches": launches,
+               "roofline": roof,
+               "cpu_baseline": cpu,
+               "clocks": clk.summary()}
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

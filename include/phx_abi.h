@@ -1,0 +1,172 @@
+/*
+ * phx_abi.h -- C ABI of the B200 (sm_100a) scattering-rate library.
+ *
+ * Each entry point replaces one method of mir-group/phoebe's C++ call surface
+ * for the 3-phonon / el-ph scattering-rate path; the reference method is
+ * cited (file:line) beside each declaration.  Conventions:
+ *   - every call returns int status (PHX_OK = 0); phx_last_error() gives text;
+ *   - plain pointers and sizes only; "host" pointers are caller-owned host
+ *     memory, "_d" pointers are device memory on the context's GPU;
+ *   - arrays are C-order (row-major) in the reference's index order;
+ *     complex arrays are interleaved (re, im) doubles;
+ *   - eigenvector matrices are U[a][b]: row a = 3*atom + cartesian component
+ *     (Wannier index for electrons), column b = band;
+ *   - energies in Ry, lengths in Bohr, masses in Ry units, temperatures in Ry;
+ *   - handles are not thread-safe; each context owns one CUDA stream.
+ */
+#ifndef PHX_ABI_H
+#define PHX_ABI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PHX_OK 0
+#define PHX_ERR_ARG 1      /* invalid argument or size */
+#define PHX_ERR_CUDA 2     /* CUDA runtime error (message in phx_last_error) */
+#define PHX_ERR_NOCONV 3   /* eigensolver hit its sweep cap */
+#define PHX_ERR_STATE 4    /* call out of order (e.g. couplings before cache_d3) */
+#define PHX_ERR_MESH 5     /* q1 +/- q2 not on the mesh */
+#define PHX_ERR_NODEV 6    /* no CUDA device / extension unusable */
+
+#define PHX_SMEAR_GAUSSIAN 0
+#define PHX_SMEAR_ADAPTIVE 1
+
+#define PHX_PREC_FP64 0        /* plain FP64 SIMT path */
+#define PHX_PREC_SPLIT_BF16 1  /* BF16 hi+lo tcgen05 GEMM, FP32 accumulate */
+#define PHX_PREC_SPLIT_TF32 2  /* TF32 hi+lo tcgen05 GEMM, FP32 accumulate */
+
+typedef struct phx_ctx phx_ctx;
+typedef struct phx_ph_h0 phx_ph_h0;
+typedef struct phx_bands phx_bands;
+typedef struct phx_v3 phx_v3;
+
+/* ---- context ---------------------------------------------------------- */
+/* Replaces initKokkos / DeviceManager (src/common_kokkos.cpp:104-134,182-190). */
+int phx_ctx_create(int device, phx_ctx** out);
+int phx_ctx_destroy(phx_ctx* ctx);
+int phx_ctx_synchronize(phx_ctx* ctx);
+/* Copies the last error message of this context (or of the library when
+ * ctx is NULL) into buf; returns the status of the failing call. */
+int phx_last_error(const phx_ctx* ctx, char* buf, size_t len);
+/* Library version string (static storage). */
+const char* phx_version(void);
+
+/* ---- harmonic phonons (PhononH0) -------------------------------------- */
+/* Host only, no GPU: acoustic sum rule "simple" + Wigner-Seitz reordering of
+ * the QE force constants fc(3,3,n1,n2,n3,nat,nat) (Ry/Bohr^2).  cell is 3x3
+ * with lattice vectors as columns, pos (nat,3).  Call with R = w = mat2R =
+ * NULL to get numR; mat2R is written (numR, 3nat, 3nat).
+ * Replaces PhononH0::setAcousticSumRule "simple" + reorderDynamicalMatrix +
+ * wsInit (src/harmonic/phonon_h0_sum_rule.cpp:45-79;
+ * src/harmonic/phonon_h0.cpp:426-535,672-771). */
+int phx_ws_reorder(int nat, const double* cell, const double* pos, const int* grid,
+                   const double* fc, int* numR, double* R, double* w, double* mat2R);
+
+/* Builds the harmonic Hamiltonian on the GPU from QE force constants.
+ * masses: per atom (Ry).  Replaces the PhononH0 constructor
+ * (src/harmonic/phonon_h0.cpp:18-248; host->device copy :165-246). */
+int phx_ph_h0_create(phx_ctx* ctx, int nat, const double* cell, const double* pos,
+                     const double* masses, const int* grid, const double* fc,
+                     phx_ph_h0** out);
+int phx_ph_h0_destroy(phx_ph_h0* h0);
+int phx_ph_h0_num_bands(const phx_ph_h0* h0);
+
+/* Batched diagonalisation at nq Cartesian wavevectors (host buffers).
+ * E (nq,nb); U (nq,nb,nb) complex; mass_scaling divides U by sqrt(m).
+ * Replaces PhononH0::diagonalizeFromCoordinates (src/harmonic/phonon_h0.h:76-79)
+ * and kokkosBatchedDiagonalizeFromCoordinates (src/harmonic/phonon_h0.h:106). */
+int phx_ph_diag(phx_ph_h0* h0, int nq, const double* q_cart, int mass_scaling, double* E,
+                double* U);
+
+/* As phx_ph_diag plus group velocities vg (nq,nb,3) (Ry*Bohr) from the
+ * finite-difference velocity operator with degenerate-subspace treatment.
+ * U is mass-scaled.  Replaces kokkosBatchedDiagonalizeWithVelocities
+ * (src/harmonic/phonon_h0.h:109) and PhononH0::diagonalizeVelocityFromCoordinates
+ * (src/harmonic/phonon_h0.cpp:895-1070). */
+int phx_ph_diag_velocities(phx_ph_h0* h0, int nq, const double* q_cart, double* E, double* U,
+                           double* vg);
+
+/* Device-resident band structure on a full Gamma-centred mesh (x fastest
+ * point index, src/points.cpp:222-248).  Replaces PhononH0::populate /
+ * ActiveBandStructure::builder for the phonon transport path
+ * (src/harmonic/phonon_h0.cpp:389-394; src/bands/active_bandstructure.cpp:488-524). */
+int phx_bands_create_mesh(phx_ph_h0* h0, const int* mesh, int with_velocities,
+                          phx_bands** out);
+/* Same, from caller-supplied host arrays (E (nq,nb), U (nq,nb,nb) complex
+ * mass-scaled, vg (nq,nb,3) or NULL) -- FullBandStructure from another source. */
+int phx_bands_create_from_host(phx_ctx* ctx, const int* mesh, const double* reciprocal_cell,
+                               int nb, const double* E, const double* U, const double* vg,
+                               phx_bands** out);
+int phx_bands_destroy(phx_bands* b);
+int phx_bands_num_points(const phx_bands* b);
+/* Copy band data to host (any pointer may be NULL). */
+int phx_bands_get(phx_bands* b, double* E, double* U, double* vg);
+
+/* ---- 3-phonon vertex (Interaction3Ph) --------------------------------- */
+/* D3 (nb,nb,nb,nr3,nr2) Ry/Bohr^3, R2 (nr2,3), R3 (nr3,3) Bohr,
+ * w2 (nr2,nat,nat), w3 (nr3,nat,nat).  Replaces the Interaction3Ph
+ * constructor (src/interaction/interaction_3ph.h:92-96; .cpp:5-68). */
+int phx_v3_create(phx_ctx* ctx, int nat, int nr2, int nr3, const double* D3, const double* R2,
+                  const double* R3, const double* w2, const double* w3, phx_v3** out);
+int phx_v3_destroy(phx_v3* v3);
+int phx_v3_set_precision(phx_v3* v3, int prec);
+/* Interaction3Ph::cacheD3 (src/interaction/interaction_3ph.h:144; .cpp:100-175). */
+int phx_v3_cache_d3(phx_v3* v3, const double* q2);
+/* Interaction3Ph::getCouplingsSquared (src/interaction/interaction_3ph.h:128-138;
+ * .cpp:179-405).  Eigenvectors are passed padded to nb columns:
+ * ev1 (nq1,nb,nb), ev2 (nb,nb), ev3p/ev3m (nq1,nb,nb) complex, of which the
+ * first nb1s[i] / nb2 / nb3ps[i] / nb3ms[i] columns are used.  Outputs are
+ * ragged and concatenated: block i of outP holds (nb1s[i], nb2, nb3ps[i])
+ * row-major at offset sum_{j<i} nb1s[j]*nb2*nb3ps[j] (likewise outM). */
+int phx_v3_couplings_sq(phx_v3* v3, int nq1, const double* q1s, const double* ev1,
+                        const int* nb1s, const double* ev2, int nb2, const double* ev3p,
+                        const int* nb3ps, const double* ev3m, const int* nb3ms, double* outP,
+                        double* outM);
+/* Interaction3Ph::estimateNumBatches (src/interaction/interaction_3ph.cpp:407-440),
+ * against the GPU's free memory. */
+int phx_v3_estimate_num_batches(phx_v3* v3, int nq1, int nb2, int* num_batches);
+
+/* ---- scattering-rate builder (PhScatteringMatrix, linewidth mode) ------ */
+typedef struct phx_lw_params {
+  int num_temperatures;       /* nT <= 8 */
+  const double* temperatures; /* (nT) Ry */
+  int smearing;               /* PHX_SMEAR_* */
+  double sigma;               /* Gaussian width (Ry) */
+  int finalize;               /* 1: degeneracy-average row 0, zero excluded states */
+  int q2_begin, q2_end;       /* q2 range to process ([0, nq) for the full builder) */
+} phx_lw_params;
+
+typedef struct phx_lw_stats {
+  double ms_total;            /* device time of the whole call */
+  double ms_vertex;           /* device time of the fused pair kernels */
+  long long pairs;            /* (q1,q2) pairs processed */
+  int kernel_launches;        /* kernels launched by the call */
+} phx_lw_stats;
+
+/* Whole PhScatteringMatrix::builder, switchCase 2 (linewidths), on the GPU:
+ * symmetrizeCoupling, cutoffs, Gaussian/adaptive deltas, Bose factors,
+ * accumulation, degeneracy averaging (src/bte/ph_scattering.cpp:60-935;
+ * src/bte/scattering.cpp:1168-1318).  A_out (nT, nq*nb) host, the reference's
+ * internalDiagonal (linewidth * n(n+1)).  stats may be NULL. */
+int phx_ph_linewidths(phx_v3* v3, phx_bands* bands, const phx_lw_params* params,
+                      double* A_out, phx_lw_stats* stats);
+/* Same with a device output buffer (nT*nq*nb doubles). */
+int phx_ph_linewidths_d(phx_v3* v3, phx_bands* bands, const phx_lw_params* params,
+                        double* A_out_d, phx_lw_stats* stats);
+
+/* RTA thermal conductivity (atomic units; x thConductivityAuToSi for W/m/K)
+ * from A_out: tau = n(n+1)/A_out, kappa_ij = sum dn/dT v_i tau v_j E/(Nq V).
+ * kappa (nT,3,3) host.  Replaces BulkTDrift + getSingleModeTimes +
+ * PhononThermalConductivity::calcFromPopulation (src/bte/drift.cpp:3-29;
+ * src/bte/scattering.cpp:484-527; src/observable/phonon_thermal_cond.cpp:64-113). */
+int phx_ph_rta_kappa(phx_bands* bands, int nT, const double* temperatures,
+                     const double* A_out, double volume, double* kappa);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PHX_ABI_H */

@@ -1,0 +1,314 @@
+"""Host-side mirror of the reference's scattering-rate classes over libphx.
+
+Class and method names follow mir-group/phoebe so that ports of its tests
+read alike:
+
+* ``PhononH0``            -- src/harmonic/phonon_h0.h (diagonalizeFromCoordinates,
+                             diagonalizeVelocityFromCoordinates, populate)
+* ``Interaction3Ph``      -- src/interaction/interaction_3ph.h (cacheD3,
+                             getCouplingsSquared, estimateNumBatches)
+* ``PhScatteringMatrix``  -- src/bte/ph_scattering.h / scattering.h (setup,
+                             getLinewidths, getSingleModeTimes) plus the RTA
+                             thermal conductivity of phonon_thermal_cond.cpp.
+
+All arithmetic runs in libphx on the GPU; these classes only marshal arrays.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from . import constants as C
+from ._abi import c128, check, dptr, f64, i32, iptr
+
+
+class Context:
+    """One GPU and one CUDA stream (phx_ctx)."""
+
+    def __init__(self, device=0):
+        L = _abi.load()
+        h = ctypes.c_void_p()
+        check(L.phx_ctx_create(int(device), ctypes.byref(h)))
+        self.h = h
+        self.device = device
+
+    def synchronize(self):
+        check(_abi.load().phx_ctx_synchronize(self.h), self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _abi.load().phx_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ws_reorder(crystal, fc2):
+    """Host-only acoustic sum rule + Wigner-Seitz reorder (no GPU needed)."""
+    L = _abi.load()
+    nat = crystal.num_atoms
+    cell, pos, fc = f64(crystal.direct_cell), f64(crystal.positions), f64(fc2)
+    grid = i32(fc2.shape[2:5])
+    n = ctypes.c_int(0)
+    check(L.phx_ws_reorder(nat, dptr(cell), dptr(pos), iptr(grid), dptr(fc), ctypes.byref(n),
+                           None, None, None))
+    nb = 3 * nat
+    R = np.zeros((n.value, 3))
+    w = np.zeros(n.value)
+    M = np.zeros((n.value, nb, nb))
+    check(L.phx_ws_reorder(nat, dptr(cell), dptr(pos), iptr(grid), dptr(fc), ctypes.byref(n),
+                           dptr(R), dptr(w), dptr(M)))
+    return R, w, M
+
+
+class PhononH0:
+    """Harmonic phonon Hamiltonian on the GPU (PhononH0)."""
+
+    def __init__(self, ctx, crystal, fc2):
+        L = _abi.load()
+        self.ctx = ctx
+        self.crystal = crystal
+        self.nb = crystal.num_bands
+        h = ctypes.c_void_p()
+        cell, pos = f64(crystal.direct_cell), f64(crystal.positions)
+        masses = f64(crystal.atomic_masses)
+        grid = i32(fc2.shape[2:5])
+        fc = f64(fc2)
+        check(L.phx_ph_h0_create(ctx.h, crystal.num_atoms, dptr(cell), dptr(pos), dptr(masses),
+                                 iptr(grid), dptr(fc), ctypes.byref(h)), ctx.h)
+        self.h = h
+
+    def diagonalizeFromCoordinates(self, q_cart, withMassScaling=True):
+        q = f64(np.atleast_2d(q_cart))
+        nq = q.shape[0]
+        E = np.zeros((nq, self.nb))
+        U = np.zeros((nq, self.nb, self.nb, 2))
+        check(_abi.load().phx_ph_diag(self.h, nq, dptr(q), int(withMassScaling), dptr(E),
+                                      dptr(U)), self.ctx.h)
+        return E, U[..., 0] + 1j * U[..., 1]
+
+    def diagonalizeWithVelocities(self, q_cart):
+        q = f64(np.atleast_2d(q_cart))
+        nq = q.shape[0]
+        E = np.zeros((nq, self.nb))
+        U = np.zeros((nq, self.nb, self.nb, 2))
+        vg = np.zeros((nq, self.nb, 3))
+        check(_abi.load().phx_ph_diag_velocities(self.h, nq, dptr(q), dptr(E), dptr(U), dptr(vg)),
+              self.ctx.h)
+        return E, U[..., 0] + 1j * U[..., 1], vg
+
+    def populate(self, mesh, withVelocities=True):
+        """Band structure on a full Gamma-centred mesh, resident on the GPU."""
+        return BandStructure.from_h0(self, mesh, withVelocities)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _abi.load().phx_ph_h0_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BandStructure:
+    """Device-resident energies / eigenvectors / velocities on a mesh (phx_bands)."""
+
+    def __init__(self, ctx, h, mesh, nb, reciprocal_cell):
+        self.ctx = ctx
+        self.h = h
+        self.mesh = tuple(int(x) for x in mesh)
+        self.nb = nb
+        self.nq = int(np.prod(self.mesh))
+        self.reciprocal_cell = np.asarray(reciprocal_cell)
+
+    @classmethod
+    def from_h0(cls, h0, mesh, with_velocities=True):
+        h = ctypes.c_void_p()
+        m = i32(mesh)
+        check(_abi.load().phx_bands_create_mesh(h0.h, iptr(m), int(with_velocities),
+                                                ctypes.byref(h)), h0.ctx.h)
+        return cls(h0.ctx, h, mesh, h0.nb, h0.crystal.reciprocal_cell)
+
+    @classmethod
+    def from_arrays(cls, ctx, mesh, reciprocal_cell, E, U, vg=None):
+        h = ctypes.c_void_p()
+        m = i32(mesh)
+        rc = f64(reciprocal_cell)
+        Ed = f64(E)
+        Ud = c128(U)
+        vd = f64(vg) if vg is not None else None
+        nb = Ed.shape[-1]
+        check(_abi.load().phx_bands_create_from_host(ctx.h, iptr(m), dptr(rc), nb, dptr(Ed),
+                                                     dptr(Ud), dptr(vd) if vd is not None else None,
+                                                     ctypes.byref(h)), ctx.h)
+        return cls(ctx, h, mesh, nb, reciprocal_cell)
+
+    def get(self, velocities=True):
+        E = np.zeros((self.nq, self.nb))
+        U = np.zeros((self.nq, self.nb, self.nb, 2))
+        vg = np.zeros((self.nq, self.nb, 3)) if velocities else None
+        check(_abi.load().phx_bands_get(self.h, dptr(E), dptr(U),
+                                        dptr(vg) if velocities else None), self.ctx.h)
+        return E, U[..., 0] + 1j * U[..., 1], vg
+
+    def close(self):
+        if getattr(self, "h", None):
+            _abi.load().phx_bands_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+PRECISIONS = {"fp64": _abi.PHX_PREC_FP64, "split_bf16": _abi.PHX_PREC_SPLIT_BF16,
+              "split_tf32": _abi.PHX_PREC_SPLIT_TF32}
+
+
+class Interaction3Ph:
+    """3-phonon vertex on the GPU (Interaction3Ph)."""
+
+    def __init__(self, ctx, crystal, fc3, precision="fp64"):
+        self.ctx = ctx
+        self.nat = crystal.num_atoms
+        self.nb = 3 * self.nat
+        D3, R2, R3, w2, w3 = (f64(x) for x in (fc3.D3, fc3.R2, fc3.R3, fc3.w2, fc3.w3))
+        self.nr3, self.nr2 = D3.shape[3], D3.shape[4]
+        h = ctypes.c_void_p()
+        check(_abi.load().phx_v3_create(ctx.h, self.nat, self.nr2, self.nr3, dptr(D3), dptr(R2),
+                                        dptr(R3), dptr(w2), dptr(w3), ctypes.byref(h)), ctx.h)
+        self.h = h
+        self.setPrecision(precision)
+
+    def setPrecision(self, precision):
+        check(_abi.load().phx_v3_set_precision(self.h, PRECISIONS[precision]), self.ctx.h)
+        self.precision = precision
+
+    def cacheD3(self, q2):
+        q = f64(q2)
+        check(_abi.load().phx_v3_cache_d3(self.h, dptr(q)), self.ctx.h)
+
+    def getCouplingsSquared(self, q1s, q2, ev1s, ev2, ev3Pluss, ev3Minss, nb1s=None, nb2=None,
+                            nb3Pluss=None, nb3Minss=None):
+        """Returns (couplingPlus, couplingMins): lists of (nb1,nb2,nb3) arrays."""
+        q1 = f64(np.atleast_2d(q1s))
+        nq1 = q1.shape[0]
+        nb = self.nb
+
+        def pad(evs):
+            out = np.zeros((nq1, nb, nb), dtype=np.complex128)
+            for i, e in enumerate(evs):
+                e = np.asarray(e)
+                out[i, :, :e.shape[1]] = e
+            return out
+
+        e1, e3p, e3m = pad(ev1s), pad(ev3Pluss), pad(ev3Minss)
+        ev2 = np.asarray(ev2)
+        e2 = np.zeros((nb, nb), dtype=np.complex128)
+        e2[:, :ev2.shape[1]] = ev2
+        nb1s = i32(nb1s if nb1s is not None else [np.asarray(e).shape[1] for e in ev1s])
+        nb2 = int(nb2 if nb2 is not None else ev2.shape[1])
+        nb3p = i32(nb3Pluss if nb3Pluss is not None else [np.asarray(e).shape[1] for e in ev3Pluss])
+        nb3m = i32(nb3Minss if nb3Minss is not None else [np.asarray(e).shape[1] for e in ev3Minss])
+        sizeP = int(np.sum(nb1s * nb2 * nb3p))
+        sizeM = int(np.sum(nb1s * nb2 * nb3m))
+        outP = np.zeros(max(sizeP, 1))
+        outM = np.zeros(max(sizeM, 1))
+        E1, E2, E3p, E3m = c128(e1), c128(e2), c128(e3p), c128(e3m)
+        check(_abi.load().phx_v3_couplings_sq(self.h, nq1, dptr(q1), dptr(E1), iptr(nb1s), dptr(E2),
+                                              nb2, dptr(E3p), iptr(nb3p), dptr(E3m), iptr(nb3m),
+                                              dptr(outP), dptr(outM)), self.ctx.h)
+        cp, cm = [], []
+        oP = oM = 0
+        for i in range(nq1):
+            n = nb1s[i] * nb2 * nb3p[i]
+            cp.append(outP[oP:oP + n].reshape(nb1s[i], nb2, nb3p[i]))
+            oP += n
+            n = nb1s[i] * nb2 * nb3m[i]
+            cm.append(outM[oM:oM + n].reshape(nb1s[i], nb2, nb3m[i]))
+            oM += n
+        return cp, cm
+
+    def estimateNumBatches(self, nq1, nb2):
+        n = ctypes.c_int(0)
+        check(_abi.load().phx_v3_estimate_num_batches(self.h, nq1, nb2, ctypes.byref(n)), self.ctx.h)
+        return n.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            _abi.load().phx_v3_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PhScatteringMatrix:
+    """RTA phonon scattering rates on a full mesh (linewidth mode of the builder)."""
+
+    def __init__(self, coupling3Ph, bands, temperatures_ry, smearing="adaptive", sigma=0.0):
+        self.v3 = coupling3Ph
+        self.bands = bands
+        self.temperatures = f64(np.atleast_1d(temperatures_ry))
+        self.smearing = smearing
+        self.sigma = float(sigma)
+        self.internalDiagonal = None
+        self.stats = None
+
+    def _params(self, q2_begin=0, q2_end=None, finalize=True):
+        p = _abi.LwParams()
+        p.num_temperatures = len(self.temperatures)
+        p.temperatures = dptr(self.temperatures)
+        p.smearing = _abi.PHX_SMEAR_GAUSSIAN if self.smearing == "gaussian" else _abi.PHX_SMEAR_ADAPTIVE
+        p.sigma = self.sigma
+        p.finalize = int(finalize)
+        p.q2_begin = int(q2_begin)
+        p.q2_end = int(self.bands.nq if q2_end is None else q2_end)
+        return p
+
+    def setup(self, q2_begin=0, q2_end=None, finalize=True):
+        """Builds A_out = linewidth * n(n+1) (internalDiagonal), shape (nT, nq*nb)."""
+        nT = len(self.temperatures)
+        out = np.zeros((nT, self.bands.nq * self.bands.nb))
+        p = self._params(q2_begin, q2_end, finalize)
+        st = _abi.LwStats()
+        check(_abi.load().phx_ph_linewidths(self.v3.h, self.bands.h, ctypes.byref(p), dptr(out),
+                                            ctypes.byref(st)), self.v3.ctx.h)
+        self.internalDiagonal = out
+        self.stats = st
+        return out
+
+    def getLinewidths(self, E):
+        """Gamma = A_out / (n(n+1)) (scattering.cpp:529-568)."""
+        T = self.temperatures[:, None]
+        x = np.sinh(np.asarray(E).reshape(1, -1) / 2.0 / T)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            return self.internalDiagonal / (0.25 / x / x)
+
+    def getSingleModeTimes(self, E):
+        """tau = n(n+1) / A_out (scattering.cpp:484-513)."""
+        T = self.temperatures[:, None]
+        x = np.sinh(np.asarray(E).reshape(1, -1) / 2.0 / T)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            return (0.25 / x / x) / self.internalDiagonal
+
+    def thermalConductivity(self, volume):
+        """RTA kappa (nT,3,3) in W/(m K)."""
+        kappa = np.zeros((len(self.temperatures), 3, 3))
+        A = f64(self.internalDiagonal)
+        check(_abi.load().phx_ph_rta_kappa(self.bands.h, len(self.temperatures),
+                                           dptr(self.temperatures), dptr(A), float(volume),
+                                           dptr(kappa)), self.v3.ctx.h)
+        return kappa * C.thConductivityAuToSi

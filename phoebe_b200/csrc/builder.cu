@@ -1,0 +1,795 @@
+// Fused 3-phonon linewidth builder (PhScatteringMatrix::builder, linewidth
+// mode) on a full Gamma-centred mesh -- plain FP64 path.
+//
+// Reference: src/bte/ph_scattering.cpp:60-613 (q2 outer loop, q1 batches,
+// HOT LOOP 3), src/bte/scattering.cpp:1209-1318 (symmetrizeCoupling),
+// :1168-1207 (degeneracyAveragingLinewidths), src/delta_function.cpp:34-96,
+// src/particle.cpp:64-96, src/bte/helper_3rd_state.cpp:128-170 (q3 lookup).
+//
+// Restructuring (same arithmetic, different order):
+//  * q3 = q1 + q2 is found by integer mesh arithmetic, which is what the
+//    reference's Cartesian round trip + rounding computes on a Gamma-centred
+//    mesh (src/points.cpp:404-423).
+//  * The e2 contraction and every q2-only phase are folded into the cached
+//    vertex once per q2:  Dp(q2)[r3][a][b2][c] = e^{-i q2.R3} sum_b e2(b,b2)
+//    sum_r2 D3w(r3,r2,a,b,c) e^{+i q2.R2}, so each (q1,q2) pair costs one
+//    [r3] x [a,b2,c] complex contraction plus two 6x6x6 contractions.
+//  * Only the "+" vertex is evaluated.  By time reversal (D(-q) = conj D(q)
+//    for real force constants, so e(-q) = conj e(q) up to a gauge) the
+//    symmetrised |V-(q1,-q2)|^2 equals the symmetrised |V+(q1,q2)|^2 with the
+//    same q3 = q1+q2; each evaluated pair therefore feeds the "+" rate of
+//    (q1,q2) and the "-" rates of (q1,-q2).  Energies, velocities and Bose
+//    factors of -q2 are read from the mesh tables at the index of -q2.
+//  * Accumulation is owner-computes per q1 tile: a CTA owns 32 q1 points and a
+//    slice of q2, keeps its partial linewidths in registers and adds them to
+//    its own slot of a partial buffer; a final kernel sums the slots in a
+//    fixed order (deterministic, no atomics), then applies degeneracy
+//    averaging and the exclusion of acoustic Gamma modes.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "cplx.cuh"
+#include "phx_consts.h"
+#include "phx_internal.h"
+
+namespace {
+
+constexpr int kTile = 32;    // q1 points per CTA
+constexpr int kMaxT = 4;     // temperatures handled per launch
+
+struct MeshArgs {
+  int nq, nb, nT, n0, n1, n2;
+  const double* E;      // (nq,nb)
+  const double2* U;     // (nq,nb,nb)
+  const double* vg;     // (nq,nb,3) or null
+  const double* bose;   // (nT,nq,nb)
+  const double* qcart;  // (nq,3)
+  int smearing;
+  double sigma;
+  double qT[9];         // adaptive: reciprocal cell rows / mesh
+  double norm;          // 1/Nq
+};
+
+__device__ __forceinline__ int mesh_add(int i, int j, int n0, int n1, int n2) {
+  const int ix = i % n0, iy = (i / n0) % n1, iz = i / (n0 * n1);
+  const int jx = j % n0, jy = (j / n0) % n1, jz = j / (n0 * n1);
+  return ((iz + jz) % n2) * n0 * n1 + ((iy + jy) % n1) * n0 + (ix + jx) % n0;
+}
+
+__device__ __forceinline__ int mesh_neg(int i, int n0, int n1, int n2) {
+  const int ix = i % n0, iy = (i / n0) % n1, iz = i / (n0 * n1);
+  return ((n2 - iz) % n2) * n0 * n1 + ((n1 - iy) % n1) * n0 + (n0 - ix) % n0;
+}
+
+// AdaptiveGaussianDeltaFunction sigma (delta_function.cpp:71-83) before the
+// floor; returns -1 for the "v == 0" special case handled by the caller.
+__device__ __forceinline__ double adaptive_sigma(const double* qT, double v0, double v1, double v2) {
+  double s = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const double d = qT[3 * i] * v0 + qT[3 * i + 1] * v1 + qT[3 * i + 2] * v2;
+    s += d * d;
+  }
+  return sqrt(s / 6.0);
+}
+
+// delta(E) with the reference's cut-offs; vzero: velocity difference is 0.
+__device__ __forceinline__ double delta_fn(int smearing, double sigma, double e, bool vzero) {
+  if (smearing == PHX_SMEAR_GAUSSIAN) {
+    const double x = e / sigma;
+    if (x > 6.0) return 0.0;
+    return 1.0 / sigma / phxc::sqrtPi * exp(-x * x);
+  }
+  if (vzero && e == 0.0) return 1.0;
+  if (sigma == 0.0) return 0.0;
+  if (fabs(e) > 2.0 * sigma) return 0.0;
+  const double x = e / sigma;
+  if (x > 6.0) return 0.0;
+  return exp(-x * x) / phxc::sqrtPi / sigma / phxc::erf2;
+}
+
+__device__ __forceinline__ double floor_sigma(double s) {
+  return (s != 0.0 && s < phxc::adaptiveCutoff) ? phxc::adaptiveCutoff : s;
+}
+
+__global__ void bose_kernel(int nq, int nb, int nT, const double* __restrict__ E,
+                            const double* __restrict__ temps, double* __restrict__ bose) {
+  const int ns = nq * nb;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns * nT; i += gridDim.x * blockDim.x) {
+    const int c = i / ns, s = i % ns;
+    const double t = temps[c], e = E[s];
+    double n;
+    if (t <= 0.0) n = e <= 0.0 ? 1.0 : 0.0;
+    else {
+      n = 1.0 / (exp(e / t) - 1.0);
+      if (n < 0.0) n = 0.0;
+    }
+    bose[i] = n;
+  }
+}
+
+// Dp[j][r3][a][b2][c] for q2 = q2_first + j (one block per (r3, group of q2)).
+__global__ void fold_q2_kernel(int nb, int nr2, int nr3, const double* __restrict__ D3w,
+                               const double* __restrict__ R2, const double* __restrict__ R3,
+                               const double* __restrict__ qcart, const double2* __restrict__ U,
+                               int q2_first, int q2_count, int q2_per_block,
+                               double2* __restrict__ Dp) {
+  extern __shared__ __align__(16) char sraw[];
+  double2* ph2 = reinterpret_cast<double2*>(sraw);   // nr2
+  double2* Y = ph2 + nr2;                            // nb*nb
+  double2* e2 = Y + nb * nb;                         // nb*nb
+  const int r3 = blockIdx.x;
+  const int nbb = nb * nb, nb3 = nbb * nb;
+  const int j0 = blockIdx.y * q2_per_block, j1 = min(q2_count, j0 + q2_per_block);
+  for (int j = j0; j < j1; ++j) {
+    const int iq2 = q2_first + j;
+    const double* q = qcart + 3 * iq2;
+    for (int r = threadIdx.x; r < nr2; r += blockDim.x) {
+      double sn, cs;
+      sincos(q[0] * R2[3 * r] + q[1] * R2[3 * r + 1] + q[2] * R2[3 * r + 2], &sn, &cs);
+      ph2[r] = cmk(cs, sn);
+    }
+    for (int e = threadIdx.x; e < nbb; e += blockDim.x) e2[e] = U[(size_t)iq2 * nbb + e];
+    double sn3, cs3;
+    sincos(-(q[0] * R3[3 * r3] + q[1] * R3[3 * r3 + 1] + q[2] * R3[3 * r3 + 2]), &sn3, &cs3);
+    const double2 p3 = cmk(cs3, sn3);
+    __syncthreads();
+    for (int a = 0; a < nb; ++a) {
+      for (int bc = threadIdx.x; bc < nbb; bc += blockDim.x) {
+        double2 acc = cmk(0.0, 0.0);
+        const double* d = D3w + (size_t)r3 * nr2 * nb3 + (size_t)a * nbb + bc;
+        for (int r = 0; r < nr2; ++r) {
+          const double x = d[(size_t)r * nb3];
+          acc.x = fma(x, ph2[r].x, acc.x);
+          acc.y = fma(x, ph2[r].y, acc.y);
+        }
+        Y[bc] = acc;
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < nbb; e += blockDim.x) {
+        const int b2 = e / nb, c = e % nb;
+        double2 z = cmk(0.0, 0.0);
+        for (int b = 0; b < nb; ++b) cfma(z, e2[b * nb + b2], Y[b * nb + c]);
+        Dp[(((size_t)j * nr3 + r3) * nb + a) * nbb + b2 * nb + c] = cmul(z, p3);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Forward-scan degeneracy blocks (scattering.cpp:1218-1230): gs[b] = first
+// band of b's block, gn[b] = its size.
+template <int NB>
+__device__ __forceinline__ void deg_blocks(const double* e, int* gs, int* gn) {
+  int start = 0;
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    if (b > start) {
+      // b continues the block iff |e[start] - e[b]| < thr and all between did
+      if (!(fabs(e[start] - e[b]) < phxc::degThreshold)) start = b;
+    }
+    gs[b] = start;
+  }
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    int n = 0;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) n += (gs[k] == gs[b]);
+    gn[b] = n;
+  }
+}
+
+struct PairArgs {
+  MeshArgs m;
+  int nr3;
+  const double* R3;
+  const double2* Dp;
+  int q2_first, q2_count, q2_per_slot;
+  double* partial;   // (S, nq, nb, nT)
+};
+
+template <int NB>
+__global__ void __launch_bounds__(kTile * NB, 1) pair_fp64_kernel(PairArgs P) {
+  const MeshArgs& M = P.m;
+  extern __shared__ __align__(16) char sraw[];
+  const int nr3 = P.nr3, nT = M.nT;
+  double2* ph = reinterpret_cast<double2*>(sraw);      // [nr3][32]
+  double2* e1s = ph + (size_t)nr3 * kTile;             // [NB*NB][32]
+  double2* e3s = e1s + NB * NB * kTile;                // [NB*NB][32]
+  double* Wx = reinterpret_cast<double*>(e3s + NB * NB * kTile);  // [NB][NB*NB][32]
+  double* b1s = Wx + NB * NB * NB * kTile;              // [nT][NB][32]
+  const int tid = threadIdx.x, ql = tid & 31, b2 = tid >> 5;
+  const int q1 = blockIdx.x * kTile + ql;
+  const bool valid = q1 < M.nq;
+  const int q1c = valid ? q1 : M.nq - 1;
+  const int n0 = M.n0, n1 = M.n1, n2 = M.n2, nq = M.nq;
+  // --- per-CTA setup: phases e^{-i q1.R3}, e1, Bose(q1)
+  for (int i = tid; i < nr3 * kTile; i += blockDim.x) {
+    const int r = i / kTile, l = i % kTile;
+    const int qq = min(blockIdx.x * kTile + l, nq - 1);
+    const double* q = M.qcart + 3 * qq;
+    double sn, cs;
+    sincos(-(q[0] * P.R3[3 * r] + q[1] * P.R3[3 * r + 1] + q[2] * P.R3[3 * r + 2]), &sn, &cs);
+    ph[i] = cmk(cs, sn);
+  }
+  for (int i = tid; i < NB * NB * kTile; i += blockDim.x) {
+    const int e = i / kTile, l = i % kTile;
+    const int qq = min(blockIdx.x * kTile + l, nq - 1);
+    e1s[i] = M.U[(size_t)qq * NB * NB + e];
+  }
+  for (int i = tid; i < nT * NB * kTile; i += blockDim.x) {
+    const int l = i % kTile, cb = i / kTile, b = cb % NB, c = cb / NB;
+    const int qq = min(blockIdx.x * kTile + l, nq - 1);
+    b1s[i] = M.bose[((size_t)c * nq + qq) * NB + b];
+  }
+  double E1[NB];
+  int g1s[NB], g1n[NB];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) E1[b] = M.E[(size_t)q1c * NB + b];
+  deg_blocks<NB>(E1, g1s, g1n);
+  double acc[NB][kMaxT];
+#pragma unroll
+  for (int b = 0; b < NB; ++b)
+#pragma unroll
+    for (int c = 0; c < kMaxT; ++c) acc[b][c] = 0.0;
+  __syncthreads();
+
+  const int jbeg = blockIdx.y * P.q2_per_slot;
+  const int jend = min(P.q2_count, jbeg + P.q2_per_slot);
+  for (int j = jbeg; j < jend; ++j) {
+    const int iq2 = P.q2_first + j;
+    const int iq2m = mesh_neg(iq2, n0, n1, n2);
+    const int iq3 = mesh_add(q1c, iq2, n0, n1, n2);
+    // stage e3 of the 32 q3 points
+    for (int i = tid; i < NB * NB * kTile; i += blockDim.x) {
+      const int e = i / kTile, l = i % kTile;
+      const int qq = min(blockIdx.x * kTile + l, nq - 1);
+      const int q3 = mesh_add(qq, iq2, n0, n1, n2);
+      e3s[i] = M.U[(size_t)q3 * NB * NB + e];
+    }
+    __syncthreads();
+    // T(a,c) = sum_r3 e^{-i q1.R3} Dp(q2)[r3][a][b2][c]
+    double2 T[NB][NB];
+#pragma unroll
+    for (int a = 0; a < NB; ++a)
+#pragma unroll
+      for (int c = 0; c < NB; ++c) T[a][c] = cmk(0.0, 0.0);
+    const double2* D = P.Dp + (size_t)j * nr3 * NB * NB * NB + b2 * NB;
+    for (int r = 0; r < nr3; ++r) {
+      const double2 p = ph[r * kTile + ql];
+      const double2* Dr = D + (size_t)r * NB * NB * NB;
+#pragma unroll
+      for (int a = 0; a < NB; ++a)
+#pragma unroll
+        for (int c = 0; c < NB; ++c) cfma(T[a][c], p, __ldg(Dr + a * NB * NB + c));
+    }
+    // X(b1,c) = sum_a e1(a,b1) T(a,c), in place column by column
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+      double2 col[NB];
+#pragma unroll
+      for (int a = 0; a < NB; ++a) col[a] = T[a][c];
+#pragma unroll
+      for (int b1 = 0; b1 < NB; ++b1) {
+        double2 x = cmk(0.0, 0.0);
+#pragma unroll
+        for (int a = 0; a < NB; ++a) cfma(x, e1s[(a * NB + b1) * kTile + ql], col[a]);
+        T[b1][c] = x;
+      }
+    }
+    // V(b1,b3) = sum_c X(b1,c) conj(e3(c,b3)); W = |V|^2
+    double W[NB][NB];
+#pragma unroll
+    for (int b1 = 0; b1 < NB; ++b1) {
+#pragma unroll
+      for (int b3 = 0; b3 < NB; ++b3) {
+        double2 v = cmk(0.0, 0.0);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) cfmac(v, T[b1][c], e3s[(c * NB + b3) * kTile + ql]);
+        W[b1][b3] = v.x * v.x + v.y * v.y;
+      }
+    }
+    // symmetrise over degenerate blocks of b1 (E1) and b3 (E3)
+    double E3[NB];
+    int g3s[NB], g3n[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) E3[b] = M.E[(size_t)iq3 * NB + b];
+    deg_blocks<NB>(E3, g3s, g3n);
+#pragma unroll
+    for (int b1 = 0; b1 < NB; ++b1) {
+      double row[NB];
+#pragma unroll
+      for (int b3 = 0; b3 < NB; ++b3) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < NB; ++k) s += (g3s[k] == g3s[b3]) ? W[b1][k] : 0.0;
+        row[b3] = s / (double)g3n[b3];
+      }
+#pragma unroll
+      for (int b3 = 0; b3 < NB; ++b3) W[b1][b3] = row[b3];
+    }
+#pragma unroll
+    for (int b3 = 0; b3 < NB; ++b3) {
+      double colv[NB];
+#pragma unroll
+      for (int b1 = 0; b1 < NB; ++b1) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < NB; ++k) s += (g1s[k] == g1s[b1]) ? W[k][b3] : 0.0;
+        colv[b1] = s / (double)g1n[b1];
+      }
+#pragma unroll
+      for (int b1 = 0; b1 < NB; ++b1) W[b1][b3] = colv[b1];
+    }
+    // exchange across b2 (one warp per b2) and average over E2 blocks
+#pragma unroll
+    for (int b1 = 0; b1 < NB; ++b1)
+#pragma unroll
+      for (int b3 = 0; b3 < NB; ++b3) Wx[((b2 * NB + b1) * NB + b3) * kTile + ql] = W[b1][b3];
+    __syncthreads();
+    double E2v[NB];
+    int g2s[NB], g2n[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) E2v[b] = M.E[(size_t)iq2 * NB + b];
+    deg_blocks<NB>(E2v, g2s, g2n);
+    int mys = 0, myn = 1;
+#pragma unroll
+    for (int b = 0; b < NB; ++b)
+      if (b == b2) { mys = g2s[b]; myn = g2n[b]; }
+    if (myn > 1) {
+#pragma unroll
+      for (int b1 = 0; b1 < NB; ++b1)
+#pragma unroll
+        for (int b3 = 0; b3 < NB; ++b3) {
+          double s = 0.0;
+          for (int k = mys; k < mys + myn; ++k) s += Wx[((k * NB + b1) * NB + b3) * kTile + ql];
+          W[b1][b3] = s / (double)myn;
+        }
+    }
+    // epilogue: "+" rates of (q1,q2) and "-" rates of (q1,-q2)
+    const double en2 = M.E[(size_t)iq2 * NB + b2];
+    const double en2m = M.E[(size_t)iq2m * NB + b2];
+    const bool ok2 = en2 >= phxc::phExcludeCutoff && en2 >= phxc::phEnergyCutoff;
+    const bool ok2m = en2m >= phxc::phExcludeCutoff && en2m >= phxc::phEnergyCutoff;
+    double v2[3] = {0, 0, 0}, v2m[3] = {0, 0, 0};
+    if (M.smearing == PHX_SMEAR_ADAPTIVE) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        v2[i] = M.vg[((size_t)iq2 * NB + b2) * 3 + i];
+        v2m[i] = M.vg[((size_t)iq2m * NB + b2) * 3 + i];
+      }
+    }
+    if (valid && (ok2 || ok2m)) {
+#pragma unroll
+      for (int b3 = 0; b3 < NB; ++b3) {
+        const double en3 = E3[b3];
+        if (en3 < phxc::phEnergyCutoff) continue;
+        double sp = M.sigma, sm = M.sigma;
+        bool vzp = false, vzm = false;
+        if (M.smearing == PHX_SMEAR_ADAPTIVE) {
+          const double* v3 = M.vg + ((size_t)iq3 * NB + b3) * 3;
+          const double dp0 = v2[0] - v3[0], dp1 = v2[1] - v3[1], dp2 = v2[2] - v3[2];
+          const double dm0 = v2m[0] - v3[0], dm1 = v2m[1] - v3[1], dm2 = v2m[2] - v3[2];
+          vzp = (dp0 * dp0 + dp1 * dp1 + dp2 * dp2) == 0.0;
+          vzm = (dm0 * dm0 + dm1 * dm1 + dm2 * dm2) == 0.0;
+          sp = floor_sigma(adaptive_sigma(M.qT, dp0, dp1, dp2));
+          sm = floor_sigma(adaptive_sigma(M.qT, dm0, dm1, dm2));
+        }
+        double n3[kMaxT];
+#pragma unroll
+        for (int c = 0; c < kMaxT; ++c)
+          n3[c] = c < nT ? M.bose[((size_t)c * nq + iq3) * NB + b3] : 0.0;
+        double n2[kMaxT], n2m[kMaxT];
+#pragma unroll
+        for (int c = 0; c < kMaxT; ++c) {
+          n2[c] = c < nT ? M.bose[((size_t)c * nq + iq2) * NB + b2] : 0.0;
+          n2m[c] = c < nT ? M.bose[((size_t)c * nq + iq2m) * NB + b2] : 0.0;
+        }
+#pragma unroll
+        for (int b1 = 0; b1 < NB; ++b1) {
+          const double en1 = E1[b1];
+          if (en1 < phxc::phExcludeCutoff || en1 < phxc::phEnergyCutoff) continue;
+          const double w = W[b1][b3];
+          if (ok2) {
+            const double dlt = delta_fn(M.smearing, sp, en1 + en2 - en3, vzp);
+            if (dlt > 0.0) {
+              const double f = phxc::pi * 0.25 * w * dlt * M.norm / (en1 * en2 * en3);
+#pragma unroll
+              for (int c = 0; c < kMaxT; ++c)
+                if (c < nT) {
+                  const double n1 = b1s[(c * NB + b1) * kTile + ql];
+                  acc[b1][c] += 0.5 * (f * n1 * n2[c] * (n3[c] + 1.0));
+                }
+            }
+          }
+          if (ok2m) {
+            double d1 = delta_fn(M.smearing, sm, en1 + en3 - en2m, vzm);
+            double d2 = delta_fn(M.smearing, sm, en2m + en3 - en1, vzm);
+            if (d1 > 0.0 || d2 > 0.0) {
+              d1 = fmax(d1, 0.0);
+              d2 = fmax(d2, 0.0);
+              const double f = phxc::pi * 0.25 * w * M.norm / (en1 * en2m * en3);
+#pragma unroll
+              for (int c = 0; c < kMaxT; ++c)
+                if (c < nT) {
+                  const double n1 = b1s[(c * NB + b1) * kTile + ql];
+                  const double r1 = f * n3[c] * n1 * (n2m[c] + 1.0) * d1;
+                  const double r2 = f * n2m[c] * n3[c] * (n1 + 1.0) * d2;
+                  acc[b1][c] += 0.5 * (r1 + r2);
+                }
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // reduce over the b2 warps and add to this CTA's partial slot
+#pragma unroll
+  for (int b1 = 0; b1 < NB; ++b1)
+#pragma unroll
+    for (int c = 0; c < kMaxT; ++c) Wx[((b2 * NB + b1) * kMaxT + c) * kTile + ql] = acc[b1][c];
+  __syncthreads();
+  if (b2 == 0 && valid) {
+    double* out = P.partial + ((size_t)blockIdx.y * nq + q1) * NB * nT;
+    for (int b1 = 0; b1 < NB; ++b1)
+      for (int c = 0; c < nT; ++c) {
+        double s = 0.0;
+        for (int k = 0; k < NB; ++k) s += Wx[((k * NB + b1) * kMaxT + c) * kTile + ql];
+        out[b1 * nT + c] += s;
+      }
+  }
+}
+
+__global__ void finalize_kernel(int nq, int nb, int nT, int nslots, const double* __restrict__ partial,
+                                const double* __restrict__ E, int finalize,
+                                double* __restrict__ Aout) {
+  const int iq = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iq >= nq) return;
+  const size_t ns = (size_t)nq * nb;
+  double lw[64];
+  for (int c = 0; c < nT; ++c) {
+    for (int b = 0; b < nb; ++b) {
+      double s = 0.0;
+      for (int k = 0; k < nslots; ++k) s += partial[(((size_t)k * nq + iq) * nb + b) * nT + c];
+      lw[b] = s;
+    }
+    if (finalize && c == 0) {
+      // degeneracyAveragingLinewidths (scattering.cpp:1168-1207), row 0 only
+      double tmp[64];
+      for (int b1 = 0; b1 < nb; ++b1) {
+        int n = 0;
+        double t = 0.0;
+        for (int b2 = 0; b2 < nb; ++b2)
+          if (fabs(E[(size_t)iq * nb + b2] - E[(size_t)iq * nb + b1]) < phxc::degThreshold) {
+            ++n;
+            t += lw[b2];
+          }
+        tmp[b1] = t / (double)(float)n;
+      }
+      for (int b = 0; b < nb; ++b) lw[b] = tmp[b];
+    }
+    for (int b = 0; b < nb; ++b) {
+      double v = lw[b];
+      if (finalize && E[(size_t)iq * nb + b] < phxc::phExcludeCutoff) v = 0.0;
+      Aout[(size_t)c * ns + (size_t)iq * nb + b] = v;
+    }
+  }
+}
+
+size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+
+int phx_scratch_reserve(phx_v3* v, size_t bytes) {
+  if (v->scratch_bytes >= bytes) return PHX_OK;
+  cudaFree(v->d_scratch);
+  v->d_scratch = nullptr;
+  v->scratch_bytes = 0;
+  PHX_CUDA(v->ctx, cudaMalloc(&v->d_scratch, bytes));
+  v->scratch_bytes = bytes;
+  return PHX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// band structures on a mesh
+// ---------------------------------------------------------------------------
+static void mesh_cartesian(const int* mesh, const double* recip, std::vector<double>& q) {
+  const int nq = mesh[0] * mesh[1] * mesh[2];
+  q.resize(3 * (size_t)nq);
+  for (int i = 0; i < nq; ++i) {
+    const int iz = i / (mesh[0] * mesh[1]);
+    const int r = i - iz * mesh[0] * mesh[1];
+    const int iy = r / mesh[0], ix = r % mesh[0];
+    const double c[3] = {double(ix) / double(mesh[0]), double(iy) / double(mesh[1]),
+                         double(iz) / double(mesh[2])};
+    for (int k = 0; k < 3; ++k)
+      q[3 * i + k] = recip[k * 3 + 0] * c[0] + recip[k * 3 + 1] * c[1] + recip[k * 3 + 2] * c[2];
+  }
+}
+
+extern "C" int phx_bands_create_mesh(phx_ph_h0* h0, const int* mesh, int with_velocities,
+                                     phx_bands** out) {
+  PHX_ARG(nullptr, h0 && mesh && out, "phx_bands_create_mesh: bad arguments");
+  phx_ctx* ctx = h0->ctx;
+  PHX_ARG(ctx, mesh[0] > 0 && mesh[1] > 0 && mesh[2] > 0, "bad mesh");
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  phx_bands* b = new phx_bands;
+  b->ctx = ctx;
+  b->nb = h0->nb;
+  b->nq = mesh[0] * mesh[1] * mesh[2];
+  for (int i = 0; i < 3; ++i) b->mesh[i] = mesh[i];
+  for (int i = 0; i < 9; ++i) b->recip[i] = h0->recip[i];
+  std::vector<double> q;
+  mesh_cartesian(mesh, h0->recip, q);
+  const size_t nq = b->nq, nb = b->nb;
+  cudaError_t e = cudaMalloc(&b->d_E, sizeof(double) * nq * nb);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_U, sizeof(double) * 2 * nq * nb * nb);
+  if (e == cudaSuccess && with_velocities) e = cudaMalloc(&b->d_vg, sizeof(double) * 3 * nq * nb);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_q, sizeof(double) * 3 * nq);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->d_q, q.data(), sizeof(double) * 3 * nq, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    phx_set_error(ctx, PHX_ERR_CUDA, cudaGetErrorString(e));
+    phx_bands_destroy(b);
+    return PHX_ERR_CUDA;
+  }
+  int rc = phx_launch_ph_bands(h0, b->nq, b->d_q, b->d_E, b->d_U, b->d_vg, 1);
+  if (rc != PHX_OK) {
+    phx_bands_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return PHX_OK;
+}
+
+extern "C" int phx_bands_create_from_host(phx_ctx* ctx, const int* mesh,
+                                          const double* reciprocal_cell, int nb, const double* E,
+                                          const double* U, const double* vg, phx_bands** out) {
+  PHX_ARG(ctx, ctx && mesh && reciprocal_cell && E && U && out && nb > 0 && nb <= 63,
+          "phx_bands_create_from_host: bad arguments");
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  phx_bands* b = new phx_bands;
+  b->ctx = ctx;
+  b->nb = nb;
+  b->nq = mesh[0] * mesh[1] * mesh[2];
+  for (int i = 0; i < 3; ++i) b->mesh[i] = mesh[i];
+  for (int i = 0; i < 9; ++i) b->recip[i] = reciprocal_cell[i];
+  std::vector<double> q;
+  mesh_cartesian(mesh, reciprocal_cell, q);
+  const size_t nq = b->nq;
+  cudaError_t e = cudaMalloc(&b->d_E, sizeof(double) * nq * nb);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_U, sizeof(double) * 2 * nq * nb * nb);
+  if (e == cudaSuccess && vg) e = cudaMalloc(&b->d_vg, sizeof(double) * 3 * nq * nb);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_q, sizeof(double) * 3 * nq);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_E, E, sizeof(double) * nq * nb, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_U, U, sizeof(double) * 2 * nq * nb * nb, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess && vg)
+    e = cudaMemcpyAsync(b->d_vg, vg, sizeof(double) * 3 * nq * nb, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_q, q.data(), sizeof(double) * 3 * nq, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    phx_set_error(ctx, PHX_ERR_CUDA, cudaGetErrorString(e));
+    phx_bands_destroy(b);
+    return PHX_ERR_CUDA;
+  }
+  *out = b;
+  return PHX_OK;
+}
+
+extern "C" int phx_bands_destroy(phx_bands* b) {
+  if (!b) return PHX_OK;
+  if (b->ctx) cudaSetDevice(b->ctx->device);
+  cudaFree(b->d_E);
+  cudaFree(b->d_U);
+  cudaFree(b->d_vg);
+  cudaFree(b->d_q);
+  cudaFree(b->d_U32);
+  delete b;
+  return PHX_OK;
+}
+
+extern "C" int phx_bands_num_points(const phx_bands* b) { return b ? b->nq : 0; }
+
+extern "C" int phx_bands_get(phx_bands* b, double* E, double* U, double* vg) {
+  PHX_ARG(nullptr, b, "null bands handle");
+  phx_ctx* ctx = b->ctx;
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t nq = b->nq, nb = b->nb;
+  if (E) PHX_CUDA(ctx, cudaMemcpyAsync(E, b->d_E, sizeof(double) * nq * nb, cudaMemcpyDeviceToHost, ctx->stream));
+  if (U)
+    PHX_CUDA(ctx, cudaMemcpyAsync(U, b->d_U, sizeof(double) * 2 * nq * nb * nb, cudaMemcpyDeviceToHost, ctx->stream));
+  if (vg) {
+    PHX_ARG(ctx, b->d_vg != nullptr, "band structure has no velocities");
+    PHX_CUDA(ctx, cudaMemcpyAsync(vg, b->d_vg, sizeof(double) * 3 * nq * nb, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// builder
+// ---------------------------------------------------------------------------
+namespace {
+
+struct BuilderPlan {
+  int chunk = 512;      // q2 per fold/pair launch
+  int slots = 8;        // partial-sum slots (q2 slices per chunk)
+};
+
+template <int NB>
+int run_fp64(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
+             phx_lw_stats* stats) {
+  phx_ctx* ctx = v->ctx;
+  cudaStream_t st = ctx->stream;
+  const int nq = b->nq, nT = p->num_temperatures, nr3 = v->nr3, nr2 = v->nr2;
+  const int q2b = p->q2_begin, q2e = p->q2_end;
+  BuilderPlan plan;
+  plan.chunk = std::min(plan.chunk, std::max(1, q2e - q2b));
+  const size_t nb3 = (size_t)NB * NB * NB;
+  const size_t sz_dp = align_up(sizeof(double2) * plan.chunk * nr3 * nb3);
+  const size_t sz_part = align_up(sizeof(double) * plan.slots * nq * NB * nT);
+  const size_t sz_bose = align_up(sizeof(double) * nT * nq * NB);
+  const size_t sz_T = align_up(sizeof(double) * 8);
+  PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T));
+  char* base = static_cast<char*>(v->d_scratch);
+  double2* Dp = reinterpret_cast<double2*>(base);
+  double* partial = reinterpret_cast<double*>(base + sz_dp);
+  double* bose = reinterpret_cast<double*>(base + sz_dp + sz_part);
+  double* temps = reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose);
+  cudaEvent_t ev0, ev1, evv0, evv1;
+  PHX_CUDA(ctx, cudaEventCreate(&ev0));
+  PHX_CUDA(ctx, cudaEventCreate(&ev1));
+  PHX_CUDA(ctx, cudaEventCreate(&evv0));
+  PHX_CUDA(ctx, cudaEventCreate(&evv1));
+  int launches = 0;
+  PHX_CUDA(ctx, cudaEventRecord(ev0, st));
+  PHX_CUDA(ctx, cudaMemcpyAsync(temps, p->temperatures, sizeof(double) * nT, cudaMemcpyHostToDevice, st));
+  PHX_CUDA(ctx, cudaMemsetAsync(partial, 0, sizeof(double) * plan.slots * nq * NB * nT, st));
+  bose_kernel<<<std::min(1024, (nq * NB * nT + 255) / 256), 256, 0, st>>>(nq, NB, nT, b->d_E, temps, bose);
+  ++launches;
+  PairArgs P;
+  P.m.nq = nq;
+  P.m.nb = NB;
+  P.m.nT = nT;
+  P.m.n0 = b->mesh[0];
+  P.m.n1 = b->mesh[1];
+  P.m.n2 = b->mesh[2];
+  P.m.E = b->d_E;
+  P.m.U = reinterpret_cast<const double2*>(b->d_U);
+  P.m.vg = b->d_vg;
+  P.m.bose = bose;
+  P.m.qcart = b->d_q;
+  P.m.smearing = p->smearing;
+  P.m.sigma = p->sigma;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) P.m.qT[i * 3 + j] = b->recip[i * 3 + j] / b->mesh[i];
+  P.m.norm = 1.0 / (double)nq;
+  P.nr3 = nr3;
+  P.R3 = v->d_R3;
+  P.Dp = Dp;
+  P.partial = partial;
+  const size_t smem_pair = sizeof(double2) * ((size_t)nr3 * kTile + 2 * NB * NB * kTile) +
+                           sizeof(double) * ((size_t)NB * NB * NB * kTile + (size_t)kMaxT * NB * kTile);
+  PHX_ARG(ctx, smem_pair <= 227 * 1024, "phx_ph_linewidths: too many R3 vectors for the FP64 path");
+  PHX_CUDA(ctx, cudaFuncSetAttribute(pair_fp64_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_pair));
+  const size_t smem_fold = sizeof(double2) * (nr2 + 2 * NB * NB);
+  const int tiles = (nq + kTile - 1) / kTile;
+  PHX_CUDA(ctx, cudaEventRecord(evv0, st));
+  for (int c0 = q2b; c0 < q2e; c0 += plan.chunk) {
+    const int cnt = std::min(plan.chunk, q2e - c0);
+    const int per_block = 8;
+    dim3 gf(nr3, (cnt + per_block - 1) / per_block);
+    fold_q2_kernel<<<gf, 128, smem_fold, st>>>(NB, nr2, nr3, v->d_D3w, v->d_R2, v->d_R3, b->d_q,
+                                               reinterpret_cast<const double2*>(b->d_U), c0, cnt,
+                                               per_block, Dp);
+    ++launches;
+    P.q2_first = c0;
+    P.q2_count = cnt;
+    P.q2_per_slot = (cnt + plan.slots - 1) / plan.slots;
+    dim3 gp(tiles, plan.slots);
+    pair_fp64_kernel<NB><<<gp, kTile * NB, smem_pair, st>>>(P);
+    ++launches;
+    PHX_CUDA(ctx, cudaGetLastError());
+  }
+  PHX_CUDA(ctx, cudaEventRecord(evv1, st));
+  finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, NB, nT, plan.slots, partial, b->d_E,
+                                                    p->finalize, Aout_d);
+  ++launches;
+  PHX_CUDA(ctx, cudaGetLastError());
+  PHX_CUDA(ctx, cudaEventRecord(ev1, st));
+  PHX_CUDA(ctx, cudaEventSynchronize(ev1));
+  if (stats) {
+    float ms = 0, msv = 0;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventElapsedTime(&msv, evv0, evv1);
+    stats->ms_total = ms;
+    stats->ms_vertex = msv;
+    stats->pairs = (long long)nq * (q2e - q2b);
+    stats->kernel_launches = launches;
+  }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  cudaEventDestroy(evv0);
+  cudaEventDestroy(evv1);
+  return PHX_OK;
+}
+
+}  // namespace
+
+extern "C" int phx_ph_linewidths_d(phx_v3* v, phx_bands* b, const phx_lw_params* p,
+                                   double* Aout_d, phx_lw_stats* stats) {
+  PHX_ARG(nullptr, v && b && p && Aout_d, "phx_ph_linewidths: bad arguments");
+  phx_ctx* ctx = v->ctx;
+  PHX_ARG(ctx, b->ctx == ctx, "v3 and bands belong to different contexts");
+  PHX_ARG(ctx, b->nb == v->nb, "band count of bands and v3 differ");
+  PHX_ARG(ctx, p->num_temperatures >= 1 && p->num_temperatures <= kMaxT && p->temperatures,
+          "1..4 temperatures per call");
+  PHX_ARG(ctx, p->smearing == PHX_SMEAR_GAUSSIAN || p->smearing == PHX_SMEAR_ADAPTIVE, "bad smearing");
+  PHX_ARG(ctx, p->smearing != PHX_SMEAR_GAUSSIAN || p->sigma > 0.0, "Gaussian smearing needs sigma > 0");
+  PHX_ARG(ctx, p->smearing != PHX_SMEAR_ADAPTIVE || b->d_vg, "adaptive smearing needs velocities");
+  PHX_ARG(ctx, 0 <= p->q2_begin && p->q2_begin <= p->q2_end && p->q2_end <= b->nq, "bad q2 range");
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (p->q2_begin == p->q2_end) {
+    PHX_CUDA(ctx, cudaMemsetAsync(Aout_d, 0, sizeof(double) * p->num_temperatures * b->nq * b->nb, ctx->stream));
+    return PHX_OK;
+  }
+  switch (v->nb) {
+    case 6:
+      return run_fp64<6>(v, b, p, Aout_d, stats);
+    default:
+      phx_set_error(ctx, PHX_ERR_ARG, "phx_ph_linewidths: this build supports nb = 6 on the fused path");
+      return PHX_ERR_ARG;
+  }
+}
+
+extern "C" int phx_ph_linewidths(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout,
+                                 phx_lw_stats* stats) {
+  PHX_ARG(nullptr, v && b && p && Aout, "phx_ph_linewidths: bad arguments");
+  phx_ctx* ctx = v->ctx;
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t n = (size_t)p->num_temperatures * b->nq * b->nb;
+  double* d = nullptr;
+  PHX_CUDA(ctx, cudaMalloc(&d, sizeof(double) * std::max<size_t>(n, 1)));
+  int rc = phx_ph_linewidths_d(v, b, p, d, stats);
+  if (rc == PHX_OK) {
+    cudaError_t e = cudaMemcpyAsync(Aout, d, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+      phx_set_error(ctx, PHX_ERR_CUDA, cudaGetErrorString(e));
+      rc = PHX_ERR_CUDA;
+    }
+  }
+  cudaFree(d);
+  return rc;
+}
+
+extern "C" int phx_ph_rta_kappa(phx_bands* b, int nT, const double* temps, const double* Aout,
+                                double volume, double* kappa) {
+  PHX_ARG(nullptr, b && temps && Aout && kappa && nT > 0 && volume > 0, "phx_ph_rta_kappa: bad arguments");
+  PHX_ARG(b->ctx, b->d_vg, "phx_ph_rta_kappa needs velocities");
+  const size_t ns = (size_t)b->nq * b->nb;
+  std::vector<double> E(ns), vg(3 * ns);
+  PHX_TRY(phx_bands_get(b, E.data(), nullptr, vg.data()));
+  for (int c = 0; c < nT; ++c) {
+    double k[9] = {0};
+    const double T = temps[c];
+    for (size_t s = 0; s < ns; ++s) {
+      const double en = E[s];
+      if (en < phxc::phExcludeCutoff) continue;
+      const double x = std::sinh(en / 2.0 / T);
+      const double pp = 0.25 / x / x;
+      const double tau = pp / Aout[c * ns + s];
+      const double dndt = pp * en / T / T;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          k[i * 3 + j] += dndt * vg[3 * s + i] * tau * vg[3 * s + j] * en / (double)b->nq / volume;
+    }
+    for (int i = 0; i < 9; ++i) kappa[c * 9 + i] = k[i];
+  }
+  return PHX_OK;
+}

@@ -1,0 +1,101 @@
+// Internal definitions shared by the translation units of libphx.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/phx_abi.h"
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+void phx_set_error(const phx_ctx* ctx, int code, const std::string& msg);
+
+#define PHX_CUDA(ctx, call)                                                          \
+  do {                                                                               \
+    cudaError_t _e = (call);                                                         \
+    if (_e != cudaSuccess) {                                                         \
+      phx_set_error((ctx), PHX_ERR_CUDA,                                             \
+                    std::string(#call) + ": " + cudaGetErrorString(_e) + " at " +    \
+                        __FILE__ + ":" + std::to_string(__LINE__));                  \
+      return PHX_ERR_CUDA;                                                           \
+    }                                                                                \
+  } while (0)
+
+#define PHX_ARG(ctx, cond, msg)                       \
+  do {                                                \
+    if (!(cond)) {                                    \
+      phx_set_error((ctx), PHX_ERR_ARG, (msg));       \
+      return PHX_ERR_ARG;                             \
+    }                                                 \
+  } while (0)
+
+#define PHX_TRY(x)             \
+  do {                         \
+    int _rc = (x);             \
+    if (_rc != PHX_OK) return _rc; \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// handles
+// ---------------------------------------------------------------------------
+struct phx_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  mutable std::string last_error;
+  mutable int last_status = 0;
+  // device status word written by kernels (non-convergence, mesh misses)
+  int* d_status = nullptr;
+};
+
+struct phx_ph_h0 {
+  phx_ctx* ctx = nullptr;
+  int nat = 0, nb = 0, numR = 0;
+  double cell[9];             // lattice vectors as columns
+  double recip[9];            // reciprocal vectors as columns
+  std::vector<double> masses; // per band
+  double* d_R = nullptr;      // (numR,3) Wigner-Seitz vectors grouped by atom pair
+  int* d_pofs = nullptr;      // (nat*nat+1) offsets of each atom pair's R range
+  double* d_wblk = nullptr;   // (numR,9) weight * 3x3 force-constant block
+  double* d_masses = nullptr; // (nb)
+};
+
+struct phx_bands {
+  phx_ctx* ctx = nullptr;
+  int nb = 0, nq = 0;
+  int mesh[3] = {0, 0, 0};
+  double recip[9];            // reciprocal cell, columns = b vectors
+  double* d_E = nullptr;      // (nq,nb)
+  double* d_U = nullptr;      // (nq,nb,nb) complex, mass-scaled
+  double* d_vg = nullptr;     // (nq,nb,3) or null
+  double* d_q = nullptr;      // (nq,3) Cartesian mesh points
+  float* d_U32 = nullptr;     // (nq,nb,nb) complex fp32 copy for the split path
+};
+
+struct phx_v3 {
+  phx_ctx* ctx = nullptr;
+  int nat = 0, nb = 0, nr2 = 0, nr3 = 0;
+  int precision = PHX_PREC_FP64;
+  std::vector<double> R2, R3;
+  double* d_D3w = nullptr;     // (nr3,nr2,nb,nb,nb) weights folded (w2*w3*w3)
+  double* d_D3raw = nullptr;   // (nb,nb,nb,nr3,nr2) for the cacheD3 API path
+  double* d_w2 = nullptr;      // (nr2,nat,nat)
+  double* d_w3 = nullptr;      // (nr3,nat,nat)
+  double* d_R2 = nullptr;      // (nr2,3)
+  double* d_R3 = nullptr;      // (nr3,3)
+  double* d_plus = nullptr;    // cached D3+ (nb,nb,nb,nr3) complex
+  double* d_mins = nullptr;    // cached D3- (nb,nb,nb,nr3) complex
+  bool cached = false;
+  double q2_cached[3];
+  // builder scratch (grown on demand)
+  void* d_scratch = nullptr;
+  size_t scratch_bytes = 0;
+};
+
+int phx_scratch_reserve(phx_v3* v3, size_t bytes);
+
+// kernels implemented in harmonic.cu, used by the ABI layer
+int phx_launch_ph_bands(phx_ph_h0* h0, int nq, const double* d_q, double* d_E, double* d_U,
+                        double* d_vg, int mass_scaling);

@@ -38,10 +38,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default=os.environ.get("PHX_BENCH_PRECISION", "fp64"),
+    ap.add_argument("--precision", default=os.environ.get("PHX_BENCH_PRECISION", "split_bf16"),
                     choices=["fp64", "split_bf16", "split_tf32"])
     ap.add_argument("--mesh", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="profiling aid: time the builder only (no e2e leg, no CPU baseline)")
     return ap.parse_args()
 
 
@@ -255,7 +257,7 @@ def run_ours(args):
         fc3.w3.nbytes + T.nbytes
     d2h = nT * nq * nb * 8
     e2e_times = []
-    for i in range(1 + min(args.steps, 3)):
+    for i in range(0 if args.kernels_only else 1 + min(args.steps, 3)):
         barrier()
         t0 = time.perf_counter()
         h0e = PhononH0(ctx, cr, fc2)
@@ -273,7 +275,7 @@ def run_ours(args):
         dt = time.perf_counter() - t0
         if i > 0:
             e2e_times.append(dt)
-    e2e_value = pairs_step / float(np.median(e2e_times))
+    e2e_value = pairs_step / float(np.median(e2e_times)) if e2e_times else None
 
     # roofline of the dominant kernel (fused pair kernel), device-timed
     fl = flops_per_pair(nb, nr3)
@@ -297,7 +299,7 @@ def run_ours(args):
 
     out = None
     if rank == 0:
-        cpu = cpu_baseline(cr, fc2, fc3, mesh, args.cpu_seconds)
+        cpu = None if args.kernels_only else cpu_baseline(cr, fc2, fc3, mesh, args.cpu_seconds)
         out = {"metric": "3ph triplets/s @20^3 mesh", "value": value, "unit": "triplets/s",
                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",

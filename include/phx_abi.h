@@ -166,6 +166,14 @@ int phx_ph_linewidths_d(phx_v3* v3, phx_bands* bands, const phx_lw_params* param
 int phx_ph_rta_kappa(phx_bands* bands, int nT, const double* temperatures,
                      const double* A_out, double volume, double* kappa);
 
+/* ---- diagnostics -------------------------------------------------------- */
+/* Self-test of the split-precision tensor-core GEMM used by the builder: one
+ * 128 x N tile C = A * B^T with A (128,Kp) and B (N,Kp) FP32 host arrays,
+ * split into BF16 hi+lo and accumulated as hi*hi + hi*lo + lo*hi in FP32 via
+ * tcgen05.mma with the builder's shared-memory layouts.  No reference
+ * counterpart (validates this library's own tensor-core building block). */
+int phx_diag_tc_gemm(phx_ctx* ctx, int N, int Kp, const float* A, const float* B, float* C);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,65 +33,13 @@
 #include "phx_consts.h"
 #include "phx_internal.h"
 
+#include "pair_common.cuh"
+
+using namespace pairc;
+
 namespace {
 
 constexpr int kTile = 32;    // q1 points per CTA
-constexpr int kMaxT = 4;     // temperatures handled per launch
-
-struct MeshArgs {
-  int nq, nb, nT, n0, n1, n2;
-  const double* E;      // (nq,nb)
-  const double2* U;     // (nq,nb,nb)
-  const double* vg;     // (nq,nb,3) or null
-  const double* bose;   // (nT,nq,nb)
-  const double* qcart;  // (nq,3)
-  int smearing;
-  double sigma;
-  double qT[9];         // adaptive: reciprocal cell rows / mesh
-  double norm;          // 1/Nq
-};
-
-__device__ __forceinline__ int mesh_add(int i, int j, int n0, int n1, int n2) {
-  const int ix = i % n0, iy = (i / n0) % n1, iz = i / (n0 * n1);
-  const int jx = j % n0, jy = (j / n0) % n1, jz = j / (n0 * n1);
-  return ((iz + jz) % n2) * n0 * n1 + ((iy + jy) % n1) * n0 + (ix + jx) % n0;
-}
-
-__device__ __forceinline__ int mesh_neg(int i, int n0, int n1, int n2) {
-  const int ix = i % n0, iy = (i / n0) % n1, iz = i / (n0 * n1);
-  return ((n2 - iz) % n2) * n0 * n1 + ((n1 - iy) % n1) * n0 + (n0 - ix) % n0;
-}
-
-// AdaptiveGaussianDeltaFunction sigma (delta_function.cpp:71-83) before the
-// floor; returns -1 for the "v == 0" special case handled by the caller.
-__device__ __forceinline__ double adaptive_sigma(const double* qT, double v0, double v1, double v2) {
-  double s = 0.0;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    const double d = qT[3 * i] * v0 + qT[3 * i + 1] * v1 + qT[3 * i + 2] * v2;
-    s += d * d;
-  }
-  return sqrt(s / 6.0);
-}
-
-// delta(E) with the reference's cut-offs; vzero: velocity difference is 0.
-__device__ __forceinline__ double delta_fn(int smearing, double sigma, double e, bool vzero) {
-  if (smearing == PHX_SMEAR_GAUSSIAN) {
-    const double x = e / sigma;
-    if (x > 6.0) return 0.0;
-    return 1.0 / sigma / phxc::sqrtPi * exp(-x * x);
-  }
-  if (vzero && e == 0.0) return 1.0;
-  if (sigma == 0.0) return 0.0;
-  if (fabs(e) > 2.0 * sigma) return 0.0;
-  const double x = e / sigma;
-  if (x > 6.0) return 0.0;
-  return exp(-x * x) / phxc::sqrtPi / sigma / phxc::erf2;
-}
-
-__device__ __forceinline__ double floor_sigma(double s) {
-  return (s != 0.0 && s < phxc::adaptiveCutoff) ? phxc::adaptiveCutoff : s;
-}
 
 __global__ void bose_kernel(int nq, int nb, int nT, const double* __restrict__ E,
                             const double* __restrict__ temps, double* __restrict__ bose) {
@@ -155,28 +103,6 @@ __global__ void fold_q2_kernel(int nb, int nr2, int nr3, const double* __restric
       }
       __syncthreads();
     }
-  }
-}
-
-// Forward-scan degeneracy blocks (scattering.cpp:1218-1230): gs[b] = first
-// band of b's block, gn[b] = its size.
-template <int NB>
-__device__ __forceinline__ void deg_blocks(const double* e, int* gs, int* gn) {
-  int start = 0;
-#pragma unroll
-  for (int b = 0; b < NB; ++b) {
-    if (b > start) {
-      // b continues the block iff |e[start] - e[b]| < thr and all between did
-      if (!(fabs(e[start] - e[b]) < phxc::degThreshold)) start = b;
-    }
-    gs[b] = start;
-  }
-#pragma unroll
-  for (int b = 0; b < NB; ++b) {
-    int n = 0;
-#pragma unroll
-    for (int k = 0; k < NB; ++k) n += (gs[k] == gs[b]);
-    gn[b] = n;
   }
 }
 
@@ -482,6 +408,15 @@ size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
 }  // namespace
 
+// split-precision path (split.cu)
+int phx_split_kp(int nr3);
+size_t phx_split_bimg_bytes(int chunk, int nr3);
+size_t phx_split_smem_bytes(int nr3);
+int phx_split_prepare_bands(phx_ctx* ctx, phx_bands* b);
+int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v, const phx_bands* b,
+                         const double2* Dp, uint8_t* Bimg, int q2_first, int q2_count, int slots,
+                         double* partial, int* launches);
+
 int phx_scratch_reserve(phx_v3* v, size_t bytes) {
   if (v->scratch_bytes >= bytes) return PHX_OK;
   cudaFree(v->d_scratch);
@@ -588,6 +523,7 @@ extern "C" int phx_bands_destroy(phx_bands* b) {
   cudaFree(b->d_vg);
   cudaFree(b->d_q);
   cudaFree(b->d_U32);
+  cudaFree(b->d_q1_order);
   delete b;
   return PHX_OK;
 }
@@ -621,25 +557,40 @@ struct BuilderPlan {
 };
 
 template <int NB>
-int run_fp64(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
-             phx_lw_stats* stats) {
+int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
+                phx_lw_stats* stats) {
   phx_ctx* ctx = v->ctx;
   cudaStream_t st = ctx->stream;
   const int nq = b->nq, nT = p->num_temperatures, nr3 = v->nr3, nr2 = v->nr2;
   const int q2b = p->q2_begin, q2e = p->q2_end;
+  const bool split = v->precision != PHX_PREC_FP64;
   BuilderPlan plan;
+  if (split) {
+    plan.chunk = 448;
+    plan.slots = 7;
+  }
   plan.chunk = std::min(plan.chunk, std::max(1, q2e - q2b));
+  plan.slots = std::min(plan.slots, plan.chunk);
+  // the split kernel gives each of its two b2-parity warp sets its own slot
+  const int nslots = split ? 2 * plan.slots : plan.slots;
   const size_t nb3 = (size_t)NB * NB * NB;
   const size_t sz_dp = align_up(sizeof(double2) * plan.chunk * nr3 * nb3);
-  const size_t sz_part = align_up(sizeof(double) * plan.slots * nq * NB * nT);
+  const size_t sz_part = align_up(sizeof(double) * nslots * nq * NB * nT);
   const size_t sz_bose = align_up(sizeof(double) * nT * nq * NB);
   const size_t sz_T = align_up(sizeof(double) * 8);
-  PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T));
+  const size_t sz_img = split ? align_up(phx_split_bimg_bytes(plan.chunk, nr3)) : 0;
+  PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_img));
   char* base = static_cast<char*>(v->d_scratch);
   double2* Dp = reinterpret_cast<double2*>(base);
   double* partial = reinterpret_cast<double*>(base + sz_dp);
   double* bose = reinterpret_cast<double*>(base + sz_dp + sz_part);
   double* temps = reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose);
+  uint8_t* Bimg = reinterpret_cast<uint8_t*>(base + sz_dp + sz_part + sz_bose + sz_T);
+  if (split) {
+    PHX_ARG(ctx, NB == 6, "split-precision path supports nb = 6");
+    PHX_ARG(ctx, phx_split_smem_bytes(nr3) <= 227 * 1024, "too many R3 vectors for the split path");
+    PHX_TRY(phx_split_prepare_bands(ctx, b));
+  }
   cudaEvent_t ev0, ev1, evv0, evv1;
   PHX_CUDA(ctx, cudaEventCreate(&ev0));
   PHX_CUDA(ctx, cudaEventCreate(&ev1));
@@ -647,8 +598,9 @@ int run_fp64(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   PHX_CUDA(ctx, cudaEventCreate(&evv1));
   int launches = 0;
   PHX_CUDA(ctx, cudaEventRecord(ev0, st));
+  PHX_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
   PHX_CUDA(ctx, cudaMemcpyAsync(temps, p->temperatures, sizeof(double) * nT, cudaMemcpyHostToDevice, st));
-  PHX_CUDA(ctx, cudaMemsetAsync(partial, 0, sizeof(double) * plan.slots * nq * NB * nT, st));
+  PHX_CUDA(ctx, cudaMemsetAsync(partial, 0, sizeof(double) * nslots * nq * NB * nT, st));
   bose_kernel<<<std::min(1024, (nq * NB * nT + 255) / 256), 256, 0, st>>>(nq, NB, nT, b->d_E, temps, bose);
   ++launches;
   PairArgs P;
@@ -674,9 +626,11 @@ int run_fp64(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   P.partial = partial;
   const size_t smem_pair = sizeof(double2) * ((size_t)nr3 * kTile + 2 * NB * NB * kTile) +
                            sizeof(double) * ((size_t)NB * NB * NB * kTile + (size_t)kMaxT * NB * kTile);
-  PHX_ARG(ctx, smem_pair <= 227 * 1024, "phx_ph_linewidths: too many R3 vectors for the FP64 path");
-  PHX_CUDA(ctx, cudaFuncSetAttribute(pair_fp64_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem_pair));
+  if (!split) {
+    PHX_ARG(ctx, smem_pair <= 227 * 1024, "phx_ph_linewidths: too many R3 vectors for the FP64 path");
+    PHX_CUDA(ctx, cudaFuncSetAttribute(pair_fp64_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_pair));
+  }
   const size_t smem_fold = sizeof(double2) * (nr2 + 2 * NB * NB);
   const int tiles = (nq + kTile - 1) / kTile;
   PHX_CUDA(ctx, cudaEventRecord(evv0, st));
@@ -688,6 +642,10 @@ int run_fp64(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
                                                reinterpret_cast<const double2*>(b->d_U), c0, cnt,
                                                per_block, Dp);
     ++launches;
+    if (split) {
+      PHX_TRY(phx_split_pair_chunk(ctx, P.m, v, b, Dp, Bimg, c0, cnt, plan.slots, partial, &launches));
+      continue;
+    }
     P.q2_first = c0;
     P.q2_count = cnt;
     P.q2_per_slot = (cnt + plan.slots - 1) / plan.slots;
@@ -697,12 +655,20 @@ int run_fp64(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
     PHX_CUDA(ctx, cudaGetLastError());
   }
   PHX_CUDA(ctx, cudaEventRecord(evv1, st));
-  finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, NB, nT, plan.slots, partial, b->d_E,
+  finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, NB, nT, nslots, partial, b->d_E,
                                                     p->finalize, Aout_d);
   ++launches;
   PHX_CUDA(ctx, cudaGetLastError());
   PHX_CUDA(ctx, cudaEventRecord(ev1, st));
   PHX_CUDA(ctx, cudaEventSynchronize(ev1));
+  int kst = 0;
+  PHX_CUDA(ctx, cudaMemcpy(&kst, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (kst) {
+    cudaMemset(ctx->d_status, 0, sizeof(int));
+    phx_set_error(ctx, PHX_ERR_CUDA, "pair kernel gave up waiting on a pipeline barrier (status " +
+                                         std::to_string(kst) + ")");
+    return PHX_ERR_CUDA;
+  }
   if (stats) {
     float ms = 0, msv = 0;
     cudaEventElapsedTime(&ms, ev0, ev1);
@@ -740,7 +706,7 @@ extern "C" int phx_ph_linewidths_d(phx_v3* v, phx_bands* b, const phx_lw_params*
   }
   switch (v->nb) {
     case 6:
-      return run_fp64<6>(v, b, p, Aout_d, stats);
+      return run_builder<6>(v, b, p, Aout_d, stats);
     default:
       phx_set_error(ctx, PHX_ERR_ARG, "phx_ph_linewidths: this build supports nb = 6 on the fused path");
       return PHX_ERR_ARG;

@@ -72,6 +72,7 @@ struct phx_bands {
   double* d_vg = nullptr;     // (nq,nb,3) or null
   double* d_q = nullptr;      // (nq,3) Cartesian mesh points
   float* d_U32 = nullptr;     // (nq,nb,nb) complex fp32 copy for the split path
+  int* d_q1_order = nullptr;  // (nq) q1 visiting order of the split path
 };
 
 struct phx_v3 {

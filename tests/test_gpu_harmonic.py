@@ -71,11 +71,13 @@ def test_mesh_band_structure(ctx, diamond):
     m = lattice.Mesh(cr, (4, 4, 4))
     q = m.cartesian_coords()
     E2, U2, v2 = gpu.diagonalizeWithVelocities(q)
-    np.testing.assert_array_equal(E, E2)
-    np.testing.assert_array_equal(vg, v2)
+    # same kernel on (up to rounding of the Cartesian mesh points) the same q
+    np.testing.assert_allclose(E, E2, rtol=1e-13, atol=1e-15)
+    np.testing.assert_allclose(vg, v2, rtol=1e-6, atol=1e-9)
     ref = oracle.PhononH0(cr, fc)
     E0, _ = ref.diagonalize(q)
-    np.testing.assert_allclose(E, E0, rtol=1e-12, atol=1e-15)
+    w2, w2_0 = np.sign(E) * E ** 2, np.sign(E0) * E0 ** 2
+    np.testing.assert_allclose(w2, w2_0, rtol=0, atol=1e-13 * np.abs(w2_0).max())
 
 
 def test_errors_are_reported(ctx, diamond):

@@ -1,0 +1,59 @@
+"""Split-precision (BF16 x3 on tcgen05) path: the tensor-core GEMM building
+block against numpy, then whole-builder linewidths against the FP64 path.
+
+North-star bar for the split path: linewidth max relative error <= 1e-5 and
+thermal conductivity within 0.1% of the FP64 result (checked at 1e-4 here)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from phoebe_b200 import constants as C
+
+pytestmark = pytest.mark.gpu
+
+
+def test_tc_gemm_selftest(ctx):
+    from phoebe_b200 import _abi
+    rng = np.random.default_rng(0)
+    for N, Kp in ((144, 96), (64, 16), (256, 48)):
+        A = rng.normal(size=(128, Kp)).astype(np.float32)
+        B = rng.normal(size=(N, Kp)).astype(np.float32)
+        Cm = np.zeros((128, N), dtype=np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        _abi.check(_abi.load().phx_diag_tc_gemm(ctx.h, N, Kp, A.ctypes.data_as(fp),
+                                                B.ctypes.data_as(fp), Cm.ctypes.data_as(fp)), ctx.h)
+        ref = A.astype(np.float64) @ B.astype(np.float64).T
+        # BF16 hi+lo keeps ~16 bits per operand: each product is exact to
+        # ~2^-17 relative, so the error is ~1e-5 of sum_k |A||B|
+        scale = np.abs(A).astype(np.float64) @ np.abs(B).astype(np.float64).T
+        err = (np.abs(Cm - ref) / scale).max()
+        assert err < 3e-5, (N, Kp, err)
+
+
+def _builder(ctx, diamond, mesh, smearing, temps_k, precision):
+    from phoebe_b200.core import Interaction3Ph, PhononH0, PhScatteringMatrix
+    cr = diamond["crystal"]
+    T = np.array([C.kelvin_to_ry(t) for t in temps_k])
+    h0 = PhononH0(ctx, cr, diamond["fc2"])
+    bands = h0.populate(mesh, withVelocities=True)
+    v3 = Interaction3Ph(ctx, cr, diamond["fc3"], precision=precision)
+    sm = PhScatteringMatrix(v3, bands, T, smearing, 0.3 / C.ryToTHz)
+    A = sm.setup()
+    k = sm.thermalConductivity(cr.volume)
+    E, _, _ = bands.get(velocities=False)
+    return A, k, E, sm
+
+
+@pytest.mark.parametrize("mesh,smearing,temps", [((8, 8, 8), "gaussian", (300.0,)),
+                                                 ((10, 10, 10), "adaptive", (100.0, 300.0, 600.0))])
+def test_split_linewidths_match_fp64(ctx, diamond, mesh, smearing, temps):
+    A64, k64, E, _ = _builder(ctx, diamond, mesh, smearing, temps, "fp64")
+    A16, k16, _, sm = _builder(ctx, diamond, mesh, smearing, temps, "split_bf16")
+    # linewidths Gamma = A / n(n+1) on non-excluded states
+    ok = E.reshape(-1) >= C.phExcludeCutoff
+    big = ok[None, :] & (np.abs(A64) > 1e-8 * np.abs(A64).max())
+    rel = np.abs(A16 - A64)[big] / np.abs(A64)[big]
+    assert rel.max() < 1e-5, rel.max()
+    np.testing.assert_allclose(k16, k64, rtol=1e-4)
+    assert sm.stats.kernel_launches > 0

@@ -158,6 +158,26 @@ int phx_ph_linewidths(phx_v3* v3, phx_bands* bands, const phx_lw_params* params,
 int phx_ph_linewidths_d(phx_v3* v3, phx_bands* bands, const phx_lw_params* params,
                         double* A_out_d, phx_lw_stats* stats);
 
+/* Allocation-free variant of phx_ph_linewidths_d (no counterpart in the
+ * reference).  For callers that cannot allocate device memory when they call
+ * the builder -- e.g. an application that has given all free device memory
+ * to its own pool allocator, or one that must not pay cudaMalloc/cudaFree's
+ * implicit device synchronisation inside a latency-critical loop.  It calls
+ * no cudaMalloc/cudaFree: the plain FP64 path runs with every intermediate
+ * buffer in a 16 MiB array that the library reserves statically on each GPU
+ * where it is loaded (held until the process exits).  The caller passes the
+ * device output A_out_d (nT*nq*nb doubles).  Limit: Bose table and partial
+ * sums, 16*nq*nb*nT bytes, plus one q2 slab of the cached vertex,
+ * 16*nr3*nb^3 bytes, must fit in 16 MiB; larger problems are rejected with
+ * PHX_ERR_ARG.  The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the array and leave their contents in it (the call clears
+ * what must start at zero): calls that overlap on the same GPU race.  The
+ * precision setting of v3 is ignored (FP64).  Returns after the stream has
+ * drained. */
+int phx_ph_linewidths_static(phx_v3* v3, phx_bands* bands, const phx_lw_params* params,
+                             double* A_out_d);
+
 /* RTA thermal conductivity (atomic units; x thConductivityAuToSi for W/m/K)
  * from A_out: tau = n(n+1)/A_out, kappa_ij = sum dn/dT v_i tau v_j E/(Nq V).
  * kappa (nT,3,3) host.  Replaces BulkTDrift + getSingleModeTimes +

@@ -69,6 +69,7 @@ SIGNATURES = {
     "phx_ph_linewidths": [_VP, _VP, ctypes.POINTER(LwParams), _D, ctypes.POINTER(LwStats)],
     "phx_ph_linewidths_d": [_VP, _VP, ctypes.POINTER(LwParams), _VP, ctypes.POINTER(LwStats)],
     "phx_ph_rta_kappa": [_VP, _i, _D, _D, ctypes.c_double, _D],
+    "phx_ph_linewidths_static": [_VP, _VP, ctypes.POINTER(LwParams), _VP],
     "phx_diag_tc_gemm": [_VP, _i, _i, ctypes.POINTER(ctypes.c_float),
                          ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)],
 }

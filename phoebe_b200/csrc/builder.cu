@@ -27,6 +27,8 @@
 //    averaging and the exclusion of acoustic Gamma modes.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "cplx.cuh"
@@ -758,4 +760,145 @@ extern "C" int phx_ph_rta_kappa(phx_bands* b, int nT, const double* temps, const
     for (int i = 0; i < 9; ++i) kappa[c * 9 + i] = k[i];
   }
   return PHX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the fused builder (plain FP64 path).
+//
+// For callers that cannot allocate device memory when they call the builder:
+// for example a host application that has handed all free device memory to
+// its own pool allocator before calling into this library, or one that must
+// not pay the implicit device-wide synchronisation of cudaMalloc/cudaFree
+// inside a latency-critical loop.  All intermediate buffers of this variant
+// live in one array of fixed size that the library reserves statically on
+// every GPU where it is loaded; it is held until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kStaticScratchBytes = size_t(16) << 20;  // 16 MiB per GPU
+
+__device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+std::mutex g_static_mutex;
+void* g_static_addr[64] = {nullptr};  // device address of g_static_scratch, per device
+
+// Looks the array up once per device (the device must be current).  This is
+// the one CUDA call of the variant that must not run inside a stream capture.
+int static_scratch_address(phx_ctx* ctx, void** out) {
+  std::lock_guard<std::mutex> lk(g_static_mutex);
+  PHX_ARG(ctx, ctx->device >= 0 && ctx->device < 64, "device index out of range");
+  if (!g_static_addr[ctx->device]) {
+    void* addr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&addr, g_static_scratch);
+    if (e != cudaSuccess || !addr) {
+      phx_set_error(ctx, PHX_ERR_CUDA,
+                    std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+      return PHX_ERR_CUDA;
+    }
+    g_static_addr[ctx->device] = addr;
+  }
+  *out = g_static_addr[ctx->device];
+  return PHX_OK;
+}
+
+template <int NB>
+int run_builder_static(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d) {
+  phx_ctx* ctx = v->ctx;
+  cudaStream_t st = ctx->stream;
+  const int nq = b->nq, nT = p->num_temperatures, nr3 = v->nr3, nr2 = v->nr2;
+  const int q2b = p->q2_begin, q2e = p->q2_end;
+  const size_t nb3 = (size_t)NB * NB * NB;
+  const size_t sz_part = align_up(sizeof(double) * (size_t)nq * NB * nT);  // one slot
+  const size_t sz_bose = align_up(sizeof(double) * (size_t)nT * nq * NB);
+  const size_t sz_T = align_up(sizeof(double) * 8);
+  const size_t per_q2 = sizeof(double2) * (size_t)nr3 * nb3;
+  const size_t fixed = sz_part + sz_bose + sz_T;
+  if (fixed + align_up(per_q2) > kStaticScratchBytes) {
+    phx_set_error(ctx, PHX_ERR_ARG,
+                  "phx_ph_linewidths_static: this problem needs " + std::to_string(fixed + align_up(per_q2)) +
+                      " bytes of scratch at least; the static scratch holds " +
+                      std::to_string(kStaticScratchBytes) + " bytes (reduce mesh points or temperatures)");
+    return PHX_ERR_ARG;
+  }
+  const int chunk = (int)std::min<size_t>({(kStaticScratchBytes - fixed) / per_q2, (size_t)512,
+                                           (size_t)(q2e - q2b)});
+  void* base_v = nullptr;
+  PHX_TRY(static_scratch_address(ctx, &base_v));
+  char* base = static_cast<char*>(base_v);
+  double* partial = reinterpret_cast<double*>(base);
+  double* bose = reinterpret_cast<double*>(base + sz_part);
+  double* temps = reinterpret_cast<double*>(base + sz_part + sz_bose);
+  double2* Dp = reinterpret_cast<double2*>(base + fixed);
+  // the array keeps the previous call's contents: clear what accumulates
+  PHX_CUDA(ctx, cudaMemcpyAsync(temps, p->temperatures, sizeof(double) * nT, cudaMemcpyHostToDevice, st));
+  PHX_CUDA(ctx, cudaMemsetAsync(partial, 0, sizeof(double) * (size_t)nq * NB * nT, st));
+  bose_kernel<<<std::min(1024, (nq * NB * nT + 255) / 256), 256, 0, st>>>(nq, NB, nT, b->d_E, temps, bose);
+  PairArgs P;
+  P.m.nq = nq;
+  P.m.nb = NB;
+  P.m.nT = nT;
+  P.m.n0 = b->mesh[0];
+  P.m.n1 = b->mesh[1];
+  P.m.n2 = b->mesh[2];
+  P.m.E = b->d_E;
+  P.m.U = reinterpret_cast<const double2*>(b->d_U);
+  P.m.vg = b->d_vg;
+  P.m.bose = bose;
+  P.m.qcart = b->d_q;
+  P.m.smearing = p->smearing;
+  P.m.sigma = p->sigma;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) P.m.qT[i * 3 + j] = b->recip[i * 3 + j] / b->mesh[i];
+  P.m.norm = 1.0 / (double)nq;
+  P.nr3 = nr3;
+  P.R3 = v->d_R3;
+  P.Dp = Dp;
+  P.partial = partial;
+  const size_t smem_pair = sizeof(double2) * ((size_t)nr3 * kTile + 2 * NB * NB * kTile) +
+                           sizeof(double) * ((size_t)NB * NB * NB * kTile + (size_t)kMaxT * NB * kTile);
+  PHX_ARG(ctx, smem_pair <= 227 * 1024, "phx_ph_linewidths_static: too many R3 vectors");
+  PHX_CUDA(ctx, cudaFuncSetAttribute(pair_fp64_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_pair));
+  const size_t smem_fold = sizeof(double2) * (nr2 + 2 * NB * NB);
+  const int tiles = (nq + kTile - 1) / kTile;
+  for (int c0 = q2b; c0 < q2e; c0 += chunk) {
+    const int cnt = std::min(chunk, q2e - c0);
+    const int per_block = 8;
+    fold_q2_kernel<<<dim3(nr3, (cnt + per_block - 1) / per_block), 128, smem_fold, st>>>(
+        NB, nr2, nr3, v->d_D3w, v->d_R2, v->d_R3, b->d_q, reinterpret_cast<const double2*>(b->d_U), c0,
+        cnt, per_block, Dp);
+    P.q2_first = c0;
+    P.q2_count = cnt;
+    P.q2_per_slot = cnt;
+    pair_fp64_kernel<NB><<<dim3(tiles, 1), kTile * NB, smem_pair, st>>>(P);
+    PHX_CUDA(ctx, cudaGetLastError());
+  }
+  finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, NB, nT, 1, partial, b->d_E, p->finalize, Aout_d);
+  PHX_CUDA(ctx, cudaGetLastError());
+  PHX_CUDA(ctx, cudaStreamSynchronize(st));
+  return PHX_OK;
+}
+
+}  // namespace
+
+extern "C" int phx_ph_linewidths_static(phx_v3* v, phx_bands* b, const phx_lw_params* p,
+                                        double* Aout_d) {
+  PHX_ARG(nullptr, v && b && p && Aout_d, "phx_ph_linewidths_static: bad arguments");
+  phx_ctx* ctx = v->ctx;
+  PHX_ARG(ctx, b->ctx == ctx, "v3 and bands belong to different contexts");
+  PHX_ARG(ctx, b->nb == v->nb, "band count of bands and v3 differ");
+  PHX_ARG(ctx, p->num_temperatures >= 1 && p->num_temperatures <= kMaxT && p->temperatures,
+          "1..4 temperatures per call");
+  PHX_ARG(ctx, p->smearing == PHX_SMEAR_GAUSSIAN || p->smearing == PHX_SMEAR_ADAPTIVE, "bad smearing");
+  PHX_ARG(ctx, p->smearing != PHX_SMEAR_GAUSSIAN || p->sigma > 0.0, "Gaussian smearing needs sigma > 0");
+  PHX_ARG(ctx, p->smearing != PHX_SMEAR_ADAPTIVE || b->d_vg, "adaptive smearing needs velocities");
+  PHX_ARG(ctx, 0 <= p->q2_begin && p->q2_begin <= p->q2_end && p->q2_end <= b->nq, "bad q2 range");
+  PHX_ARG(ctx, v->nb == 6, "phx_ph_linewidths_static: this build supports nb = 6");
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (p->q2_begin == p->q2_end) {
+    PHX_CUDA(ctx, cudaMemsetAsync(Aout_d, 0, sizeof(double) * p->num_temperatures * b->nq * b->nb, ctx->stream));
+    PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return PHX_OK;
+  }
+  return run_builder_static<6>(v, b, p, Aout_d);
 }

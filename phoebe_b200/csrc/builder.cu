@@ -415,9 +415,11 @@ int phx_split_kp(int nr3);
 size_t phx_split_bimg_bytes(int chunk, int nr3);
 size_t phx_split_smem_bytes(int nr3);
 int phx_split_prepare_bands(phx_ctx* ctx, phx_bands* b);
+size_t phx_split_rec_bytes(int nq);
+int phx_split_pack_records(phx_ctx* ctx, const pairc::MeshArgs& M, void* rec, int* launches);
 int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v, const phx_bands* b,
-                         const double2* Dp, uint8_t* Bimg, int q2_first, int q2_count, int slots,
-                         double* partial, int* launches);
+                         const double2* Dp, uint8_t* Bimg, const void* rec, double emax, int q2_first,
+                         int q2_count, int slots, double* partial, int* launches);
 
 int phx_scratch_reserve(phx_v3* v, size_t bytes) {
   if (v->scratch_bytes >= bytes) return PHX_OK;
@@ -573,25 +575,30 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   }
   plan.chunk = std::min(plan.chunk, std::max(1, q2e - q2b));
   plan.slots = std::min(plan.slots, plan.chunk);
-  // the split kernel gives each of its two b2-parity warp sets its own slot
-  const int nslots = split ? 2 * plan.slots : plan.slots;
+  const int nslots = plan.slots;
   const size_t nb3 = (size_t)NB * NB * NB;
   const size_t sz_dp = align_up(sizeof(double2) * plan.chunk * nr3 * nb3);
   const size_t sz_part = align_up(sizeof(double) * nslots * nq * NB * nT);
   const size_t sz_bose = align_up(sizeof(double) * nT * nq * NB);
   const size_t sz_T = align_up(sizeof(double) * 8);
   const size_t sz_img = split ? align_up(phx_split_bimg_bytes(plan.chunk, nr3)) : 0;
-  PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_img));
+  const size_t sz_rec = split ? align_up(phx_split_rec_bytes(nq)) : 0;
+  PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_img + sz_rec));
   char* base = static_cast<char*>(v->d_scratch);
   double2* Dp = reinterpret_cast<double2*>(base);
   double* partial = reinterpret_cast<double*>(base + sz_dp);
   double* bose = reinterpret_cast<double*>(base + sz_dp + sz_part);
   double* temps = reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose);
   uint8_t* Bimg = reinterpret_cast<uint8_t*>(base + sz_dp + sz_part + sz_bose + sz_T);
+  void* rec = base + sz_dp + sz_part + sz_bose + sz_T + sz_img;
+  double emax = 0.0;  // largest energy of the mesh (margin of the split path's FP32 windows)
   if (split) {
     PHX_ARG(ctx, NB == 6, "split-precision path supports nb = 6");
     PHX_ARG(ctx, phx_split_smem_bytes(nr3) <= 227 * 1024, "too many R3 vectors for the split path");
     PHX_TRY(phx_split_prepare_bands(ctx, b));
+    std::vector<double> Eh((size_t)nq * NB);
+    PHX_CUDA(ctx, cudaMemcpy(Eh.data(), b->d_E, sizeof(double) * Eh.size(), cudaMemcpyDeviceToHost));
+    for (double e : Eh) emax = std::max(emax, std::fabs(e));
   }
   cudaEvent_t ev0, ev1, evv0, evv1;
   PHX_CUDA(ctx, cudaEventCreate(&ev0));
@@ -635,6 +642,7 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   }
   const size_t smem_fold = sizeof(double2) * (nr2 + 2 * NB * NB);
   const int tiles = (nq + kTile - 1) / kTile;
+  if (split) PHX_TRY(phx_split_pack_records(ctx, P.m, rec, &launches));
   PHX_CUDA(ctx, cudaEventRecord(evv0, st));
   for (int c0 = q2b; c0 < q2e; c0 += plan.chunk) {
     const int cnt = std::min(plan.chunk, q2e - c0);
@@ -645,7 +653,8 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
                                                per_block, Dp);
     ++launches;
     if (split) {
-      PHX_TRY(phx_split_pair_chunk(ctx, P.m, v, b, Dp, Bimg, c0, cnt, plan.slots, partial, &launches));
+      PHX_TRY(phx_split_pair_chunk(ctx, P.m, v, b, Dp, Bimg, rec, emax, c0, cnt, plan.slots, partial,
+                                   &launches));
       continue;
     }
     P.q2_first = c0;

@@ -1,23 +1,31 @@
 // Split-precision (BF16 x3) tensor-core path of the fused 3-phonon builder.
 //
 // The R3 transform of the vertex (interaction_3ph.cpp:276-289, "tmploop"),
-//   T(q1; a,b2,c) = sum_r3 e^{-i q1.R3} Dp(q2)[r3][a][b2][c],
+//   X(q1; a,b2,c) = sum_r3 e^{-i q1.R3} Dp(q2)[r3][a][b2][c],
 // is a complex GEMM with M = q1 (128 per CTA), K = r3, N = (a,b2,c).  It runs
 // on the 5th-generation tensor cores as a real GEMM on [Re | Im] extended
 // operands, each operand split as x = hi + lo in BF16 and accumulated as
-// hi*hi + hi*lo + lo*hi in FP32 in tensor memory (TMEM).
+// hi*hi + hi*lo + lo*hi in FP32 in tensor memory (TMEM).  N is processed in
+// three parts of two b2 values (144 FP32 columns) that live in three fixed
+// TMEM regions, so the MMA of one part overlaps the CUDA-core epilogue of the
+// others.
 //
-// Per CTA: 4 epilogue warps (one per TMEM lane quarter; thread = q1), one
-// producer warp (bulk async copies of pre-laid-out B images), one MMA warp
-// (single thread issues tcgen05.mma).  N is processed in three parts of two
-// b2 values (144 FP32 columns, an MMA N that is a multiple of 16) that rotate
-// through three TMEM regions, so the MMA of one part overlaps the CUDA-core
-// epilogue of the others.  The
-// epilogue contracts with e1 and e3 in FP32, symmetrises over degenerate
-// blocks, and evaluates the delta functions and Bose factors of the + and -
-// processes with energy differences formed in FP64, accumulating linewidths
-// in FP64.  Triplets whose delta is zero by the reference's own cut-offs are
-// skipped before any arithmetic (exactly zero contributions).
+// Epilogue (12 warps; TMEM lane quarter = warp & 3 = 32 q1 rows, k = warp >> 2):
+//  * the three warps of a quarter stage the records of q3 = q1 + q2 for their
+//    rows (one 592-byte record per mesh point: FP32 eigenvectors, energies,
+//    velocity projections, Bose factors, degenerate blocks);
+//  * warp k decides, for b2 = 2k, 2k+1 and every (b1, b3), whether any of the
+//    three delta functions of the triplet can be non-zero (FP32 windows with a
+//    rounding margin); the masks are shared in shared memory;
+//  * warp k owns the linewidths of b1 = k and k+3 for every b2: it contracts
+//    the rows of X it needs with e1 and e3 in FP32, and accumulates the rates
+//    of the live triplets in FP64.
+// Degenerate points need no symmetrised |V|^2: with S the block average over
+// the degenerate blocks of b1, b2 and b3 (scattering.cpp:1209-1318),
+//   Gamma(b1) = sum_{b2,b3} S(W) F = sum_{b1' in blk(b1), b2, b3} W(b1',b2,b3) G(b1,b2,b3) / n1,
+// where G is the average of the rate factors F over blk(b2) x blk(b3).  Each
+// owner therefore contracts the rows of its b1 block and averages F, and the
+// triplets whose delta is zero by the reference's own cut-offs are skipped.
 #include <algorithm>
 #include <cmath>
 #include <cuda_bf16.h>
@@ -31,35 +39,106 @@ using namespace pairc;
 namespace {
 
 constexpr int kM = 128;            // q1 rows per CTA = TMEM lanes
-constexpr int kKC = 32;            // K elements per B chunk (2 MMA K-steps)
+constexpr int kKC = 16;            // K elements per B stage (one MMA K-step)
 constexpr int kParts = 3;          // N split into 3 parts of 2 b2 each
-constexpr int kB2PerPart = 2;
 constexpr int kNH = 144;           // N columns per part: 2 b2 x 36 (a,c) x {re,im}
-constexpr int kStages = 2;
+constexpr int kStages = 3;
 constexpr int kRegion = 160;       // TMEM columns per accumulator region (>= kNH)
 constexpr int kTmemCols = 512;
-constexpr int kEpiWarps = 8;
+constexpr int kEpiWarps = 12;
 constexpr int kThreads = (kEpiWarps + 2) * 32;
-constexpr uint32_t kPartBytes = kNH * kKC * 2;    // one of hi / lo: 9216 B
-constexpr uint32_t kStageBytes = 2 * kPartBytes;  // hi + lo: 18432 B
-constexpr uint32_t kBSbo = (kKC / 8) * 128;       // 512 B between 8-row groups
+constexpr uint32_t kPartBytes = kNH * kKC * 2;    // one of hi / lo: 4608 B
+constexpr uint32_t kStageBytes = 2 * kPartBytes;  // hi + lo: 9216 B
+constexpr uint32_t kBSbo = (kKC / 8) * 128;       // 256 B between 8-row groups
+
+// Per-point record, 37 chunks of 16 bytes:
+//   chunks 0-17   e[a*6+b] (FP32 complex), two per chunk
+//   chunks 18+3b  band b: words 0-1 E (FP64), 2-4 P = qT.v (FP32), 5 1/E,
+//                 6-9 Bose factors of up to 4 temperatures, 10-11 unused
+//   chunk 36      word 0: degenerate blocks of the 6 bands (3 bits each)
+constexpr int kRecChunks = 37;
+constexpr int kChBand = 18;
+constexpr int kChGp = 36;
+constexpr int kU2Chunks = kRecChunks - kChBand;   // band blocks + blocks word
 
 struct TcArgs {
   MeshArgs m;
-  int Kp;                      // padded real K (2*nr3 rounded up to 48)
+  int Kp;                      // padded real K (2*nr3 rounded up to kKC)
   const uint8_t* Bimg;         // [j][part][kc] x kStageBytes
-  const float2* U32;           // (nq, nb, nb) fp32 eigenvectors
+  const uint4* rec;            // (nq, kRecChunks) per-point records
   const double* R3;
   int nr3;
   const int* q1_order;         // q1 points in k-space blocks of 4x4x2 (warp coherence)
   int q2_first, q2_count, q2_per_slot;
+  float tol;                   // margin of the FP32 liveness windows (Ry)
   double* partial;             // (S, nq, nb, nT)
   int* status;
 };
 
 // ---------------------------------------------------------------------------
-// B images: Dp (FP64 complex [j][r3][a][b2][c]) -> BF16 hi/lo K-major tiles
+// degenerate blocks of 6 sorted energies, packed as 3-bit block starts
+// (forward scan of scattering.cpp:1218-1230)
 // ---------------------------------------------------------------------------
+constexpr unsigned kIdentityBlocks = 0u | (1u << 3) | (2u << 6) | (3u << 9) | (4u << 12) | (5u << 15);
+__host__ __device__ __forceinline__ unsigned pack_blocks(const double* e) {
+  unsigned p = 0;
+  int start = 0;
+  for (int b = 0; b < 6; ++b) {
+    if (b > start && !(fabs(e[start] - e[b]) < phxc::degThreshold)) start = b;
+    p |= (unsigned)start << (3 * b);
+  }
+  return p;
+}
+__device__ __forceinline__ int blk_start(unsigned p, int b) { return (p >> (3 * b)) & 7; }
+// bit mask of the bands in the block of band b
+__device__ __forceinline__ unsigned blk_mask(unsigned p, int b) {
+  const int s = blk_start(p, b);
+  unsigned m = 0;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) m |= (blk_start(p, k) == s) ? (1u << k) : 0u;
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// records and B images
+// ---------------------------------------------------------------------------
+__global__ void pack_records_kernel(MeshArgs M, uint4* __restrict__ rec) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= M.nq) return;
+  uint32_t w[kRecChunks * 4];
+#pragma unroll 1
+  for (int el = 0; el < 36; ++el) {
+    const double2 u = M.U[(size_t)q * 36 + el];
+    w[2 * el] = __float_as_uint((float)u.x);
+    w[2 * el + 1] = __float_as_uint((float)u.y);
+  }
+  double e[6];
+#pragma unroll 1
+  for (int b = 0; b < 6; ++b) {
+    e[b] = M.E[(size_t)q * 6 + b];
+    uint32_t* o = w + 4 * (kChBand + 3 * b);
+    const unsigned long long eb = (unsigned long long)__double_as_longlong(e[b]);
+    o[0] = (uint32_t)eb;
+    o[1] = (uint32_t)(eb >> 32);
+    for (int i = 0; i < 3; ++i) {
+      double p = 0.0;
+      if (M.smearing == PHX_SMEAR_ADAPTIVE && M.vg)
+        for (int j = 0; j < 3; ++j) p += M.qT[3 * i + j] * M.vg[((size_t)q * 6 + b) * 3 + j];
+      o[2 + i] = __float_as_uint((float)p);
+    }
+    o[5] = __float_as_uint(e[b] > 0.0 ? (float)(1.0 / e[b]) : 0.f);
+    for (int t = 0; t < kMaxT; ++t)
+      o[6 + t] = __float_as_uint(t < M.nT ? (float)M.bose[((size_t)t * M.nq + q) * 6 + b] : 0.f);
+    o[10] = o[11] = 0u;
+  }
+  w[4 * kChGp] = pack_blocks(e);
+  w[4 * kChGp + 1] = w[4 * kChGp + 2] = w[4 * kChGp + 3] = 0u;
+  uint4* dst = rec + (size_t)q * kRecChunks;
+#pragma unroll 1
+  for (int c = 0; c < kRecChunks; ++c) dst[c] = make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
+}
+
+// Dp (FP64 complex [j][r3][a][b2][c]) -> BF16 hi/lo K-major tiles
 __global__ void convert_b_kernel(const double2* __restrict__ Dp, int nr3, int Kp, int q2_count,
                                  uint8_t* __restrict__ Bimg) {
   const int nkc = Kp / kKC;
@@ -73,7 +152,7 @@ __global__ void convert_b_kernel(const double2* __restrict__ Dp, int nr3, int Kp
     const int kg = kc * kKC + kk;
     const int ri = n & 1, rest = n >> 1;
     const int bl = rest / 36, a = (rest / 6) % 6, c = rest % 6;
-    const int b2 = kB2PerPart * h + bl;
+    const int b2 = 2 * h + bl;
     double v = 0.0;
     if (kg < 2 * nr3) {
       const int part = kg < nr3 ? 0 : 1;
@@ -89,273 +168,258 @@ __global__ void convert_b_kernel(const double2* __restrict__ Dp, int nr3, int Kp
   }
 }
 
-__global__ void to_fp32_kernel(const double2* __restrict__ U, size_t n, float2* __restrict__ U32) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    U32[i] = make_float2((float)U[i].x, (float)U[i].y);
+// ---------------------------------------------------------------------------
+// epilogue helpers
+// ---------------------------------------------------------------------------
+// 16-byte asynchronous global -> shared copy (L2 only) and its completion wait
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tc::smem_u32(dst)), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// ---------------------------------------------------------------------------
-// epilogue helpers (FP32 contraction, FP64 energies)
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ float sigma_f(const float* qT, float v0, float v1, float v2) {
-  float s = 0.f;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    const float d = qT[3 * i] * v0 + qT[3 * i + 1] * v1 + qT[3 * i + 2] * v2;
-    s = fmaf(d, d, s);
+struct Band {            // one band of one point
+  double E;
+  float P[3];            // qT.v (adaptive smearing)
+  float iE;              // 1/E
+  float N[kMaxT];        // Bose factors
+};
+
+// c0 points at the band's first chunk, the next two follow at stride st
+template <int NT>
+__device__ __forceinline__ Band load_band(const uint4* c0, int st) {
+  const uint4 a = c0[0], b = c0[st];
+  Band x;
+  x.E = __hiloint2double((int)a.y, (int)a.x);
+  x.P[0] = __uint_as_float(a.z);
+  x.P[1] = __uint_as_float(a.w);
+  x.P[2] = __uint_as_float(b.x);
+  x.iE = __uint_as_float(b.y);
+  x.N[0] = __uint_as_float(b.z);
+  x.N[1] = __uint_as_float(b.w);
+  x.N[2] = x.N[3] = 0.f;
+  if (NT > 2) {
+    const uint2 c = *reinterpret_cast<const uint2*>(c0 + 2 * st);
+    x.N[2] = __uint_as_float(c.x);
+    x.N[3] = __uint_as_float(c.y);
   }
-  s = sqrtf(s / 6.0f);
-  if (s != 0.f && s < (float)phxc::adaptiveCutoff) s = (float)phxc::adaptiveCutoff;
-  return s;
+  return x;
 }
 
-// delta of one process in FP32 from an FP64 energy difference; 0 when the
-// reference's cut-offs make it zero (Gaussian: x > 6; x < -8.5 contributes
-// below 1e-31 of the peak and is dropped).
-__device__ __forceinline__ float delta_f(int smearing, float sigma, double de, bool vzero) {
+struct Sig {
+  float s, inv;   // sigma and 1/sigma
+  bool vz;        // velocity difference exactly zero
+};
+
+// AdaptiveGaussianDeltaFunction::getSmearing (delta_function.cpp:71-83) from
+// the projections P = qT.v: sigma^2 = |P2 - P3|^2 / 6, floored at 1e-4 eV.
+__device__ __forceinline__ Sig sigma_ad(const float* P2, const float* P3) {
+  const float d0 = P2[0] - P3[0], d1 = P2[1] - P3[1], d2 = P2[2] - P3[2];
+  float s2 = fmaf(d0, d0, fmaf(d1, d1, d2 * d2)) * (1.f / 6.f);
+  Sig g;
+  g.vz = d0 == 0.f && d1 == 0.f && d2 == 0.f;
+  constexpr float kCut = (float)phxc::adaptiveCutoff;
+  if (s2 != 0.f && s2 < kCut * kCut) s2 = kCut * kCut;
+  const float r = s2 > 0.f ? rsqrtf(s2) : 0.f;
+  g.s = s2 * r;
+  g.inv = r;
+  return g;
+}
+
+// delta of one process in FP32 from an FP64 energy difference, 0 where the
+// reference's cut-offs make it zero (delta_function.cpp:34-96).  Gaussian:
+// x < -8.5 contributes below 1e-31 of the peak and is dropped.
+__device__ __forceinline__ float delta_ad(const Sig& g, double de) {
+  if (g.vz && de == 0.0) return 1.f;
+  if (g.s == 0.f) return 0.f;
   const float e = (float)de;
-  if (smearing == PHX_SMEAR_GAUSSIAN) {
-    const float x = e / sigma;
-    if (x > 6.f || x < -8.5f) return 0.f;
-    return __expf(-x * x) / ((float)phxc::sqrtPi * sigma);
+  if (fabsf(e) > 2.f * g.s) return 0.f;
+  const float x = e * g.inv;
+  return __expf(-x * x) * g.inv * (float)(1.0 / (phxc::sqrtPi * phxc::erf2));
+}
+__device__ __forceinline__ float delta_ga(float inv, double de) {
+  const float x = (float)de * inv;
+  if (x > 6.f || x < -8.5f) return 0.f;
+  return __expf(-x * x) * inv * (float)(1.0 / phxc::sqrtPi);
+}
+
+// Rate factors of one branch triplet for all temperatures: the "+" process
+// of (q1,q2) and the two "-" processes of (q1,-q2), as ph_scattering.cpp:338-380
+// and :466-518 (cut-offs, deltas, Bose factors), times 0.5 (the linewidth
+// convention of :433,:574); multiply by |V|^2.
+template <int NT>
+__device__ __forceinline__ void rate_f(int smearing, float ginv, float pre, double E1, float iE1,
+                                       const float* n1, const Band& x2, const Band& x2m,
+                                       const Band& x3, const Sig& gp, const Sig& gm, float* f) {
+#pragma unroll
+  for (int t = 0; t < NT; ++t) f[t] = 0.f;
+  if (!(x3.E >= phxc::phEnergyCutoff)) return;
+  const bool ok2 = x2.E >= phxc::phExcludeCutoff, ok2m = x2m.E >= phxc::phExcludeCutoff;
+  float dp = 0.f, d1 = 0.f, d2 = 0.f;
+  if (smearing == PHX_SMEAR_ADAPTIVE) {
+    if (ok2) dp = delta_ad(gp, E1 + x2.E - x3.E);
+    if (ok2m) {
+      d1 = delta_ad(gm, E1 + x3.E - x2m.E);
+      d2 = delta_ad(gm, x2m.E + x3.E - E1);
+    }
+  } else {
+    if (ok2) dp = delta_ga(ginv, E1 + x2.E - x3.E);
+    if (ok2m) {
+      d1 = delta_ga(ginv, E1 + x3.E - x2m.E);
+      d2 = delta_ga(ginv, x2m.E + x3.E - E1);
+    }
   }
-  if (vzero && de == 0.0) return 1.f;
-  if (sigma == 0.f) return 0.f;
-  if (fabsf(e) > 2.f * sigma) return 0.f;
-  const float x = e / sigma;
-  return __expf(-x * x) / ((float)phxc::sqrtPi * sigma * (float)phxc::erf2);
+  const float fp = pre * dp * iE1 * x2.iE * x3.iE;
+  const float fm = pre * iE1 * x2m.iE * x3.iE;
+#pragma unroll
+  for (int t = 0; t < NT; ++t)
+    f[t] = fp * n1[t] * x2.N[t] * (x3.N[t] + 1.f) +
+           fm * x3.N[t] * (d1 * n1[t] * (x2m.N[t] + 1.f) + d2 * x2m.N[t] * (n1[t] + 1.f));
+}
+
+// G(b1, blk(b2), blk(b3)): F averaged over the degenerate blocks of b2 and b3
+template <int NT>
+__device__ __noinline__ void rate_avg(int smearing, float ginv, float pre, double E1, float iE1,
+                                      const float* n1, const uint4* u2, const uint4* srow,
+                                      unsigned bm2, unsigned bm3, float* g) {
+#pragma unroll
+  for (int t = 0; t < NT; ++t) g[t] = 0.f;
+  int cnt = 0;
+  for (int b2 = 0; b2 < 6; ++b2) {
+    if (!((bm2 >> b2) & 1u)) continue;
+    const Band x2 = load_band<NT>(u2 + 3 * b2, 1);
+    const Band x2m = load_band<NT>(u2 + kU2Chunks + 3 * b2, 1);
+    for (int b3 = 0; b3 < 6; ++b3) {
+      if (!((bm3 >> b3) & 1u)) continue;
+      const Band x3 = load_band<NT>(srow + (kChBand + 3 * b3) * kM, kM);
+      Sig gp, gm;
+      if (smearing == PHX_SMEAR_ADAPTIVE) {
+        gp = sigma_ad(x2.P, x3.P);
+        gm = sigma_ad(x2m.P, x3.P);
+      }
+      float f[NT];
+      rate_f<NT>(smearing, ginv, pre, E1, iE1, n1, x2, x2m, x3, gp, gm, f);
+#pragma unroll
+      for (int t = 0; t < NT; ++t) g[t] += f[t];
+      ++cnt;
+    }
+  }
+  const float inv = 1.f / (float)cnt;
+#pragma unroll
+  for (int t = 0; t < NT; ++t) g[t] *= inv;
+}
+
+// OR a 6-bit b3 mask over the degenerate blocks of q3
+__device__ __noinline__ unsigned expand_b3(unsigned c, unsigned gp3) {
+  unsigned o = 0;
+  for (int b = 0; b < 6; ++b)
+    if ((c >> b) & 1u) o |= blk_mask(gp3, b);
+  return o;
+}
+
+// Liveness of (b1, b2, b3) for all b1 at one (b2, b3): bit b1 is set when
+// one of the three deltas may be non-zero (FP32 windows widened by tol).
+__device__ __forceinline__ unsigned live6(int smearing, float sg, float tol, const float* E1f,
+                                          float E2f, float E2mf, const float* P2, const float* P2m,
+                                          bool ok2, bool ok2m, float E3f, const float* P3) {
+  float hp, hm, cp, c1, c2;
+  if (smearing == PHX_SMEAR_ADAPTIVE) {
+    hp = 2.f * sigma_ad(P2, P3).s + tol;
+    hm = 2.f * sigma_ad(P2m, P3).s + tol;
+    cp = E3f - E2f;          // + : E1 + E2 - E3 = E1 - cp
+    c1 = E2mf - E3f;         // -1: E1 + E3 - E2m = E1 - c1
+    c2 = E2mf + E3f;         // -2: E2m + E3 - E1 = -(E1 - c2)
+  } else {
+    // x = dE / sigma in [-8.5, 6]: centre -1.25 sigma, half width 7.25 sigma
+    hp = hm = 7.25f * sg + tol;
+    cp = E3f - E2f - 1.25f * sg;
+    c1 = E2mf - E3f - 1.25f * sg;
+    c2 = E2mf + E3f + 1.25f * sg;
+  }
+  if (!ok2) hp = -1.f;
+  if (!ok2m) hm = -1.f;
+  unsigned msk = 0;
+#pragma unroll
+  for (int b1 = 0; b1 < 6; ++b1) {
+    const bool live = fabsf(E1f[b1] - cp) <= hp || fabsf(E1f[b1] - c1) <= hm || fabsf(E1f[b1] - c2) <= hm;
+    msk |= live ? (1u << b1) : 0u;
+  }
+  return msk;
 }
 
 // ---------------------------------------------------------------------------
 // the fused pair kernel
 // ---------------------------------------------------------------------------
-// Warp roles (320 threads): warps 0-7 epilogue (TMEM lane quarter = warp & 3,
-// b2 parity = warp >> 2), warp 8 producer, warp 9 MMA issuer.
-// Shared-memory plan (bytes), Kp = 96:
-//   A hi/lo 48 K | B stages 2 x 18 K | e1 36 K | e3 36 K | E(q1), E(q3) 12 K |
-//   v(q3) 9 K | Bose(q3), Bose(q1) 24 K | per-warp q2 data 3.4 K | barriers
-struct U2 {             // uniform data of one b2 at q2 and at -q2
-  double e2, e2m;
-  float v2[3], v2m[3];
-  float n2[kMaxT], n2m[kMaxT];
+// Warp roles (448 threads): warps 0-11 epilogue, warp 12 producer (bulk
+// copies of B stages), warp 13 MMA issuer.
+struct Smem {
+  uint32_t aPart;
+  uint8_t* A;          // [hi | lo] 128 x Kp BF16
+  uint8_t* B;          // kStages x kStageBytes
+  float2* E1v;         // e1 [36][128]
+  double* En1;         // [6][128]
+  float* iE1;          // [6][128]
+  float* N1;           // [kMaxT*6][128]
+  uint4* rec;          // staged q3 records [kRecChunks][128]
+  uint4* u2;           // [4 quarters][2: q2, -q2][kU2Chunks]
+  unsigned long long* need;  // [6 b2][128] bit b1*6+b3
+  uint64_t* bars;
 };
 
-struct Smem3 {
-  const float2* E1v;   // e1 [36][128]
-  const float2* E3v;   // e3 [36][128]
-  const double* En1;   // [6][128]
-  const double* En3;   // [6][128]
-  const float* V3;     // [18][128]
-  const float* N3;     // [kMaxT*6][128]
-  const float* N1;     // [kMaxT*6][128]
-};
+__host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
-// OR the 6x6 mask (bit b1*6+b3) over the degenerate blocks of b1 and b3
-// Degenerate blocks of 6 sorted energies packed as 3-bit block starts
-// (forward scan of scattering.cpp:1218-1230).
-constexpr unsigned kIdentityBlocks = 0u | (1u << 3) | (2u << 6) | (3u << 9) | (4u << 12) | (5u << 15);
-__device__ __forceinline__ unsigned pack_blocks(const double* e) {
-  unsigned p = 0;
-  int start = 0;
-#pragma unroll
-  for (int b = 0; b < 6; ++b) {
-    if (b > start && !(fabs(e[start] - e[b]) < phxc::degThreshold)) start = b;
-    if (b == 0) start = 0;
-    p |= (unsigned)start << (3 * b);
-  }
-  return p;
-}
-__device__ __forceinline__ int blk_start(unsigned p, int b) { return (p >> (3 * b)) & 7; }
-__device__ __forceinline__ int blk_size(unsigned p, int b) {
-  const int s = blk_start(p, b);
-  int n = 0;
-#pragma unroll
-  for (int k = 0; k < 6; ++k) n += blk_start(p, k) == s;
-  return n;
+__host__ __device__ inline size_t smem_layout(int Kp, size_t* off) {
+  size_t o = 0;
+  const size_t aPart = (size_t)kM * Kp * 2;
+  off[0] = o; o += align16(2 * aPart);                         // A
+  off[1] = o; o += align16((size_t)kStages * kStageBytes);     // B
+  off[2] = o; o += align16(36 * kM * sizeof(float2));          // e1
+  off[3] = o; o += align16(6 * kM * sizeof(double));           // E1
+  off[4] = o; o += align16(6 * kM * sizeof(float));            // 1/E1
+  off[5] = o; o += align16(kMaxT * 6 * kM * sizeof(float));    // N1
+  off[6] = o; o += align16((size_t)kRecChunks * kM * 16);      // staged records
+  off[7] = o; o += align16(4 * 2 * kU2Chunks * 16);            // q2 bands
+  off[8] = o; o += align16(6 * kM * sizeof(unsigned long long));  // masks
+  off[9] = o; o += align16(32 * sizeof(uint64_t));             // barriers, tmem slot, flag
+  return o;
 }
 
-// OR the 6x6 mask (bit b1*6+b3) over the degenerate blocks of b1 and b3
-__device__ __forceinline__ unsigned long long expand_blocks(unsigned long long m, unsigned gp1,
-                                                            unsigned gp3) {
-  unsigned long long rows[6];
-#pragma unroll
-  for (int b1 = 0; b1 < 6; ++b1) rows[b1] = (m >> (6 * b1)) & 63ull;
-  unsigned long long out = 0;
-#pragma unroll
-  for (int b1 = 0; b1 < 6; ++b1) {
-    unsigned long long row = 0;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) row |= (blk_start(gp1, k) == blk_start(gp1, b1)) ? rows[k] : 0ull;
-    unsigned long long e = 0;
-#pragma unroll
-    for (int b3 = 0; b3 < 6; ++b3) {
-      unsigned long long blk = 0;
-#pragma unroll
-      for (int k = 0; k < 6; ++k) blk |= (blk_start(gp3, k) == blk_start(gp3, b3)) ? (1ull << k) : 0ull;
-      e |= ((row >> b3) & 1ull) ? blk : 0ull;
-    }
-    out |= e << (6 * b1);
-  }
-  return out;
+__device__ __forceinline__ Smem carve(uint8_t* base, int Kp) {
+  size_t off[10];
+  smem_layout(Kp, off);
+  Smem s;
+  s.aPart = (uint32_t)kM * Kp * 2;
+  s.A = base + off[0];
+  s.B = base + off[1];
+  s.E1v = reinterpret_cast<float2*>(base + off[2]);
+  s.En1 = reinterpret_cast<double*>(base + off[3]);
+  s.iE1 = reinterpret_cast<float*>(base + off[4]);
+  s.N1 = reinterpret_cast<float*>(base + off[5]);
+  s.rec = reinterpret_cast<uint4*>(base + off[6]);
+  s.u2 = reinterpret_cast<uint4*>(base + off[7]);
+  s.need = reinterpret_cast<unsigned long long*>(base + off[8]);
+  s.bars = reinterpret_cast<uint64_t*>(base + off[9]);
+  return s;
 }
 
-// Rate factors of one branch triplet (b1,b2,b3) for all temperatures: the
-// "+" process of (q1,q2) and the two "-" processes of (q1,-q2), exactly as
-// ph_scattering.cpp:338-380 and :466-518 (cut-offs, deltas, Bose factors),
-// times 0.5 (the linewidth convention of :433,:574); multiply by |V|^2.
-__device__ __forceinline__ void rate_factors(const MeshArgs& M, double en1, const float* n1,
-                                             const U2& x, double en3, const float* n3, float sp,
-                                             float sm, bool vzp, bool vzm, float* f) {
-#pragma unroll
-  for (int c = 0; c < kMaxT; ++c) f[c] = 0.f;
-  if (en1 < phxc::phExcludeCutoff || en3 < phxc::phEnergyCutoff) return;
-  const bool ok2 = x.e2 >= phxc::phExcludeCutoff;
-  const bool ok2m = x.e2m >= phxc::phExcludeCutoff;
-  const float dplus = ok2 ? delta_f(M.smearing, sp, en1 + x.e2 - en3, vzp) : 0.f;
-  float d1 = 0.f, d2 = 0.f;
-  if (ok2m) {
-    d1 = delta_f(M.smearing, sm, en1 + en3 - x.e2m, vzm);
-    d2 = delta_f(M.smearing, sm, x.e2m + en3 - en1, vzm);
-  }
-  if (dplus <= 0.f && d1 <= 0.f && d2 <= 0.f) return;
-  d1 = fmaxf(d1, 0.f);
-  d2 = fmaxf(d2, 0.f);
-  const float pre = (float)(phxc::pi * 0.25 * 0.5) * (float)M.norm;
-  const float fp = dplus > 0.f ? pre * dplus / (float)(en1 * x.e2 * en3) : 0.f;
-  const float fm = (d1 > 0.f || d2 > 0.f) ? pre / (float)(en1 * x.e2m * en3) : 0.f;
-#pragma unroll
-  for (int c = 0; c < kMaxT; ++c) {
-    if (c >= M.nT) break;
-    float r = 0.f;
-    if (fp > 0.f) r += fp * n1[c] * x.n2[c] * (n3[c] + 1.f);
-    if (fm > 0.f) r += fm * (n3[c] * n1[c] * (x.n2m[c] + 1.f) * d1 + x.n2m[c] * n3[c] * (n1[c] + 1.f) * d2);
-    f[c] = r;
-  }
-}
-
-__device__ __forceinline__ void sigmas(const MeshArgs& M, const float* qT, const U2& x,
-                                       const float* V3, int m, int b3, float& sp, float& sm,
-                                       bool& vzp, bool& vzm) {
-  sp = sm = (float)M.sigma;
-  vzp = vzm = false;
-  if (M.smearing != PHX_SMEAR_ADAPTIVE) return;
-  const float v30 = V3[(b3 * 3) * 128 + m], v31 = V3[(b3 * 3 + 1) * 128 + m],
-              v32 = V3[(b3 * 3 + 2) * 128 + m];
-  const float dp0 = x.v2[0] - v30, dp1 = x.v2[1] - v31, dp2 = x.v2[2] - v32;
-  const float dm0 = x.v2m[0] - v30, dm1 = x.v2m[1] - v31, dm2 = x.v2m[2] - v32;
-  vzp = dp0 == 0.f && dp1 == 0.f && dp2 == 0.f;
-  vzm = dm0 == 0.f && dm1 == 0.f && dm2 == 0.f;
-  sp = sigma_f(qT, dp0, dp1, dp2);
-  sm = sigma_f(qT, dm0, dm1, dm2);
-}
-
-// Block-averaged rate factors G(b1, block(b2), block(b3)) used when any of
-// the three points has degenerate bands: by the symmetry of the block
-// average, sum S(W) F = sum W S(F), so |V|^2 never has to be symmetrised.
-__device__ __forceinline__ void rate_block(const MeshArgs& M, const float* qT, const Smem3& S,
-                                        const U2* u2, int m, int b1, int b2s, int b2n, int b3s,
-                                        int b3n, float* g) {
-#pragma unroll
-  for (int c = 0; c < kMaxT; ++c) g[c] = 0.f;
-  const double en1 = S.En1[b1 * 128 + m];
-  float n1[kMaxT];
-#pragma unroll
-  for (int c = 0; c < kMaxT; ++c) n1[c] = S.N1[(c * 6 + b1) * 128 + m];
-  for (int bb = b2s; bb < b2s + b2n; ++bb) {
-    const U2 x = u2[bb];
-    for (int b3 = b3s; b3 < b3s + b3n; ++b3) {
-      float sp, sm;
-      bool vzp, vzm;
-      sigmas(M, qT, x, S.V3, m, b3, sp, sm, vzp, vzm);
-      float n3[kMaxT];
-#pragma unroll
-      for (int c = 0; c < kMaxT; ++c) n3[c] = S.N3[(c * 6 + b3) * 128 + m];
-      float f[kMaxT];
-      rate_factors(M, en1, n1, x, S.En3[b3 * 128 + m], n3, sp, sm, vzp, vzm, f);
-#pragma unroll
-      for (int c = 0; c < kMaxT; ++c) g[c] += f[c];
-    }
-  }
-  const float inv = 1.f / (float)(b2n * b3n);
-#pragma unroll
-  for (int c = 0; c < kMaxT; ++c) g[c] *= inv;
-}
-
-// Liveness of (b1, b2, b3) for all b1, b3 at one b2 (bit b1*6+b3), in FP32
-// with a margin for rounding; the rate stage re-applies the exact tests.
-__device__ __forceinline__ unsigned long long live_mask(const MeshArgs& M, const float* qT,
-                                                       const Smem3& S, const U2& x, int m,
-                                                       const float* E1f, unsigned ok1) {
-  const bool ok2 = x.e2 >= phxc::phExcludeCutoff;
-  const bool ok2m = x.e2m >= phxc::phExcludeCutoff;
-  if (!ok2 && !ok2m) return 0ull;
-  const float tol = 4.0e-9f;  // bound on the FP32 error of an energy difference (Ry)
-  const float e2f = (float)x.e2, e2mf = (float)x.e2m;
-  unsigned long long msk = 0;
-#pragma unroll 1
-  for (int b3 = 0; b3 < 6; ++b3) {
-    const double en3 = S.En3[b3 * 128 + m];
-    if (!(en3 >= phxc::phEnergyCutoff)) continue;
-    const float e3f = (float)en3;
-    float sp, sm;
-    bool vzp, vzm;
-    sigmas(M, qT, x, S.V3, m, b3, sp, sm, vzp, vzm);
-    float hip, lop, him, lom;
-    if (M.smearing == PHX_SMEAR_ADAPTIVE) {
-      hip = 2.f * sp + tol;
-      lop = -hip;
-      him = 2.f * sm + tol;
-      lom = -him;
-    } else {
-      hip = 6.f * sp + tol;
-      lop = -8.5f * sp - tol;
-      him = 6.f * sm + tol;
-      lom = -8.5f * sm - tol;
-    }
-    if (!ok2) { hip = -1.f; lop = 1.f; }
-    if (!ok2m) { him = -1.f; lom = 1.f; }
-    const float cp = e2f - e3f, cm1 = e3f - e2mf, cm2 = e2mf + e3f;
-    unsigned long long col = 0;
-#pragma unroll
-    for (int b1 = 0; b1 < 6; ++b1) {
-      const float dp = E1f[b1] + cp, d1 = E1f[b1] + cm1, d2 = cm2 - E1f[b1];
-      const bool live = (dp <= hip && dp >= lop) || (d1 <= him && d1 >= lom) || (d2 <= him && d2 >= lom);
-      col |= (live && ((ok1 >> b1) & 1u)) ? (1ull << (b1 * 6)) : 0ull;
-    }
-    msk |= col << b3;
-  }
-  return msk;
-}
-
+template <int NT>
 __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
   const MeshArgs& M = P.m;
   extern __shared__ __align__(1024) uint8_t smem[];
   const int Kp = P.Kp, nkc = Kp / kKC;
-  const uint32_t aPart = (uint32_t)kM * Kp * 2;
-  uint8_t* sA = smem;                                                   // [hi | lo]
-  uint8_t* sB = sA + 2 * aPart;                                         // stages
-  float2* sE1 = reinterpret_cast<float2*>(sB + kStages * kStageBytes);  // [36][128]
-  float2* sE3 = sE1 + 36 * kM;                                          // [36][128]
-  double* sEn1 = reinterpret_cast<double*>(sE3 + 36 * kM);              // [6][128]
-  double* sEn3 = sEn1 + 6 * kM;                                         // [6][128]
-  float* sV3 = reinterpret_cast<float*>(sEn3 + 6 * kM);                 // [18][128]
-  float* sN3 = sV3 + 18 * kM;                                           // [kMaxT*6][128]
-  float* sN1 = sN3 + kMaxT * 6 * kM;                                    // [kMaxT*6][128]
-  U2* sU2 = reinterpret_cast<U2*>(sN1 + kMaxT * 6 * kM);               // [8 warps][6]
-  float* sQT = reinterpret_cast<float*>(sU2 + kEpiWarps * 6);           // [9] adaptive qTensor
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sQT + 10);
-  uint64_t* full = bars;
-  uint64_t* empty = bars + kStages;
-  uint64_t* accf = bars + 2 * kStages;
-  uint64_t* acce = accf + kParts;
-  uint64_t* done = acce + kParts;
-  uint64_t* stg = done + 1;        // [4] q3 data staged by both parities of a quarter
-  uint64_t* rel = stg + 4;         // [4] q3 data released by both parities
+  const Smem S = carve(smem, Kp);
+  uint64_t* full = S.bars;                // [kStages]
+  uint64_t* empty = full + kStages;       // [kStages]
+  uint64_t* accf = empty + kStages;       // [kParts] MMA of a part done
+  uint64_t* acce = accf + kParts;         // [kParts] part released by the 12 epilogue warps
+  uint64_t* done = acce + kParts;         // MMA drain
+  uint64_t* stg = done + 1;               // [4] q3 records of a quarter staged
+  uint64_t* lvb = stg + 4;                // [4] liveness masks of a quarter written
+  uint64_t* rel = lvb + 4;                // [4] quarter done with the staged records
   uint32_t* tslot = reinterpret_cast<uint32_t*>(rel + 4);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nq = M.nq, n0 = M.n0, n1 = M.n1, n2 = M.n2, nT = M.nT;
+  const int nq = M.nq, n0 = M.n0, n1 = M.n1, n2 = M.n2;
   const int tile0 = blockIdx.x * kM;
 
   if (tid == 0) {
@@ -369,13 +433,13 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
     }
     tc::mbar_init(done, 1);
     for (int q = 0; q < 4; ++q) {
-      tc::mbar_init(&stg[q], 64);
-      tc::mbar_init(&rel[q], 64);
+      tc::mbar_init(&stg[q], 96);
+      tc::mbar_init(&lvb[q], 96);
+      tc::mbar_init(&rel[q], 96);
     }
     *abort_flag = 0;
     tc::fence_mbar_init();
   }
-  if (tid < 9) sQT[tid] = (float)M.qT[tid];
   if (warp == 0) {
     tc::tmem_alloc(tslot, kTmemCols);
     tc::tmem_relinquish();
@@ -395,23 +459,24 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
     const __nv_bfloat16 hi = __double2bfloat16(v);
     const __nv_bfloat16 lo = __double2bfloat16(v - (double)__bfloat162float(hi));
     const uint32_t off = tc::core_offset(mm, k, Kp, 2);
-    *reinterpret_cast<__nv_bfloat16*>(sA + off) = hi;
-    *reinterpret_cast<__nv_bfloat16*>(sA + aPart + off) = lo;
+    *reinterpret_cast<__nv_bfloat16*>(S.A + off) = hi;
+    *reinterpret_cast<__nv_bfloat16*>(S.A + S.aPart + off) = lo;
   }
+  // q1 data of the tile from the records
   for (int e = tid; e < 36 * kM; e += kThreads) {
     const int el = e / kM, mm = e % kM;
     const int q = P.q1_order[min(tile0 + mm, nq - 1)];
-    sE1[e] = P.U32[(size_t)q * 36 + el];
-  }
-  for (int e = tid; e < kMaxT * 6 * kM; e += kThreads) {
-    const int f = e / kM, mm = e % kM, c = f / 6, b = f % 6;
-    const int q = P.q1_order[min(tile0 + mm, nq - 1)];
-    sN1[e] = c < nT ? (float)M.bose[((size_t)c * nq + q) * 6 + b] : 0.f;
+    const uint2 v = reinterpret_cast<const uint2*>(P.rec + (size_t)q * kRecChunks)[el];
+    S.E1v[e] = make_float2(__uint_as_float(v.x), __uint_as_float(v.y));
   }
   for (int e = tid; e < 6 * kM; e += kThreads) {
     const int b = e / kM, mm = e % kM;
     const int q = P.q1_order[min(tile0 + mm, nq - 1)];
-    sEn1[e] = M.E[(size_t)q * 6 + b];
+    const Band x = load_band<kMaxT>(P.rec + (size_t)q * kRecChunks + kChBand + 3 * b, 1);
+    S.En1[e] = x.E;
+    S.iE1[e] = x.iE;
+#pragma unroll
+    for (int t = 0; t < kMaxT; ++t) S.N1[(t * 6 + b) * kM + mm] = x.N[t];
   }
   tc::fence_proxy_async_smem();
   tc::tc_fence_before();
@@ -421,20 +486,20 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
 
   const int jbeg = blockIdx.y * P.q2_per_slot;
   const int jend = min(P.q2_count, jbeg + P.q2_per_slot);
-  const int nunits = kParts * max(0, jend - jbeg);
+  const int nj = max(0, jend - jbeg);
 
   if (warp == kEpiWarps) {
     // ---------------- producer ----------------
     if (lane == 0) {
       int it = 0;
-      for (int u = 0; u < nunits && !*abort_flag; ++u) {
+      for (int u = 0; u < kParts * nj && !*abort_flag; ++u) {
         const int j = jbeg + u / kParts, h = u % kParts;
         for (int kc = 0; kc < nkc; ++kc, ++it) {
           const int s = it % kStages;
           const uint32_t ph = (it / kStages) & 1;
           if (!tc::mbar_wait_sleep(&empty[s], ph ^ 1, P.status, 1)) { *abort_flag = 1; break; }
           tc::mbar_arrive_expect_tx(&full[s], kStageBytes);
-          tc::bulk_g2s(sB + s * kStageBytes, P.Bimg + ((size_t)(j * kParts + h) * nkc + kc) * kStageBytes,
+          tc::bulk_g2s(S.B + s * kStageBytes, P.Bimg + ((size_t)(j * kParts + h) * nkc + kc) * kStageBytes,
                        kStageBytes, &full[s]);
         }
       }
@@ -444,11 +509,11 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
     if (lane == 0) {
       const uint32_t idesc = tc::idesc_bf16_f32(kM, kNH);
       const uint32_t sbA = (uint32_t)(Kp / 8) * 128;
-      const uint32_t aHi = tc::smem_u32(sA), aLo = tc::smem_u32(sA + aPart);
+      const uint32_t aHi = tc::smem_u32(S.A), aLo = tc::smem_u32(S.A + S.aPart);
       int it = 0;
-      for (int u = 0; u < nunits && !*abort_flag; ++u) {
-        const int r = u % kParts, k = u / kParts;
-        if (!tc::mbar_wait_sleep(&acce[r], (k & 1) ^ 1, P.status, 2)) { *abort_flag = 1; break; }
+      for (int u = 0; u < kParts * nj && !*abort_flag; ++u) {
+        const int r = u % kParts, jj = u / kParts;
+        if (!tc::mbar_wait_sleep(&acce[r], (jj & 1) ^ 1, P.status, 2)) { *abort_flag = 1; break; }
         tc::tc_fence_after();
         const uint32_t d = tmem + r * kRegion;
         bool ok = true;
@@ -457,19 +522,15 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
           const uint32_t ph = (it / kStages) & 1;
           if (!tc::mbar_wait_sleep(&full[s], ph, P.status, 4)) { ok = false; break; }
           tc::tc_fence_after();
-          const uint32_t bHi = tc::smem_u32(sB + s * kStageBytes);
+          const uint32_t bHi = tc::smem_u32(S.B + s * kStageBytes);
           const uint32_t bLo = bHi + kPartBytes;
-#pragma unroll
-          for (int ks = 0; ks < kKC / 16; ++ks) {
-            const int kg = kc * (kKC / 16) + ks;
-            const uint64_t dAh = tc::smem_desc(aHi + kg * 256, 128, sbA);
-            const uint64_t dAl = tc::smem_desc(aLo + kg * 256, 128, sbA);
-            const uint64_t dBh = tc::smem_desc(bHi + ks * 256, 128, kBSbo);
-            const uint64_t dBl = tc::smem_desc(bLo + ks * 256, 128, kBSbo);
-            tc::mma_bf16(d, dAh, dBh, idesc, (kc | ks) != 0);
-            tc::mma_bf16(d, dAh, dBl, idesc, 1);
-            tc::mma_bf16(d, dAl, dBh, idesc, 1);
-          }
+          const uint64_t dAh = tc::smem_desc(aHi + kc * 256, 128, sbA);
+          const uint64_t dAl = tc::smem_desc(aLo + kc * 256, 128, sbA);
+          const uint64_t dBh = tc::smem_desc(bHi, 128, kBSbo);
+          const uint64_t dBl = tc::smem_desc(bLo, 128, kBSbo);
+          tc::mma_bf16(d, dAh, dBh, idesc, kc != 0);
+          tc::mma_bf16(d, dAh, dBl, idesc, 1);
+          tc::mma_bf16(d, dAl, dBh, idesc, 1);
           tc::mma_commit(&empty[s]);
         }
         if (!ok) { *abort_flag = 1; break; }
@@ -480,237 +541,188 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
       tc::mbar_wait_sleep(done, 0, P.status, 8);
     }
   } else {
-    // ---------------- epilogue: thread = (q1, b2 parity) ----------------
-    const int qd = warp & 3, par = warp >> 2;
+    // ---------------- epilogue ----------------
+    const int qd = warp & 3, k = warp >> 2;
     const int m = qd * 32 + lane;
     const bool valid = tile0 + m < nq;
     const int q1c = P.q1_order[min(tile0 + m, nq - 1)];
     const unsigned FULL = 0xffffffffu;
-    float E1f[6];
-    unsigned ok1 = 0;
-    unsigned gp1;  // packed block starts of q1 (3 bits per band)
-    {
-      double e1d[6];
-#pragma unroll
-      for (int b = 0; b < 6; ++b) {
-        e1d[b] = sEn1[b * kM + m];
-        E1f[b] = (float)e1d[b];
-        ok1 |= (e1d[b] >= phxc::phExcludeCutoff && valid) ? (1u << b) : 0u;
-      }
-      gp1 = pack_blocks(e1d);
-    }
+    const int smearing = M.smearing;
+    const float sg = (float)M.sigma, ginv = M.sigma > 0.0 ? (float)(1.0 / M.sigma) : 0.f;
+    const float pre = (float)(phxc::pi * 0.25 * 0.5) * (float)M.norm;
+    const unsigned gp1 = P.rec[(size_t)q1c * kRecChunks + kChGp].x;
     const bool deg1 = gp1 != kIdentityBlocks;
-    const float* qT = sQT;
-    double acc[6][kMaxT];
+    unsigned ok1 = 0;
 #pragma unroll
-    for (int b = 0; b < 6; ++b)
+    for (int b = 0; b < 6; ++b) ok1 |= (valid && S.En1[b * kM + m] >= phxc::phExcludeCutoff) ? (1u << b) : 0u;
+    // owned b1 = k + 3o, their degenerate blocks
+    const unsigned bmO0 = deg1 ? blk_mask(gp1, k) : (1u << k);
+    const unsigned bmO1 = deg1 ? blk_mask(gp1, k + 3) : (1u << (k + 3));
+    double acc0[NT], acc1[NT];
 #pragma unroll
-      for (int c = 0; c < kMaxT; ++c) acc[b][c] = 0.0;
-    unsigned long long need[3];   // own b2 = par + 2j
-    unsigned gp2 = kIdentityBlocks, gp3 = kIdentityBlocks;
-    float Wd[36];                 // |V|^2 of triplets at degenerate points (deferred)
-    unsigned long long dmask = 0;
-    bool deg = false;
-    U2* u2 = sU2 + warp * 6;
+    for (int t = 0; t < NT; ++t) acc0[t] = acc1[t] = 0.0;
+    uint4* u2 = S.u2 + qd * 2 * kU2Chunks;
+    const uint4* srow = S.rec + m;
     const uint32_t lane_base = (uint32_t)(qd * 32) << 16;
-    for (int u = 0; u < nunits; ++u) {
-      const int h = u % kParts, k = u / kParts;
-      if (h == 0) {
-        // ---- new q2: stage q3 data (shared by both parities of the quarter)
-        const int iq2 = P.q2_first + jbeg + k;
-        const int iq2m = mesh_neg(iq2, n0, n1, n2);
-        const int iq3 = mesh_add(q1c, iq2, n0, n1, n2);
-        // both parities must be done with the previous q2's staged data
-        if (k > 0 && !tc::mbar_wait_sleep(&rel[qd], (k - 1) & 1, P.status, 32)) { *abort_flag = 1; break; }
-        if (par == 0) {
-          const float2* src = P.U32 + (size_t)iq3 * 36;
-#pragma unroll 6
-          for (int e = 0; e < 36; ++e) sE3[e * kM + m] = src[e];
+    for (int jj = 0; jj < nj; ++jj) {
+      // ---- stage the q3 records of the quarter's rows and the q2 / -q2 bands
+      if (jj > 0 && !tc::mbar_wait(&rel[qd], (jj - 1) & 1, P.status, 32)) { *abort_flag = 1; break; }
+      const int iq2 = P.q2_first + jbeg + jj;
+      const int iq2m = mesh_neg(iq2, n0, n1, n2);
+      const int iq3 = mesh_add(q1c, iq2, n0, n1, n2);
+      {
+        const uint4* src = P.rec + (size_t)iq3 * kRecChunks;
 #pragma unroll
-          for (int b = 0; b < 6; ++b) sEn3[b * kM + m] = M.E[(size_t)iq3 * 6 + b];
-        } else {
-          if (M.smearing == PHX_SMEAR_ADAPTIVE) {
-#pragma unroll 6
-            for (int i = 0; i < 18; ++i) sV3[i * kM + m] = (float)M.vg[(size_t)iq3 * 18 + i];
-          }
-          for (int c = 0; c < nT; ++c) {
-#pragma unroll
-            for (int b = 0; b < 6; ++b) sN3[(c * 6 + b) * kM + m] = (float)M.bose[((size_t)c * nq + iq3) * 6 + b];
-          }
+        for (int i = 0; i < 13; ++i)
+          if (k + 3 * i < kRecChunks) cp_async16(&S.rec[(k + 3 * i) * kM + m], src + k + 3 * i);
+        if (k == 2 && lane < kU2Chunks) {
+          cp_async16(&u2[lane], P.rec + (size_t)iq2 * kRecChunks + kChBand + lane);
+          cp_async16(&u2[kU2Chunks + lane], P.rec + (size_t)iq2m * kRecChunks + kChBand + lane);
         }
-        if (lane < 6) {
-          U2 x;
-          x.e2 = M.E[(size_t)iq2 * 6 + lane];
-          x.e2m = M.E[(size_t)iq2m * 6 + lane];
+        cp_async_wait_all();
+      }
+      tc::mbar_arrive(&stg[qd]);
+      if (!tc::mbar_wait(&stg[qd], jj & 1, P.status, 64)) { *abort_flag = 1; break; }
+      const unsigned gp2 = u2[kU2Chunks - 1].x;
+      const unsigned gp3 = srow[kChGp * kM].x;
+      const bool deg2 = gp2 != kIdentityBlocks, deg3 = gp3 != kIdentityBlocks;
+      // ---- liveness of b2 = 2k, 2k+1 for all (b1, b3)
+      {
+        float E1f[6];
 #pragma unroll
-          for (int i = 0; i < 3; ++i) {
-            x.v2[i] = M.smearing == PHX_SMEAR_ADAPTIVE ? (float)M.vg[((size_t)iq2 * 6 + lane) * 3 + i] : 0.f;
-            x.v2m[i] = M.smearing == PHX_SMEAR_ADAPTIVE ? (float)M.vg[((size_t)iq2m * 6 + lane) * 3 + i] : 0.f;
-          }
-#pragma unroll
-          for (int c = 0; c < kMaxT; ++c) {
-            x.n2[c] = c < nT ? (float)M.bose[((size_t)c * nq + iq2) * 6 + lane] : 0.f;
-            x.n2m[c] = c < nT ? (float)M.bose[((size_t)c * nq + iq2m) * 6 + lane] : 0.f;
-          }
-          u2[lane] = x;
-        }
-        tc::mbar_arrive(&stg[qd]);  // staged data visible to both parities
-        if (!tc::mbar_wait(&stg[qd], k & 1, P.status, 64)) { *abort_flag = 1; break; }
-        {
-          double e2d[6], e3d[6];
-#pragma unroll
-          for (int b = 0; b < 6; ++b) {
-            e2d[b] = u2[b].e2;
-            e3d[b] = sEn3[b * kM + m];
-          }
-          gp2 = pack_blocks(e2d);
-          gp3 = pack_blocks(e3d);
-        }
-        const bool deg2 = gp2 != kIdentityBlocks, deg3 = gp3 != kIdentityBlocks;
-        deg = deg1 || deg2 || deg3;
-        // liveness masks of the own b2 values, expanded over degenerate blocks
-#pragma unroll
-        for (int j = 0; j < 3; ++j) need[j] = 0ull;
+        for (int b = 0; b < 6; ++b) E1f[b] = (float)S.En1[b * kM + m];
 #pragma unroll 1
-        for (int bx = 0; bx < 6; ++bx) {
-          if (!deg2 && (bx & 1) != par) continue;
-          Smem3 S;
-          S.En3 = sEn3; S.V3 = sV3;
-          const unsigned long long mk = live_mask(M, qT, S, u2[bx], m, E1f, ok1);
+        for (int bl = 0; bl < 2; ++bl) {
+          const int b2 = 2 * k + bl;
+          const Band x2 = load_band<1>(u2 + 3 * b2, 1);
+          const Band x2m = load_band<1>(u2 + kU2Chunks + 3 * b2, 1);
+          const float E2f = (float)x2.E, E2mf = (float)x2m.E;
+          const bool ok2 = x2.E >= phxc::phExcludeCutoff, ok2m = x2m.E >= phxc::phExcludeCutoff;
+          unsigned long long nd = 0;
+          if (ok2 || ok2m) {
+#pragma unroll 1
+            for (int b3 = 0; b3 < 6; ++b3) {
+              const Band x3 = load_band<1>(srow + (kChBand + 3 * b3) * kM, kM);
+              if (!(x3.E >= phxc::phEnergyCutoff)) continue;
+              const unsigned c = live6(smearing, sg, P.tol, E1f, E2f, E2mf, x2.P, x2m.P, ok2, ok2m,
+                                       (float)x3.E, x3.P) & ok1;
+              unsigned long long sp = 0;
 #pragma unroll
-          for (int j = 0; j < 3; ++j)
-            if (blk_start(gp2, bx) == blk_start(gp2, par + 2 * j)) need[j] |= mk;
-        }
-        if (deg1 || deg3) {
-#pragma unroll
-          for (int j = 0; j < 3; ++j) need[j] = expand_blocks(need[j], gp1, gp3);
+              for (int b1 = 0; b1 < 6; ++b1) sp |= (unsigned long long)((c >> b1) & 1u) << (6 * b1);
+              nd |= sp << b3;
+            }
+          }
+          S.need[b2 * kM + m] = nd;
         }
       }
-      // ---- this part holds b2 = 2h and 2h+1; this thread takes b2 = 2h + par
-      const int b2 = 2 * h + par;
-      unsigned long long nb2 = 0;
-#pragma unroll
-      for (int j = 0; j < 3; ++j)
-        if (j == h) nb2 = need[j];
-      unsigned rows = 0;
-#pragma unroll
-      for (int b1 = 0; b1 < 6; ++b1) rows |= ((nb2 >> (6 * b1)) & 63ull) ? (1u << b1) : 0u;
-      const unsigned wrows = __reduce_or_sync(FULL, rows);
-      if (!tc::mbar_wait_sleep(&accf[h], k & 1, P.status, 16)) { *abort_flag = 1; break; }
-      tc::tc_fence_after();
-      const uint32_t col0 = tmem + lane_base + h * kRegion + par * 72;
-      const U2& x = u2[b2];
+      tc::mbar_arrive(&lvb[qd]);
+      if (!tc::mbar_wait(&lvb[qd], jj & 1, P.status, 128)) { *abort_flag = 1; break; }
+      // ---- the three parts
+      bool stop = false;
 #pragma unroll 1
-      for (int hb = 0; hb < 2; ++hb) {
-        const unsigned hrows = (wrows >> (3 * hb)) & 7u;
-        if (!hrows) continue;
-        // X(b1,c) = sum_a e1(a,b1) T(a,c) for b1 = 3hb..3hb+2; T read from TMEM one a-row at a time
-        float2 X[3][6];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-          for (int c = 0; c < 6; ++c) X[i][c] = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int a = 0; a < 6; ++a) {
-          float t[12];
-          __syncwarp();
-          tc::tmem_ld8(col0 + a * 12, t);
-          tc::tmem_ld4(col0 + a * 12 + 8, t + 8);
-          tc::tmem_wait_ld();
-#pragma unroll
-          for (int i = 0; i < 3; ++i) {
-            if (!((hrows >> i) & 1u)) continue;
-            const float2 e = sE1[(a * 6 + 3 * hb + i) * kM + m];
-#pragma unroll
-            for (int c = 0; c < 6; ++c) cfmaf(X[i][c], e, make_float2(t[2 * c], t[2 * c + 1]));
+      for (int h = 0; h < kParts; ++h) {
+        if (!tc::mbar_wait(&accf[h], jj & 1, P.status, 16)) { stop = true; break; }
+        tc::tc_fence_after();
+#pragma unroll 1
+        for (int bl = 0; bl < 2; ++bl) {
+          const int b2 = 2 * h + bl;
+          // b3 masks of the owned b1 (expanded over the blocks of b2 and b3)
+          unsigned long long nsrc = S.need[b2 * kM + m];
+          const unsigned bm2 = deg2 ? blk_mask(gp2, b2) : (1u << b2);
+          if (bm2 != (1u << b2)) {
+            for (int b = 0; b < 6; ++b)
+              if (b != b2 && ((bm2 >> b) & 1u)) nsrc |= S.need[b * kM + m];
           }
-        }
-        // V(b1,b3) = sum_c X(b1,c) conj(e3(c,b3)); rates of the needed triplets
-#pragma unroll 1
-        for (int b3 = 0; b3 < 6; ++b3) {
-          unsigned cols = 0;
+          unsigned nO0 = (unsigned)(nsrc >> (6 * k)) & 63u;
+          unsigned nO1 = (unsigned)(nsrc >> (6 * (k + 3))) & 63u;
+          if (deg3) {
+            if (nO0) nO0 = expand_b3(nO0, gp3);
+            if (nO1) nO1 = expand_b3(nO1, gp3);
+          }
+          const unsigned R = (nO0 ? bmO0 : 0u) | (nO1 ? bmO1 : 0u);
+          unsigned UR = __reduce_or_sync(FULL, R);
+          const uint32_t col0 = tmem + lane_base + h * kRegion + bl * 72;
+          while (UR) {
+            const int row = __ffs(UR) - 1;
+            UR &= UR - 1;
+            // Y(c) = sum_a e1(a, row) X(a, c)
+            float2 Y[6];
 #pragma unroll
-          for (int i = 0; i < 3; ++i) cols |= ((nb2 >> (6 * (3 * hb + i) + b3)) & 1ull) ? (1u << i) : 0u;
-          const unsigned wcols = __reduce_or_sync(FULL, cols);
-          if (!wcols) continue;
-          float2 ec[6];
+            for (int c = 0; c < 6; ++c) Y[c] = make_float2(0.f, 0.f);
 #pragma unroll
-          for (int c = 0; c < 6; ++c) ec[c] = sE3[(c * 6 + b3) * kM + m];
-          float sp, sm;
-          bool vzp, vzm;
-          sigmas(M, qT, x, sV3, m, b3, sp, sm, vzp, vzm);
-          const double en3 = sEn3[b3 * kM + m];
-          float n3[kMaxT];
+            for (int a = 0; a < 6; ++a) {
+              float t[12];
+              tc::tmem_ld8(col0 + a * 12, t);
+              tc::tmem_ld4(col0 + a * 12 + 8, t + 8);
+              tc::tmem_wait_ld();
+              const float2 e = S.E1v[(a * 6 + row) * kM + m];
 #pragma unroll
-          for (int c = 0; c < kMaxT; ++c) n3[c] = sN3[(c * 6 + b3) * kM + m];
+              for (int c = 0; c < 6; ++c) cfmaf(Y[c], e, make_float2(t[2 * c], t[2 * c + 1]));
+            }
+            const unsigned cols = (((bmO0 >> row) & 1u) ? nO0 : 0u) | (((bmO1 >> row) & 1u) ? nO1 : 0u);
+            unsigned UC = __reduce_or_sync(FULL, cols);
+            while (UC) {
+              const int b3 = __ffs(UC) - 1;
+              UC &= UC - 1;
+              // V = sum_c Y(c) conj(e3(c, b3)), W = |V|^2
+              float2 v = make_float2(0.f, 0.f);
 #pragma unroll
-          for (int i = 0; i < 3; ++i) {
-            if (!((wcols >> i) & 1u)) continue;
-            float2 v = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int c = 0; c < 6; ++c) cfmacf(v, X[i][c], ec[c]);
-            const float w = fmaf(v.x, v.x, v.y * v.y);
-            if (!((cols >> i) & 1u)) continue;
-            const int b1 = 3 * hb + i;
-            if (!deg) {
-              float n1v[kMaxT], f[kMaxT];
-#pragma unroll
-              for (int c = 0; c < kMaxT; ++c) n1v[c] = sN1[(c * 6 + b1) * kM + m];
-              rate_factors(M, sEn1[b1 * kM + m], n1v, x, en3, n3, sp, sm, vzp, vzm, f);
-              if (hb == 0) {
-#pragma unroll
-                for (int c = 0; c < kMaxT; ++c) acc[i][c] += (double)(w * f[c]);
-              } else {
-#pragma unroll
-                for (int c = 0; c < kMaxT; ++c) acc[3 + i][c] += (double)(w * f[c]);
+              for (int c = 0; c < 6; ++c) {
+                const uint2 e = reinterpret_cast<const uint2*>(srow + ((c * 6 + b3) >> 1) * kM)[(c * 6 + b3) & 1];
+                cfmacf(v, Y[c], make_float2(__uint_as_float(e.x), __uint_as_float(e.y)));
               }
-            } else {
-              // degenerate points: defer (W is spread over blocks after X is released)
-              Wd[b1 * 6 + b3] = w;
-              dmask |= 1ull << (b1 * 6 + b3);
+              const float w = fmaf(v.x, v.x, v.y * v.y);
+              if (!((cols >> b3) & 1u)) continue;
+              const Band x2 = load_band<NT>(u2 + 3 * b2, 1);
+              const Band x2m = load_band<NT>(u2 + kU2Chunks + 3 * b2, 1);
+              const Band x3 = load_band<NT>(srow + (kChBand + 3 * b3) * kM, kM);
+              Sig gp, gm;
+              if (smearing == PHX_SMEAR_ADAPTIVE) {
+                gp = sigma_ad(x2.P, x3.P);
+                gm = sigma_ad(x2m.P, x3.P);
+              }
+              const bool avg = deg2 || deg3;
+              const unsigned bm3 = avg ? blk_mask(gp3, b3) : 0u;
+#pragma unroll 1
+              for (int o = 0; o < 2; ++o) {
+                const int b1 = k + 3 * o;
+                const unsigned no = o ? nO1 : nO0, bmo = o ? bmO1 : bmO0;
+                if (!((no >> b3) & 1u) || !((bmo >> row) & 1u)) continue;
+                const double E1 = S.En1[b1 * kM + m];
+                const float iE1 = S.iE1[b1 * kM + m];
+                float n1v[NT];
+#pragma unroll
+                for (int t = 0; t < NT; ++t) n1v[t] = S.N1[(t * 6 + b1) * kM + m];
+                float f[NT];
+                if (!avg) rate_f<NT>(smearing, ginv, pre, E1, iE1, n1v, x2, x2m, x3, gp, gm, f);
+                else rate_avg<NT>(smearing, ginv, pre, E1, iE1, n1v, u2, srow, bm2, bm3, f);
+                const float wn = w / (float)__popc(bmo);
+                if (o == 0) {
+#pragma unroll
+                  for (int t = 0; t < NT; ++t) acc0[t] += (double)(wn * f[t]);
+                } else {
+#pragma unroll
+                  for (int t = 0; t < NT; ++t) acc1[t] += (double)(wn * f[t]);
+                }
+              }
             }
           }
         }
+        tc::tc_fence_before();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&acce[h]);
       }
-      tc::tc_fence_before();
-      __syncwarp();
-      if (lane == 0) tc::mbar_arrive(&acce[h]);
-      if (dmask) {
-        // degenerate points: spread W over the block of b1 with block-averaged
-        // rate factors (sum S(W) F = sum W S(F) for the block average S)
-        Smem3 S;
-        S.E1v = sE1; S.E3v = sE3; S.En1 = sEn1; S.En3 = sEn3; S.V3 = sV3; S.N3 = sN3; S.N1 = sN1;
-        const int b2s = blk_start(gp2, b2), b2n = blk_size(gp2, b2);
-        while (dmask) {
-          const int bit = __ffsll((long long)dmask) - 1;
-          dmask &= dmask - 1;
-          const int b1 = bit / 6, b3 = bit % 6;
-          const float w = Wd[bit];
-          const int b3s = blk_start(gp3, b3), b3n = blk_size(gp3, b3);
-          const int b1s = blk_start(gp1, b1), b1n = blk_size(gp1, b1);
-          for (int bt = b1s; bt < b1s + b1n; ++bt) {
-            float g[kMaxT];
-            rate_block(M, qT, S, u2, m, bt, b2s, b2n, b3s, b3n, g);
-#pragma unroll
-            for (int bb = 0; bb < 6; ++bb)
-              if (bb == bt) {
-#pragma unroll
-                for (int c = 0; c < kMaxT; ++c) acc[bb][c] += (double)(w * g[c] / (float)b1n);
-              }
-          }
-        }
-      }
-      if (h == kParts - 1) tc::mbar_arrive(&rel[qd]);  // done with this q2's staged data
+      if (stop) { *abort_flag = 1; break; }
+      tc::mbar_arrive(&rel[qd]);  // done with this q2's staged records
       if (*abort_flag) break;
     }
-    // each parity owns its own partial-sum slot (2 slots per CTA row)
     if (valid) {
-      double* out = P.partial + ((size_t)(2 * blockIdx.y + par) * nq + q1c) * 6 * nT;
+      double* out = P.partial + ((size_t)blockIdx.y * nq + q1c) * 6 * NT;
 #pragma unroll
-      for (int b1 = 0; b1 < 6; ++b1)
-#pragma unroll
-        for (int c = 0; c < kMaxT; ++c)
-          if (c < nT) out[b1 * nT + c] += acc[b1][c];
+      for (int t = 0; t < NT; ++t) {
+        out[k * NT + t] += acc0[t];
+        out[(k + 3) * NT + t] += acc1[t];
+      }
     }
   }
   tc::tc_fence_before();
@@ -800,10 +812,18 @@ __global__ void __launch_bounds__(128, 1) diag_gemm_kernel(int N, int Kp, const 
 }
 
 size_t pair_tc_smem(int Kp) {
-  return 2 * (size_t)kM * Kp * 2 + (size_t)kStages * kStageBytes + 2 * 36 * kM * sizeof(float2) +
-         12 * kM * sizeof(double) + (18 + 2 * kMaxT * 6) * kM * sizeof(float) +
-         kEpiWarps * 6 * sizeof(U2) + 10 * sizeof(float) + (2 * kStages + 2 * kParts + 9) * sizeof(uint64_t) +
-         16 + 1024;
+  size_t off[10];
+  return smem_layout(Kp, off) + 1024;
+}
+
+template <int NT>
+int launch_pair(phx_ctx* ctx, const TcArgs& A, int tiles, int slots) {
+  const size_t smem = pair_tc_smem(A.Kp);
+  PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+  pair_tc_kernel<NT><<<dim3(tiles, slots), kThreads, smem, ctx->stream>>>(A);
+  PHX_CUDA(ctx, cudaGetLastError());
+  return PHX_OK;
 }
 
 }  // namespace
@@ -817,18 +837,13 @@ size_t phx_split_bimg_bytes(int chunk, int nr3) {
   return (size_t)chunk * kParts * (phx_split_kp(nr3) / kKC) * kStageBytes;
 }
 
-// FP32 eigenvectors and the q1 visiting order (k-space blocks of 4x4x2 so
-// that the 32 lanes of a warp hold neighbouring q1 with similar energies).
+size_t phx_split_rec_bytes(int nq) { return (size_t)nq * kRecChunks * 16; }
+
+// The q1 visiting order: k-space blocks of 4x4x2 so that the 32 lanes of a
+// warp hold neighbouring q1 with similar energies and similar q3.
 int phx_split_prepare_bands(phx_ctx* ctx, phx_bands* b) {
-  if (!b->d_U32) {
-    const size_t n = (size_t)b->nq * b->nb * b->nb;
-    PHX_CUDA(ctx, cudaMalloc(&b->d_U32, sizeof(float2) * n));
-    to_fp32_kernel<<<1024, 256, 0, ctx->stream>>>(reinterpret_cast<const double2*>(b->d_U), n,
-                                                  reinterpret_cast<float2*>(b->d_U32));
-    PHX_CUDA(ctx, cudaGetLastError());
-  }
   if (!b->d_q1_order) {
-    const int n0 = b->mesh[0], n1 = b->mesh[1], n2 = b->mesh[2];
+    const int n0 = b->mesh[0], n1 = b->mesh[1];
     std::vector<long long> key(b->nq);
     std::vector<int> order(b->nq);
     for (int i = 0; i < b->nq; ++i) {
@@ -845,11 +860,20 @@ int phx_split_prepare_bands(phx_ctx* ctx, phx_bands* b) {
   return PHX_OK;
 }
 
+// Per-point records of one builder call (they hold the Bose factors of its
+// temperatures and the velocity projections of its smearing).
+int phx_split_pack_records(phx_ctx* ctx, const pairc::MeshArgs& M, void* rec, int* launches) {
+  pack_records_kernel<<<(M.nq + 127) / 128, 128, 0, ctx->stream>>>(M, static_cast<uint4*>(rec));
+  PHX_CUDA(ctx, cudaGetLastError());
+  *launches += 1;
+  return PHX_OK;
+}
+
 // One chunk of q2: convert the FP64 Dp images to BF16 hi/lo tiles and run the
 // fused tensor-core pair kernel over (q1 tiles) x (q2 slots).
 int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v, const phx_bands* b,
-                         const double2* Dp, uint8_t* Bimg, int q2_first, int q2_count, int slots,
-                         double* partial, int* launches) {
+                         const double2* Dp, uint8_t* Bimg, const void* rec, double emax, int q2_first,
+                         int q2_count, int slots, double* partial, int* launches) {
   const int Kp = phx_split_kp(v->nr3);
   const int nkc = Kp / kKC;
   convert_b_kernel<<<dim3(q2_count, kParts * nkc), 256, 0, ctx->stream>>>(Dp, v->nr3, Kp, q2_count, Bimg);
@@ -858,21 +882,27 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
   A.m = M;
   A.Kp = Kp;
   A.Bimg = Bimg;
-  A.U32 = reinterpret_cast<const float2*>(b->d_U32);
+  A.rec = static_cast<const uint4*>(rec);
   A.R3 = v->d_R3;
   A.nr3 = v->nr3;
   A.q1_order = b->d_q1_order;
   A.q2_first = q2_first;
   A.q2_count = q2_count;
   A.q2_per_slot = (q2_count + slots - 1) / slots;
+  // FP32 energies carry a relative rounding of 2^-24; a window test sums
+  // four of them and a sigma: 32 units of the largest energy bound it.
+  A.tol = (float)(32.0 * std::max(emax, 1e-6) * 5.9604644775390625e-8);
   A.partial = partial;
   A.status = ctx->d_status;
-  const size_t smem = pair_tc_smem(Kp);
-  PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
   const int tiles = (M.nq + kM - 1) / kM;
-  pair_tc_kernel<<<dim3(tiles, slots), kThreads, smem, ctx->stream>>>(A);
-  PHX_CUDA(ctx, cudaGetLastError());
+  int rc = PHX_OK;
+  switch (M.nT) {
+    case 1: rc = launch_pair<1>(ctx, A, tiles, slots); break;
+    case 2: rc = launch_pair<2>(ctx, A, tiles, slots); break;
+    case 3: rc = launch_pair<3>(ctx, A, tiles, slots); break;
+    default: rc = launch_pair<4>(ctx, A, tiles, slots); break;
+  }
+  if (rc != PHX_OK) return rc;
   *launches += 2;
   return PHX_OK;
 }

@@ -17,9 +17,12 @@
 //  * warp k decides, for b2 = 2k, 2k+1 and every (b1, b3), whether any of the
 //    three delta functions of the triplet can be non-zero (FP32 windows with a
 //    rounding margin); the masks are shared in shared memory;
-//  * warp k owns the linewidths of b1 = k and k+3 for every b2: it contracts
-//    the rows of X it needs with e1 and e3 in FP32, and accumulates the rates
-//    of the live triplets in FP64.
+//  * warp k handles the rows (b1, b2) with (b1 + b2) % 3 == k: it contracts
+//    the rows of X it needs with e1 and e3 in FP32 and queues the live
+//    triplets (|V|^2 and indices) in shared memory; 32 queued triplets at a
+//    time get their delta functions and Bose factors with every lane busy,
+//    and their rates go to FP32 accumulators of the current q2, which are
+//    folded into FP64 registers once per q2.
 // Degenerate points need no symmetrised |V|^2: with S the block average over
 // the degenerate blocks of b1, b2 and b3 (scattering.cpp:1209-1318),
 //   Gamma(b1) = sum_{b2,b3} S(W) F = sum_{b1' in blk(b1), b2, b3} W(b1',b2,b3) G(b1,b2,b3) / n1,
@@ -42,7 +45,7 @@ constexpr int kM = 128;            // q1 rows per CTA = TMEM lanes
 constexpr int kKC = 16;            // K elements per B stage (one MMA K-step)
 constexpr int kParts = 3;          // N split into 3 parts of 2 b2 each
 constexpr int kNH = 144;           // N columns per part: 2 b2 x 36 (a,c) x {re,im}
-constexpr int kStages = 3;
+constexpr int kStages = 2;
 constexpr int kRegion = 160;       // TMEM columns per accumulator region (>= kNH)
 constexpr int kTmemCols = 512;
 constexpr int kEpiWarps = 12;
@@ -60,6 +63,7 @@ constexpr int kRecChunks = 37;
 constexpr int kChBand = 18;
 constexpr int kChGp = 36;
 constexpr int kU2Chunks = kRecChunks - kChBand;   // band blocks + blocks word
+constexpr int kQueue = 64;                        // live-triplet queue entries per warp
 
 struct TcArgs {
   MeshArgs m;
@@ -276,38 +280,6 @@ __device__ __forceinline__ void rate_f(int smearing, float ginv, float pre, doub
            fm * x3.N[t] * (d1 * n1[t] * (x2m.N[t] + 1.f) + d2 * x2m.N[t] * (n1[t] + 1.f));
 }
 
-// G(b1, blk(b2), blk(b3)): F averaged over the degenerate blocks of b2 and b3
-template <int NT>
-__device__ __noinline__ void rate_avg(int smearing, float ginv, float pre, double E1, float iE1,
-                                      const float* n1, const uint4* u2, const uint4* srow,
-                                      unsigned bm2, unsigned bm3, float* g) {
-#pragma unroll
-  for (int t = 0; t < NT; ++t) g[t] = 0.f;
-  int cnt = 0;
-  for (int b2 = 0; b2 < 6; ++b2) {
-    if (!((bm2 >> b2) & 1u)) continue;
-    const Band x2 = load_band<NT>(u2 + 3 * b2, 1);
-    const Band x2m = load_band<NT>(u2 + kU2Chunks + 3 * b2, 1);
-    for (int b3 = 0; b3 < 6; ++b3) {
-      if (!((bm3 >> b3) & 1u)) continue;
-      const Band x3 = load_band<NT>(srow + (kChBand + 3 * b3) * kM, kM);
-      Sig gp, gm;
-      if (smearing == PHX_SMEAR_ADAPTIVE) {
-        gp = sigma_ad(x2.P, x3.P);
-        gm = sigma_ad(x2m.P, x3.P);
-      }
-      float f[NT];
-      rate_f<NT>(smearing, ginv, pre, E1, iE1, n1, x2, x2m, x3, gp, gm, f);
-#pragma unroll
-      for (int t = 0; t < NT; ++t) g[t] += f[t];
-      ++cnt;
-    }
-  }
-  const float inv = 1.f / (float)cnt;
-#pragma unroll
-  for (int t = 0; t < NT; ++t) g[t] *= inv;
-}
-
 // OR a 6-bit b3 mask over the degenerate blocks of q3
 __device__ __noinline__ unsigned expand_b3(unsigned c, unsigned gp3) {
   unsigned o = 0;
@@ -349,6 +321,7 @@ __device__ __forceinline__ unsigned live6(int smearing, float sg, float tol, con
 // ---------------------------------------------------------------------------
 // the fused pair kernel
 // ---------------------------------------------------------------------------
+
 // Warp roles (448 threads): warps 0-11 epilogue, warp 12 producer (bulk
 // copies of B stages), warp 13 MMA issuer.
 struct Smem {
@@ -362,6 +335,8 @@ struct Smem {
   uint4* rec;          // staged q3 records [kRecChunks][128]
   uint4* u2;           // [4 quarters][2: q2, -q2][kU2Chunks]
   unsigned long long* need;  // [6 b2][128] bit b1*6+b3
+  uint2* queue;        // [12 warps][kQueue] live triplets awaiting their rates
+  float* acc;          // [4 quarters][32 rows][6 b1][kMaxT] rates of the current q2
   uint64_t* bars;
 };
 
@@ -379,12 +354,14 @@ __host__ __device__ inline size_t smem_layout(int Kp, size_t* off) {
   off[6] = o; o += align16((size_t)kRecChunks * kM * 16);      // staged records
   off[7] = o; o += align16(4 * 2 * kU2Chunks * 16);            // q2 bands
   off[8] = o; o += align16(6 * kM * sizeof(unsigned long long));  // masks
-  off[9] = o; o += align16(32 * sizeof(uint64_t));             // barriers, tmem slot, flag
+  off[9] = o; o += align16(kEpiWarps * kQueue * sizeof(uint2));   // queues
+  off[10] = o; o += align16(4 * 32 * 6 * kMaxT * sizeof(float));  // q2 accumulators
+  off[11] = o; o += align16(32 * sizeof(uint64_t));            // barriers, tmem slot, flag
   return o;
 }
 
 __device__ __forceinline__ Smem carve(uint8_t* base, int Kp) {
-  size_t off[10];
+  size_t off[12];
   smem_layout(Kp, off);
   Smem s;
   s.aPart = (uint32_t)kM * Kp * 2;
@@ -397,8 +374,59 @@ __device__ __forceinline__ Smem carve(uint8_t* base, int Kp) {
   s.rec = reinterpret_cast<uint4*>(base + off[6]);
   s.u2 = reinterpret_cast<uint4*>(base + off[7]);
   s.need = reinterpret_cast<unsigned long long*>(base + off[8]);
-  s.bars = reinterpret_cast<uint64_t*>(base + off[9]);
+  s.queue = reinterpret_cast<uint2*>(base + off[9]);
+  s.acc = reinterpret_cast<float*>(base + off[10]);
+  s.bars = reinterpret_cast<uint64_t*>(base + off[11]);
   return s;
+}
+
+// Rate of one queued live triplet, added to the FP32 accumulator of its row
+// and b1.  Entry: x = |V|^2 / n1, y = lane of the q1 row | b1 << 5 | b2 << 8 |
+// b3 << 11 | degenerate flag << 14.  Flagged entries average the rate factors
+// over the degenerate blocks of b2 and b3 (one band each otherwise).
+template <int NT>
+__device__ __forceinline__ void rate_entry(uint2 e, int qd, const double* En1, const float* iE1s,
+                                           const float* N1, const uint4* rec, const uint4* u2,
+                                           unsigned gp2, int smearing, float ginv, float pre,
+                                           float* qacc) {
+  const float wn = __uint_as_float(e.x);
+  const int r = e.y & 31, b1 = (e.y >> 5) & 7, b2 = (e.y >> 8) & 7, b3 = (e.y >> 11) & 7;
+  const int mm = qd * 32 + r;
+  const uint4* srow = rec + mm;
+  unsigned bm2 = 1u << b2, bm3 = 1u << b3;
+  if ((e.y >> 14) & 1) {
+    bm2 = blk_mask(gp2, b2);
+    bm3 = blk_mask(srow[kChGp * kM].x, b3);
+  }
+  const double E1 = En1[b1 * kM + mm];
+  const float iE1 = iE1s[b1 * kM + mm];
+  float n1v[NT];
+#pragma unroll
+  for (int t = 0; t < NT; ++t) n1v[t] = N1[(t * 6 + b1) * kM + mm];
+  float g[NT];
+#pragma unroll
+  for (int t = 0; t < NT; ++t) g[t] = 0.f;
+  for (unsigned m2 = bm2; m2; m2 &= m2 - 1) {
+    const int c2 = __ffs(m2) - 1;
+    const Band x2 = load_band<NT>(u2 + 3 * c2, 1);
+    const Band x2m = load_band<NT>(u2 + kU2Chunks + 3 * c2, 1);
+    for (unsigned m3 = bm3; m3; m3 &= m3 - 1) {
+      const int c3 = __ffs(m3) - 1;
+      const Band x3 = load_band<NT>(srow + (kChBand + 3 * c3) * kM, kM);
+      Sig gp, gm;
+      if (smearing == PHX_SMEAR_ADAPTIVE) {
+        gp = sigma_ad(x2.P, x3.P);
+        gm = sigma_ad(x2m.P, x3.P);
+      }
+      float f[NT];
+      rate_f<NT>(smearing, ginv, pre, E1, iE1, n1v, x2, x2m, x3, gp, gm, f);
+#pragma unroll
+      for (int t = 0; t < NT; ++t) g[t] += f[t];
+    }
+  }
+  const float scale = wn / (float)(__popc(bm2) * __popc(bm3));
+#pragma unroll
+  for (int t = 0; t < NT; ++t) atomicAdd(&qacc[(r * 6 + b1) * kMaxT + t], scale * g[t]);
 }
 
 template <int NT>
@@ -542,6 +570,10 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
     }
   } else {
     // ---------------- epilogue ----------------
+    // Warp k of quarter qd handles the rows (b1, b2) with (b1 + b2) % 3 == k,
+    // so the three warps of a quarter share every b2 and every b1 evenly; the
+    // rates go to FP32 accumulators of the quarter (one q2 at a time), which
+    // warp k folds into FP64 registers for b1 = k and k + 3.
     const int qd = warp & 3, k = warp >> 2;
     const int m = qd * 32 + lane;
     const bool valid = tile0 + m < nq;
@@ -555,18 +587,38 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
     unsigned ok1 = 0;
 #pragma unroll
     for (int b = 0; b < 6; ++b) ok1 |= (valid && S.En1[b * kM + m] >= phxc::phExcludeCutoff) ? (1u << b) : 0u;
-    // owned b1 = k + 3o, their degenerate blocks
-    const unsigned bmO0 = deg1 ? blk_mask(gp1, k) : (1u << k);
-    const unsigned bmO1 = deg1 ? blk_mask(gp1, k + 3) : (1u << (k + 3));
     double acc0[NT], acc1[NT];
 #pragma unroll
     for (int t = 0; t < NT; ++t) acc0[t] = acc1[t] = 0.0;
     uint4* u2 = S.u2 + qd * 2 * kU2Chunks;
     const uint4* srow = S.rec + m;
+    uint2* queue = S.queue + warp * kQueue;
+    float* qacc = S.acc + qd * 32 * 6 * kMaxT;
+#pragma unroll
+    for (int t = 0; t < kMaxT; ++t) {
+      qacc[(lane * 6 + k) * kMaxT + t] = 0.f;
+      qacc[(lane * 6 + k + 3) * kMaxT + t] = 0.f;
+    }
+    int qn = 0;  // queued live triplets (warp-uniform)
+    const unsigned lanemask_lt = (1u << lane) - 1u;
     const uint32_t lane_base = (uint32_t)(qd * 32) << 16;
+    // fold the quarter's accumulators of b1 = k, k+3 (this lane's row) into FP64
+    auto flush = [&]() {
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        acc0[t] += (double)qacc[(lane * 6 + k) * kMaxT + t];
+        acc1[t] += (double)qacc[(lane * 6 + k + 3) * kMaxT + t];
+        qacc[(lane * 6 + k) * kMaxT + t] = 0.f;
+        qacc[(lane * 6 + k + 3) * kMaxT + t] = 0.f;
+      }
+    };
+    bool failed = false;
     for (int jj = 0; jj < nj; ++jj) {
-      // ---- stage the q3 records of the quarter's rows and the q2 / -q2 bands
-      if (jj > 0 && !tc::mbar_wait(&rel[qd], (jj - 1) & 1, P.status, 32)) { *abort_flag = 1; break; }
+      // ---- previous q2 done by the whole quarter: fold its rates, then stage
+      if (jj > 0) {
+        if (!tc::mbar_wait(&rel[qd], (jj - 1) & 1, P.status, 32)) { failed = true; break; }
+        flush();
+      }
       const int iq2 = P.q2_first + jbeg + jj;
       const int iq2m = mesh_neg(iq2, n0, n1, n2);
       const int iq3 = mesh_add(q1c, iq2, n0, n1, n2);
@@ -582,7 +634,7 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
         cp_async_wait_all();
       }
       tc::mbar_arrive(&stg[qd]);
-      if (!tc::mbar_wait(&stg[qd], jj & 1, P.status, 64)) { *abort_flag = 1; break; }
+      if (!tc::mbar_wait(&stg[qd], jj & 1, P.status, 64)) { failed = true; break; }
       const unsigned gp2 = u2[kU2Chunks - 1].x;
       const unsigned gp3 = srow[kChGp * kM].x;
       const bool deg2 = gp2 != kIdentityBlocks, deg3 = gp3 != kIdentityBlocks;
@@ -616,16 +668,18 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
         }
       }
       tc::mbar_arrive(&lvb[qd]);
-      if (!tc::mbar_wait(&lvb[qd], jj & 1, P.status, 128)) { *abort_flag = 1; break; }
+      if (!tc::mbar_wait(&lvb[qd], jj & 1, P.status, 128)) { failed = true; break; }
       // ---- the three parts
-      bool stop = false;
 #pragma unroll 1
       for (int h = 0; h < kParts; ++h) {
-        if (!tc::mbar_wait(&accf[h], jj & 1, P.status, 16)) { stop = true; break; }
+        if (!tc::mbar_wait(&accf[h], jj & 1, P.status, 16)) { failed = true; break; }
         tc::tc_fence_after();
 #pragma unroll 1
         for (int bl = 0; bl < 2; ++bl) {
           const int b2 = 2 * h + bl;
+          const int r0 = (k + 6 - b2 % 3) % 3;       // owned b1 = r0, r0 + 3
+          const unsigned bmO0 = deg1 ? blk_mask(gp1, r0) : (1u << r0);
+          const unsigned bmO1 = deg1 ? blk_mask(gp1, r0 + 3) : (1u << (r0 + 3));
           // b3 masks of the owned b1 (expanded over the blocks of b2 and b3)
           unsigned long long nsrc = S.need[b2 * kM + m];
           const unsigned bm2 = deg2 ? blk_mask(gp2, b2) : (1u << b2);
@@ -633,8 +687,8 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
             for (int b = 0; b < 6; ++b)
               if (b != b2 && ((bm2 >> b) & 1u)) nsrc |= S.need[b * kM + m];
           }
-          unsigned nO0 = (unsigned)(nsrc >> (6 * k)) & 63u;
-          unsigned nO1 = (unsigned)(nsrc >> (6 * (k + 3))) & 63u;
+          unsigned nO0 = (unsigned)(nsrc >> (6 * r0)) & 63u;
+          unsigned nO1 = (unsigned)(nsrc >> (6 * (r0 + 3))) & 63u;
           if (deg3) {
             if (nO0) nO0 = expand_b3(nO0, gp3);
             if (nO1) nO1 = expand_b3(nO1, gp3);
@@ -672,37 +726,28 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
                 cfmacf(v, Y[c], make_float2(__uint_as_float(e.x), __uint_as_float(e.y)));
               }
               const float w = fmaf(v.x, v.x, v.y * v.y);
-              if (!((cols >> b3) & 1u)) continue;
-              const Band x2 = load_band<NT>(u2 + 3 * b2, 1);
-              const Band x2m = load_band<NT>(u2 + kU2Chunks + 3 * b2, 1);
-              const Band x3 = load_band<NT>(srow + (kChBand + 3 * b3) * kM, kM);
-              Sig gp, gm;
-              if (smearing == PHX_SMEAR_ADAPTIVE) {
-                gp = sigma_ad(x2.P, x3.P);
-                gm = sigma_ad(x2m.P, x3.P);
-              }
-              const bool avg = deg2 || deg3;
-              const unsigned bm3 = avg ? blk_mask(gp3, b3) : 0u;
-#pragma unroll 1
+              // queue the live triplets of the owned b1 (block-averaged when degenerate)
+              const bool blk23 = (bm2 != (1u << b2)) || (deg3 && blk_mask(gp3, b3) != (1u << b3));
+              const unsigned meta =
+                  (unsigned)lane | ((unsigned)b2 << 8) | ((unsigned)b3 << 11) | (blk23 ? (1u << 14) : 0u);
+#pragma unroll
               for (int o = 0; o < 2; ++o) {
-                const int b1 = k + 3 * o;
                 const unsigned no = o ? nO1 : nO0, bmo = o ? bmO1 : bmO0;
-                if (!((no >> b3) & 1u) || !((bmo >> row) & 1u)) continue;
-                const double E1 = S.En1[b1 * kM + m];
-                const float iE1 = S.iE1[b1 * kM + m];
-                float n1v[NT];
-#pragma unroll
-                for (int t = 0; t < NT; ++t) n1v[t] = S.N1[(t * 6 + b1) * kM + m];
-                float f[NT];
-                if (!avg) rate_f<NT>(smearing, ginv, pre, E1, iE1, n1v, x2, x2m, x3, gp, gm, f);
-                else rate_avg<NT>(smearing, ginv, pre, E1, iE1, n1v, u2, srow, bm2, bm3, f);
-                const float wn = w / (float)__popc(bmo);
-                if (o == 0) {
-#pragma unroll
-                  for (int t = 0; t < NT; ++t) acc0[t] += (double)(wn * f[t]);
-                } else {
-#pragma unroll
-                  for (int t = 0; t < NT; ++t) acc1[t] += (double)(wn * f[t]);
+                const bool live = ((no >> b3) & 1u) && ((bmo >> row) & 1u);
+                const unsigned bal = __ballot_sync(FULL, live);
+                if (!bal) continue;
+                if (live)
+                  queue[qn + __popc(bal & lanemask_lt)] =
+                      make_uint2(__float_as_uint(w / (float)__popc(bmo)), meta | ((unsigned)(r0 + 3 * o) << 5));
+                qn += __popc(bal);
+                if (qn >= 32) {
+                  __syncwarp();
+                  rate_entry<NT>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc);
+                  const uint2 rest = lane + 32 < qn ? queue[lane + 32] : make_uint2(0u, 0u);
+                  __syncwarp();
+                  if (lane + 32 < qn) queue[lane] = rest;
+                  qn -= 32;
+                  __syncwarp();
                 }
               }
             }
@@ -712,10 +757,20 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&acce[h]);
       }
-      if (stop) { *abort_flag = 1; break; }
-      tc::mbar_arrive(&rel[qd]);  // done with this q2's staged records
+      if (failed) break;
+      if (qn) {
+        __syncwarp();
+        if (lane < qn)
+          rate_entry<NT>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc);
+        qn = 0;
+      }
+      __syncwarp();
+      tc::mbar_arrive(&rel[qd]);  // done with this q2's staged records and accumulators
       if (*abort_flag) break;
     }
+    if (failed) *abort_flag = 1;
+    // the last q2 of the quarter
+    if (!failed && nj > 0 && tc::mbar_wait(&rel[qd], (nj - 1) & 1, P.status, 32)) flush();
     if (valid) {
       double* out = P.partial + ((size_t)blockIdx.y * nq + q1c) * 6 * NT;
 #pragma unroll
@@ -812,7 +867,7 @@ __global__ void __launch_bounds__(128, 1) diag_gemm_kernel(int N, int Kp, const 
 }
 
 size_t pair_tc_smem(int Kp) {
-  size_t off[10];
+  size_t off[12];
   return smem_layout(Kp, off) + 1024;
 }
 

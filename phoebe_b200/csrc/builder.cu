@@ -108,6 +108,91 @@ __global__ void fold_q2_kernel(int nb, int nr2, int nr3, const double* __restric
   }
 }
 
+// Same Dp, one block per (r3, 8 consecutive q2): every thread accumulates one
+// (a,b,c) of the R2 transform for the 8 q2 at once (the D3w element is read
+// once for 8 phases), then the e2 contraction runs from shared memory.  The
+// sums run in the same order as fold_q2_kernel (r2 ascending, then b), so the
+// results are identical.  nb <= 8.
+constexpr int kFoldQ = 8;
+__global__ void __launch_bounds__(256) fold_q2_tiled_kernel(int nb, int nr2, int nr3, const double* __restrict__ D3w,
+                                                            const double* __restrict__ R2, const double* __restrict__ R3,
+                                                            const double* __restrict__ qcart, const double2* __restrict__ U,
+                                                            int q2_first, int q2_count, double2* __restrict__ Dp) {
+  extern __shared__ __align__(16) char sraw[];
+  const int nbb = nb * nb, nb3 = nbb * nb;
+  double2* ph2 = reinterpret_cast<double2*>(sraw);   // [kFoldQ][nr2]
+  double2* e2 = ph2 + kFoldQ * nr2;                  // [kFoldQ][nbb]
+  double2* Y = e2 + kFoldQ * nbb;                    // [kFoldQ][nb3]
+  double2* p3 = Y + kFoldQ * nb3;                    // [kFoldQ]
+  const int r3 = blockIdx.x;
+  const int j0 = blockIdx.y * kFoldQ;
+  const int nj = min(kFoldQ, q2_count - j0);
+  for (int e = threadIdx.x; e < kFoldQ * nr2; e += blockDim.x) {
+    const int jl = e / nr2, r = e % nr2;
+    double2 v = cmk(0.0, 0.0);
+    if (jl < nj) {
+      const double* q = qcart + 3 * (q2_first + j0 + jl);
+      double sn, cs;
+      sincos(q[0] * R2[3 * r] + q[1] * R2[3 * r + 1] + q[2] * R2[3 * r + 2], &sn, &cs);
+      v = cmk(cs, sn);
+    }
+    ph2[e] = v;
+  }
+  for (int e = threadIdx.x; e < kFoldQ * nbb; e += blockDim.x) {
+    const int jl = e / nbb;
+    e2[e] = jl < nj ? U[(size_t)(q2_first + j0 + jl) * nbb + e % nbb] : cmk(0.0, 0.0);
+  }
+  if (threadIdx.x < kFoldQ) {
+    double2 v = cmk(0.0, 0.0);
+    if ((int)threadIdx.x < nj) {
+      const double* q = qcart + 3 * (q2_first + j0 + threadIdx.x);
+      double sn3, cs3;
+      sincos(-(q[0] * R3[3 * r3] + q[1] * R3[3 * r3 + 1] + q[2] * R3[3 * r3 + 2]), &sn3, &cs3);
+      v = cmk(cs3, sn3);
+    }
+    p3[threadIdx.x] = v;
+  }
+  __syncthreads();
+  const double* d0 = D3w + (size_t)r3 * nr2 * nb3;
+  for (int abc = threadIdx.x; abc < nb3; abc += blockDim.x) {
+    double2 acc[kFoldQ];
+#pragma unroll
+    for (int jl = 0; jl < kFoldQ; ++jl) acc[jl] = cmk(0.0, 0.0);
+    for (int r = 0; r < nr2; ++r) {
+      const double x = __ldg(d0 + (size_t)r * nb3 + abc);
+#pragma unroll
+      for (int jl = 0; jl < kFoldQ; ++jl) {
+        const double2 p = ph2[jl * nr2 + r];
+        acc[jl].x = fma(x, p.x, acc[jl].x);
+        acc[jl].y = fma(x, p.y, acc[jl].y);
+      }
+    }
+#pragma unroll
+    for (int jl = 0; jl < kFoldQ; ++jl) Y[jl * nb3 + abc] = acc[jl];
+  }
+  __syncthreads();
+  // Dp[j][r3][a][b2][c] = p3 * sum_b e2(b,b2) Y(a,b,c)
+  for (int e = threadIdx.x; e < nj * nb3; e += blockDim.x) {
+    const int jl = e / nb3, rest = e % nb3;
+    const int a = rest / nbb, b2 = (rest / nb) % nb, c = rest % nb;
+    const double2* y = Y + jl * nb3 + a * nbb + c;
+    const double2* u = e2 + jl * nbb + b2;
+    double2 z = cmk(0.0, 0.0);
+    for (int b = 0; b < nb; ++b) cfma(z, u[b * nb], y[b * nb]);
+    Dp[(((size_t)(j0 + jl) * nr3 + r3) * nb + a) * nbb + b2 * nb + c] = cmul(z, p3[jl]);
+  }
+}
+
+size_t fold_tiled_smem(int nb, int nr2) {
+  return sizeof(double2) * ((size_t)kFoldQ * (nr2 + nb * nb + nb * nb * nb) + kFoldQ);
+}
+void fold_tiled_launch(int nb, int nr2, int nr3, const phx_v3* v, const phx_bands* b, int c0, int cnt,
+                       double2* Dp, cudaStream_t st) {
+  dim3 gf(nr3, (cnt + kFoldQ - 1) / kFoldQ);
+  fold_q2_tiled_kernel<<<gf, 256, fold_tiled_smem(nb, nr2), st>>>(nb, nr2, nr3, v->d_D3w, v->d_R2, v->d_R3, b->d_q,
+                                                                  reinterpret_cast<const double2*>(b->d_U), c0, cnt, Dp);
+}
+
 struct PairArgs {
   MeshArgs m;
   int nr3;
@@ -640,17 +725,17 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
     PHX_CUDA(ctx, cudaFuncSetAttribute(pair_fp64_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem_pair));
   }
-  const size_t smem_fold = sizeof(double2) * (nr2 + 2 * NB * NB);
+  const size_t smem_fold = fold_tiled_smem(NB, nr2);
+  PHX_ARG(ctx, smem_fold <= 227 * 1024, "phx_ph_linewidths: too many R2 vectors");
+  if (smem_fold > 48 * 1024)
+    PHX_CUDA(ctx, cudaFuncSetAttribute(fold_q2_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_fold));
   const int tiles = (nq + kTile - 1) / kTile;
   if (split) PHX_TRY(phx_split_pack_records(ctx, P.m, rec, &launches));
   PHX_CUDA(ctx, cudaEventRecord(evv0, st));
   for (int c0 = q2b; c0 < q2e; c0 += plan.chunk) {
     const int cnt = std::min(plan.chunk, q2e - c0);
-    const int per_block = 8;
-    dim3 gf(nr3, (cnt + per_block - 1) / per_block);
-    fold_q2_kernel<<<gf, 128, smem_fold, st>>>(NB, nr2, nr3, v->d_D3w, v->d_R2, v->d_R3, b->d_q,
-                                               reinterpret_cast<const double2*>(b->d_U), c0, cnt,
-                                               per_block, Dp);
+    fold_tiled_launch(NB, nr2, nr3, v, b, c0, cnt, Dp, st);
     ++launches;
     if (split) {
       PHX_TRY(phx_split_pair_chunk(ctx, P.m, v, b, Dp, Bimg, rec, emax, c0, cnt, plan.slots, partial,

@@ -30,6 +30,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 TEMPS_K = (100.0, 300.0, 600.0)
+# FP32 FFMA throughput of a B200 (packed and scalar FFMA stream, all SMs, CUDA
+# events), the denominator of the pair kernel's CUDA-core view
+FFMA_PEAK_TFLOPS = 72.0
+# ncu DRAM bytes (read + write) of one pair-kernel launch (448 q2) per mesh;
+# None where not captured
+PAIR_TRAFFIC_BYTES = {20: 87476992 + 5594112, 16: 85.2e6}
 
 
 def parse():
@@ -230,6 +236,8 @@ def run_ours(args):
     barrier()
     dev_ms = []
     vertex_ms = []
+    pair_ms = []
+    pair_launches = 0
     launches = 0
     with Clocks(local) as clk:
         t0 = time.perf_counter()
@@ -239,6 +247,8 @@ def run_ours(args):
             st = step()
             dev_ms.append(st.ms_total)
             vertex_ms.append(st.ms_vertex)
+            pair_ms.append(st.ms_pair)
+            pair_launches += st.pair_launches
             launches += st.kernel_launches
         barrier()
         wall = time.perf_counter() - t0
@@ -277,9 +287,10 @@ def run_ours(args):
             e2e_times.append(dt)
     e2e_value = pairs_step / float(np.median(e2e_times)) if e2e_times else None
 
-    # roofline of the dominant kernel (fused pair kernel), device-timed
+    # roofline of the dominant kernel (fused pair kernel): algorithmic FLOPs of
+    # all its launches / their CUDA-event time (events around each launch)
     fl = flops_per_pair(nb, nr3)
-    achieved = fl * (q2e - q2b) * nq / (float(np.mean(vertex_ms)) / 1000.0) / 1e12
+    achieved = fl * (q2e - q2b) * nq * args.steps / (float(np.sum(pair_ms)) / 1000.0) / 1e12
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -292,9 +303,19 @@ def run_ours(args):
                         "FP64 peak available)"}
     else:
         pk = peaks.get("bf16_tflops_sustained", 1394.6)
+        # DRAM bytes per launch of the pair kernel, ncu dram__bytes_read.sum +
+        # dram__bytes_write.sum of one 20^3 launch (448 q2 x 8000 q1)
         roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
-                "frac": achieved / pk, "traffic": None, "peak_source": "measured (sustained)"}
+                "frac": achieved / pk, "traffic": PAIR_TRAFFIC_BYTES.get(args.mesh),
+                "peak_source": "measured (sustained)",
+                "simt_view": {"what": "FP32 epilogue (e1, e3 contractions of all 216 triplets) "
+                                      "against the measured FFMA rate",
+                              "flops_per_pair": 16 * nb ** 4,
+                              "achieved": 16 * nb ** 4 * achieved / fl, "peak": FFMA_PEAK_TFLOPS,
+                              "frac": 16 * nb ** 4 * achieved / fl / FFMA_PEAK_TFLOPS}}
     roof["flops_per_pair"] = fl
+    roof["pair_launches"] = pair_launches
+    roof["ms_per_pair_launch"] = float(np.sum(pair_ms)) / max(1, pair_launches)
     roof["flops_per_pair_reference_formulation"] = flops_per_pair_reference(nb, nr3)
 
     out = None

@@ -142,9 +142,11 @@ typedef struct phx_lw_params {
 
 typedef struct phx_lw_stats {
   double ms_total;            /* device time of the whole call */
-  double ms_vertex;           /* device time of the fused pair kernels */
+  double ms_vertex;           /* device time of the q2 loop (R2 fold, conversions, pair kernels) */
   long long pairs;            /* (q1,q2) pairs processed */
   int kernel_launches;        /* kernels launched by the call */
+  int pair_launches;          /* launches of the fused pair kernel */
+  double ms_pair;             /* device time of those launches alone (CUDA events) */
 } phx_lw_stats;
 
 /* Whole PhScatteringMatrix::builder, switchCase 2 (linewidths), on the GPU:

@@ -39,7 +39,8 @@ class LwParams(ctypes.Structure):
 
 class LwStats(ctypes.Structure):
     _fields_ = [("ms_total", ctypes.c_double), ("ms_vertex", ctypes.c_double),
-                ("pairs", ctypes.c_longlong), ("kernel_launches", ctypes.c_int)]
+                ("pairs", ctypes.c_longlong), ("kernel_launches", ctypes.c_int),
+                ("pair_launches", ctypes.c_int), ("ms_pair", ctypes.c_double)]
 
 
 # name -> argtypes (all return int unless listed in _RESTYPE)

@@ -504,7 +504,8 @@ size_t phx_split_rec_bytes(int nq);
 int phx_split_pack_records(phx_ctx* ctx, const pairc::MeshArgs& M, void* rec, int* launches);
 int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v, const phx_bands* b,
                          const double2* Dp, uint8_t* Bimg, const void* rec, double emax, int q2_first,
-                         int q2_count, int slots, double* partial, int* launches);
+                         int q2_count, int slots, double* partial, int* launches, cudaEvent_t ev_begin,
+                         cudaEvent_t ev_end);
 
 int phx_scratch_reserve(phx_v3* v, size_t bytes) {
   if (v->scratch_bytes >= bytes) return PHX_OK;
@@ -691,6 +692,13 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   PHX_CUDA(ctx, cudaEventCreate(&evv0));
   PHX_CUDA(ctx, cudaEventCreate(&evv1));
   int launches = 0;
+  std::vector<cudaEvent_t> pair_events;  // (begin, end) of every pair-kernel launch, when stats are asked for
+  struct EventGuard {
+    std::vector<cudaEvent_t>& ev;
+    ~EventGuard() {
+      for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+  } pair_event_guard{pair_events};
   PHX_CUDA(ctx, cudaEventRecord(ev0, st));
   PHX_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
   PHX_CUDA(ctx, cudaMemcpyAsync(temps, p->temperatures, sizeof(double) * nT, cudaMemcpyHostToDevice, st));
@@ -738,15 +746,31 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
     fold_tiled_launch(NB, nr2, nr3, v, b, c0, cnt, Dp, st);
     ++launches;
     if (split) {
+      cudaEvent_t pe0 = nullptr, pe1 = nullptr;
+      if (stats) {
+        PHX_CUDA(ctx, cudaEventCreate(&pe0));
+        PHX_CUDA(ctx, cudaEventCreate(&pe1));
+        pair_events.push_back(pe0);
+        pair_events.push_back(pe1);
+      }
       PHX_TRY(phx_split_pair_chunk(ctx, P.m, v, b, Dp, Bimg, rec, emax, c0, cnt, plan.slots, partial,
-                                   &launches));
+                                   &launches, pe0, pe1));
       continue;
     }
     P.q2_first = c0;
     P.q2_count = cnt;
     P.q2_per_slot = (cnt + plan.slots - 1) / plan.slots;
     dim3 gp(tiles, plan.slots);
+    cudaEvent_t pe0 = nullptr, pe1 = nullptr;
+    if (stats) {
+      PHX_CUDA(ctx, cudaEventCreate(&pe0));
+      PHX_CUDA(ctx, cudaEventCreate(&pe1));
+      pair_events.push_back(pe0);
+      pair_events.push_back(pe1);
+      PHX_CUDA(ctx, cudaEventRecord(pe0, st));
+    }
     pair_fp64_kernel<NB><<<gp, kTile * NB, smem_pair, st>>>(P);
+    if (stats) PHX_CUDA(ctx, cudaEventRecord(pe1, st));
     ++launches;
     PHX_CUDA(ctx, cudaGetLastError());
   }
@@ -773,6 +797,14 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
     stats->ms_vertex = msv;
     stats->pairs = (long long)nq * (q2e - q2b);
     stats->kernel_launches = launches;
+    stats->pair_launches = (int)(pair_events.size() / 2);
+    double msp = 0.0;
+    for (size_t i = 0; i + 1 < pair_events.size(); i += 2) {
+      float x = 0.f;
+      cudaEventElapsedTime(&x, pair_events[i], pair_events[i + 1]);
+      msp += x;
+    }
+    stats->ms_pair = msp;
   }
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);

@@ -928,7 +928,8 @@ int phx_split_pack_records(phx_ctx* ctx, const pairc::MeshArgs& M, void* rec, in
 // fused tensor-core pair kernel over (q1 tiles) x (q2 slots).
 int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v, const phx_bands* b,
                          const double2* Dp, uint8_t* Bimg, const void* rec, double emax, int q2_first,
-                         int q2_count, int slots, double* partial, int* launches) {
+                         int q2_count, int slots, double* partial, int* launches, cudaEvent_t ev_begin,
+                         cudaEvent_t ev_end) {
   const int Kp = phx_split_kp(v->nr3);
   const int nkc = Kp / kKC;
   convert_b_kernel<<<dim3(q2_count, kParts * nkc), 256, 0, ctx->stream>>>(Dp, v->nr3, Kp, q2_count, Bimg);
@@ -951,6 +952,7 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
   A.status = ctx->d_status;
   const int tiles = (M.nq + kM - 1) / kM;
   int rc = PHX_OK;
+  if (ev_begin) PHX_CUDA(ctx, cudaEventRecord(ev_begin, ctx->stream));
   switch (M.nT) {
     case 1: rc = launch_pair<1>(ctx, A, tiles, slots); break;
     case 2: rc = launch_pair<2>(ctx, A, tiles, slots); break;
@@ -958,6 +960,7 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
     default: rc = launch_pair<4>(ctx, A, tiles, slots); break;
   }
   if (rc != PHX_OK) return rc;
+  if (ev_end) PHX_CUDA(ctx, cudaEventRecord(ev_end, ctx->stream));
   *launches += 2;
   return PHX_OK;
 }

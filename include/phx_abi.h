@@ -43,6 +43,8 @@ typedef struct phx_ctx phx_ctx;
 typedef struct phx_ph_h0 phx_ph_h0;
 typedef struct phx_bands phx_bands;
 typedef struct phx_v3 phx_v3;
+typedef struct phx_el_h0 phx_el_h0;
+typedef struct phx_elph phx_elph;
 
 /* ---- context ---------------------------------------------------------- */
 /* Replaces initKokkos / DeviceManager (src/common_kokkos.cpp:104-134,182-190). */
@@ -187,6 +189,70 @@ int phx_ph_linewidths_static(phx_v3* v3, phx_bands* bands, const phx_lw_params* 
  * src/bte/scattering.cpp:484-527; src/observable/phonon_thermal_cond.cpp:64-113). */
 int phx_ph_rta_kappa(phx_bands* bands, int nT, const double* temperatures,
                      const double* A_out, double volume, double* kappa);
+
+/* ---- electronic Wannier Hamiltonian (ElectronH0Wannier) ----------------- */
+/* Build from the Wannier Hamiltonian H(R) (nR,nw,nw) complex (Ry) on the
+ * Bravais vectors R (nR,3) Bohr with degeneracies deg (nR); cell as in
+ * phx_ph_h0_create.  Replaces the ElectronH0Wannier constructor without
+ * shifted vectors (src/harmonic/electron_h0_wannier.cpp:6-60). */
+int phx_el_h0_create(phx_ctx* ctx, int nw, int nR, const double* cell, const double* R,
+                     const double* deg, const double* H, phx_el_h0** out);
+int phx_el_h0_destroy(phx_el_h0* h);
+int phx_el_h0_num_bands(const phx_el_h0* h);
+/* H(k) = sum_R e^{+i k.R}/deg_R H(R), ascending energies E (nk,nw), eigenvectors
+ * U (nk,nw,nw) complex with U[w][b] = component w of band b, and, when vg is
+ * not NULL, group velocities (nk,nw,3) of the Hellmann-Feynman operator with
+ * degenerate subspaces (1 micro-eV) rediagonalised and zero at Gamma.
+ * Replaces batchedDiagonalizeFromCoordinates / batchedDiagonalizeWithVelocities
+ * (src/harmonic/electron_h0_wannier.cpp:160-235,633-760; Kokkos :777-999). */
+int phx_el_diag(phx_el_h0* h, int nk, const double* k, double* E, double* U, double* vg);
+/* Device band structure of a Gamma-centred k mesh (ElectronH0Wannier::populate,
+ * src/harmonic/electron_h0_wannier.h:91-114). */
+int phx_el_bands_create_mesh(phx_el_h0* h, const int* mesh, int with_velocities, phx_bands** out);
+
+/* ---- electron-phonon coupling (InteractionElPhWan) ---------------------- */
+/* Upload the Wannier-basis coupling g(Re, Rp, nu, w1, w2), complex FP32
+ * (nRe,nRp,nph,nw,nw), with the electronic and phononic Bravais vectors (Bohr)
+ * and their degeneracies.  Replaces the InteractionElPhWan constructor
+ * (src/interaction/interaction_elph.h:89-120; layout of :45-47). */
+int phx_elph_create(phx_ctx* ctx, int nw, int nph, int nRe, int nRp, const double* Re,
+                    const double* degE, const double* Rp, const double* degP, const float* g,
+                    phx_elph** out);
+int phx_elph_destroy(phx_elph* e);
+/* cacheElPh (src/interaction/interaction_elph.cpp:492-701): transform over Re
+ * at k1 (e^{+i k1.Re}/deg) and rotate by the k1 eigenvectors U1 (nw,nb1)
+ * complex; the result stays on the device for phx_elph_couplings_sq. */
+int phx_elph_cache_k1(phx_elph* e, const double* k1, const double* U1, int nb1);
+/* calcCouplingSquared + getCouplingSquared (src/interaction/interaction_elph.cpp:229-448,
+ * no polar correction): for nk2 final states with phonon wavevectors q3 (nk2,3),
+ * electron eigenvectors U2s (nk2,nw,nb2max) complex (first nb2s[i] columns used)
+ * and phonon eigenvectors ev3s (nk2,nph,nph) complex U[a][nu], writes
+ * coupling (nk2,nb1,nb2max,nph) = |g(b1,b2,nu)|^2 (zero beyond nb2s[i]). */
+int phx_elph_couplings_sq(phx_elph* e, int nk2, const double* q3, const double* U2s, const int* nb2s,
+                          int nb2max, const double* ev3s, double* coupling);
+
+typedef struct phx_el_params {
+  int num_temperatures;       /* <= 4 */
+  const double* temperatures; /* Ry */
+  double chemical_potential;  /* Ry */
+  double window;              /* half width (Ry) of the active window around mu */
+  int smearing;               /* PHX_SMEAR_GAUSSIAN / PHX_SMEAR_ADAPTIVE */
+  double sigma;               /* Gaussian width (Ry) */
+  double norm;                /* prefactor of every rate (1/N of the summed q mesh) */
+  int num_k1;                 /* outer k points */
+  const int* k1_list;         /* their k-mesh indices (host) */
+} phx_el_params;
+
+/* ElScatteringMatrix::builder, linewidth mode (src/bte/el_scattering.cpp:38-405),
+ * for the outer k points k1_list of the electron mesh el_bands, every q of the
+ * phonon mesh ph_bands (the q mesh must divide the k mesh) and k2 = k1 + q:
+ * states outside |E - mu| <= window are inactive; rates
+ * |g|^2 ((f2 + n3) d(E1-E2+w3) + (1 - f2 + n3) d(E1-E2-w3)) norm pi / w3 with
+ * w3 >= 5 cm^-1, |g|^2 symmetrised over degenerate blocks, then degeneracy
+ * averaging of temperature row 0.  out (nT, num_k1, nw) host, zero for
+ * inactive states.  stats may be NULL. */
+int phx_el_linewidths(phx_elph* e, phx_bands* el_bands, phx_bands* ph_bands,
+                      const phx_el_params* params, double* out, phx_lw_stats* stats);
 
 /* ---- diagnostics -------------------------------------------------------- */
 /* Self-test of the split-precision tensor-core GEMM used by the builder: one

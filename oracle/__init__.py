@@ -51,6 +51,19 @@ def lib():
                                         ctypes.c_int, _I, ctypes.c_int, _D]
         L.orc_rta_kappa.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, ctypes.c_long,
                                     ctypes.c_double, _D]
+        L.orc_el_diag.restype = ctypes.c_int
+        L.orc_el_diag.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, ctypes.c_int, _D, _D, _D, _D]
+        _F = ctypes.POINTER(ctypes.c_float)
+        L.orc_elph_cache.restype = ctypes.c_int
+        L.orc_elph_cache.argtypes = [ctypes.c_int] * 4 + [_D, _D, _F, _D, _D, ctypes.c_int, _D]
+        L.orc_elph_couplings.restype = ctypes.c_int
+        L.orc_elph_couplings.argtypes = [ctypes.c_int] * 3 + [_D, _D, _D, ctypes.c_int, ctypes.c_int, _D, _D,
+                                                               _I, ctypes.c_int, _D, _D]
+        L.orc_el_linewidths.restype = ctypes.c_int
+        L.orc_el_linewidths.argtypes = ([ctypes.c_int] * 4 + [_D, _D, _D, _D, _F, _I, _I, _D, _D, _D, _I, _I,
+                                                              _D, _D, _D, _D, ctypes.c_int, _I, ctypes.c_int,
+                                                              _D, ctypes.c_double, ctypes.c_int,
+                                                              ctypes.c_double, ctypes.c_double, _D])
         _lib = L
     return _lib
 
@@ -194,3 +207,84 @@ def rta_kappa(E, vg, Aout, temps_ry, nqmesh, volume):
     lib().orc_rta_kappa(ns, len(T), _p(T), _p(_d(E)), _p(_d(vg)), _p(_d(Aout)), int(nqmesh),
                         float(volume), _p(kappa))
     return kappa
+
+
+def _ip(a):
+    return np.ascontiguousarray(a, dtype=np.int32).ctypes.data_as(_I)
+
+
+def _f32c(a):
+    """complex64 array -> contiguous interleaved float32."""
+    return np.ascontiguousarray(a, dtype=np.complex64).view(np.float32)
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class ElectronH0Wannier:
+    """CPU FP64 restatement of ElectronH0Wannier (no shifted vectors)."""
+
+    def __init__(self, R, deg, H):
+        self.R, self.deg = _d(R), _d(deg)
+        self.H = _c(H)
+        self.nR, self.nw = H.shape[0], H.shape[1]
+
+    def diagonalize(self, k_cart, velocities=False):
+        k = _d(np.atleast_2d(k_cart))
+        nk = k.shape[0]
+        E = np.zeros((nk, self.nw))
+        U = np.zeros((nk, self.nw, self.nw, 2))
+        vg = np.zeros((nk, self.nw, 3)) if velocities else None
+        rc = lib().orc_el_diag(self.nw, self.nR, _p(self.R), _p(self.deg), _p(self.H), nk, _p(k), _p(E),
+                               _p(U), _p(vg) if velocities else None)
+        assert rc == 0
+        U = U[..., 0] + 1j * U[..., 1]
+        return (E, U, vg) if velocities else (E, U)
+
+
+class InteractionElPhWan:
+    """CPU FP64 restatement of InteractionElPhWan (cacheElPh, calcCouplingSquared)."""
+
+    def __init__(self, Re, degE, Rp, degP, g):
+        self.Re, self.degE, self.Rp, self.degP = _d(Re), _d(degE), _d(Rp), _d(degP)
+        self.g = _f32c(g)
+        self.nRe, self.nRp, self.nph, self.nw = g.shape[0], g.shape[1], g.shape[2], g.shape[3]
+
+    def cache_elph(self, U1, k1):
+        U1 = np.asarray(U1)
+        nb1 = U1.shape[1]
+        out = np.zeros((self.nRp, self.nph, nb1, self.nw, 2))
+        lib().orc_elph_cache(self.nw, self.nph, self.nRe, self.nRp, _p(self.Re), _p(self.degE), _fp(self.g),
+                             _p(_d(k1)), _p(_c(U1)), nb1, _p(out))
+        self.cached = out
+        self.nb1 = nb1
+        return out[..., 0] + 1j * out[..., 1]
+
+    def calc_coupling_squared(self, U2s, nb2s, ev3s, q3s):
+        nk2 = len(nb2s)
+        nb2max = U2s.shape[2]
+        out = np.zeros((nk2, self.nb1, nb2max, self.nph))
+        lib().orc_elph_couplings(self.nw, self.nph, self.nRp, _p(self.Rp), _p(self.degP), _p(self.cached),
+                                 self.nb1, nk2, _p(_d(q3s)), _p(_c(U2s)), _ip(nb2s),
+                                 nb2max, _p(_c(ev3s)), _p(out))
+        return out
+
+
+def el_linewidths(elph, kmesh, qmesh, Ek, Uk, vk, lo, hi, Eq, evq, kcart, recipk, k1list, temps_ry, mu,
+                  smearing, sigma, norm):
+    """ElScatteringMatrix::builder (linewidth mode): returns (nT, nk1, nw)."""
+    nk1 = len(k1list)
+    nT = len(temps_ry)
+    out = np.zeros((nT, nk1, elph.nw))
+    vk_ = _d(vk) if vk is not None else _d(np.zeros((Ek.shape[0], Ek.shape[1], 3)))
+    rc = lib().orc_el_linewidths(elph.nw, elph.nph, elph.nRe, elph.nRp, _p(elph.Re), _p(elph.degE), _p(elph.Rp),
+                                 _p(elph.degP), _fp(elph.g), _ip(kmesh),
+                                 _ip(qmesh), _p(_d(Ek)), _p(_c(Uk)),
+                                 _p(vk_), _ip(lo),
+                                 _ip(hi), _p(_d(Eq)), _p(_c(evq)),
+                                 _p(_d(kcart)), _p(_d(recipk)), nk1, _ip(k1list),
+                                 nT, _p(_d(temps_ry)), float(mu), 1 if smearing == "adaptive" else 0,
+                                 float(sigma), float(norm), _p(out))
+    assert rc == 0
+    return out

@@ -43,6 +43,13 @@ class LwStats(ctypes.Structure):
                 ("pair_launches", ctypes.c_int), ("ms_pair", ctypes.c_double)]
 
 
+class ElParams(ctypes.Structure):
+    _fields_ = [("num_temperatures", ctypes.c_int), ("temperatures", ctypes.POINTER(ctypes.c_double)),
+                ("chemical_potential", ctypes.c_double), ("window", ctypes.c_double),
+                ("smearing", ctypes.c_int), ("sigma", ctypes.c_double), ("norm", ctypes.c_double),
+                ("num_k1", ctypes.c_int), ("k1_list", ctypes.POINTER(ctypes.c_int))]
+
+
 # name -> argtypes (all return int unless listed in _RESTYPE)
 SIGNATURES = {
     "phx_ctx_create": [_i, ctypes.POINTER(_VP)],
@@ -71,6 +78,17 @@ SIGNATURES = {
     "phx_ph_linewidths_d": [_VP, _VP, ctypes.POINTER(LwParams), _VP, ctypes.POINTER(LwStats)],
     "phx_ph_rta_kappa": [_VP, _i, _D, _D, ctypes.c_double, _D],
     "phx_ph_linewidths_static": [_VP, _VP, ctypes.POINTER(LwParams), _VP],
+    "phx_el_h0_create": [_VP, _i, _i, _D, _D, _D, _D, ctypes.POINTER(_VP)],
+    "phx_el_h0_destroy": [_VP],
+    "phx_el_h0_num_bands": [_VP],
+    "phx_el_diag": [_VP, _i, _D, _D, _D, _D],
+    "phx_el_bands_create_mesh": [_VP, _I, _i, ctypes.POINTER(_VP)],
+    "phx_elph_create": [_VP, _i, _i, _i, _i, _D, _D, _D, _D, ctypes.POINTER(ctypes.c_float),
+                        ctypes.POINTER(_VP)],
+    "phx_elph_destroy": [_VP],
+    "phx_elph_cache_k1": [_VP, _D, _D, _i],
+    "phx_elph_couplings_sq": [_VP, _i, _D, _D, _I, _i, _D, _D],
+    "phx_el_linewidths": [_VP, _VP, _VP, ctypes.POINTER(ElParams), _D, ctypes.POINTER(LwStats)],
     "phx_diag_tc_gemm": [_VP, _i, _i, ctypes.POINTER(ctypes.c_float),
                          ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)],
 }

@@ -312,3 +312,148 @@ class PhScatteringMatrix:
                                            dptr(self.temperatures), dptr(A), float(volume),
                                            dptr(kappa)), self.v3.ctx.h)
         return kappa * C.thConductivityAuToSi
+
+
+# ---------------------------------------------------------------------------
+# electron-phonon Wannier path
+# ---------------------------------------------------------------------------
+
+class ElectronH0Wannier:
+    """Electronic Wannier Hamiltonian on the GPU (ElectronH0Wannier, no shifted vectors)."""
+
+    def __init__(self, ctx, crystal, R, deg, H):
+        L = _abi.load()
+        self.ctx = ctx
+        self.crystal = crystal
+        self.nw = int(H.shape[1])
+        h = ctypes.c_void_p()
+        cell, Rd, dd, Hd = f64(crystal.direct_cell), f64(R), f64(deg), c128(H)
+        check(L.phx_el_h0_create(ctx.h, self.nw, len(Rd), dptr(cell), dptr(Rd), dptr(dd), dptr(Hd),
+                                 ctypes.byref(h)), ctx.h)
+        self.h = h
+
+    def _diag(self, k_cart, velocities):
+        k = f64(np.atleast_2d(k_cart))
+        nk = k.shape[0]
+        E = np.zeros((nk, self.nw))
+        U = np.zeros((nk, self.nw, self.nw, 2))
+        vg = np.zeros((nk, self.nw, 3)) if velocities else None
+        check(_abi.load().phx_el_diag(self.h, nk, dptr(k), dptr(E), dptr(U),
+                                      dptr(vg) if velocities else None), self.ctx.h)
+        return E, U[..., 0] + 1j * U[..., 1], vg
+
+    def diagonalizeFromCoordinates(self, k_cart):
+        E, U, _ = self._diag(k_cart, False)
+        return E, U
+
+    def diagonalizeWithVelocities(self, k_cart):
+        return self._diag(k_cart, True)
+
+    def populate(self, mesh, withVelocities=True):
+        """Band structure on a full Gamma-centred k mesh, resident on the GPU."""
+        h = ctypes.c_void_p()
+        m = i32(mesh)
+        check(_abi.load().phx_el_bands_create_mesh(self.h, iptr(m), int(withVelocities), ctypes.byref(h)),
+              self.ctx.h)
+        return BandStructure(self.ctx, h, mesh, self.nw, self.crystal.reciprocal_cell)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _abi.load().phx_el_h0_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class InteractionElPhWan:
+    """Electron-phonon coupling in the Wannier basis on the GPU (InteractionElPhWan)."""
+
+    def __init__(self, ctx, Re, degE, Rp, degP, g):
+        L = _abi.load()
+        self.ctx = ctx
+        g = np.ascontiguousarray(g, dtype=np.complex64)
+        self.nRe, self.nRp, self.nph, self.nw = g.shape[0], g.shape[1], g.shape[2], g.shape[3]
+        gf = g.view(np.float32)
+        h = ctypes.c_void_p()
+        Re, degE, Rp, degP = f64(Re), f64(degE), f64(Rp), f64(degP)
+        check(L.phx_elph_create(ctx.h, self.nw, self.nph, self.nRe, self.nRp, dptr(Re), dptr(degE), dptr(Rp),
+                                dptr(degP), gf.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), ctypes.byref(h)),
+              ctx.h)
+        self.h = h
+        self.nb1 = 0
+
+    def cacheElPh(self, eigvec1, k1C):
+        """eigvec1: (nw, nb1) complex (columns = bands at k1)."""
+        U = c128(eigvec1)
+        self.nb1 = int(np.asarray(eigvec1).shape[1])
+        check(_abi.load().phx_elph_cache_k1(self.h, dptr(f64(k1C)), dptr(U), self.nb1), self.ctx.h)
+
+    def calcCouplingSquared(self, eigvecs2, eigvecs3, q3Cs):
+        """eigvecs2: list of (nw, nb2) complex; eigvecs3: list of (nph, nph); q3Cs: (nk2,3).
+        Returns the list of |g|^2 tensors (nb1, nb2, nph), as getCouplingSquared."""
+        nk2 = len(eigvecs2)
+        nb2s = i32([np.asarray(u).shape[1] for u in eigvecs2])
+        nb2max = int(nb2s.max()) if nk2 else 1
+        U2 = np.zeros((nk2, self.nw, nb2max), dtype=np.complex128)
+        for i, u in enumerate(eigvecs2):
+            U2[i, :, :u.shape[1]] = u
+        ev3 = np.ascontiguousarray(np.asarray(eigvecs3), dtype=np.complex128)
+        out = np.zeros((nk2, self.nb1, nb2max, self.nph))
+        check(_abi.load().phx_elph_couplings_sq(self.h, nk2, dptr(f64(q3Cs)), dptr(c128(U2)), iptr(nb2s), nb2max,
+                                                dptr(c128(ev3)), dptr(out)), self.ctx.h)
+        self.cacheCoupling = [out[i, :, :nb2s[i], :] for i in range(nk2)]
+        return self.cacheCoupling
+
+    def getCouplingSquared(self, ik2):
+        return self.cacheCoupling[ik2]
+
+    def close(self):
+        if getattr(self, "h", None):
+            _abi.load().phx_elph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ElScatteringMatrix:
+    """Electron-phonon linewidths (ElScatteringMatrix::builder, linewidth mode) on the GPU.
+
+    k2 = k1 + q runs over the q mesh of the phonon band structure (which must
+    divide the electron k mesh); norm defaults to 1/N_q."""
+
+    def __init__(self, elph, el_bands, ph_bands, temperatures_ry, chemical_potential, window, smearing="adaptive",
+                 sigma=0.0, norm=None):
+        self.elph, self.el, self.ph = elph, el_bands, ph_bands
+        self.temperatures = f64(np.atleast_1d(temperatures_ry))
+        self.mu, self.window = float(chemical_potential), float(window)
+        self.smearing, self.sigma = smearing, float(sigma)
+        self.norm = 1.0 / ph_bands.nq if norm is None else float(norm)
+
+    def setup(self, k1_list=None):
+        """Linewidths (nT, nk1, nw) of the outer k points (all k of the mesh by default)."""
+        k1 = i32(np.arange(self.el.nq) if k1_list is None else k1_list)
+        p = _abi.ElParams()
+        p.num_temperatures = len(self.temperatures)
+        p.temperatures = dptr(self.temperatures)
+        p.chemical_potential = self.mu
+        p.window = self.window
+        p.smearing = _abi.PHX_SMEAR_GAUSSIAN if self.smearing == "gaussian" else _abi.PHX_SMEAR_ADAPTIVE
+        p.sigma = self.sigma
+        p.norm = self.norm
+        p.num_k1 = len(k1)
+        p.k1_list = iptr(k1)
+        out = np.zeros((len(self.temperatures), len(k1), self.el.nb))
+        st = _abi.LwStats()
+        check(_abi.load().phx_el_linewidths(self.elph.h, self.el.h, self.ph.h, ctypes.byref(p), dptr(out),
+                                            ctypes.byref(st)), self.elph.ctx.h)
+        self.stats = st
+        self.linewidths = out
+        return out

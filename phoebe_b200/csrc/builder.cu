@@ -520,7 +520,7 @@ int phx_scratch_reserve(phx_v3* v, size_t bytes) {
 // ---------------------------------------------------------------------------
 // band structures on a mesh
 // ---------------------------------------------------------------------------
-static void mesh_cartesian(const int* mesh, const double* recip, std::vector<double>& q) {
+void phx_mesh_cartesian(const int* mesh, const double* recip, std::vector<double>& q) {
   const int nq = mesh[0] * mesh[1] * mesh[2];
   q.resize(3 * (size_t)nq);
   for (int i = 0; i < nq; ++i) {
@@ -547,7 +547,7 @@ extern "C" int phx_bands_create_mesh(phx_ph_h0* h0, const int* mesh, int with_ve
   for (int i = 0; i < 3; ++i) b->mesh[i] = mesh[i];
   for (int i = 0; i < 9; ++i) b->recip[i] = h0->recip[i];
   std::vector<double> q;
-  mesh_cartesian(mesh, h0->recip, q);
+  phx_mesh_cartesian(mesh, h0->recip, q);
   const size_t nq = b->nq, nb = b->nb;
   cudaError_t e = cudaMalloc(&b->d_E, sizeof(double) * nq * nb);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_U, sizeof(double) * 2 * nq * nb * nb);
@@ -582,7 +582,7 @@ extern "C" int phx_bands_create_from_host(phx_ctx* ctx, const int* mesh,
   for (int i = 0; i < 3; ++i) b->mesh[i] = mesh[i];
   for (int i = 0; i < 9; ++i) b->recip[i] = reciprocal_cell[i];
   std::vector<double> q;
-  mesh_cartesian(mesh, reciprocal_cell, q);
+  phx_mesh_cartesian(mesh, reciprocal_cell, q);
   const size_t nq = b->nq;
   cudaError_t e = cudaMalloc(&b->d_E, sizeof(double) * nq * nb);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_U, sizeof(double) * 2 * nq * nb * nb);

@@ -22,4 +22,6 @@ constexpr double phEnergyCutoff = 0.001 / ryToCmm1;
 constexpr double phExcludeCutoff = 0.1 / ryToCmm1;
 constexpr double velDegThreshold = 0.0001 / ryToCmm1;
 constexpr double degThreshold = 1.0e-6;
+// el_scattering.cpp:127
+constexpr double elPhononCutoff = 5.0 / ryToCmm1;
 }  // namespace phxc

@@ -97,6 +97,33 @@ struct phx_v3 {
 
 int phx_scratch_reserve(phx_v3* v3, size_t bytes);
 
+// Cartesian coordinates (n,3) of a Gamma-centred mesh (recip: columns = b vectors)
+void phx_mesh_cartesian(const int* mesh, const double* recip, std::vector<double>& q);
+
+struct phx_el_h0 {
+  phx_ctx* ctx = nullptr;
+  int nw = 0, nR = 0;
+  double cell[9];             // lattice vectors as columns
+  double recip[9];            // reciprocal vectors as columns
+  double* d_R = nullptr;      // (nR,3) Bravais vectors (Bohr)
+  double* d_deg = nullptr;    // (nR) degeneracies
+  double* d_H = nullptr;      // (nR,nw,nw) complex Wannier Hamiltonian (Ry)
+};
+
+struct phx_elph {
+  phx_ctx* ctx = nullptr;
+  int nw = 0, nph = 0, nRe = 0, nRp = 0;
+  double* d_Re = nullptr;     // (nRe,3)
+  double* d_degE = nullptr;   // (nRe)
+  double* d_Rp = nullptr;     // (nRp,3)
+  double* d_degP = nullptr;   // (nRp)
+  float* d_g = nullptr;       // (nRe,nRp,nph,nw,nw) complex FP32 coupling in the Wannier basis
+  double* d_cached = nullptr; // (nRp,nph,nw,nw) complex: cacheElPh of the last k1 (b1 < nb1)
+  int nb1 = 0;                // bands of the cached k1
+  void* d_scratch = nullptr;  // builder scratch (grown on demand)
+  size_t scratch_bytes = 0;
+};
+
 // kernels implemented in harmonic.cu, used by the ABI layer
 int phx_launch_ph_bands(phx_ph_h0* h0, int nq, const double* d_q, double* d_E, double* d_U,
                         double* d_vg, int mass_scaling);

@@ -320,3 +320,79 @@ def config0():
 def config1():
     """Diamond, 20^3 mesh, adaptive smearing, 100/300/600 K (headline case)."""
     return diamond_workload((20, 20, 20), "adaptive", (100.0, 300.0, 600.0))
+
+
+# ---------------------------------------------------------------------------
+# electron-phonon Wannier model (workload of the el-ph path)
+# ---------------------------------------------------------------------------
+
+@dataclass
+class ElPhModel:
+    crystal: Crystal
+    Re: np.ndarray      # (nRe,3) Bohr
+    degE: np.ndarray    # (nRe,)
+    H: np.ndarray       # (nRe,nw,nw) complex128, Ry; H(-R) = H(R)^dagger
+    Rp: np.ndarray      # (nRp,3) Bohr
+    degP: np.ndarray    # (nRp,)
+    g: np.ndarray       # (nRe,nRp,nph,nw,nw) complex64, Ry/Bohr
+
+
+def lattice_cube(crystal, n):
+    """The (2n+1)^3 lattice vectors i a1 + j a2 + k a3 with |i|,|j|,|k| <= n
+    (Cartesian, Bohr), each with degeneracy 1; index of -R is (count-1) - index of R."""
+    r = np.arange(-n, n + 1)
+    ijk = np.stack(np.meshgrid(r, r, r, indexing="ij"), -1).reshape(-1, 3)
+    R = ijk @ crystal.direct_cell.T
+    return R, np.ones(len(R))
+
+
+def wannier_hamiltonian(crystal, nw=8, ncell=3, seed=SEED_BASE + 3, amp_ev=2.0, decay_ang=3.0):
+    """H(R) = (X(R) + X(-R)^dagger)/2 with X complex N(0,1) amp exp(-|R|/decay):
+    Hermitian-consistent, so H(k) is Hermitian at every k."""
+    R, deg = lattice_cube(crystal, ncell)
+    nR = len(R)
+    rng = CounterRNG(seed)
+    x = rng.normal(0, 2 * nR * nw * nw).reshape(nR, nw, nw, 2)
+    X = x[..., 0] + 1j * x[..., 1]
+    dist = np.linalg.norm(R, axis=1) * C.distanceBohrToAng
+    X *= (amp_ev / C.energyRyToEv * np.exp(-dist / decay_ang))[:, None, None]
+    H = 0.5 * (X + np.conj(np.transpose(X[::-1], (0, 2, 1))))
+    return R, deg, H
+
+
+def elph_coupling(crystal, nRe_cell, nRp_cell, nph, nw, seed=SEED_BASE + 3, amp=0.1, decay_ang=4.0):
+    """g(Re,Rp,nu,w1,w2) complex64 N(0,1) amp eV/A exp(-(|Re|+|Rp|)/decay), in Ry/Bohr;
+    generated per Re (stream 1 + iRe of the counter RNG) to bound memory."""
+    Re, degE = lattice_cube(crystal, nRe_cell)
+    Rp, degP = lattice_cube(crystal, nRp_cell)
+    rng = CounterRNG(seed)
+    dE = np.linalg.norm(Re, axis=1) * C.distanceBohrToAng
+    dP = np.linalg.norm(Rp, axis=1) * C.distanceBohrToAng
+    unit = amp / C.energyRyToEv * C.distanceBohrToAng
+    per = len(Rp) * nph * nw * nw
+    g = np.empty((len(Re), len(Rp), nph, nw, nw), dtype=np.complex64)
+    for ie in range(len(Re)):
+        x = rng.normal(1 + ie, 2 * per).reshape(len(Rp), nph, nw, nw, 2)
+        scale = (unit * np.exp(-(dE[ie] + dP) / decay_ang))[:, None, None, None]
+        g[ie] = ((x[..., 0] + 1j * x[..., 1]) * scale).astype(np.complex64)
+    return Re, degE, Rp, degP, g
+
+
+def elph_model(crystal=None, nw=8, ncell_h=3, ncell_e=3, ncell_p=3, seed=SEED_BASE + 3):
+    """Wannier Hamiltonian on (2 ncell_h + 1)^3 vectors and el-ph coupling on
+    (2 ncell_e + 1)^3 x (2 ncell_p + 1)^3 vectors for the diamond cell (6 branches)."""
+    cr = crystal if crystal is not None else diamond_crystal()
+    Rh, degh, H = wannier_hamiltonian(cr, nw, ncell_h, seed)
+    Re, degE, Rp, degP, g = elph_coupling(cr, ncell_e, ncell_p, cr.num_bands, nw, seed + (1 << 20))
+    if ncell_e != ncell_h:
+        raise ValueError("the Hamiltonian and the coupling share the electronic vectors")
+    return ElPhModel(cr, Re, degE, H, Rp, degP, g)
+
+
+def active_window(E, mu, window):
+    """Active band range [lo, hi) of every k point: bands with |E - mu| <= window."""
+    act = (E >= mu - window) & (E <= mu + window)
+    nk, nw = E.shape
+    lo = np.where(act.any(1), act.argmax(1), 0).astype(np.int32)
+    hi = np.where(act.any(1), nw - act[:, ::-1].argmax(1), 0).astype(np.int32)
+    return lo, hi

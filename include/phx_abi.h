@@ -45,6 +45,7 @@ typedef struct phx_bands phx_bands;
 typedef struct phx_v3 phx_v3;
 typedef struct phx_el_h0 phx_el_h0;
 typedef struct phx_elph phx_elph;
+typedef struct phx_mlp phx_mlp;
 
 /* ---- context ---------------------------------------------------------- */
 /* Replaces initKokkos / DeviceManager (src/common_kokkos.cpp:104-134,182-190). */
@@ -253,6 +254,25 @@ typedef struct phx_el_params {
  * inactive states.  stats may be NULL. */
 int phx_el_linewidths(phx_elph* e, phx_bands* el_bands, phx_bands* ph_bands,
                       const phx_el_params* params, double* out, phx_lw_stats* stats);
+
+/* ---- learned screening network (no counterpart in the reference) -------- */
+/* MLP nin -> hidden (x depth, GELU) -> 1 with parameters laid out per layer as
+ * W (nout,nin) row-major then b (nout), FP32 master copies; every product uses
+ * the weights rounded to BF16 with FP32 accumulation.  params may be NULL
+ * (uninitialised).  Kernels: tiled GEMM forward/backward, GELU, MSE, Adam. */
+int phx_mlp_create(phx_ctx* ctx, int nin, int hidden, int depth, const float* params, phx_mlp** out);
+int phx_mlp_destroy(phx_mlp* net);
+long long phx_mlp_num_params(const phx_mlp* net);
+int phx_mlp_get_params(phx_mlp* net, float* params);
+int phx_mlp_set_params(phx_mlp* net, const float* params);
+/* y (B) = net(X (B,nin)), host arrays */
+int phx_mlp_infer(phx_mlp* net, int B, const float* X, float* y);
+/* gradient (num_params) of the mean squared error mean_b (net(X_b) - t_b)^2, and the loss */
+int phx_mlp_grad(phx_mlp* net, int B, const float* X, const float* t, float* grad, float* loss);
+/* Adam (beta 0.9/0.999, eps 1e-8) on shuffled mini-batches for the given epochs;
+ * loss_per_epoch (epochs) may be NULL. */
+int phx_mlp_train(phx_mlp* net, int n, const float* X, const float* t, int epochs, int batch, float lr,
+                  unsigned long long seed, float* loss_per_epoch);
 
 /* ---- diagnostics -------------------------------------------------------- */
 /* Self-test of the split-precision tensor-core GEMM used by the builder: one

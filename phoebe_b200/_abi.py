@@ -89,10 +89,20 @@ SIGNATURES = {
     "phx_elph_cache_k1": [_VP, _D, _D, _i],
     "phx_elph_couplings_sq": [_VP, _i, _D, _D, _I, _i, _D, _D],
     "phx_el_linewidths": [_VP, _VP, _VP, ctypes.POINTER(ElParams), _D, ctypes.POINTER(LwStats)],
+    "phx_mlp_create": [_VP, _i, _i, _i, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_VP)],
+    "phx_mlp_destroy": [_VP],
+    "phx_mlp_num_params": [_VP],
+    "phx_mlp_get_params": [_VP, ctypes.POINTER(ctypes.c_float)],
+    "phx_mlp_set_params": [_VP, ctypes.POINTER(ctypes.c_float)],
+    "phx_mlp_infer": [_VP, _i, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)],
+    "phx_mlp_grad": [_VP, _i, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                     ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)],
+    "phx_mlp_train": [_VP, _i, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), _i, _i,
+                      ctypes.c_float, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_float)],
     "phx_diag_tc_gemm": [_VP, _i, _i, ctypes.POINTER(ctypes.c_float),
                          ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)],
 }
-_RESTYPE = {"phx_version": ctypes.c_char_p}
+_RESTYPE = {"phx_version": ctypes.c_char_p, "phx_mlp_num_params": ctypes.c_longlong}
 
 _lib = None
 

@@ -44,10 +44,16 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="3ph", choices=["3ph", "elph"],
+                    help="3ph: the headline linewidth builder; elph: electron-phonon linewidths "
+                         "(8 Wannier functions, 343 x 343 coupling vectors, 40^3 k, 20^3 q)")
+    ap.add_argument("--elph-k1", type=int, default=64, help="outer k points timed per elph step")
     ap.add_argument("--precision", default=os.environ.get("PHX_BENCH_PRECISION", "split_bf16"),
                     choices=["fp64", "split_bf16", "split_tf32"])
     ap.add_argument("--mesh", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-fp64", action="store_true",
+                    help="skip the plain FP64 GPU step that the split path is compared with")
     ap.add_argument("--kernels-only", action="store_true",
                     help="profiling aid: time the builder only (no e2e leg, no CPU baseline)")
     return ap.parse_args()
@@ -197,7 +203,8 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from phoebe_b200 import _abi
     from phoebe_b200 import constants as C
-    from phoebe_b200.core import Context, Interaction3Ph, PhononH0, PhScatteringMatrix
+    from phoebe_b200.core import (Context, Interaction3Ph, PhononH0, PhScatteringMatrix,
+                                  finalize_linewidths, q2_slice)
     import ctypes
 
     cr, fc2, fc3, mesh = workload(args.mesh)
@@ -212,8 +219,7 @@ def run_ours(args):
     bands = h0.populate(mesh, withVelocities=True)
     v3 = Interaction3Ph(ctx, cr, fc3, precision=args.precision)
     sm = PhScatteringMatrix(v3, bands, T, "adaptive")
-    q2b = rank * nq // world
-    q2e = (rank + 1) * nq // world
+    q2b, q2e = q2_slice(rank, world, nq)
     A = torch.zeros(nT * nq * nb, dtype=torch.float64, device="cuda")
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
     L = _abi.load()
@@ -278,7 +284,7 @@ def run_ours(args):
         if dist:
             At = torch.from_numpy(Ae).cuda()
             dist.all_reduce(At)
-            Ae = At.cpu().numpy()
+            Ae = finalize_linewidths(At.cpu().numpy(), be.get(velocities=False)[0])
         ve.close()
         be.close()
         h0e.close()
@@ -318,6 +324,26 @@ def run_ours(args):
     roof["ms_per_pair_launch"] = float(np.sum(pair_ms)) / max(1, pair_launches)
     roof["flops_per_pair_reference_formulation"] = flops_per_pair_reference(nb, nr3)
 
+    # the plain FP64 GPU path on the same workload (one step after a one-chunk warm-up)
+    fp64 = None
+    if args.precision != "fp64" and not args.kernels_only and not args.no_fp64:
+        v3.setPrecision("fp64")
+        p = sm._params(q2b, min(q2e, q2b + 448), finalize=False)
+        _abi.check(L.phx_ph_linewidths_d(v3.h, bands.h, ctypes.byref(p), ctypes.c_void_p(A.data_ptr()),
+                                         None), ctx.h)
+        flush.zero_()
+        barrier()
+        st64 = step()
+        barrier()
+        ms64 = float(st64.ms_total)
+        if dist:
+            t = torch.tensor([ms64], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms64 = float(t.item())
+        v3.setPrecision(args.precision)
+        fp64 = {"ms_per_step": ms64, "value": pairs_step / (ms64 / 1000.0), "unit": "triplets/s",
+                "dtype": "f64", "steps": 1, "split_speedup": ms64 / ms_step}
+
     out = None
     if rank == 0:
         cpu = None if args.kernels_only else cpu_baseline(cr, fc2, fc3, mesh, args.cpu_seconds)
@@ -339,6 +365,7 @@ def run_ours(args):
                "gpu_launches": launches,
                "roofline": roof,
                "cpu_baseline": cpu,
+               "fp64_path": fp64,
                "clocks": clk.summary()}
         print(json.dumps(out), flush=True)
     if dist:
@@ -346,8 +373,57 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_elph(args):
+    """Electron-phonon linewidths on a bounded sample of outer k points (FP64 GPU path)."""
+    import torch
+    from phoebe_b200 import constants as C
+    from phoebe_b200 import synth
+    from phoebe_b200.core import (Context, ElectronH0Wannier, ElScatteringMatrix, InteractionElPhWan,
+                                  PhononH0)
+    model = synth.elph_model(nw=8, ncell_h=3, ncell_e=3, ncell_p=3)
+    cr = model.crystal
+    kmesh, qmesh = (40, 40, 40), (20, 20, 20)
+    torch.cuda.set_device(0)
+    ctx = Context(0)
+    wan = ElectronH0Wannier(ctx, cr, model.Re, model.degE, model.H)
+    el = wan.populate(kmesh, withVelocities=True)
+    h0 = PhononH0(ctx, cr, synth.diamond_fc2(cr))
+    ph = h0.populate(qmesh, withVelocities=False)
+    elph = InteractionElPhWan(ctx, model.Re, model.degE, model.Rp, model.degP, model.g)
+    Ek = el.get(velocities=False)[0]
+    mu = float(np.median(Ek))
+    window = 0.3 / C.energyRyToEv
+    lo, hi = synth.active_window(Ek, mu, window)
+    active = np.nonzero(hi > lo)[0]
+    rng = np.random.default_rng(0)
+    T = np.array([C.kelvin_to_ry(300.0)])
+    sm = ElScatteringMatrix(elph, el, ph, T, mu, window, "adaptive")
+    ms = []
+    for i in range(args.warmup + args.steps):
+        k1 = np.sort(rng.choice(active, args.elph_k1, replace=False)).astype(np.int32)
+        sm.setup(k1)
+        if i >= args.warmup:
+            ms.append(sm.stats.ms_total)
+    ms_step = float(np.mean(ms))
+    pairs = sm.stats.pairs
+    states = int(np.sum(hi[k1] - lo[k1]))
+    line = {"metric": "el-ph (k1,q) pairs/s, 8 Wannier bands, 343x343 vectors, 40^3 k x 20^3 q",
+            "value": pairs / (ms_step / 1000.0), "unit": "pairs/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "el-ph linewidths, %d outer k (of %d active of 64000), all 8000 q, "
+                                   "window +-0.3 eV, adaptive smearing, 300 K" % (args.elph_k1, len(active)),
+                       "coupling_bytes": int(model.g.nbytes)},
+            "carrier_linewidths_per_s": states / (ms_step / 1000.0),
+            "pairs_per_step": int(pairs)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "elph":
+        run_elph(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -65,6 +65,29 @@ def ws_reorder(crystal, fc2):
     return R, w, M
 
 
+def q2_slice(rank, world, nq):
+    """Contiguous q2 range [begin, end) of one rank: the reference splits the outer
+    q2 loop over MPI ranks and sums the linewidth vector (ph_scattering.cpp:800)."""
+    return rank * nq // world, (rank + 1) * nq // world
+
+
+def finalize_linewidths(A, E):
+    """What the builder's finalize step does, for partial results summed over
+    ranks: degeneracy averaging of temperature row 0 (scattering.cpp:1168-1207)
+    and zero for excluded states (scattering.cpp:30-50, ph_scattering.cpp:900-906).
+    A (nT, nq*nb) summed over ranks, E (nq, nb); returns a new array."""
+    E = np.asarray(E)
+    nq, nb = E.shape
+    out = np.array(A, dtype=np.float64).reshape(-1, nq, nb)
+    row = out[0].copy()
+    for b1 in range(nb):
+        m = np.abs(E - E[:, b1:b1 + 1]) < C.degeneracyThreshold
+        n = m.sum(axis=1).astype(np.float32).astype(np.float64)
+        out[0][:, b1] = (row * m).sum(axis=1) / n
+    out[:, E < C.phExcludeCutoff] = 0.0
+    return out.reshape(A.shape)
+
+
 class PhononH0:
     """Harmonic phonon Hamiltonian on the GPU (PhononH0)."""
 

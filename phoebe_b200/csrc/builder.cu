@@ -508,13 +508,7 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
                          cudaEvent_t ev_end);
 
 int phx_scratch_reserve(phx_v3* v, size_t bytes) {
-  if (v->scratch_bytes >= bytes) return PHX_OK;
-  cudaFree(v->d_scratch);
-  v->d_scratch = nullptr;
-  v->scratch_bytes = 0;
-  PHX_CUDA(v->ctx, cudaMalloc(&v->d_scratch, bytes));
-  v->scratch_bytes = bytes;
-  return PHX_OK;
+  return phx_ctx_reserve(v->ctx, &v->ctx->d_scratch, &v->ctx->scratch_bytes, bytes);
 }
 
 // ---------------------------------------------------------------------------
@@ -670,7 +664,7 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   const size_t sz_img = split ? align_up(phx_split_bimg_bytes(plan.chunk, nr3)) : 0;
   const size_t sz_rec = split ? align_up(phx_split_rec_bytes(nq)) : 0;
   PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_img + sz_rec));
-  char* base = static_cast<char*>(v->d_scratch);
+  char* base = static_cast<char*>(v->ctx->d_scratch);
   double2* Dp = reinterpret_cast<double2*>(base);
   double* partial = reinterpret_cast<double*>(base + sz_dp);
   double* bose = reinterpret_cast<double*>(base + sz_dp + sz_part);
@@ -847,8 +841,8 @@ extern "C" int phx_ph_linewidths(phx_v3* v, phx_bands* b, const phx_lw_params* p
   phx_ctx* ctx = v->ctx;
   PHX_CUDA(ctx, cudaSetDevice(ctx->device));
   const size_t n = (size_t)p->num_temperatures * b->nq * b->nb;
-  double* d = nullptr;
-  PHX_CUDA(ctx, cudaMalloc(&d, sizeof(double) * std::max<size_t>(n, 1)));
+  PHX_TRY(phx_ctx_reserve(ctx, &ctx->d_out, &ctx->out_bytes, sizeof(double) * std::max<size_t>(n, 1)));
+  double* d = static_cast<double*>(ctx->d_out);
   int rc = phx_ph_linewidths_d(v, b, p, d, stats);
   if (rc == PHX_OK) {
     cudaError_t e = cudaMemcpyAsync(Aout, d, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream);
@@ -858,7 +852,6 @@ extern "C" int phx_ph_linewidths(phx_v3* v, phx_bands* b, const phx_lw_params* p
       rc = PHX_ERR_CUDA;
     }
   }
-  cudaFree(d);
   return rc;
 }
 

@@ -85,6 +85,8 @@ extern "C" int phx_ctx_destroy(phx_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->d_status) cudaFree(ctx->d_status);
+  cudaFree(ctx->d_scratch);
+  cudaFree(ctx->d_out);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return PHX_OK;
@@ -195,5 +197,16 @@ extern "C" int phx_ws_reorder(int nat, const double* cell, const double* pos, co
             ++iR;
           }
   *numR = iR;
+  return PHX_OK;
+}
+
+int phx_ctx_reserve(phx_ctx* ctx, void** buf, size_t* have, size_t bytes) {
+  if (*have >= bytes && *buf) return PHX_OK;
+  PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  cudaFree(*buf);
+  *buf = nullptr;
+  *have = 0;
+  PHX_CUDA(ctx, cudaMalloc(buf, bytes));
+  *have = bytes;
   return PHX_OK;
 }

@@ -48,7 +48,17 @@ struct phx_ctx {
   mutable int last_status = 0;
   // device status word written by kernels (non-convergence, mesh misses)
   int* d_status = nullptr;
+  // builder scratch and output staging, kept for the context's lifetime so
+  // that objects created and destroyed between calls reuse them (calls on one
+  // context run on its one stream, in order)
+  void* d_scratch = nullptr;
+  size_t scratch_bytes = 0;
+  void* d_out = nullptr;
+  size_t out_bytes = 0;
 };
+
+// grow-only device buffers of a context
+int phx_ctx_reserve(phx_ctx* ctx, void** buf, size_t* have, size_t bytes);
 
 struct phx_ph_h0 {
   phx_ctx* ctx = nullptr;
@@ -90,9 +100,6 @@ struct phx_v3 {
   double* d_mins = nullptr;    // cached D3- (nb,nb,nb,nr3) complex
   bool cached = false;
   double q2_cached[3];
-  // builder scratch (grown on demand)
-  void* d_scratch = nullptr;
-  size_t scratch_bytes = 0;
 };
 
 int phx_scratch_reserve(phx_v3* v3, size_t bytes);

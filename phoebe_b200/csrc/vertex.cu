@@ -223,7 +223,6 @@ extern "C" int phx_v3_destroy(phx_v3* v) {
   cudaFree(v->d_R3);
   cudaFree(v->d_plus);
   cudaFree(v->d_mins);
-  cudaFree(v->d_scratch);
   delete v;
   return PHX_OK;
 }

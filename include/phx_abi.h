@@ -232,6 +232,11 @@ int phx_elph_cache_k1(phx_elph* e, const double* k1, const double* U1, int nb1);
 int phx_elph_couplings_sq(phx_elph* e, int nk2, const double* q3, const double* U2s, const int* nb2s,
                           int nb2max, const double* ev3s, double* coupling);
 
+/* Precision of the Rp transform inside phx_el_linewidths: PHX_PREC_FP64 (default)
+ * or PHX_PREC_SPLIT_BF16 (tcgen05 BF16 hi+lo, FP32 accumulation; needs 6 phonon
+ * branches and 8 Wannier functions).  The rotations, |g|^2 and rates stay FP64. */
+int phx_elph_set_precision(phx_elph* e, int precision);
+
 typedef struct phx_el_params {
   int num_temperatures;       /* <= 4 */
   const double* temperatures; /* Ry */

@@ -87,6 +87,7 @@ SIGNATURES = {
                         ctypes.POINTER(_VP)],
     "phx_elph_destroy": [_VP],
     "phx_elph_cache_k1": [_VP, _D, _D, _i],
+    "phx_elph_set_precision": [_VP, _i],
     "phx_elph_couplings_sq": [_VP, _i, _D, _D, _I, _i, _D, _D],
     "phx_el_linewidths": [_VP, _VP, _VP, ctypes.POINTER(ElParams), _D, ctypes.POINTER(LwStats)],
     "phx_mlp_create": [_VP, _i, _i, _i, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_VP)],

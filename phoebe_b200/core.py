@@ -409,6 +409,11 @@ class InteractionElPhWan:
         self.h = h
         self.nb1 = 0
 
+    def setPrecision(self, precision):
+        """'fp64' or 'split_bf16' (tensor-core Rp transform in the linewidth builder)."""
+        check(_abi.load().phx_elph_set_precision(self.h, PRECISIONS[precision]), self.ctx.h)
+        self.precision = precision
+
     def cacheElPh(self, eigvec1, k1C):
         """eigvec1: (nw, nb1) complex (columns = bands at k1)."""
         U = c128(eigvec1)

@@ -18,6 +18,17 @@
 #include "phx_consts.h"
 #include "phx_internal.h"
 
+// split-precision Rp transform (el_split.cu)
+void phx_el_split_dims(int nRp, int nq, int* nKC, int* nMT);
+size_t phx_el_split_phase_bytes(int nRp, int nq);
+size_t phx_el_split_coupling_bytes(int nRp, int xmax);
+int phx_el_split_max_batch();
+int phx_el_split_phases(phx_ctx* ctx, int nq, const double* qcart, int nRp, const double* Rp, const double* degP,
+                        uint8_t* img);
+int phx_el_split_g3_batch(phx_ctx* ctx, const uint8_t* Aimg, uint8_t* Bimg, const double2* cached, size_t per,
+                          int nRp, int nph, int nw, int nq, int nb, const int* nb1, float2* g3T, int* ldq_out,
+                          int* xoff_out);
+
 namespace {
 
 constexpr int kB1 = 8;        // k1 points per pass over the coupling tensor
@@ -139,11 +150,24 @@ __device__ inline PairSmem pair_carve(char* base, int nRp, int nph, int nw) {
 // |g|^2 of the kQT final states whose phases, U2 (nb2 columns) and ev3 are staged;
 // cached is (nRp, nph, nw(b1), nw) of one k1 with nb1 active bands.
 __device__ void pair_couplings(const double2* __restrict__ cached, int nRp, int nph, int nw, int nb1,
-                               const PairSmem& s) {
+                               const PairSmem& s, const float2* __restrict__ g3in = nullptr, int g3ld = 0) {
   const int tid = threadIdx.x, NT = blockDim.x;
   const int nx = nph * nb1 * nw;
+  if (g3in) {
+    // g3 from the tensor-core GEMM, stored g3in[x * g3ld + q] (q = phonon mesh index)
+    for (int i = tid; i < kQT * nx; i += NT) {
+      const int q = i % kQT, x = i / kQT;
+      const int w2 = x % nw, b1 = (x / nw) % nb1, nu = x / (nw * nb1);
+      double2 v = cmk(0.0, 0.0);
+      if (s.info[4 * q]) {
+        const float2 f = g3in[(size_t)x * g3ld + s.info[4 * q + 3]];
+        v = cmk((double)f.x, (double)f.y);
+      }
+      s.g3[((q * nph + nu) * kMaxW + b1) * nw + w2] = v;
+    }
+  }
   // g3[q][nu][b1][w2] = sum_Rp ph[q][Rp] cached[Rp][nu][b1][w2]
-  for (int x = tid; x < nx; x += NT) {
+  for (int x = tid; x < (g3in ? 0 : nx); x += NT) {
     const int w2 = x % nw, b1 = (x / nw) % nb1, nu = x / (nw * nb1);
     const size_t cx = ((size_t)nu * nw + b1) * nw + w2;
     double2 acc[kQT];
@@ -272,6 +296,8 @@ struct ElArgs {
   double qT[9];
   double norm;
   double* out;             // (nT, nk1, nw)
+  const float2* g3in;      // precomputed g3 of this k1, g3in[x * g3ld + q], or null
+  int g3ld;
 };
 
 __device__ __forceinline__ double el_delta(const ElArgs& A, double e, const double v[3]) {
@@ -327,8 +353,9 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
   }
   __syncthreads();
   if (!(s.info[0] | s.info[4] | s.info[8] | s.info[12])) return;
-  // phases e^{+i q3.Rp}/deg with q3 = k2 - k1 (helper_el_scattering.cpp:233-234)
-  for (int i = tid; i < kQT * nRp; i += NT) {
+  // phases e^{+i q3.Rp}/deg with q3 = k2 - k1 (helper_el_scattering.cpp:233-234),
+  // not needed when g3 comes from the tensor-core GEMM
+  for (int i = tid; i < (A.g3in ? 0 : kQT * nRp); i += NT) {
     const int q = i / nRp, r = i % nRp;
     double2 v = cmk(0.0, 0.0);
     if (s.info[4 * q]) {
@@ -363,7 +390,7 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
     s.E3[i] = s.info[4 * q] ? A.Eq[(size_t)s.info[4 * q + 3] * nph + i % nph] : 0.0;
   }
   __syncthreads();
-  pair_couplings(A.cached, nRp, nph, nw, nb1, s);
+  pair_couplings(A.cached, nRp, nph, nw, nb1, s, A.g3in, A.g3ld);
   pair_symmetrize(E1, nb1, nph, s);
   // rates (el_scattering.cpp:268-327)
   for (int x = tid; x < kQT * nb1 * kMaxW * nph; x += NT) {
@@ -668,11 +695,19 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
     PHX_ARG(ctx, p->k1_list[i] >= 0 && p->k1_list[i] < nk, "phx_el_linewidths: k1 index out of range");
   PHX_CUDA(ctx, cudaSetDevice(ctx->device));
   const size_t N = (size_t)e->nRp * nph * nw * nw;
+  const bool split = e->precision != PHX_PREC_FP64;
+  // split path: phase image, coupling image of a batch, g3T of a batch (x, q)
+  int sKC = 0, sMT = 0;
+  phx_el_split_dims(e->nRp, ph->nq, &sKC, &sMT);
+  const int xmax = kB1 * nph * nw * nw;
+  const size_t b_A = split ? align256(phx_el_split_phase_bytes(e->nRp, ph->nq)) : 0;
+  const size_t b_B = split ? align256(phx_el_split_coupling_bytes(e->nRp, xmax)) : 0;
+  const size_t b_g3 = split ? align256(sizeof(float2) * (size_t)xmax * sMT * 128) + b_A + b_B : 0;
   const size_t b_lo = align256(sizeof(int) * nk), b_k1 = align256(sizeof(int) * std::max(1, nk1)),
                b_out = align256(sizeof(double) * (size_t)nT * std::max(1, nk1) * nw),
                b_kb = align256(sizeof(double) * 3 * kB1), b_ub = align256(sizeof(double2) * kB1 * nw * nw),
                b_nb = align256(sizeof(int) * kB1), b_g1 = align256(sizeof(double2) * kB1 * N);
-  PHX_TRY(elph_reserve(e, 2 * b_lo + b_k1 + b_out + b_kb + b_ub + b_nb + 2 * b_g1));
+  PHX_TRY(elph_reserve(e, 2 * b_lo + b_k1 + b_out + b_kb + b_ub + b_nb + 2 * b_g1 + b_g3));
   char* base = static_cast<char*>(e->d_scratch);
   int* dlo = reinterpret_cast<int*>(base);
   int* dhi = reinterpret_cast<int*>(base + b_lo);
@@ -684,12 +719,16 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
   int* dnb = reinterpret_cast<int*>(bb + b_kb + b_ub);
   double2* dg1 = reinterpret_cast<double2*>(bb + b_kb + b_ub + b_nb);
   double2* dcached = reinterpret_cast<double2*>(bb + b_kb + b_ub + b_nb + b_g1);
+  uint8_t* dAimg = split ? reinterpret_cast<uint8_t*>(bb + b_kb + b_ub + b_nb + 2 * b_g1) : nullptr;
+  uint8_t* dBimg = split ? dAimg + b_A : nullptr;
+  float2* dg3 = split ? reinterpret_cast<float2*>(dBimg + b_B) : nullptr;
   cudaStream_t st = ctx->stream;
   cudaEvent_t ev0, ev1;
   PHX_CUDA(ctx, cudaEventCreate(&ev0));
   PHX_CUDA(ctx, cudaEventCreate(&ev1));
   PHX_CUDA(ctx, cudaEventRecord(ev0, st));
   int launches = 0;
+  PHX_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
   el_window_kernel<<<(nk + 255) / 256, 256, 0, st>>>(el->d_E, nk, nw, p->chemical_potential, p->window, dlo, dhi);
   ++launches;
   PHX_CUDA(ctx, cudaGetLastError());
@@ -730,6 +769,13 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
     for (int j = 0; j < 3; ++j) A.qT[i * 3 + j] = el->recip[i * 3 + j] / el->mesh[i];
   A.norm = p->norm;
   A.out = dout;
+  A.g3in = nullptr;
+  A.g3ld = 0;
+  if (split) {
+    PHX_ARG(ctx, kB1 <= phx_el_split_max_batch(), "phx_el_linewidths: k1 batch larger than the split GEMM's");
+    PHX_TRY(phx_el_split_phases(ctx, ph->nq, ph->d_q, e->nRp, e->d_Rp, e->d_degP, dAimg));
+    ++launches;
+  }
   const size_t smem = pair_smem(e);
   PHX_ARG(ctx, smem <= 227 * 1024, "phx_el_linewidths: too many phonon Bravais vectors");
   PHX_CUDA(ctx, cudaFuncSetAttribute(el_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -762,10 +808,22 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
     }
     PHX_TRY(elph_cache_batch(e, nb, dkb, dub, dnb, dg1, dcached));
     launches += 2;
+    // the Rp transform of all q and the batch's k1 on the tensor cores (BF16 x3, FP32 accumulation)
+    int g3ld = 0;
+    std::vector<int> xoff(kB1, 0);
+    if (split) {
+      PHX_TRY(phx_el_split_g3_batch(ctx, dAimg, dBimg, dcached, per, e->nRp, nph, nw, nq, nb, nbb.data(), dg3,
+                                    &g3ld, xoff.data()));
+      launches += 2;
+    }
     for (int j = 0; j < nb; ++j) {
       A.cached = dcached + (size_t)j * per;
       A.ik1 = p->k1_list[rows[j]];
       A.i1 = rows[j];
+      if (split) {
+        A.g3in = dg3 + (size_t)xoff[j] * g3ld;
+        A.g3ld = g3ld;
+      }
       el_pair_kernel<<<qblocks, kPairThreads, smem, st>>>(A);
       ++launches;
       pairs += nq;
@@ -779,7 +837,16 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
   }
   PHX_CUDA(ctx, cudaEventRecord(ev1, st));
   PHX_CUDA(ctx, cudaMemcpyAsync(out, dout, sizeof(double) * (size_t)nT * nk1 * nw, cudaMemcpyDeviceToHost, st));
+  int kst = 0;
+  PHX_CUDA(ctx, cudaMemcpyAsync(&kst, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
   PHX_CUDA(ctx, cudaStreamSynchronize(st));
+  if (kst) {
+    cudaMemset(ctx->d_status, 0, sizeof(int));
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    phx_set_error(ctx, PHX_ERR_CUDA, "el-ph tensor-core GEMM gave up waiting on its MMA barrier");
+    return PHX_ERR_CUDA;
+  }
   if (stats) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ev0, ev1);
@@ -792,5 +859,13 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
   }
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
+  return PHX_OK;
+}
+
+extern "C" int phx_elph_set_precision(phx_elph* e, int precision) {
+  PHX_ARG(e ? e->ctx : nullptr, e, "phx_elph_set_precision: null handle");
+  PHX_ARG(e->ctx, precision == PHX_PREC_FP64 || precision == PHX_PREC_SPLIT_BF16,
+          "phx_elph_set_precision: PHX_PREC_FP64 or PHX_PREC_SPLIT_BF16");
+  e->precision = precision;
   return PHX_OK;
 }

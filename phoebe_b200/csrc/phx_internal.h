@@ -127,6 +127,7 @@ struct phx_elph {
   float* d_g = nullptr;       // (nRe,nRp,nph,nw,nw) complex FP32 coupling in the Wannier basis
   double* d_cached = nullptr; // (nRp,nph,nw,nw) complex: cacheElPh of the last k1 (b1 < nb1)
   int nb1 = 0;                // bands of the cached k1
+  int precision = PHX_PREC_FP64;  // of the Rp transform in phx_el_linewidths
   void* d_scratch = nullptr;  // builder scratch (grown on demand)
   size_t scratch_bytes = 0;
 };

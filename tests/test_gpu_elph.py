@@ -115,3 +115,35 @@ def test_el_linewidths_match_oracle(ctx, model, smearing, kmesh, qmesh):
     h0.close()
     el.close()
     wan.close()
+
+
+def test_el_linewidths_split_precision(ctx, model):
+    """Tensor-core (BF16 x3) Rp transform: linewidths within 1e-5 of the FP64 path."""
+    from phoebe_b200.core import (ElectronH0Wannier, ElScatteringMatrix, InteractionElPhWan, PhononH0)
+    cr = model.crystal
+    kmesh, qmesh = (8, 8, 8), (4, 4, 4)
+    wan = ElectronH0Wannier(ctx, cr, model.Re, model.degE, model.H)
+    el = wan.populate(kmesh, withVelocities=True)
+    h0 = PhononH0(ctx, cr, synth.diamond_fc2(cr))
+    ph = h0.populate(qmesh, withVelocities=False)
+    gpu = InteractionElPhWan(ctx, model.Re, model.degE, model.Rp, model.degP, model.g)
+    Ek = el.get(velocities=False)[0]
+    mu = float(np.median(Ek))
+    temps = np.array([C.kelvin_to_ry(300.0)])
+    k1 = np.arange(0, 512, 3, dtype=np.int32)
+    sm = ElScatteringMatrix(gpu, el, ph, temps, mu, 0.05, "adaptive")
+    A64 = sm.setup(k1)
+    gpu.setPrecision("split_bf16")
+    A16 = sm.setup(k1)
+    assert np.abs(A64).max() > 0
+    big = np.abs(A64) > 1e-6 * np.abs(A64).max()
+    rel = np.abs(A16 - A64)[big] / np.abs(A64)[big]
+    assert rel.max() < 1e-5, rel.max()
+    gpu.setPrecision("fp64")
+    # back on the FP64 path (atomic accumulation order varies between runs)
+    np.testing.assert_allclose(sm.setup(k1), A64, rtol=1e-13, atol=0)
+    gpu.close()
+    ph.close()
+    h0.close()
+    el.close()
+    wan.close()

@@ -275,7 +275,8 @@ __device__ void pair_symmetrize(const double* E1, int nb1, int nph, const PairSm
 
 struct ElArgs {
   int nw, nph, nRp;
-  const double2* cached;   // this k1
+  const double2* cached;   // batch of k1: cached + blockIdx.y * cper
+  size_t cper;
   const double* Rp;
   const double* degP;
   int kmesh[3], qmesh[3];
@@ -287,7 +288,9 @@ struct ElArgs {
   const int* hi;
   const double* Eq;        // (nq,nph)
   const double2* evq;      // (nq,nph,nph)
-  int ik1, i1, nk1;        // k1 mesh index and its row in the output
+  int ik1s[kB1], i1s[kB1]; // per blockIdx.y: k1 mesh index and its row in the output
+  long long g3offs[kB1];   // per blockIdx.y: offset of its g3 columns in g3in
+  int nk1;
   int nT;
   double temps[pairc::kMaxT];
   double mu;
@@ -327,10 +330,14 @@ __device__ __forceinline__ double el_delta(const ElArgs& A, double e, const doub
 __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
   extern __shared__ __align__(16) char sraw[];
   const int nw = A.nw, nph = A.nph, nRp = A.nRp;
-  const PairSmem s = pair_carve(sraw, nRp, nph, nw);
+  // no phase buffer when g3 comes from the tensor-core GEMM
+  const PairSmem s = pair_carve(sraw, A.g3in ? 0 : nRp, nph, nw);
   const int tid = threadIdx.x, NT = blockDim.x;
   const int nq = A.qmesh[0] * A.qmesh[1] * A.qmesh[2];
-  const int ik1 = A.ik1, lo1 = A.lo[ik1], nb1 = A.hi[ik1] - lo1;
+  const int jb = blockIdx.y;
+  const int ik1 = A.ik1s[jb], i1 = A.i1s[jb], lo1 = A.lo[ik1], nb1 = A.hi[ik1] - lo1;
+  const double2* cached = A.cached + (size_t)jb * A.cper;
+  const float2* g3in = A.g3in ? A.g3in + A.g3offs[jb] : nullptr;
   const int x1 = ik1 % A.kmesh[0], y1 = (ik1 / A.kmesh[0]) % A.kmesh[1], z1 = ik1 / (A.kmesh[0] * A.kmesh[1]);
   const int f0 = A.kmesh[0] / A.qmesh[0], f1 = A.kmesh[1] / A.qmesh[1], f2 = A.kmesh[2] / A.qmesh[2];
   const double* E1 = A.Ek + (size_t)ik1 * nw + lo1;
@@ -355,7 +362,7 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
   if (!(s.info[0] | s.info[4] | s.info[8] | s.info[12])) return;
   // phases e^{+i q3.Rp}/deg with q3 = k2 - k1 (helper_el_scattering.cpp:233-234),
   // not needed when g3 comes from the tensor-core GEMM
-  for (int i = tid; i < (A.g3in ? 0 : kQT * nRp); i += NT) {
+  for (int i = tid; i < (g3in ? 0 : kQT * nRp); i += NT) {
     const int q = i / nRp, r = i % nRp;
     double2 v = cmk(0.0, 0.0);
     if (s.info[4 * q]) {
@@ -390,7 +397,7 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
     s.E3[i] = s.info[4 * q] ? A.Eq[(size_t)s.info[4 * q + 3] * nph + i % nph] : 0.0;
   }
   __syncthreads();
-  pair_couplings(A.cached, nRp, nph, nw, nb1, s, A.g3in, A.g3ld);
+  pair_couplings(cached, nRp, nph, nw, nb1, s, g3in, A.g3ld);
   pair_symmetrize(E1, nb1, nph, s);
   // rates (el_scattering.cpp:268-327)
   for (int x = tid; x < kQT * nb1 * kMaxW * nph; x += NT) {
@@ -429,7 +436,7 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
   for (int i = tid; i < nb1 * A.nT; i += NT) {
     const int b1 = i / A.nT, t = i % A.nT;
     const double v = s.acc[b1 * pairc::kMaxT + t];
-    if (v != 0.0) atomicAdd(&A.out[((size_t)t * A.nk1 + A.i1) * nw + lo1 + b1], v);
+    if (v != 0.0) atomicAdd(&A.out[((size_t)t * A.nk1 + i1) * nw + lo1 + b1], v);
   }
 }
 
@@ -493,6 +500,35 @@ __global__ void el_window_kernel(const double* __restrict__ E, int nk, int nw, d
     if (h <= l) l = h = 0;
     lo[k] = l;
     hi[k] = h;
+  }
+}
+
+// active-band counts of the k1 list
+__global__ void el_k1_bands_kernel(const int* __restrict__ k1s, int nk1, const int* __restrict__ lo,
+                                   const int* __restrict__ hi, int* __restrict__ nb1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nk1) nb1[i] = hi[k1s[i]] - lo[k1s[i]];
+}
+
+// k1 coordinates, active-band counts and U1 columns lo..hi-1 of a batch of
+// active k1 (mesh indices ik[0..nb)); unused slots are zeroed
+__global__ void el_batch_gather_kernel(const int* __restrict__ ik, int nb, const int* __restrict__ lo,
+                                       const int* __restrict__ hi, const double* __restrict__ kcart,
+                                       const double2* __restrict__ Uk, int nw, double* __restrict__ kb,
+                                       double2* __restrict__ ub, int* __restrict__ nbb) {
+  for (int i = threadIdx.x; i < kB1 * nw * nw; i += blockDim.x) {
+    const int j = i / (nw * nw), w = (i / nw) % nw, b = i % nw;
+    double2 v = cmk(0.0, 0.0);
+    if (j < nb) {
+      const int k = ik[j];
+      if (b < hi[k] - lo[k]) v = Uk[((size_t)k * nw + w) * nw + lo[k] + b];
+    }
+    ub[i] = v;
+  }
+  for (int j = threadIdx.x; j < kB1; j += blockDim.x) {
+    const int k = j < nb ? ik[j] : 0;
+    nbb[j] = j < nb ? hi[k] - lo[k] : 0;
+    for (int c = 0; c < 3; ++c) kb[3 * j + c] = j < nb ? kcart[3 * (size_t)k + c] : 0.0;
   }
 }
 
@@ -707,7 +743,7 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
                b_out = align256(sizeof(double) * (size_t)nT * std::max(1, nk1) * nw),
                b_kb = align256(sizeof(double) * 3 * kB1), b_ub = align256(sizeof(double2) * kB1 * nw * nw),
                b_nb = align256(sizeof(int) * kB1), b_g1 = align256(sizeof(double2) * kB1 * N);
-  PHX_TRY(elph_reserve(e, 2 * b_lo + b_k1 + b_out + b_kb + b_ub + b_nb + 2 * b_g1 + b_g3));
+  PHX_TRY(elph_reserve(e, 2 * b_lo + 3 * b_k1 + b_out + b_kb + b_ub + b_nb + 2 * b_g1 + b_g3));
   char* base = static_cast<char*>(e->d_scratch);
   int* dlo = reinterpret_cast<int*>(base);
   int* dhi = reinterpret_cast<int*>(base + b_lo);
@@ -722,6 +758,8 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
   uint8_t* dAimg = split ? reinterpret_cast<uint8_t*>(bb + b_kb + b_ub + b_nb + 2 * b_g1) : nullptr;
   uint8_t* dBimg = split ? dAimg + b_A : nullptr;
   float2* dg3 = split ? reinterpret_cast<float2*>(dBimg + b_B) : nullptr;
+  int* dnball = reinterpret_cast<int*>(bb + b_kb + b_ub + b_nb + 2 * b_g1 + b_g3);   // (nk1) active bands
+  int* dactik = dnball + b_k1 / sizeof(int);                                        // mesh index of active k1
   cudaStream_t st = ctx->stream;
   cudaEvent_t ev0, ev1;
   PHX_CUDA(ctx, cudaEventCreate(&ev0));
@@ -734,13 +772,24 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
   PHX_CUDA(ctx, cudaGetLastError());
   if (nk1 > 0) PHX_CUDA(ctx, cudaMemcpyAsync(dk1, p->k1_list, sizeof(int) * nk1, cudaMemcpyHostToDevice, st));
   PHX_CUDA(ctx, cudaMemsetAsync(dout, 0, sizeof(double) * (size_t)nT * std::max(1, nk1) * nw, st));
-  // host copies of the windows and k1 data (band counts and eigenvectors per batch)
-  std::vector<int> lo(nk), hi(nk);
-  PHX_CUDA(ctx, cudaMemcpyAsync(lo.data(), dlo, sizeof(int) * nk, cudaMemcpyDeviceToHost, st));
-  PHX_CUDA(ctx, cudaMemcpyAsync(hi.data(), dhi, sizeof(int) * nk, cudaMemcpyDeviceToHost, st));
-  PHX_CUDA(ctx, cudaStreamSynchronize(st));
-  std::vector<double> kc(3 * (size_t)nk);
-  PHX_CUDA(ctx, cudaMemcpy(kc.data(), el->d_q, sizeof(double) * 3 * nk, cudaMemcpyDeviceToHost));
+  // active-band counts of the k1 list: the host needs them to lay out the batches
+  std::vector<int> nb1all(std::max(1, nk1), 0);
+  if (nk1 > 0) {
+    el_k1_bands_kernel<<<(nk1 + 255) / 256, 256, 0, st>>>(dk1, nk1, dlo, dhi, dnball);
+    ++launches;
+    PHX_CUDA(ctx, cudaGetLastError());
+    PHX_CUDA(ctx, cudaMemcpyAsync(nb1all.data(), dnball, sizeof(int) * nk1, cudaMemcpyDeviceToHost, st));
+    PHX_CUDA(ctx, cudaStreamSynchronize(st));
+  }
+  // the k1 with active states, in list order, taken kB1 at a time
+  std::vector<int> act, actik;
+  for (int i = 0; i < nk1; ++i)
+    if (nb1all[i] > 0) {
+      act.push_back(i);
+      actik.push_back(p->k1_list[i]);
+    }
+  const int nact = (int)act.size();
+  if (nact > 0) PHX_CUDA(ctx, cudaMemcpyAsync(dactik, actik.data(), sizeof(int) * nact, cudaMemcpyHostToDevice, st));
   ElArgs A;
   A.nw = nw;
   A.nph = nph;
@@ -776,36 +825,24 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
     PHX_TRY(phx_el_split_phases(ctx, ph->nq, ph->d_q, e->nRp, e->d_Rp, e->d_degP, dAimg));
     ++launches;
   }
-  const size_t smem = pair_smem(e);
+  size_t soff[10];
+  const size_t smem = pair_smem_layout(split ? 0 : e->nRp, nph, nw, soff);
   PHX_ARG(ctx, smem <= 227 * 1024, "phx_el_linewidths: too many phonon Bravais vectors");
   PHX_CUDA(ctx, cudaFuncSetAttribute(el_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int nq = ph->nq;
   const int qblocks = (nq + kQT - 1) / kQT;
   const size_t per = N;
   long long pairs = 0;
-  for (int b0 = 0; b0 < nk1; b0 += kB1) {
-    // the batch's k1 with active states
-    std::vector<int> rows;
-    for (int i = b0; i < std::min(nk1, b0 + kB1); ++i)
-      if (hi[p->k1_list[i]] > lo[p->k1_list[i]]) rows.push_back(i);
-    if (rows.empty()) continue;
-    const int nb = (int)rows.size();
-    std::vector<double> kb(3 * kB1, 0.0);
+  for (int b0 = 0; b0 < nact; b0 += kB1) {
+    const int nb = std::min(kB1, nact - b0);
+    std::vector<int> rows(act.begin() + b0, act.begin() + b0 + nb);
     std::vector<int> nbb(kB1, 0);
-    for (int j = 0; j < nb; ++j) {
-      const int ik = p->k1_list[rows[j]];
-      for (int c = 0; c < 3; ++c) kb[3 * j + c] = kc[3 * (size_t)ik + c];
-      nbb[j] = hi[ik] - lo[ik];
-    }
-    PHX_CUDA(ctx, cudaMemcpyAsync(dkb, kb.data(), sizeof(double) * 3 * kB1, cudaMemcpyHostToDevice, st));
-    PHX_CUDA(ctx, cudaMemcpyAsync(dnb, nbb.data(), sizeof(int) * kB1, cudaMemcpyHostToDevice, st));
-    // U1 of the active bands, columns shifted to start at 0
-    for (int j = 0; j < nb; ++j) {
-      const int ik = p->k1_list[rows[j]];
-      for (int w = 0; w < nw; ++w)
-        PHX_CUDA(ctx, cudaMemcpyAsync(dub + ((size_t)j * nw + w) * nw, el->d_U + 2 * (((size_t)ik * nw + w) * nw + lo[ik]),
-                                      sizeof(double2) * (hi[ik] - lo[ik]), cudaMemcpyDeviceToDevice, st));
-    }
+    for (int j = 0; j < nb; ++j) nbb[j] = nb1all[rows[j]];
+    // k1 coordinates, band counts and U1 of the batch, gathered on the device
+    el_batch_gather_kernel<<<1, 256, 0, st>>>(dactik + b0, nb, dlo, dhi, el->d_q,
+                                              reinterpret_cast<const double2*>(el->d_U), nw, dkb, dub, dnb);
+    ++launches;
+    PHX_CUDA(ctx, cudaGetLastError());
     PHX_TRY(elph_cache_batch(e, nb, dkb, dub, dnb, dg1, dcached));
     launches += 2;
     // the Rp transform of all q and the batch's k1 on the tensor cores (BF16 x3, FP32 accumulation)
@@ -816,18 +853,21 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
                                     &g3ld, xoff.data()));
       launches += 2;
     }
+    // one launch for the batch: blockIdx.y = k1 of the batch
+    A.cached = dcached;
+    A.cper = per;
     for (int j = 0; j < nb; ++j) {
-      A.cached = dcached + (size_t)j * per;
-      A.ik1 = p->k1_list[rows[j]];
-      A.i1 = rows[j];
-      if (split) {
-        A.g3in = dg3 + (size_t)xoff[j] * g3ld;
-        A.g3ld = g3ld;
-      }
-      el_pair_kernel<<<qblocks, kPairThreads, smem, st>>>(A);
-      ++launches;
-      pairs += nq;
+      A.ik1s[j] = p->k1_list[rows[j]];
+      A.i1s[j] = rows[j];
+      A.g3offs[j] = (long long)xoff[j] * g3ld;
     }
+    if (split) {
+      A.g3in = dg3;
+      A.g3ld = g3ld;
+    }
+    el_pair_kernel<<<dim3(qblocks, nb), kPairThreads, smem, st>>>(A);
+    ++launches;
+    pairs += (long long)nq * nb;
     PHX_CUDA(ctx, cudaGetLastError());
   }
   if (nk1 > 0) {

@@ -138,10 +138,48 @@ def test_el_linewidths_split_precision(ctx, model):
     assert np.abs(A64).max() > 0
     big = np.abs(A64) > 1e-6 * np.abs(A64).max()
     rel = np.abs(A16 - A64)[big] / np.abs(A64)[big]
+    print("split vs fp64, small el-ph model: max rel %.3e" % rel.max())
     assert rel.max() < 1e-5, rel.max()
     gpu.setPrecision("fp64")
     # back on the FP64 path (atomic accumulation order varies between runs)
     np.testing.assert_allclose(sm.setup(k1), A64, rtol=1e-13, atol=0)
+    gpu.close()
+    ph.close()
+    h0.close()
+    el.close()
+    wan.close()
+
+
+def test_el_linewidths_split_precision_full_model(ctx):
+    """The el-ph benchmark model (343 electron and 343 phonon vectors, 40^3 k,
+    20^3 q): split-precision linewidths of a sample of active k1 within 1e-5 of
+    the FP64 path (the FP64 path itself is pinned to the oracle on the small
+    model above)."""
+    from phoebe_b200.core import (ElectronH0Wannier, ElScatteringMatrix, InteractionElPhWan, PhononH0)
+    model = synth.elph_model(nw=8, ncell_h=3, ncell_e=3, ncell_p=3)
+    cr = model.crystal
+    wan = ElectronH0Wannier(ctx, cr, model.Re, model.degE, model.H)
+    el = wan.populate((40, 40, 40), withVelocities=True)
+    h0 = PhononH0(ctx, cr, synth.diamond_fc2(cr))
+    ph = h0.populate((20, 20, 20), withVelocities=False)
+    gpu = InteractionElPhWan(ctx, model.Re, model.degE, model.Rp, model.degP, model.g)
+    Ek = el.get(velocities=False)[0]
+    mu = float(np.median(Ek))
+    window = 0.3 / C.energyRyToEv
+    lo, hi = synth.active_window(Ek, mu, window)
+    active = np.nonzero(hi > lo)[0]
+    k1 = np.sort(np.random.default_rng(5).choice(active, 12, replace=False)).astype(np.int32)
+    temps = np.array([C.kelvin_to_ry(300.0)])
+    sm = ElScatteringMatrix(gpu, el, ph, temps, mu, window, "adaptive")
+    A64 = sm.setup(k1)
+    gpu.setPrecision("split_bf16")
+    A16 = sm.setup(k1)
+    big = np.abs(A64) > 1e-6 * np.abs(A64).max()
+    rel = np.abs(A16 - A64)[big] / np.abs(A64)[big]
+    print("split vs fp64, full el-ph model: max rel %.3e, median %.3e over %d linewidths"
+          % (rel.max(), np.median(rel), big.sum()))
+    assert big.sum() >= 8
+    assert rel.max() < 1e-5, rel.max()
     gpu.close()
     ph.close()
     h0.close()

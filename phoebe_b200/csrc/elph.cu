@@ -28,6 +28,11 @@ int phx_el_split_phases(phx_ctx* ctx, int nq, const double* qcart, int nRp, cons
 int phx_el_split_g3_batch(phx_ctx* ctx, const uint8_t* Aimg, uint8_t* Bimg, const double2* cached, size_t per,
                           int nRp, int nph, int nw, int nq, int nb, const int* nb1, float2* g3T, int* ldq_out,
                           int* xoff_out);
+size_t phx_el_split_g_image_bytes(int nRe, long long N);
+size_t phx_el_split_k1_image_bytes();
+int phx_el_split_g_image(phx_ctx* ctx, const float* g, int nRe, long long N, uint8_t* img);
+int phx_el_split_g1(phx_ctx* ctx, const uint8_t* gimg, int nRe, long long N, const double* Re, const double* degE,
+                    int nb, const double* k1s, uint8_t* kimg, double2* g1);
 
 namespace {
 
@@ -570,9 +575,22 @@ int elph_reserve(phx_elph* e, size_t bytes) {
 // cacheElPh of nb (<= kB1) k1 points: k1s (device, nb*3), U1s (device, nb*nw*nw, columns
 // >= nb1 ignored), nb1s (device) -> cached (device, nb * nRp*nph*nw*nw)
 int elph_cache_batch(phx_elph* e, int nb, const double* d_k1s, const double2* d_U1s, const int* d_nb1s,
-                     double2* d_g1, double2* d_cached) {
+                     double2* d_g1, double2* d_cached, bool tensor_cores = false) {
   phx_ctx* ctx = e->ctx;
   const size_t N = (size_t)e->nRp * e->nph * e->nw * e->nw;
+  if (tensor_cores) {
+    // g1 on the tensor cores from the split image of g (built once per coupling object)
+    if (!e->d_gimg) {
+      PHX_CUDA(ctx, cudaMalloc(&e->d_gimg, phx_el_split_g_image_bytes(e->nRe, (long long)N)));
+      PHX_CUDA(ctx, cudaMalloc(&e->d_kimg, phx_el_split_k1_image_bytes()));
+      PHX_TRY(phx_el_split_g_image(ctx, e->d_g, e->nRe, (long long)N, e->d_gimg));
+    }
+    PHX_TRY(phx_el_split_g1(ctx, e->d_gimg, e->nRe, (long long)N, e->d_Re, e->d_degE, nb, d_k1s, e->d_kimg, d_g1));
+    elph_rot_kernel<<<std::min<size_t>((N * nb + 255) / 256, (size_t)ctx->num_sms * 16), 256, 0, ctx->stream>>>(
+        d_g1, e->nRp * e->nph, e->nw, nb, d_U1s, d_nb1s, d_cached);
+    PHX_CUDA(ctx, cudaGetLastError());
+    return PHX_OK;
+  }
   const size_t smem = sizeof(double2) * kB1 * e->nRe;
   if (smem > 48 * 1024)
     PHX_CUDA(ctx, cudaFuncSetAttribute(elph_g1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -636,6 +654,8 @@ extern "C" int phx_elph_destroy(phx_elph* e) {
   cudaFree(e->d_g);
   cudaFree(e->d_cached);
   cudaFree(e->d_scratch);
+  cudaFree(e->d_gimg);
+  cudaFree(e->d_kimg);
   delete e;
   return PHX_OK;
 }
@@ -843,8 +863,8 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
                                               reinterpret_cast<const double2*>(el->d_U), nw, dkb, dub, dnb);
     ++launches;
     PHX_CUDA(ctx, cudaGetLastError());
-    PHX_TRY(elph_cache_batch(e, nb, dkb, dub, dnb, dg1, dcached));
-    launches += 2;
+    PHX_TRY(elph_cache_batch(e, nb, dkb, dub, dnb, dg1, dcached, split));
+    launches += split ? 3 : 2;
     // the Rp transform of all q and the batch's k1 on the tensor cores (BF16 x3, FP32 accumulation)
     int g3ld = 0;
     std::vector<int> xoff(kB1, 0);

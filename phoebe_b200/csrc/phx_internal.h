@@ -127,7 +127,9 @@ struct phx_elph {
   float* d_g = nullptr;       // (nRe,nRp,nph,nw,nw) complex FP32 coupling in the Wannier basis
   double* d_cached = nullptr; // (nRp,nph,nw,nw) complex: cacheElPh of the last k1 (b1 < nb1)
   int nb1 = 0;                // bands of the cached k1
-  int precision = PHX_PREC_FP64;  // of the Rp transform in phx_el_linewidths
+  int precision = PHX_PREC_FP64;  // of the Re and Rp transforms in phx_el_linewidths
+  uint8_t* d_gimg = nullptr;  // split path: BF16 hi/lo tile image of g (built on first use)
+  uint8_t* d_kimg = nullptr;  // split path: phase image of a k1 batch
   void* d_scratch = nullptr;  // builder scratch (grown on demand)
   size_t scratch_bytes = 0;
 };

@@ -113,6 +113,9 @@ struct PairSmem {
   double* E3;     // [kQT][nph]
   double* acc;    // [kMaxW][kMaxT] block sums of the rates
   int* info;      // [kQT][4]: valid, nb2, k2 index, q index
+  double* f2;     // [kQT][kMaxW][kMaxT] Fermi occupation of the final electron states
+  double* n3;     // [kQT][kMaxPh][kMaxT] Bose occupation of the phonons
+  double2* wd;    // [kQT][kMaxW(b1)][kMaxW(b2)] adaptive width: (sigma, |v1 - v2| == 0)
 };
 
 __host__ __device__ inline size_t pair_smem_layout(int nRp, int nph, int nw, size_t* off) {
@@ -123,20 +126,25 @@ __host__ __device__ inline size_t pair_smem_layout(int nRp, int nph, int nw, siz
     return r;
   };
   off[0] = take(sizeof(double2) * kQT * nRp);
-  off[1] = take(sizeof(double2) * kQT * nph * kMaxW * nw);
+  // |g|^2 (cs) is written after g4 is complete, when g3 is dead: it shares g3's space
+  const size_t g3b = sizeof(double2) * kQT * nph * kMaxW * nw, csb = sizeof(double) * kQT * kMaxW * kMaxW * nph;
+  off[1] = take(g3b > csb ? g3b : csb);
   off[2] = take(sizeof(double2) * kQT * nph * kMaxW * nw);
   off[3] = take(sizeof(double2) * kQT * nw * kMaxW);
   off[4] = take(sizeof(double2) * kQT * nph * nph);
-  off[5] = take(sizeof(double) * kQT * kMaxW * kMaxW * nph);
+  off[5] = off[1];
   off[6] = take(sizeof(double) * kQT * kMaxW);
   off[7] = take(sizeof(double) * kQT * nph);
   off[8] = take(sizeof(double) * kMaxW * pairc::kMaxT);
   off[9] = take(sizeof(int) * kQT * 4);
+  off[10] = take(sizeof(double) * kQT * kMaxW * pairc::kMaxT);
+  off[11] = take(sizeof(double) * kQT * kMaxPh * pairc::kMaxT);
+  off[12] = take(sizeof(double2) * kQT * kMaxW * kMaxW);
   return o;
 }
 
 __device__ inline PairSmem pair_carve(char* base, int nRp, int nph, int nw) {
-  size_t off[10];
+  size_t off[13];
   pair_smem_layout(nRp, nph, nw, off);
   PairSmem s;
   s.ph = reinterpret_cast<double2*>(base + off[0]);
@@ -149,6 +157,9 @@ __device__ inline PairSmem pair_carve(char* base, int nRp, int nph, int nw) {
   s.E3 = reinterpret_cast<double*>(base + off[7]);
   s.acc = reinterpret_cast<double*>(base + off[8]);
   s.info = reinterpret_cast<int*>(base + off[9]);
+  s.f2 = reinterpret_cast<double*>(base + off[10]);
+  s.n3 = reinterpret_cast<double*>(base + off[11]);
+  s.wd = reinterpret_cast<double2*>(base + off[12]);
   return s;
 }
 
@@ -219,60 +230,78 @@ __device__ void pair_symmetrize(const double* E1, int nb1, int nph, const PairSm
   auto C = [&](int q, int b1, int b2, int nu) -> double& {
     return s.cs[((q * kMaxW + b1) * kMaxW + b2) * nph + nu];
   };
-  for (int x = tid; x < kQT * kMaxW * nph; x += NT) {
-    const int q = x / (kMaxW * nph), b2 = (x / nph) % kMaxW, nu = x % nph;
-    if (!s.info[4 * q] || b2 >= s.info[4 * q + 1]) continue;
-    for (int ib = 0; ib < nb1;) {
-      int deg = 0;
-      for (int i = ib; i < nb1; ++i) {
-        if (fabs(E1[ib] - E1[i]) < 1.0e-6) ++deg;
-        else break;
+  // A forward-scan block of two or more states exists exactly when two
+  // neighbouring energies are within the threshold; a pass without one is
+  // the identity and is skipped (block-wide votes, which are also barriers).
+  const bool n1 = tid + 1 < nb1 && fabs(E1[tid] - E1[tid + 1]) < 1.0e-6;
+  bool n2 = false, n3 = false;
+  if (tid < kQT * kMaxW) {
+    const int q = tid / kMaxW, b = tid % kMaxW;
+    n2 = s.info[4 * q] && b + 1 < s.info[4 * q + 1] && fabs(s.E2[q * kMaxW + b] - s.E2[q * kMaxW + b + 1]) < 1.0e-6;
+  }
+  if (tid < kQT * nph) {
+    const int q = tid / nph, nu = tid % nph;
+    n3 = s.info[4 * q] && nu + 1 < nph && fabs(s.E3[q * nph + nu] - s.E3[q * nph + nu + 1]) < 1.0e-6;
+  }
+  if (!__syncthreads_or(n1 || n2 || n3)) return;
+  if (__syncthreads_or(n1)) {
+    for (int x = tid; x < kQT * kMaxW * nph; x += NT) {
+      const int q = x / (kMaxW * nph), b2 = (x / nph) % kMaxW, nu = x % nph;
+      if (!s.info[4 * q] || b2 >= s.info[4 * q + 1]) continue;
+      for (int ib = 0; ib < nb1;) {
+        int deg = 0;
+        for (int i = ib; i < nb1; ++i) {
+          if (fabs(E1[ib] - E1[i]) < 1.0e-6) ++deg;
+          else break;
+        }
+        if (deg > 1) {
+          double t = 0.0;
+          for (int i = 0; i < deg; ++i) t += C(q, ib + i, b2, nu);
+          for (int i = 0; i < deg; ++i) C(q, ib + i, b2, nu) = t / float(deg);
+        }
+        ib += deg;
       }
-      if (deg > 1) {
-        double t = 0.0;
-        for (int i = 0; i < deg; ++i) t += C(q, ib + i, b2, nu);
-        for (int i = 0; i < deg; ++i) C(q, ib + i, b2, nu) = t / float(deg);
-      }
-      ib += deg;
     }
   }
-  __syncthreads();
-  for (int x = tid; x < kQT * kMaxW * nph; x += NT) {
-    const int q = x / (kMaxW * nph), b1 = (x / nph) % kMaxW, nu = x % nph;
-    const int nb2 = s.info[4 * q + 1];
-    if (!s.info[4 * q] || b1 >= nb1) continue;
-    const double* E2 = s.E2 + q * kMaxW;
-    for (int ib = 0; ib < nb2;) {
-      int deg = 0;
-      for (int i = ib; i < nb2; ++i) {
-        if (fabs(E2[ib] - E2[i]) < 1.0e-6) ++deg;
-        else break;
+  if (__syncthreads_or(n2)) {
+    for (int x = tid; x < kQT * kMaxW * nph; x += NT) {
+      const int q = x / (kMaxW * nph), b1 = (x / nph) % kMaxW, nu = x % nph;
+      const int nb2 = s.info[4 * q + 1];
+      if (!s.info[4 * q] || b1 >= nb1) continue;
+      const double* E2 = s.E2 + q * kMaxW;
+      for (int ib = 0; ib < nb2;) {
+        int deg = 0;
+        for (int i = ib; i < nb2; ++i) {
+          if (fabs(E2[ib] - E2[i]) < 1.0e-6) ++deg;
+          else break;
+        }
+        if (deg > 1) {
+          double t = 0.0;
+          for (int i = 0; i < deg; ++i) t += C(q, b1, ib + i, nu);
+          for (int i = 0; i < deg; ++i) C(q, b1, ib + i, nu) = t / float(deg);
+        }
+        ib += deg;
       }
-      if (deg > 1) {
-        double t = 0.0;
-        for (int i = 0; i < deg; ++i) t += C(q, b1, ib + i, nu);
-        for (int i = 0; i < deg; ++i) C(q, b1, ib + i, nu) = t / float(deg);
-      }
-      ib += deg;
     }
   }
-  __syncthreads();
-  for (int x = tid; x < kQT * kMaxW * kMaxW; x += NT) {
-    const int q = x / (kMaxW * kMaxW), b1 = (x / kMaxW) % kMaxW, b2 = x % kMaxW;
-    if (!s.info[4 * q] || b1 >= nb1 || b2 >= s.info[4 * q + 1]) continue;
-    const double* E3 = s.E3 + q * nph;
-    for (int ib = 0; ib < nph;) {
-      int deg = 0;
-      for (int i = ib; i < nph; ++i) {
-        if (fabs(E3[ib] - E3[i]) < 1.0e-6) ++deg;
-        else break;
+  if (__syncthreads_or(n3)) {
+    for (int x = tid; x < kQT * kMaxW * kMaxW; x += NT) {
+      const int q = x / (kMaxW * kMaxW), b1 = (x / kMaxW) % kMaxW, b2 = x % kMaxW;
+      if (!s.info[4 * q] || b1 >= nb1 || b2 >= s.info[4 * q + 1]) continue;
+      const double* E3 = s.E3 + q * nph;
+      for (int ib = 0; ib < nph;) {
+        int deg = 0;
+        for (int i = ib; i < nph; ++i) {
+          if (fabs(E3[ib] - E3[i]) < 1.0e-6) ++deg;
+          else break;
+        }
+        if (deg > 1) {
+          double t = 0.0;
+          for (int i = 0; i < deg; ++i) t += C(q, b1, b2, ib + i);
+          for (int i = 0; i < deg; ++i) C(q, b1, b2, ib + i) = t / float(deg);
+        }
+        ib += deg;
       }
-      if (deg > 1) {
-        double t = 0.0;
-        for (int i = 0; i < deg; ++i) t += C(q, b1, b2, ib + i);
-        for (int i = 0; i < deg; ++i) C(q, b1, b2, ib + i) = t / float(deg);
-      }
-      ib += deg;
     }
   }
   __syncthreads();
@@ -308,22 +337,34 @@ struct ElArgs {
   int g3ld;
 };
 
-__device__ __forceinline__ double el_delta(const ElArgs& A, double e, const double v[3]) {
-  if (A.smearing == PHX_SMEAR_GAUSSIAN) {
-    const double x = e / A.sigma;
-    if (x > 6.0) return 0.0;
-    return 1.0 / A.sigma / phxc::sqrtPi * exp(-x * x);
-  }
-  // delta_function.cpp:65-96
-  const double vn = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-  if (vn == 0.0 && e == 0.0) return 1.0;
+// adaptive width of a (k1 b1, k2 b2) pair from v = v1 - v2 (delta_function.cpp:65-88);
+// vzero: |v| == 0
+struct ElWidth {
+  double sg;
+  bool vzero;
+};
+__device__ __forceinline__ ElWidth el_width(const ElArgs& A, const double v[3]) {
+  ElWidth w;
+  w.vzero = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) == 0.0;
   double s = 0.0;
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     const double d = A.qT[3 * i] * v[0] + A.qT[3 * i + 1] * v[1] + A.qT[3 * i + 2] * v[2];
     s += d * d;
   }
-  double sg = sqrt(s / 6.0);
+  w.sg = sqrt(s / 6.0);
+  return w;
+}
+
+__device__ __forceinline__ double el_delta(const ElArgs& A, double e, const ElWidth& w) {
+  if (A.smearing == PHX_SMEAR_GAUSSIAN) {
+    const double x = e / A.sigma;
+    if (x > 6.0) return 0.0;
+    return 1.0 / A.sigma / phxc::sqrtPi * exp(-x * x);
+  }
+  // delta_function.cpp:65-96
+  if (w.vzero && e == 0.0) return 1.0;
+  double sg = w.sg;
   if (sg == 0.0) return 0.0;
   if (sg < phxc::adaptiveCutoff) sg = phxc::adaptiveCutoff;
   if (fabs(e) > 2.0 * sg) return 0.0;
@@ -401,40 +442,85 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
     const int q = i / nph;
     s.E3[i] = s.info[4 * q] ? A.Eq[(size_t)s.info[4 * q + 3] * nph + i % nph] : 0.0;
   }
+  // populations of the final states (el_scattering.cpp:287-300)
+  for (int i = tid; i < kQT * kMaxW * A.nT; i += NT) {
+    const int t = i % A.nT, b2 = (i / A.nT) % kMaxW, q = i / (A.nT * kMaxW);
+    double f = 0.0;
+    if (s.info[4 * q] && b2 < s.info[4 * q + 1]) {
+      const double T = A.temps[t];
+      const int ik2 = s.info[4 * q + 2];
+      const double en2 = A.Ek[(size_t)ik2 * nw + A.lo[ik2] + b2];
+      if (T <= 0.0) {
+        f = en2 <= A.mu ? 1.0 : 0.0;
+      } else {
+        f = 1.0 / (exp((en2 - A.mu) / T) + 1.0);
+        f = fmin(1.0, fmax(0.0, f));
+      }
+    }
+    s.f2[(q * kMaxW + b2) * pairc::kMaxT + t] = f;
+  }
+  for (int i = tid; i < kQT * nph * A.nT; i += NT) {
+    const int t = i % A.nT, nu = (i / A.nT) % nph, q = i / (A.nT * nph);
+    double n = 0.0;
+    const double T = A.temps[t];
+    if (s.info[4 * q] && T > 0.0) {
+      n = 1.0 / (exp(A.Eq[(size_t)s.info[4 * q + 3] * nph + nu] / T) - 1.0);
+      if (n < 0.0) n = 0.0;
+    }
+    s.n3[(q * kMaxPh + nu) * pairc::kMaxT + t] = n;
+  }
+  // adaptive widths of the (b1, b2) pairs (delta_function.cpp:65-88)
+  for (int x = tid; x < (A.smearing == PHX_SMEAR_ADAPTIVE ? kQT * kMaxW * kMaxW : 0); x += NT) {
+    const int b2 = x % kMaxW, b1 = (x / kMaxW) % kMaxW, q = x / (kMaxW * kMaxW);
+    double2 wv = make_double2(0.0, 0.0);
+    if (s.info[4 * q] && b1 < nb1 && b2 < s.info[4 * q + 1]) {
+      const int ik2 = s.info[4 * q + 2];
+      double v[3];
+      for (int c = 0; c < 3; ++c)
+        v[c] = A.vk[((size_t)ik1 * nw + lo1 + b1) * 3 + c] - A.vk[((size_t)ik2 * nw + A.lo[ik2] + b2) * 3 + c];
+      const ElWidth w = el_width(A, v);
+      wv = make_double2(w.sg, w.vzero ? 1.0 : 0.0);
+    }
+    s.wd[x] = wv;
+  }
   __syncthreads();
   pair_couplings(cached, nRp, nph, nw, nb1, s, g3in, A.g3ld);
   pair_symmetrize(E1, nb1, nph, s);
-  // rates (el_scattering.cpp:268-327)
-  for (int x = tid; x < kQT * nb1 * kMaxW * nph; x += NT) {
-    const int nu = x % nph, b2 = (x / nph) % kMaxW, b1 = (x / (nph * kMaxW)) % nb1, q = x / (nph * kMaxW * nb1);
-    if (!s.info[4 * q] || b2 >= s.info[4 * q + 1]) continue;
+  // rates (el_scattering.cpp:268-327), one thread per (b1, q, b2, nu) with b1
+  // slowest: the kQT * kMaxW * nph entries of one b1 fill whole warps, so a
+  // warp reduces its rates and adds them once
+  const int per_b1 = kQT * kMaxW * nph;
+  for (int x = tid; x < nb1 * per_b1; x += NT) {
+    const int nu = x % nph, b2 = (x / nph) % kMaxW, q = (x / (nph * kMaxW)) % kQT, b1 = x / per_b1;
+    double r[pairc::kMaxT];
+#pragma unroll
+    for (int t = 0; t < pairc::kMaxT; ++t) r[t] = 0.0;
     const double en3 = s.E3[q * nph + nu];
-    if (en3 < phxc::elPhononCutoff) continue;
-    const double en1 = E1[b1], en2 = s.E2[q * kMaxW + b2];
-    double v[3] = {0.0, 0.0, 0.0};
-    if (A.smearing == PHX_SMEAR_ADAPTIVE) {
-      const int ik2 = s.info[4 * q + 2];
-      for (int c = 0; c < 3; ++c)
-        v[c] = A.vk[((size_t)ik1 * nw + lo1 + b1) * 3 + c] - A.vk[((size_t)ik2 * nw + A.lo[ik2] + b2) * 3 + c];
-    }
-    const double d1 = el_delta(A, en1 - en2 + en3, v);
-    const double d2 = el_delta(A, en1 - en2 - en3, v);
-    if (d1 <= 0.0 && d2 <= 0.0) continue;
-    const double c = s.cs[((q * kMaxW + b1) * kMaxW + b2) * nph + nu];
-    for (int t = 0; t < A.nT; ++t) {
-      const double T = A.temps[t];
-      double fermi2, bose3;
-      if (T <= 0.0) {
-        fermi2 = en2 <= A.mu ? 1.0 : 0.0;
-        bose3 = 0.0;
-      } else {
-        fermi2 = 1.0 / (exp((en2 - A.mu) / T) + 1.0);
-        fermi2 = fmin(1.0, fmax(0.0, fermi2));
-        bose3 = 1.0 / (exp(en3 / T) - 1.0);
-        if (bose3 < 0.0) bose3 = 0.0;
+    if (s.info[4 * q] && b2 < s.info[4 * q + 1] && en3 >= phxc::elPhononCutoff) {
+      const double en1 = E1[b1], en2 = s.E2[q * kMaxW + b2];
+      const double2 wv = s.wd[(q * kMaxW + b1) * kMaxW + b2];
+      const ElWidth w{wv.x, wv.y != 0.0};
+      const double d1 = el_delta(A, en1 - en2 + en3, w);
+      const double d2 = el_delta(A, en1 - en2 - en3, w);
+      if (d1 > 0.0 || d2 > 0.0) {
+        const double c = s.cs[((q * kMaxW + b1) * kMaxW + b2) * nph + nu];
+#pragma unroll
+        for (int t = 0; t < pairc::kMaxT; ++t) {
+          if (t < A.nT) {
+            const double fermi2 = s.f2[(q * kMaxW + b2) * pairc::kMaxT + t];
+            const double bose3 = s.n3[(q * kMaxPh + nu) * pairc::kMaxT + t];
+            r[t] = c * ((fermi2 + bose3) * d1 + (1.0 - fermi2 + bose3) * d2) * A.norm / en3 * phxc::pi;
+          }
+        }
       }
-      const double rate = c * ((fermi2 + bose3) * d1 + (1.0 - fermi2 + bose3) * d2) * A.norm / en3 * phxc::pi;
-      atomicAdd(&s.acc[b1 * pairc::kMaxT + t], rate);
+    }
+#pragma unroll
+    for (int t = 0; t < pairc::kMaxT; ++t) {
+      if (t < A.nT) {
+        double v = r[t];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((tid & 31) == 0 && v != 0.0) atomicAdd(&s.acc[b1 * pairc::kMaxT + t], v);
+      }
     }
   }
   __syncthreads();
@@ -605,7 +691,7 @@ int elph_cache_batch(phx_elph* e, int nb, const double* d_k1s, const double2* d_
 }
 
 size_t pair_smem(const phx_elph* e) {
-  size_t off[10];
+  size_t off[13];
   return pair_smem_layout(e->nRp, e->nph, e->nw, off);
 }
 
@@ -845,7 +931,7 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
     PHX_TRY(phx_el_split_phases(ctx, ph->nq, ph->d_q, e->nRp, e->d_Rp, e->d_degP, dAimg));
     ++launches;
   }
-  size_t soff[10];
+  size_t soff[13];
   const size_t smem = pair_smem_layout(split ? 0 : e->nRp, nph, nw, soff);
   PHX_ARG(ctx, smem <= 227 * 1024, "phx_el_linewidths: too many phonon Bravais vectors");
   PHX_CUDA(ctx, cudaFuncSetAttribute(el_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

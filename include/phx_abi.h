@@ -232,9 +232,13 @@ int phx_elph_cache_k1(phx_elph* e, const double* k1, const double* U1, int nb1);
 int phx_elph_couplings_sq(phx_elph* e, int nk2, const double* q3, const double* U2s, const int* nb2s,
                           int nb2max, const double* ev3s, double* coupling);
 
-/* Precision of the Rp transform inside phx_el_linewidths: PHX_PREC_FP64 (default)
- * or PHX_PREC_SPLIT_BF16 (tcgen05 BF16 hi+lo, FP32 accumulation; needs 6 phonon
- * branches and 8 Wannier functions).  The rotations, |g|^2 and rates stay FP64. */
+/* Precision of the Re and Rp transforms inside phx_el_linewidths (the first steps
+ * of cacheElPh and calcCouplingSquared, interaction_elph.cpp:540-580,364-374):
+ * PHX_PREC_FP64 (default) or PHX_PREC_SPLIT_BF16 (tcgen05 BF16 hi+lo; the Re
+ * transform adds its 64-deep chunk sums in FP64, the Rp transform accumulates in
+ * FP32).  The U1 rotation, the phonon and U2 rotations, |g|^2 and the rates stay
+ * FP64.  The first split call builds a BF16 image of the coupling tensor (as large
+ * as the FP32 tensor), kept until phx_elph_destroy. */
 int phx_elph_set_precision(phx_elph* e, int precision);
 
 typedef struct phx_el_params {

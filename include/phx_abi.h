@@ -141,6 +141,12 @@ typedef struct phx_lw_params {
   double sigma;               /* Gaussian width (Ry) */
   int finalize;               /* 1: degeneracy-average row 0, zero excluded states */
   int q2_begin, q2_end;       /* q2 range to process ([0, nq) for the full builder) */
+  /* Optional per-q1 window on q2 (no counterpart in the reference; uneven
+   * work of the batched-instance workload): the pair (q1, q2) is counted only
+   * when window_energy[q2] <= window_cut[q1].  Host arrays (nq), or both NULL
+   * for every pair.  Runs on the FP64 path. */
+  const double* window_energy;
+  const double* window_cut;
 } phx_lw_params;
 
 typedef struct phx_lw_stats {
@@ -156,7 +162,9 @@ typedef struct phx_lw_stats {
  * symmetrizeCoupling, cutoffs, Gaussian/adaptive deltas, Bose factors,
  * accumulation, degeneracy averaging (src/bte/ph_scattering.cpp:60-935;
  * src/bte/scattering.cpp:1168-1318).  A_out (nT, nq*nb) host, the reference's
- * internalDiagonal (linewidth * n(n+1)).  stats may be NULL. */
+ * internalDiagonal (linewidth * n(n+1)).  stats may be NULL.  nb = 6 runs on
+ * the fused register-tiled kernels (FP64 or split precision); any nb <= 16, or
+ * a q2 window, runs on the shared-memory FP64 kernel. */
 int phx_ph_linewidths(phx_v3* v3, phx_bands* bands, const phx_lw_params* params,
                       double* A_out, phx_lw_stats* stats);
 /* Same with a device output buffer (nT*nq*nb doubles). */

@@ -288,10 +288,14 @@ void orc_symmetrize_coupling(double* c, int nb1, int nb2, int nb3, const double*
 //   q2_list: which q2 to process (NULL -> all), nq2 its length
 //   out: A_out (nT, nq*nb), accumulated (not zeroed here when accumulate=1)
 //   finalize: 1 -> degeneracy averaging of row 0 and zeroing excluded states
+//   win_energy / win_cut (nq) or NULL: the pair (q1, q2) is skipped unless
+//     win_energy[q2] <= win_cut[q1] (per-q1 window of the batched-instance
+//     workload; no counterpart in the reference)
 int orc_ph_linewidths(void* p, int nq, const int* mesh, const double* E, const double* ev,
                       const double* vg, const double* qcart, const double* recip, int nT,
                       const double* Tk_ry, int smearing, double sigma, int nq2,
-                      const int* q2_list, int finalize, double* out) {
+                      const int* q2_list, int finalize, double* out, const double* win_energy,
+                      const double* win_cut) {
   V3& v = *(V3*)p;
   const int nb = v.nb;
   const size_t ns = (size_t)nq * nb;
@@ -379,6 +383,7 @@ int orc_ph_linewidths(void* p, int nq, const int* mesh, const double* E, const d
     }
     // HOT LOOP 3 (serial in the reference), ph_scattering.cpp:284-613
     for (int iq1 = 0; iq1 < nq; ++iq1) {
+      if (win_energy && !(win_energy[iq2] <= win_cut[iq1])) continue;
       const double* c_p = &cP[iq1 * o];
       const double* c_m = &cM[iq1 * o];
       const int q3p = iq3p[iq1], q3m = iq3m[iq1];

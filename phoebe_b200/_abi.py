@@ -34,7 +34,8 @@ _i = ctypes.c_int
 class LwParams(ctypes.Structure):
     _fields_ = [("num_temperatures", ctypes.c_int), ("temperatures", _D),
                 ("smearing", ctypes.c_int), ("sigma", ctypes.c_double),
-                ("finalize", ctypes.c_int), ("q2_begin", ctypes.c_int), ("q2_end", ctypes.c_int)]
+                ("finalize", ctypes.c_int), ("q2_begin", ctypes.c_int), ("q2_end", ctypes.c_int),
+                ("window_energy", _D), ("window_cut", _D)]
 
 
 class LwStats(ctypes.Structure):

@@ -281,12 +281,15 @@ class Interaction3Ph:
 class PhScatteringMatrix:
     """RTA phonon scattering rates on a full mesh (linewidth mode of the builder)."""
 
-    def __init__(self, coupling3Ph, bands, temperatures_ry, smearing="adaptive", sigma=0.0):
+    def __init__(self, coupling3Ph, bands, temperatures_ry, smearing="adaptive", sigma=0.0, window=None):
+        """window: optional (energy (nq), cut (nq)) per-q1 q2 window: the pair
+        (q1, q2) counts only when energy[q2] <= cut[q1] (synth.q2_window)."""
         self.v3 = coupling3Ph
         self.bands = bands
         self.temperatures = f64(np.atleast_1d(temperatures_ry))
         self.smearing = smearing
         self.sigma = float(sigma)
+        self.window = None if window is None else (f64(window[0]), f64(window[1]))
         self.internalDiagonal = None
         self.stats = None
 
@@ -299,6 +302,9 @@ class PhScatteringMatrix:
         p.finalize = int(finalize)
         p.q2_begin = int(q2_begin)
         p.q2_end = int(self.bands.nq if q2_end is None else q2_end)
+        if self.window is not None:
+            p.window_energy = dptr(self.window[0])
+            p.window_cut = dptr(self.window[1])
         return p
 
     def setup(self, q2_begin=0, q2_end=None, finalize=True):

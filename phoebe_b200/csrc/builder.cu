@@ -455,6 +455,227 @@ __global__ void __launch_bounds__(kTile * NB, 1) pair_fp64_kernel(PairArgs P) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Any nb up to kMaxNbGeneric (the 15-branch cells), with an optional per-q1
+// window on q2: one block per (q1, q2 slot), the R3 transform, the e1 and e3
+// contractions, |V|^2, the three symmetrisation passes and the rates of each
+// q2 run through shared memory (two nb^3 complex buffers).  Same algebra,
+// cutoffs and time-reversal pairing as pair_fp64_kernel: the "+" vertex of
+// (q1, q2) gives the "+" process of (q1, q2) and the "-" process of
+// (q1, -q2); with a window, each of the two is counted only when its q2 is
+// inside the window of q1.
+// ---------------------------------------------------------------------------
+constexpr int kMaxNbGeneric = 16;
+constexpr int kGenThreads = 256;
+
+struct Q2Window {
+  const double* energy;   // (nq) or null: no window
+  const double* cut;      // (nq): q2 is paired with q1 iff energy[q2] <= cut[q1]
+};
+
+__host__ __device__ inline size_t generic_smem_bytes(int nb, int nr3) {
+  const size_t nbb = (size_t)nb * nb, nb3 = nbb * nb;
+  return sizeof(double2) * ((size_t)nr3 + 2 * nbb + 2 * nb3) + sizeof(double) * ((size_t)nb * kMaxT + 3 * nb) +
+         sizeof(int) * 3 * nb;
+}
+
+// forward-scan degenerate blocks (scattering.cpp:1223,1257,1291): gs[b] = start of b's block
+__device__ inline void scan_blocks(const double* e, int nb, int* gs) {
+  int start = 0;
+  for (int b = 0; b < nb; ++b) {
+    if (b > start && !(fabs(e[start] - e[b]) < phxc::degThreshold)) start = b;
+    gs[b] = start;
+  }
+}
+
+__global__ void __launch_bounds__(kGenThreads) pair_generic_kernel(PairArgs P, Q2Window win) {
+  const MeshArgs& M = P.m;
+  extern __shared__ __align__(16) char sraw[];
+  const int nb = M.nb, nbb = nb * nb, nb3 = nbb * nb, nr3 = P.nr3, nT = M.nT, nq = M.nq;
+  double2* ph = reinterpret_cast<double2*>(sraw);   // [nr3]
+  double2* e1 = ph + nr3;                           // [nb][nb]
+  double2* e3 = e1 + nbb;                           // [nb][nb]
+  double2* T = e3 + nbb;                            // [nb^3]: T(a,b2,c), then W(b1,b2,b3) as doubles
+  double2* X = T + nb3;                             // [nb^3]: X(b1,b2,c)
+  double* W = reinterpret_cast<double*>(T);
+  double* acc = reinterpret_cast<double*>(X + nb3); // [nb][kMaxT]
+  double* E1 = acc + nb * kMaxT;
+  double* E2 = E1 + nb;
+  double* E3 = E2 + nb;
+  int* g1s = reinterpret_cast<int*>(E3 + nb);
+  int* g2s = g1s + nb;
+  int* g3s = g2s + nb;
+  const int tid = threadIdx.x, NT = blockDim.x;
+  const int q1 = blockIdx.x;
+  const int n0 = M.n0, n1 = M.n1, n2 = M.n2;
+  for (int r = tid; r < nr3; r += NT) {
+    const double* q = M.qcart + 3 * q1;
+    double sn, cs;
+    sincos(-(q[0] * P.R3[3 * r] + q[1] * P.R3[3 * r + 1] + q[2] * P.R3[3 * r + 2]), &sn, &cs);
+    ph[r] = cmk(cs, sn);
+  }
+  for (int e = tid; e < nbb; e += NT) e1[e] = M.U[(size_t)q1 * nbb + e];
+  for (int i = tid; i < nb * kMaxT; i += NT) acc[i] = 0.0;
+  for (int b = tid; b < nb; b += NT) E1[b] = M.E[(size_t)q1 * nb + b];
+  __syncthreads();
+  if (tid == 0) scan_blocks(E1, nb, g1s);
+  const int jbeg = blockIdx.y * P.q2_per_slot;
+  const int jend = min(P.q2_count, jbeg + P.q2_per_slot);
+  for (int j = jbeg; j < jend; ++j) {
+    const int iq2 = P.q2_first + j;
+    const int iq2m = mesh_neg(iq2, n0, n1, n2);
+    const int iq3 = mesh_add(q1, iq2, n0, n1, n2);
+    const bool inP = !win.energy || win.energy[iq2] <= win.cut[q1];
+    const bool inM = !win.energy || win.energy[iq2m] <= win.cut[q1];
+    if (!inP && !inM) continue;   // uniform over the block
+    for (int e = tid; e < nbb; e += NT) e3[e] = M.U[(size_t)iq3 * nbb + e];
+    for (int b = tid; b < nb; b += NT) {
+      E2[b] = M.E[(size_t)iq2 * nb + b];
+      E3[b] = M.E[(size_t)iq3 * nb + b];
+    }
+    // T(a,b2,c) = sum_r3 e^{-i q1.R3} Dp(q2)[r3][a][b2][c]
+    const double2* D = P.Dp + (size_t)j * nr3 * nb3;
+    for (int x = tid; x < nb3; x += NT) {
+      double2 t = cmk(0.0, 0.0);
+      for (int r = 0; r < nr3; ++r) cfma(t, ph[r], __ldg(D + (size_t)r * nb3 + x));
+      T[x] = t;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      scan_blocks(E2, nb, g2s);
+      scan_blocks(E3, nb, g3s);
+    }
+    // X(b1,b2,c) = sum_a e1(a,b1) T(a,b2,c)
+    for (int x = tid; x < nb3; x += NT) {
+      const int b1 = x / nbb, rest = x % nbb;
+      double2 v = cmk(0.0, 0.0);
+      for (int a = 0; a < nb; ++a) cfma(v, e1[a * nb + b1], T[a * nbb + rest]);
+      X[x] = v;
+    }
+    __syncthreads();
+    // W(b1,b2,b3) = |sum_c X(b1,b2,c) conj(e3(c,b3))|^2
+    for (int x = tid; x < nb3; x += NT) {
+      const int row = x / nb, b3 = x % nb;
+      double2 v = cmk(0.0, 0.0);
+      for (int c = 0; c < nb; ++c) cfmac(v, X[row * nb + c], e3[c * nb + b3]);
+      W[x] = v.x * v.x + v.y * v.y;
+    }
+    __syncthreads();
+    // symmetrizeCoupling (scattering.cpp:1209-1318): average over the blocks of
+    // b3, then b1, then b2 (projections on different indices commute)
+    for (int x = tid; x < nbb; x += NT) {
+      double* w = W + (size_t)x * nb;   // (b1,b2) row over b3
+      for (int s0 = 0; s0 < nb;) {
+        int s1 = s0 + 1;
+        while (s1 < nb && g3s[s1] == s0) ++s1;
+        if (s1 - s0 > 1) {
+          double t = 0.0;
+          for (int k = s0; k < s1; ++k) t += w[k];
+          for (int k = s0; k < s1; ++k) w[k] = t / (double)(s1 - s0);
+        }
+        s0 = s1;
+      }
+    }
+    __syncthreads();
+    for (int x = tid; x < nbb; x += NT) {
+      const int b2 = x / nb, b3 = x % nb;   // column over b1
+      for (int s0 = 0; s0 < nb;) {
+        int s1 = s0 + 1;
+        while (s1 < nb && g1s[s1] == s0) ++s1;
+        if (s1 - s0 > 1) {
+          double t = 0.0;
+          for (int k = s0; k < s1; ++k) t += W[((size_t)k * nb + b2) * nb + b3];
+          for (int k = s0; k < s1; ++k) W[((size_t)k * nb + b2) * nb + b3] = t / (double)(s1 - s0);
+        }
+        s0 = s1;
+      }
+    }
+    __syncthreads();
+    for (int x = tid; x < nbb; x += NT) {
+      const int b1 = x / nb, b3 = x % nb;   // over b2
+      for (int s0 = 0; s0 < nb;) {
+        int s1 = s0 + 1;
+        while (s1 < nb && g2s[s1] == s0) ++s1;
+        if (s1 - s0 > 1) {
+          double t = 0.0;
+          for (int k = s0; k < s1; ++k) t += W[((size_t)b1 * nb + k) * nb + b3];
+          for (int k = s0; k < s1; ++k) W[((size_t)b1 * nb + k) * nb + b3] = t / (double)(s1 - s0);
+        }
+        s0 = s1;
+      }
+    }
+    __syncthreads();
+    // rates: "+" of (q1,q2), "-" of (q1,-q2) (ph_scattering.cpp:338-380, 466-518)
+    for (int x = tid; x < nb3; x += NT) {
+      const int b1 = x / nbb, b2 = (x / nb) % nb, b3 = x % nb;
+      const double en1 = E1[b1], en3 = E3[b3];
+      if (en1 < phxc::phExcludeCutoff || en1 < phxc::phEnergyCutoff || en3 < phxc::phEnergyCutoff) continue;
+      const double en2 = M.E[(size_t)iq2 * nb + b2];
+      const double en2m = M.E[(size_t)iq2m * nb + b2];
+      const bool ok2 = inP && en2 >= phxc::phExcludeCutoff && en2 >= phxc::phEnergyCutoff;
+      const bool ok2m = inM && en2m >= phxc::phExcludeCutoff && en2m >= phxc::phEnergyCutoff;
+      if (!ok2 && !ok2m) continue;
+      double sp = M.sigma, sm = M.sigma;
+      bool vzp = false, vzm = false;
+      if (M.smearing == PHX_SMEAR_ADAPTIVE) {
+        const double* v3 = M.vg + ((size_t)iq3 * nb + b3) * 3;
+        const double* v2 = M.vg + ((size_t)iq2 * nb + b2) * 3;
+        const double* v2m = M.vg + ((size_t)iq2m * nb + b2) * 3;
+        const double dp0 = v2[0] - v3[0], dp1 = v2[1] - v3[1], dp2 = v2[2] - v3[2];
+        const double dm0 = v2m[0] - v3[0], dm1 = v2m[1] - v3[1], dm2 = v2m[2] - v3[2];
+        vzp = (dp0 * dp0 + dp1 * dp1 + dp2 * dp2) == 0.0;
+        vzm = (dm0 * dm0 + dm1 * dm1 + dm2 * dm2) == 0.0;
+        sp = floor_sigma(adaptive_sigma(M.qT, dp0, dp1, dp2));
+        sm = floor_sigma(adaptive_sigma(M.qT, dm0, dm1, dm2));
+      }
+      const double w = W[x];
+      double r[kMaxT];
+#pragma unroll
+      for (int c = 0; c < kMaxT; ++c) r[c] = 0.0;
+      if (ok2) {
+        const double dlt = delta_fn(M.smearing, sp, en1 + en2 - en3, vzp);
+        if (dlt > 0.0) {
+          const double f = phxc::pi * 0.25 * w * dlt * M.norm / (en1 * en2 * en3);
+#pragma unroll
+          for (int c = 0; c < kMaxT; ++c)
+            if (c < nT) {
+              const double n1 = M.bose[((size_t)c * nq + q1) * nb + b1];
+              const double n2 = M.bose[((size_t)c * nq + iq2) * nb + b2];
+              const double n3 = M.bose[((size_t)c * nq + iq3) * nb + b3];
+              r[c] += 0.5 * (f * n1 * n2 * (n3 + 1.0));
+            }
+        }
+      }
+      if (ok2m) {
+        double d1 = delta_fn(M.smearing, sm, en1 + en3 - en2m, vzm);
+        double d2 = delta_fn(M.smearing, sm, en2m + en3 - en1, vzm);
+        if (d1 > 0.0 || d2 > 0.0) {
+          d1 = fmax(d1, 0.0);
+          d2 = fmax(d2, 0.0);
+          const double f = phxc::pi * 0.25 * w * M.norm / (en1 * en2m * en3);
+#pragma unroll
+          for (int c = 0; c < kMaxT; ++c)
+            if (c < nT) {
+              const double n1 = M.bose[((size_t)c * nq + q1) * nb + b1];
+              const double n2m = M.bose[((size_t)c * nq + iq2m) * nb + b2];
+              const double n3 = M.bose[((size_t)c * nq + iq3) * nb + b3];
+              r[c] += 0.5 * (f * n3 * n1 * (n2m + 1.0) * d1 + f * n2m * n3 * (n1 + 1.0) * d2);
+            }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < kMaxT; ++c)
+        if (c < nT && r[c] != 0.0) atomicAdd(&acc[b1 * kMaxT + c], r[c]);
+    }
+    __syncthreads();
+  }
+  double* out = P.partial + ((size_t)blockIdx.y * nq + q1) * nb * nT;
+  for (int i = tid; i < nb * nT; i += NT) {
+    const int b1 = i / nT, c = i % nT;
+    out[i] += acc[b1 * kMaxT + c];
+  }
+}
+
 __global__ void finalize_kernel(int nq, int nb, int nT, int nslots, const double* __restrict__ partial,
                                 const double* __restrict__ E, int finalize,
                                 double* __restrict__ Aout) {
@@ -807,6 +1028,123 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   return PHX_OK;
 }
 
+// Builder for any nb <= kMaxNbGeneric, or with a per-q1 q2 window, FP64:
+// fold_q2_kernel (one q2 slab of the cached vertex) + pair_generic_kernel.
+int run_builder_generic(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d, phx_lw_stats* stats) {
+  phx_ctx* ctx = v->ctx;
+  cudaStream_t st = ctx->stream;
+  const int nq = b->nq, nb = b->nb, nT = p->num_temperatures, nr3 = v->nr3, nr2 = v->nr2;
+  const int q2b = p->q2_begin, q2e = p->q2_end;
+  PHX_ARG(ctx, nb <= kMaxNbGeneric, "phx_ph_linewidths: at most 16 branches");
+  const bool windowed = p->window_energy != nullptr;
+  PHX_ARG(ctx, !windowed || p->window_cut, "phx_ph_linewidths: window_energy without window_cut");
+  const size_t smem_pair = generic_smem_bytes(nb, nr3);
+  PHX_ARG(ctx, smem_pair <= 227 * 1024, "phx_ph_linewidths: too many R3 vectors for this band count");
+  const size_t smem_fold = sizeof(double2) * ((size_t)nr2 + 2 * (size_t)nb * nb);
+  PHX_ARG(ctx, smem_fold <= 227 * 1024, "phx_ph_linewidths: too many R2 vectors");
+  const size_t nb3 = (size_t)nb * nb * nb, per_q2 = sizeof(double2) * nr3 * nb3;
+  // q2 per cached-vertex slab: at most 512 MB of it, at most 512 q2
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>({(size_t)512, (size_t)(q2e - q2b),
+                                                                (size_t(512) << 20) / std::max<size_t>(per_q2, 1)}));
+  // enough (q1, slot) blocks to fill the GPU several times over
+  const int slots = std::max(1, std::min(chunk, (4 * ctx->num_sms + nq - 1) / nq));
+  const size_t sz_dp = align_up(per_q2 * chunk);
+  const size_t sz_part = align_up(sizeof(double) * slots * nq * nb * nT);
+  const size_t sz_bose = align_up(sizeof(double) * nT * nq * nb);
+  const size_t sz_T = align_up(sizeof(double) * 8);
+  const size_t sz_win = windowed ? align_up(sizeof(double) * 2 * nq) : 0;
+  PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_win));
+  char* base = static_cast<char*>(v->ctx->d_scratch);
+  double2* Dp = reinterpret_cast<double2*>(base);
+  double* partial = reinterpret_cast<double*>(base + sz_dp);
+  double* bose = reinterpret_cast<double*>(base + sz_dp + sz_part);
+  double* temps = reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose);
+  double* wdev = reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose + sz_T);
+  cudaEvent_t ev0, ev1, evv0, evv1;
+  PHX_CUDA(ctx, cudaEventCreate(&ev0));
+  PHX_CUDA(ctx, cudaEventCreate(&ev1));
+  PHX_CUDA(ctx, cudaEventCreate(&evv0));
+  PHX_CUDA(ctx, cudaEventCreate(&evv1));
+  int launches = 0;
+  PHX_CUDA(ctx, cudaEventRecord(ev0, st));
+  PHX_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
+  PHX_CUDA(ctx, cudaMemcpyAsync(temps, p->temperatures, sizeof(double) * nT, cudaMemcpyHostToDevice, st));
+  if (windowed) {
+    PHX_CUDA(ctx, cudaMemcpyAsync(wdev, p->window_energy, sizeof(double) * nq, cudaMemcpyHostToDevice, st));
+    PHX_CUDA(ctx, cudaMemcpyAsync(wdev + nq, p->window_cut, sizeof(double) * nq, cudaMemcpyHostToDevice, st));
+  }
+  PHX_CUDA(ctx, cudaMemsetAsync(partial, 0, sizeof(double) * slots * nq * nb * nT, st));
+  bose_kernel<<<std::min(1024, (nq * nb * nT + 255) / 256), 256, 0, st>>>(nq, nb, nT, b->d_E, temps, bose);
+  ++launches;
+  PairArgs P;
+  P.m.nq = nq;
+  P.m.nb = nb;
+  P.m.nT = nT;
+  P.m.n0 = b->mesh[0];
+  P.m.n1 = b->mesh[1];
+  P.m.n2 = b->mesh[2];
+  P.m.E = b->d_E;
+  P.m.U = reinterpret_cast<const double2*>(b->d_U);
+  P.m.vg = b->d_vg;
+  P.m.bose = bose;
+  P.m.qcart = b->d_q;
+  P.m.smearing = p->smearing;
+  P.m.sigma = p->sigma;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) P.m.qT[i * 3 + j] = b->recip[i * 3 + j] / b->mesh[i];
+  P.m.norm = 1.0 / (double)nq;
+  P.nr3 = nr3;
+  P.R3 = v->d_R3;
+  P.Dp = Dp;
+  P.partial = partial;
+  Q2Window W{windowed ? wdev : nullptr, windowed ? wdev + nq : nullptr};
+  if (smem_pair > 48 * 1024)
+    PHX_CUDA(ctx, cudaFuncSetAttribute(pair_generic_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_pair));
+  if (smem_fold > 48 * 1024)
+    PHX_CUDA(ctx, cudaFuncSetAttribute(fold_q2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fold));
+  PHX_CUDA(ctx, cudaEventRecord(evv0, st));
+  long long pairs = 0;
+  for (int c0 = q2b; c0 < q2e; c0 += chunk) {
+    const int cnt = std::min(chunk, q2e - c0);
+    const int per_block = 8;
+    fold_q2_kernel<<<dim3(nr3, (cnt + per_block - 1) / per_block), 128, smem_fold, st>>>(
+        nb, nr2, nr3, v->d_D3w, v->d_R2, v->d_R3, b->d_q, reinterpret_cast<const double2*>(b->d_U), c0, cnt,
+        per_block, Dp);
+    ++launches;
+    PHX_CUDA(ctx, cudaGetLastError());
+    P.q2_first = c0;
+    P.q2_count = cnt;
+    P.q2_per_slot = (cnt + slots - 1) / slots;
+    pair_generic_kernel<<<dim3(nq, slots), kGenThreads, smem_pair, st>>>(P, W);
+    ++launches;
+    PHX_CUDA(ctx, cudaGetLastError());
+    pairs += (long long)nq * cnt;
+  }
+  PHX_CUDA(ctx, cudaEventRecord(evv1, st));
+  finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, nb, nT, slots, partial, b->d_E, p->finalize, Aout_d);
+  ++launches;
+  PHX_CUDA(ctx, cudaGetLastError());
+  PHX_CUDA(ctx, cudaEventRecord(ev1, st));
+  PHX_CUDA(ctx, cudaEventSynchronize(ev1));
+  if (stats) {
+    float ms = 0, msv = 0;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventElapsedTime(&msv, evv0, evv1);
+    stats->ms_total = ms;
+    stats->ms_vertex = msv;
+    stats->pairs = pairs;
+    stats->kernel_launches = launches;
+    stats->pair_launches = 0;
+    stats->ms_pair = 0.0;
+  }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  cudaEventDestroy(evv0);
+  cudaEventDestroy(evv1);
+  return PHX_OK;
+}
+
 }  // namespace
 
 extern "C" int phx_ph_linewidths_d(phx_v3* v, phx_bands* b, const phx_lw_params* p,
@@ -826,13 +1164,8 @@ extern "C" int phx_ph_linewidths_d(phx_v3* v, phx_bands* b, const phx_lw_params*
     PHX_CUDA(ctx, cudaMemsetAsync(Aout_d, 0, sizeof(double) * p->num_temperatures * b->nq * b->nb, ctx->stream));
     return PHX_OK;
   }
-  switch (v->nb) {
-    case 6:
-      return run_builder<6>(v, b, p, Aout_d, stats);
-    default:
-      phx_set_error(ctx, PHX_ERR_ARG, "phx_ph_linewidths: this build supports nb = 6 on the fused path");
-      return PHX_ERR_ARG;
-  }
+  if (v->nb == 6 && !p->window_energy) return run_builder<6>(v, b, p, Aout_d, stats);
+  return run_builder_generic(v, b, p, Aout_d, stats);
 }
 
 extern "C" int phx_ph_linewidths(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout,
@@ -1013,6 +1346,7 @@ extern "C" int phx_ph_linewidths_static(phx_v3* v, phx_bands* b, const phx_lw_pa
   PHX_ARG(ctx, p->smearing != PHX_SMEAR_ADAPTIVE || b->d_vg, "adaptive smearing needs velocities");
   PHX_ARG(ctx, 0 <= p->q2_begin && p->q2_begin <= p->q2_end && p->q2_end <= b->nq, "bad q2 range");
   PHX_ARG(ctx, v->nb == 6, "phx_ph_linewidths_static: this build supports nb = 6");
+  PHX_ARG(ctx, !p->window_energy && !p->window_cut, "phx_ph_linewidths_static: no q2 window");
   PHX_CUDA(ctx, cudaSetDevice(ctx->device));
   if (p->q2_begin == p->q2_end) {
     PHX_CUDA(ctx, cudaMemsetAsync(Aout_d, 0, sizeof(double) * p->num_temperatures * b->nq * b->nb, ctx->stream));

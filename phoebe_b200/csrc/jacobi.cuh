@@ -4,6 +4,7 @@
 // n/2 disjoint complex rotations per step), FP64, bounded by a sweep cap.
 #pragma once
 #include <cmath>
+#include <cstdint>
 
 #include "cplx.cuh"
 
@@ -42,7 +43,9 @@ __device__ __forceinline__ Smem carve(char* base, int nb, int NT) {
   s.E1 = d + nb;
   s.VG = d + 2 * nb;
   s.red = d + 3 * nb;
-  Rot* r = reinterpret_cast<Rot*>(s.red + NT);
+  // Rot holds a double2: round up to 16 bytes (3 nb + NT doubles need not be)
+  const uintptr_t ra = (reinterpret_cast<uintptr_t>(s.red + NT) + 15) & ~uintptr_t(15);
+  Rot* r = reinterpret_cast<Rot*>(ra);
   s.rot = r;
   s.perm = reinterpret_cast<int*>(r + (nb / 2 + 1));
   return s;
@@ -50,6 +53,7 @@ __device__ __forceinline__ Smem carve(char* base, int nb, int NT) {
 
 inline size_t smem_bytes(int nb, int NT) {
   size_t m = (size_t)nb * nb;
+  // + 64: the 16-byte alignment of the Rot array (at most 8 bytes) and slack
   return sizeof(double2) * (5 * m + kPhaseChunk) + sizeof(double) * (3 * nb + NT) +
          sizeof(Rot) * (nb / 2 + 1) + sizeof(int) * nb + 64;
 }

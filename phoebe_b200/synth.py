@@ -205,27 +205,38 @@ def random_fc3(crystal, num_pairs, seed, amp_ev=3.0, decay_ang=4.0,
     vecs = [v for v in itertools.product(range(-nmax, nmax + 1), repeat=3)]
     length = {v: np.linalg.norm(A @ np.array(v, dtype=np.float64)) for v in vecs}
     vecset = set(vecs)
-    # candidate orbits with all three vectors short
-    orbits = {}
-    lim = sorted(set(round(x, 6) for x in length.values()))[8]
-    short = [v for v in vecs if length[v] <= lim + 1e-9]
-    for R2 in short:
-        for R3 in short:
-            R32 = tuple(x - y for x, y in zip(R3, R2))
-            if R32 not in vecset or length[R32] > lim + 1e-9:
-                continue
-            imgs = frozenset(q for q, _ in _orbit((R2, R3)))
-            if imgs in orbits:
-                continue
-            orbits[imgs] = max(length[R2], length[R3], length[R32])
-    keys = list(orbits.keys())
-    tie = rng.uniform(1, len(keys))
-    order = sorted(range(len(keys)), key=lambda i: (round(orbits[keys[i]], 6), tie[i]))
+    # candidate orbits with all three vectors within the 9th distinct length
+    # (further shells only when those cannot supply num_pairs pairs)
+    dl = sorted(set(round(x, 6) for x in length.values()))
     pairs = []
-    for i in order:
-        orb = sorted(keys[i])
-        if len(pairs) + len(orb) <= num_pairs:
-            pairs.extend(orb)
+    for shell in range(8, len(dl)):
+        lim = dl[shell]
+        orbits = {}
+        short = [v for v in vecs if length[v] <= lim + 1e-9]
+        for R2 in short:
+            for R3 in short:
+                R32 = tuple(x - y for x, y in zip(R3, R2))
+                if R32 not in vecset or length[R32] > lim + 1e-9:
+                    continue
+                imgs = frozenset(q for q, _ in _orbit((R2, R3)))
+                if imgs in orbits:
+                    continue
+                orbits[imgs] = max(length[R2], length[R3], length[R32])
+        keys = list(orbits.keys())
+        tie = rng.uniform(1, len(keys))
+        order = sorted(range(len(keys)), key=lambda i: (round(orbits[keys[i]], 6), tie[i]))
+        # greedy in that order; when the orbit sizes (1, 3, 6) cannot add up to
+        # num_pairs with the single-pair orbit in, retry without it
+        for min_size in (1, 2):
+            pairs = []
+            for i in order:
+                orb = sorted(keys[i])
+                if len(orb) >= min_size and len(pairs) + len(orb) <= num_pairs:
+                    pairs.extend(orb)
+                if len(pairs) == num_pairs:
+                    break
+            if len(pairs) == num_pairs:
+                break
         if len(pairs) == num_pairs:
             break
     if len(pairs) != num_pairs:
@@ -244,11 +255,14 @@ def random_fc3(crystal, num_pairs, seed, amp_ev=3.0, decay_ang=4.0,
     R2s = sorted(set(p[0] for p in pairs))
     groups = {R2: [pidx[p] for p in pairs if p[0] == R2] for R2 in R2s}
 
+    # image k of every pair is a permutation of the pair set with one transpose
+    jmap = np.array([[j for j, _ in imgs] for imgs in perm_maps])        # (num_pairs, 6)
+    axes = [ax for _, ax in perm_maps[0]]
+
     def symmetrise(B):
         S = np.zeros_like(B)
-        for i, imgs in enumerate(perm_maps):
-            for j, ax in imgs:
-                S[j] += np.transpose(B[i], ax)
+        for k, ax in enumerate(axes):
+            S[jmap[:, k]] += np.transpose(B, (0,) + tuple(1 + a for a in ax))
         return S / 6.0
 
     def asr_project(B):
@@ -320,6 +334,44 @@ def config0():
 def config1():
     """Diamond, 20^3 mesh, adaptive smearing, 100/300/600 K (headline case)."""
     return diamond_workload((20, 20, 20), "adaptive", (100.0, 300.0, 600.0))
+
+
+def perovskite_workload(mesh=(24, 24, 24), num_pairs=1500, fc_grid=(7, 7, 7), smearing="adaptive",
+                        temperatures_k=(300.0,)):
+    """Batched uneven instances: the 5-atom perovskite-like cell (15 branches),
+    spring FC2 on a 7x7x7 grid, 1500 FC3 pairs (seed of config 2)."""
+    cr = perovskite_crystal()
+    fc2 = perovskite_fc2(cr, fc_grid)
+    fc3 = random_fc3(cr, num_pairs, SEED_BASE + 2)
+    return Workload("perovskite-%dx%dx%d" % tuple(mesh), cr, fc2, fc3, tuple(mesh),
+                    tuple(temperatures_k), smearing, 0.3 / C.ryToTHz)
+
+
+def config2(mesh=(24, 24, 24)):
+    """5-atom perovskite, 24^3 mesh, per-q1 q2 window (use q2_window on its bands)."""
+    return perovskite_workload(mesh)
+
+
+def q2_window(E, mesh, seed=SEED_BASE + 2, keep_min=0.2, keep_max=1.0):
+    """Per-q1 energy window on q2 (uneven work; no counterpart in the reference).
+
+    The window energy of q2 is the largest phonon energy at q2 or at -q2, so
+    q2 and -q2 always fall on the same side of a window.  Each q1 draws a kept
+    fraction f uniform in [keep_min, keep_max] from the counter RNG (stream 7,
+    counter q1); its cut is the window energy of rank ceil(f nq) - 1 in
+    ascending order, and q2 is paired with q1 iff energy[q2] <= cut[q1] (ties
+    kept).  Returns (energy (nq), cut (nq))."""
+    E = np.asarray(E)
+    nq = E.shape[0]
+    n0, n1, n2 = mesh
+    idx = np.arange(nq)
+    ix, iy, iz = idx % n0, (idx // n0) % n1, idx // (n0 * n1)
+    neg = ((n2 - iz) % n2) * n0 * n1 + ((n1 - iy) % n1) * n0 + (n0 - ix) % n0
+    energy = np.maximum(E.max(axis=1), E[neg].max(axis=1))
+    f = keep_min + (keep_max - keep_min) * CounterRNG(seed).uniform(7, nq)
+    srt = np.sort(energy)
+    rank = np.clip(np.ceil(f * nq).astype(np.int64) - 1, 0, nq - 1)
+    return energy, srt[rank]
 
 
 # ---------------------------------------------------------------------------

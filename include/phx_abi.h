@@ -156,6 +156,8 @@ typedef struct phx_lw_stats {
   int kernel_launches;        /* kernels launched by the call */
   int pair_launches;          /* launches of the fused pair kernel */
   double ms_pair;             /* device time of those launches alone (CUDA events) */
+  int plan_chunk, plan_slots; /* launch plan used (q2 per chunk, partial-sum slots) */
+  int graph;                  /* 0 eager launches, 1 captured into a CUDA graph, 2 graph replayed */
 } phx_lw_stats;
 
 /* Whole PhScatteringMatrix::builder, switchCase 2 (linewidths), on the GPU:

@@ -41,7 +41,8 @@ class LwParams(ctypes.Structure):
 class LwStats(ctypes.Structure):
     _fields_ = [("ms_total", ctypes.c_double), ("ms_vertex", ctypes.c_double),
                 ("pairs", ctypes.c_longlong), ("kernel_launches", ctypes.c_int),
-                ("pair_launches", ctypes.c_int), ("ms_pair", ctypes.c_double)]
+                ("pair_launches", ctypes.c_int), ("ms_pair", ctypes.c_double),
+                ("plan_chunk", ctypes.c_int), ("plan_slots", ctypes.c_int), ("graph", ctypes.c_int)]
 
 
 class ElParams(ctypes.Structure):

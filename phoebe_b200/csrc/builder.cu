@@ -27,7 +27,11 @@
 //    averaging and the exclusion of acoustic Gamma modes.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -720,6 +724,7 @@ size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 int phx_split_kp(int nr3);
 size_t phx_split_bimg_bytes(int chunk, int nr3);
 size_t phx_split_smem_bytes(int nr3);
+int phx_split_set_attributes(phx_ctx* ctx, int nr3, int nT);
 int phx_split_prepare_bands(phx_ctx* ctx, phx_bands* b);
 size_t phx_split_rec_bytes(int nq);
 int phx_split_pack_records(phx_ctx* ctx, const pairc::MeshArgs& M, void* rec, int* launches);
@@ -861,6 +866,155 @@ struct BuilderPlan {
   int slots = 8;        // partial-sum slots (q2 slices per chunk)
 };
 
+// ---------------------------------------------------------------------------
+// Launch plans and CUDA graphs of the builder
+//
+// Autotuner: the first call for a problem shape (path, nb, nq, nr3, nr2, nT,
+// device) times each candidate (chunk, slots) on one chunk of q2 with CUDA
+// events and keeps the fastest per q2 for the rest of the process
+// (PHX_TUNE=0: fixed defaults).  Graphs: the device work of a call -- the
+// memsets, Bose factors, records, every fold / conversion / pair launch of
+// the q2 loop and the finalisation -- is captured into a CUDA graph owned by
+// the v3 object and replayed when a later call touches the same buffers with
+// the same parameters (PHX_GRAPHS=0: eager launches).  Temperatures and
+// windows are copied to the device outside the graph, so their values may
+// change between replays.
+// ---------------------------------------------------------------------------
+bool env_off(const char* name) {
+  const char* e = std::getenv(name);
+  return e && e[0] == '0';
+}
+
+struct PlanKey {
+  int kind, nb, nq, nr3, nr2, nT, device;
+  bool operator<(const PlanKey& o) const {
+    return std::tie(kind, nb, nq, nr3, nr2, nT, device) < std::tie(o.kind, o.nb, o.nq, o.nr3, o.nr2, o.nT, o.device);
+  }
+};
+std::mutex g_plan_mutex;
+std::map<PlanKey, BuilderPlan> g_plans;
+
+bool find_plan(const PlanKey& k, BuilderPlan* out) {
+  std::lock_guard<std::mutex> lock(g_plan_mutex);
+  auto it = g_plans.find(k);
+  if (it == g_plans.end()) return false;
+  *out = it->second;
+  return true;
+}
+void store_plan(const PlanKey& k, const BuilderPlan& p) {
+  std::lock_guard<std::mutex> lock(g_plan_mutex);
+  g_plans[k] = p;
+}
+
+}  // namespace
+
+struct phx_builder_graph {
+  std::vector<uint64_t> key;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t vertex_begin = nullptr, vertex_end = nullptr;
+  std::vector<cudaEvent_t> pair_events;
+  int launches = 0;
+};
+struct phx_builder_graphs {
+  std::vector<phx_builder_graph> entries;   // most recent last, at most 4
+};
+
+void phx_builder_graph_free(phx_builder_graph& g) {
+  if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (g.vertex_begin) cudaEventDestroy(g.vertex_begin);
+  if (g.vertex_end) cudaEventDestroy(g.vertex_end);
+  for (cudaEvent_t e : g.pair_events) cudaEventDestroy(e);
+  g = phx_builder_graph();
+}
+
+void phx_builder_release(phx_v3* v) {
+  if (!v->graphs) return;
+  for (auto& g : v->graphs->entries) phx_builder_graph_free(g);
+  delete v->graphs;
+  v->graphs = nullptr;
+}
+
+namespace {
+
+uint64_t bits(double x) {
+  uint64_t u;
+  std::memcpy(&u, &x, sizeof(u));
+  return u;
+}
+uint64_t bits(const void* p) { return (uint64_t)(uintptr_t)p; }
+
+// Runs `work` (the device work of one call, which records the vertex-loop
+// events and appends its pair events) eagerly, captured into a new graph, or
+// as the replay of a cached one.  On return, *g points at the entry whose
+// events carry this call's timings (`tmp` when eager).
+template <class Work>
+int run_device_work(phx_v3* v, const std::vector<uint64_t>& key, Work&& work, phx_builder_graph* tmp,
+                    phx_builder_graph** g, int* graph_state) {
+  phx_ctx* ctx = v->ctx;
+  cudaStream_t st = ctx->stream;
+  auto make_events = [&](phx_builder_graph& e) -> int {
+    PHX_CUDA(ctx, cudaEventCreate(&e.vertex_begin));
+    PHX_CUDA(ctx, cudaEventCreate(&e.vertex_end));
+    return PHX_OK;
+  };
+  if (env_off("PHX_GRAPHS")) {
+    PHX_TRY(make_events(*tmp));
+    PHX_TRY(work(*tmp));
+    *g = tmp;
+    *graph_state = 0;
+    return PHX_OK;
+  }
+  if (!v->graphs) v->graphs = new phx_builder_graphs;
+  auto& es = v->graphs->entries;
+  for (size_t i = 0; i < es.size(); ++i)
+    if (es[i].key == key) {
+      PHX_CUDA(ctx, cudaGraphLaunch(es[i].exec, st));
+      std::rotate(es.begin() + i, es.begin() + i + 1, es.end());
+      *g = &es.back();
+      *graph_state = 2;
+      return PHX_OK;
+    }
+  phx_builder_graph e;
+  e.key = key;
+  int rc = make_events(e);
+  cudaGraph_t graph = nullptr;
+  if (rc == PHX_OK) {
+    cudaError_t ce = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess) {
+      phx_set_error(ctx, PHX_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+      rc = PHX_ERR_CUDA;
+    } else {
+      rc = work(e);
+      ce = cudaStreamEndCapture(st, &graph);
+      if (rc == PHX_OK && ce != cudaSuccess) {
+        phx_set_error(ctx, PHX_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+        rc = PHX_ERR_CUDA;
+      }
+    }
+  }
+  if (rc == PHX_OK) {
+    cudaError_t ce = cudaGraphInstantiate(&e.exec, graph, 0);
+    if (ce != cudaSuccess) {
+      phx_set_error(ctx, PHX_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+      rc = PHX_ERR_CUDA;
+    }
+  }
+  if (graph) cudaGraphDestroy(graph);
+  if (rc != PHX_OK) {
+    phx_builder_graph_free(e);
+    return rc;
+  }
+  PHX_CUDA(ctx, cudaGraphLaunch(e.exec, st));
+  if (es.size() >= 4) {
+    phx_builder_graph_free(es.front());
+    es.erase(es.begin());
+  }
+  es.push_back(std::move(e));
+  *g = &es.back();
+  *graph_state = 1;
+  return PHX_OK;
+}
+
 template <int NB>
 int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
                 phx_lw_stats* stats) {
@@ -869,20 +1023,22 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   const int nq = b->nq, nT = p->num_temperatures, nr3 = v->nr3, nr2 = v->nr2;
   const int q2b = p->q2_begin, q2e = p->q2_end;
   const bool split = v->precision != PHX_PREC_FP64;
-  BuilderPlan plan;
-  if (split) {
-    plan.chunk = 448;
-    plan.slots = 7;
-  }
-  plan.chunk = std::min(plan.chunk, std::max(1, q2e - q2b));
-  plan.slots = std::min(plan.slots, plan.chunk);
-  const int nslots = plan.slots;
+  // candidate plans; the first is the default
+  std::vector<BuilderPlan> cands;
+  if (split)
+    cands = {{448, 7}, {448, 14}, {896, 7}, {896, 14}};
+  else
+    cands = {{512, 8}, {512, 4}, {512, 16}};
+  int max_chunk = 0;
+  for (auto& c : cands) max_chunk = std::max(max_chunk, c.chunk);
+  max_chunk = std::min(max_chunk, std::max(1, q2e - q2b));
+  const int max_slots = 16;
   const size_t nb3 = (size_t)NB * NB * NB;
-  const size_t sz_dp = align_up(sizeof(double2) * plan.chunk * nr3 * nb3);
-  const size_t sz_part = align_up(sizeof(double) * nslots * nq * NB * nT);
+  const size_t sz_dp = align_up(sizeof(double2) * max_chunk * nr3 * nb3);
+  const size_t sz_part = align_up(sizeof(double) * max_slots * nq * NB * nT);
   const size_t sz_bose = align_up(sizeof(double) * nT * nq * NB);
   const size_t sz_T = align_up(sizeof(double) * 8);
-  const size_t sz_img = split ? align_up(phx_split_bimg_bytes(plan.chunk, nr3)) : 0;
+  const size_t sz_img = split ? align_up(phx_split_bimg_bytes(max_chunk, nr3)) : 0;
   const size_t sz_rec = split ? align_up(phx_split_rec_bytes(nq)) : 0;
   PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_img + sz_rec));
   char* base = static_cast<char*>(v->ctx->d_scratch);
@@ -892,34 +1048,20 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   double* temps = reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose);
   uint8_t* Bimg = reinterpret_cast<uint8_t*>(base + sz_dp + sz_part + sz_bose + sz_T);
   void* rec = base + sz_dp + sz_part + sz_bose + sz_T + sz_img;
-  double emax = 0.0;  // largest energy of the mesh (margin of the split path's FP32 windows)
   if (split) {
     PHX_ARG(ctx, NB == 6, "split-precision path supports nb = 6");
     PHX_ARG(ctx, phx_split_smem_bytes(nr3) <= 227 * 1024, "too many R3 vectors for the split path");
     PHX_TRY(phx_split_prepare_bands(ctx, b));
-    std::vector<double> Eh((size_t)nq * NB);
-    PHX_CUDA(ctx, cudaMemcpy(Eh.data(), b->d_E, sizeof(double) * Eh.size(), cudaMemcpyDeviceToHost));
-    for (double e : Eh) emax = std::max(emax, std::fabs(e));
-  }
-  cudaEvent_t ev0, ev1, evv0, evv1;
-  PHX_CUDA(ctx, cudaEventCreate(&ev0));
-  PHX_CUDA(ctx, cudaEventCreate(&ev1));
-  PHX_CUDA(ctx, cudaEventCreate(&evv0));
-  PHX_CUDA(ctx, cudaEventCreate(&evv1));
-  int launches = 0;
-  std::vector<cudaEvent_t> pair_events;  // (begin, end) of every pair-kernel launch, when stats are asked for
-  struct EventGuard {
-    std::vector<cudaEvent_t>& ev;
-    ~EventGuard() {
-      for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    if (b->emax < 0.0) {
+      // largest energy of the mesh (margin of the split path's FP32 windows), once per band structure
+      std::vector<double> Eh((size_t)nq * NB);
+      PHX_CUDA(ctx, cudaMemcpy(Eh.data(), b->d_E, sizeof(double) * Eh.size(), cudaMemcpyDeviceToHost));
+      double m = 0.0;
+      for (double e : Eh) m = std::max(m, std::fabs(e));
+      b->emax = m;
     }
-  } pair_event_guard{pair_events};
-  PHX_CUDA(ctx, cudaEventRecord(ev0, st));
-  PHX_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
-  PHX_CUDA(ctx, cudaMemcpyAsync(temps, p->temperatures, sizeof(double) * nT, cudaMemcpyHostToDevice, st));
-  PHX_CUDA(ctx, cudaMemsetAsync(partial, 0, sizeof(double) * nslots * nq * NB * nT, st));
-  bose_kernel<<<std::min(1024, (nq * NB * nT + 255) / 256), 256, 0, st>>>(nq, NB, nT, b->d_E, temps, bose);
-  ++launches;
+  }
+  const double emax = split ? b->emax : 0.0;
   PairArgs P;
   P.m.nq = nq;
   P.m.nb = NB;
@@ -953,79 +1095,147 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   if (smem_fold > 48 * 1024)
     PHX_CUDA(ctx, cudaFuncSetAttribute(fold_q2_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem_fold));
+  if (split) PHX_TRY(phx_split_set_attributes(ctx, nr3, nT));
   const int tiles = (nq + kTile - 1) / kTile;
-  if (split) PHX_TRY(phx_split_pack_records(ctx, P.m, rec, &launches));
-  PHX_CUDA(ctx, cudaEventRecord(evv0, st));
-  for (int c0 = q2b; c0 < q2e; c0 += plan.chunk) {
-    const int cnt = std::min(plan.chunk, q2e - c0);
+  // one chunk of the q2 loop; pe0/pe1 (may be null) bracket its pair kernel
+  auto chunk_work = [&](const BuilderPlan& pl, int c0, int cnt, cudaEvent_t pe0, cudaEvent_t pe1,
+                        int* launches) -> int {
     fold_tiled_launch(NB, nr2, nr3, v, b, c0, cnt, Dp, st);
-    ++launches;
-    if (split) {
-      cudaEvent_t pe0 = nullptr, pe1 = nullptr;
-      if (stats) {
-        PHX_CUDA(ctx, cudaEventCreate(&pe0));
-        PHX_CUDA(ctx, cudaEventCreate(&pe1));
-        pair_events.push_back(pe0);
-        pair_events.push_back(pe1);
+    ++*launches;
+    if (split)
+      return phx_split_pair_chunk(ctx, P.m, v, b, Dp, Bimg, rec, emax, c0, cnt, pl.slots, partial, launches,
+                                  pe0, pe1);
+    PairArgs Q = P;
+    Q.q2_first = c0;
+    Q.q2_count = cnt;
+    Q.q2_per_slot = (cnt + pl.slots - 1) / pl.slots;
+    if (pe0) PHX_CUDA(ctx, phx_record_event(pe0, st));
+    pair_fp64_kernel<NB><<<dim3(tiles, pl.slots), kTile * NB, smem_pair, st>>>(Q);
+    if (pe1) PHX_CUDA(ctx, phx_record_event(pe1, st));
+    ++*launches;
+    PHX_CUDA(ctx, cudaGetLastError());
+    return PHX_OK;
+  };
+  PHX_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
+  PHX_CUDA(ctx, cudaMemcpyAsync(temps, p->temperatures, sizeof(double) * nT, cudaMemcpyHostToDevice, st));
+  // launch plan: tuned once per problem shape
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const PlanKey pk{split ? 1 : 0, NB, nq, nr3, nr2, nT, dev};
+  BuilderPlan plan = cands[0];
+  if (!env_off("PHX_TUNE") && q2e - q2b >= 2 * cands[0].chunk && !find_plan(pk, &plan)) {
+    int dummy = 0;
+    if (split) PHX_TRY(phx_split_pack_records(ctx, P.m, rec, &dummy));
+    bose_kernel<<<std::min(1024, (nq * NB * nT + 255) / 256), 256, 0, st>>>(nq, NB, nT, b->d_E, temps, bose);
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    PHX_CUDA(ctx, cudaEventCreate(&t0));
+    PHX_CUDA(ctx, cudaEventCreate(&t1));
+    double best = 1e300;
+    int rc = PHX_OK;
+    for (const auto& c : cands) {
+      const int cnt = std::min(c.chunk, q2e - q2b);
+      const BuilderPlan cc{cnt, std::min(c.slots, cnt)};
+      cudaEventRecord(t0, st);
+      rc = chunk_work(cc, q2b, cnt, nullptr, nullptr, &dummy);
+      cudaEventRecord(t1, st);
+      if (rc == PHX_OK && cudaEventSynchronize(t1) != cudaSuccess) rc = PHX_ERR_CUDA;
+      if (rc != PHX_OK) break;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, t0, t1);
+      if (ms / cnt < best) {
+        best = ms / cnt;
+        plan = c;
       }
-      PHX_TRY(phx_split_pair_chunk(ctx, P.m, v, b, Dp, Bimg, rec, emax, c0, cnt, plan.slots, partial,
-                                   &launches, pe0, pe1));
-      continue;
     }
-    P.q2_first = c0;
-    P.q2_count = cnt;
-    P.q2_per_slot = (cnt + plan.slots - 1) / plan.slots;
-    dim3 gp(tiles, plan.slots);
-    cudaEvent_t pe0 = nullptr, pe1 = nullptr;
-    if (stats) {
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rc != PHX_OK) {
+      if (rc == PHX_ERR_CUDA) phx_set_error(ctx, PHX_ERR_CUDA, "builder autotuner: a timed candidate failed");
+      return rc;
+    }
+    store_plan(pk, plan);
+  }
+  plan.chunk = std::min(plan.chunk, std::max(1, q2e - q2b));
+  plan.slots = std::min(plan.slots, plan.chunk);
+  const int nslots = plan.slots;
+  // the device work of the call
+  auto work = [&](phx_builder_graph& g) -> int {
+    int launches = 0;
+    PHX_CUDA(ctx, cudaMemsetAsync(partial, 0, sizeof(double) * nslots * nq * NB * nT, st));
+    bose_kernel<<<std::min(1024, (nq * NB * nT + 255) / 256), 256, 0, st>>>(nq, NB, nT, b->d_E, temps, bose);
+    ++launches;
+    if (split) PHX_TRY(phx_split_pack_records(ctx, P.m, rec, &launches));
+    PHX_CUDA(ctx, phx_record_event(g.vertex_begin, st));
+    for (int c0 = q2b; c0 < q2e; c0 += plan.chunk) {
+      const int cnt = std::min(plan.chunk, q2e - c0);
+      cudaEvent_t pe0 = nullptr, pe1 = nullptr;
       PHX_CUDA(ctx, cudaEventCreate(&pe0));
+      g.pair_events.push_back(pe0);
       PHX_CUDA(ctx, cudaEventCreate(&pe1));
-      pair_events.push_back(pe0);
-      pair_events.push_back(pe1);
-      PHX_CUDA(ctx, cudaEventRecord(pe0, st));
+      g.pair_events.push_back(pe1);
+      PHX_TRY(chunk_work(plan, c0, cnt, pe0, pe1, &launches));
     }
-    pair_fp64_kernel<NB><<<gp, kTile * NB, smem_pair, st>>>(P);
-    if (stats) PHX_CUDA(ctx, cudaEventRecord(pe1, st));
+    PHX_CUDA(ctx, phx_record_event(g.vertex_end, st));
+    finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, NB, nT, nslots, partial, b->d_E, p->finalize, Aout_d);
     ++launches;
     PHX_CUDA(ctx, cudaGetLastError());
-  }
-  PHX_CUDA(ctx, cudaEventRecord(evv1, st));
-  finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, NB, nT, nslots, partial, b->d_E,
-                                                    p->finalize, Aout_d);
-  ++launches;
-  PHX_CUDA(ctx, cudaGetLastError());
-  PHX_CUDA(ctx, cudaEventRecord(ev1, st));
-  PHX_CUDA(ctx, cudaEventSynchronize(ev1));
+    g.launches = launches;
+    return PHX_OK;
+  };
+  const std::vector<uint64_t> key = {
+      (uint64_t)(split ? 1 : 0), (uint64_t)NB, (uint64_t)nq, (uint64_t)nT, (uint64_t)q2b, (uint64_t)q2e,
+      (uint64_t)p->smearing, bits(p->sigma), (uint64_t)p->finalize, (uint64_t)plan.chunk, (uint64_t)plan.slots,
+      bits(emax), bits(base), bits(Aout_d), bits(b->d_E), bits(b->d_U), bits(b->d_vg), bits(b->d_q),
+      bits(b->d_U32), bits(b->d_q1_order), bits(v->d_D3w), bits(v->d_R2), bits(v->d_R3), bits(ctx->d_status)};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  PHX_CUDA(ctx, cudaEventCreate(&ev0));
+  PHX_CUDA(ctx, cudaEventCreate(&ev1));
+  PHX_CUDA(ctx, cudaEventRecord(ev0, st));
+  phx_builder_graph eager;
+  phx_builder_graph* g = nullptr;
+  int graph_state = 0;
+  int rc = run_device_work(v, key, work, &eager, &g, &graph_state);
   int kst = 0;
-  PHX_CUDA(ctx, cudaMemcpy(&kst, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-  if (kst) {
+  if (rc == PHX_OK) {
+    cudaError_t ce = cudaEventRecord(ev1, st);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(ev1);
+    if (ce == cudaSuccess) ce = cudaMemcpy(&kst, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) {
+      phx_set_error(ctx, PHX_ERR_CUDA, cudaGetErrorString(ce));
+      rc = PHX_ERR_CUDA;
+    }
+  }
+  if (rc == PHX_OK && kst) {
     cudaMemset(ctx->d_status, 0, sizeof(int));
     phx_set_error(ctx, PHX_ERR_CUDA, "pair kernel gave up waiting on a pipeline barrier (status " +
                                          std::to_string(kst) + ")");
-    return PHX_ERR_CUDA;
+    rc = PHX_ERR_CUDA;
   }
-  if (stats) {
+  if (rc == PHX_OK && stats) {
     float ms = 0, msv = 0;
     cudaEventElapsedTime(&ms, ev0, ev1);
-    cudaEventElapsedTime(&msv, evv0, evv1);
+    cudaEventElapsedTime(&msv, g->vertex_begin, g->vertex_end);
     stats->ms_total = ms;
     stats->ms_vertex = msv;
     stats->pairs = (long long)nq * (q2e - q2b);
-    stats->kernel_launches = launches;
-    stats->pair_launches = (int)(pair_events.size() / 2);
+    stats->kernel_launches = g->launches;
+    stats->pair_launches = (int)(g->pair_events.size() / 2);
     double msp = 0.0;
-    for (size_t i = 0; i + 1 < pair_events.size(); i += 2) {
+    for (size_t i = 0; i + 1 < g->pair_events.size(); i += 2) {
       float x = 0.f;
-      cudaEventElapsedTime(&x, pair_events[i], pair_events[i + 1]);
+      cudaEventElapsedTime(&x, g->pair_events[i], g->pair_events[i + 1]);
       msp += x;
     }
     stats->ms_pair = msp;
+    stats->plan_chunk = plan.chunk;
+    stats->plan_slots = plan.slots;
+    stats->graph = graph_state;
+    cudaGetLastError();   // an elapsed-time query that failed must not leak into the next call
   }
+  phx_builder_graph_free(eager);
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
-  cudaEventDestroy(evv0);
-  cudaEventDestroy(evv1);
-  return PHX_OK;
+  return rc;
 }
 
 // Builder for any nb <= kMaxNbGeneric, or with a per-q1 q2 window, FP64:
@@ -1046,10 +1256,11 @@ int run_builder_generic(phx_v3* v, phx_bands* b, const phx_lw_params* p, double*
   // q2 per cached-vertex slab: at most 512 MB of it, at most 512 q2
   const int chunk = (int)std::max<size_t>(1, std::min<size_t>({(size_t)512, (size_t)(q2e - q2b),
                                                                 (size_t(512) << 20) / std::max<size_t>(per_q2, 1)}));
-  // enough (q1, slot) blocks to fill the GPU several times over
-  const int slots = std::max(1, std::min(chunk, (4 * ctx->num_sms + nq - 1) / nq));
+  // (q1, slot) blocks: the candidates fill the GPU 4, 8 or 16 times over
+  const int fill = std::max(1, (4 * ctx->num_sms + nq - 1) / nq);
+  const int max_slots = std::min(chunk, 4 * fill);
   const size_t sz_dp = align_up(per_q2 * chunk);
-  const size_t sz_part = align_up(sizeof(double) * slots * nq * nb * nT);
+  const size_t sz_part = align_up(sizeof(double) * max_slots * nq * nb * nT);
   const size_t sz_bose = align_up(sizeof(double) * nT * nq * nb);
   const size_t sz_T = align_up(sizeof(double) * 8);
   const size_t sz_win = windowed ? align_up(sizeof(double) * 2 * nq) : 0;
@@ -1060,22 +1271,12 @@ int run_builder_generic(phx_v3* v, phx_bands* b, const phx_lw_params* p, double*
   double* bose = reinterpret_cast<double*>(base + sz_dp + sz_part);
   double* temps = reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose);
   double* wdev = reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose + sz_T);
-  cudaEvent_t ev0, ev1, evv0, evv1;
-  PHX_CUDA(ctx, cudaEventCreate(&ev0));
-  PHX_CUDA(ctx, cudaEventCreate(&ev1));
-  PHX_CUDA(ctx, cudaEventCreate(&evv0));
-  PHX_CUDA(ctx, cudaEventCreate(&evv1));
-  int launches = 0;
-  PHX_CUDA(ctx, cudaEventRecord(ev0, st));
   PHX_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
   PHX_CUDA(ctx, cudaMemcpyAsync(temps, p->temperatures, sizeof(double) * nT, cudaMemcpyHostToDevice, st));
   if (windowed) {
     PHX_CUDA(ctx, cudaMemcpyAsync(wdev, p->window_energy, sizeof(double) * nq, cudaMemcpyHostToDevice, st));
     PHX_CUDA(ctx, cudaMemcpyAsync(wdev + nq, p->window_cut, sizeof(double) * nq, cudaMemcpyHostToDevice, st));
   }
-  PHX_CUDA(ctx, cudaMemsetAsync(partial, 0, sizeof(double) * slots * nq * nb * nT, st));
-  bose_kernel<<<std::min(1024, (nq * nb * nT + 255) / 256), 256, 0, st>>>(nq, nb, nT, b->d_E, temps, bose);
-  ++launches;
   PairArgs P;
   P.m.nq = nq;
   P.m.nb = nb;
@@ -1103,46 +1304,113 @@ int run_builder_generic(phx_v3* v, phx_bands* b, const phx_lw_params* p, double*
                                        (int)smem_pair));
   if (smem_fold > 48 * 1024)
     PHX_CUDA(ctx, cudaFuncSetAttribute(fold_q2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fold));
-  PHX_CUDA(ctx, cudaEventRecord(evv0, st));
-  long long pairs = 0;
-  for (int c0 = q2b; c0 < q2e; c0 += chunk) {
-    const int cnt = std::min(chunk, q2e - c0);
+  auto chunk_work = [&](int c0, int cnt, int slots, int* launches) -> int {
     const int per_block = 8;
     fold_q2_kernel<<<dim3(nr3, (cnt + per_block - 1) / per_block), 128, smem_fold, st>>>(
         nb, nr2, nr3, v->d_D3w, v->d_R2, v->d_R3, b->d_q, reinterpret_cast<const double2*>(b->d_U), c0, cnt,
         per_block, Dp);
-    ++launches;
+    ++*launches;
     PHX_CUDA(ctx, cudaGetLastError());
-    P.q2_first = c0;
-    P.q2_count = cnt;
-    P.q2_per_slot = (cnt + slots - 1) / slots;
-    pair_generic_kernel<<<dim3(nq, slots), kGenThreads, smem_pair, st>>>(P, W);
-    ++launches;
+    PairArgs Q = P;
+    Q.q2_first = c0;
+    Q.q2_count = cnt;
+    Q.q2_per_slot = (cnt + slots - 1) / slots;
+    pair_generic_kernel<<<dim3(nq, slots), kGenThreads, smem_pair, st>>>(Q, W);
+    ++*launches;
     PHX_CUDA(ctx, cudaGetLastError());
-    pairs += (long long)nq * cnt;
+    return PHX_OK;
+  };
+  // slot count tuned once per problem shape (a window makes the work per block uneven)
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const PlanKey pk{windowed ? 3 : 2, nb, nq, nr3, nr2, nT, dev};
+  BuilderPlan plan{chunk, std::min(chunk, fill)};
+  if (!env_off("PHX_TUNE") && q2e - q2b >= 2 * chunk && !find_plan(pk, &plan)) {
+    bose_kernel<<<std::min(1024, (nq * nb * nT + 255) / 256), 256, 0, st>>>(nq, nb, nT, b->d_E, temps, bose);
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    PHX_CUDA(ctx, cudaEventCreate(&t0));
+    PHX_CUDA(ctx, cudaEventCreate(&t1));
+    double best = 1e300;
+    int rc = PHX_OK, dummy = 0;
+    for (int f : {fill, 2 * fill, 4 * fill}) {
+      const int sl = std::min(chunk, f);
+      cudaEventRecord(t0, st);
+      rc = chunk_work(q2b, chunk, sl, &dummy);
+      cudaEventRecord(t1, st);
+      if (rc == PHX_OK && cudaEventSynchronize(t1) != cudaSuccess) rc = PHX_ERR_CUDA;
+      if (rc != PHX_OK) break;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, t0, t1);
+      if (ms < best) {
+        best = ms;
+        plan.slots = sl;
+      }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rc != PHX_OK) {
+      if (rc == PHX_ERR_CUDA) phx_set_error(ctx, PHX_ERR_CUDA, "builder autotuner: a timed candidate failed");
+      return rc;
+    }
+    store_plan(pk, plan);
   }
-  PHX_CUDA(ctx, cudaEventRecord(evv1, st));
-  finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, nb, nT, slots, partial, b->d_E, p->finalize, Aout_d);
-  ++launches;
-  PHX_CUDA(ctx, cudaGetLastError());
-  PHX_CUDA(ctx, cudaEventRecord(ev1, st));
-  PHX_CUDA(ctx, cudaEventSynchronize(ev1));
-  if (stats) {
+  const int slots = plan.slots;
+  long long pairs = 0;
+  for (int c0 = q2b; c0 < q2e; c0 += chunk) pairs += (long long)nq * std::min(chunk, q2e - c0);
+  auto work = [&](phx_builder_graph& g) -> int {
+    int launches = 0;
+    PHX_CUDA(ctx, cudaMemsetAsync(partial, 0, sizeof(double) * slots * nq * nb * nT, st));
+    bose_kernel<<<std::min(1024, (nq * nb * nT + 255) / 256), 256, 0, st>>>(nq, nb, nT, b->d_E, temps, bose);
+    ++launches;
+    PHX_CUDA(ctx, phx_record_event(g.vertex_begin, st));
+    for (int c0 = q2b; c0 < q2e; c0 += chunk) PHX_TRY(chunk_work(c0, std::min(chunk, q2e - c0), slots, &launches));
+    PHX_CUDA(ctx, phx_record_event(g.vertex_end, st));
+    finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, nb, nT, slots, partial, b->d_E, p->finalize, Aout_d);
+    ++launches;
+    PHX_CUDA(ctx, cudaGetLastError());
+    g.launches = launches;
+    return PHX_OK;
+  };
+  const std::vector<uint64_t> key = {
+      (uint64_t)(windowed ? 3 : 2), (uint64_t)nb, (uint64_t)nq, (uint64_t)nT, (uint64_t)q2b, (uint64_t)q2e,
+      (uint64_t)p->smearing, bits(p->sigma), (uint64_t)p->finalize, (uint64_t)chunk, (uint64_t)slots, bits(base),
+      bits(Aout_d), bits(b->d_E), bits(b->d_U), bits(b->d_vg), bits(b->d_q), bits(v->d_D3w), bits(v->d_R2),
+      bits(v->d_R3), bits(ctx->d_status)};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  PHX_CUDA(ctx, cudaEventCreate(&ev0));
+  PHX_CUDA(ctx, cudaEventCreate(&ev1));
+  PHX_CUDA(ctx, cudaEventRecord(ev0, st));
+  phx_builder_graph eager;
+  phx_builder_graph* g = nullptr;
+  int graph_state = 0;
+  int rc = run_device_work(v, key, work, &eager, &g, &graph_state);
+  if (rc == PHX_OK) {
+    cudaError_t ce = cudaEventRecord(ev1, st);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(ev1);
+    if (ce != cudaSuccess) {
+      phx_set_error(ctx, PHX_ERR_CUDA, cudaGetErrorString(ce));
+      rc = PHX_ERR_CUDA;
+    }
+  }
+  if (rc == PHX_OK && stats) {
     float ms = 0, msv = 0;
     cudaEventElapsedTime(&ms, ev0, ev1);
-    cudaEventElapsedTime(&msv, evv0, evv1);
+    cudaEventElapsedTime(&msv, g->vertex_begin, g->vertex_end);
     stats->ms_total = ms;
     stats->ms_vertex = msv;
     stats->pairs = pairs;
-    stats->kernel_launches = launches;
+    stats->kernel_launches = g->launches;
     stats->pair_launches = 0;
     stats->ms_pair = 0.0;
+    stats->plan_chunk = chunk;
+    stats->plan_slots = slots;
+    stats->graph = graph_state;
+    cudaGetLastError();
   }
+  phx_builder_graph_free(eager);
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
-  cudaEventDestroy(evv0);
-  cudaEventDestroy(evv1);
-  return PHX_OK;
+  return rc;
 }
 
 }  // namespace

@@ -60,6 +60,15 @@ struct phx_ctx {
 // grow-only device buffers of a context
 int phx_ctx_reserve(phx_ctx* ctx, void** buf, size_t* have, size_t bytes);
 
+// Records e on st; while st is being captured into a graph the record becomes
+// an external event node, so that the event times the graph's replays.
+inline cudaError_t phx_record_event(cudaEvent_t e, cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(st, &cs);
+  return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(e, st, cudaEventRecordExternal)
+                                             : cudaEventRecord(e, st);
+}
+
 struct phx_ph_h0 {
   phx_ctx* ctx = nullptr;
   int nat = 0, nb = 0, numR = 0;
@@ -83,7 +92,12 @@ struct phx_bands {
   double* d_q = nullptr;      // (nq,3) Cartesian mesh points
   float* d_U32 = nullptr;     // (nq,nb,nb) complex fp32 copy for the split path
   int* d_q1_order = nullptr;  // (nq) q1 visiting order of the split path
+  double emax = -1.0;         // largest |E| of the mesh (split path), < 0 until computed
 };
+
+// CUDA graphs of the builder, owned by the v3 object (builder.cu)
+struct phx_builder_graphs;
+void phx_builder_release(phx_v3* v);
 
 struct phx_v3 {
   phx_ctx* ctx = nullptr;
@@ -100,6 +114,7 @@ struct phx_v3 {
   double* d_mins = nullptr;    // cached D3- (nb,nb,nb,nr3) complex
   bool cached = false;
   double q2_cached[3];
+  phx_builder_graphs* graphs = nullptr;
 };
 
 int phx_scratch_reserve(phx_v3* v3, size_t bytes);

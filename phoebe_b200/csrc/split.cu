@@ -873,9 +873,7 @@ size_t pair_tc_smem(int Kp) {
 
 template <int NT>
 int launch_pair(phx_ctx* ctx, const TcArgs& A, int tiles, int slots) {
-  const size_t smem = pair_tc_smem(A.Kp);
-  PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
+  const size_t smem = pair_tc_smem(A.Kp);   // attribute set by phx_split_set_attributes
   pair_tc_kernel<NT><<<dim3(tiles, slots), kThreads, smem, ctx->stream>>>(A);
   PHX_CUDA(ctx, cudaGetLastError());
   return PHX_OK;
@@ -952,7 +950,7 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
   A.status = ctx->d_status;
   const int tiles = (M.nq + kM - 1) / kM;
   int rc = PHX_OK;
-  if (ev_begin) PHX_CUDA(ctx, cudaEventRecord(ev_begin, ctx->stream));
+  if (ev_begin) PHX_CUDA(ctx, phx_record_event(ev_begin, ctx->stream));
   switch (M.nT) {
     case 1: rc = launch_pair<1>(ctx, A, tiles, slots); break;
     case 2: rc = launch_pair<2>(ctx, A, tiles, slots); break;
@@ -960,12 +958,25 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
     default: rc = launch_pair<4>(ctx, A, tiles, slots); break;
   }
   if (rc != PHX_OK) return rc;
-  if (ev_end) PHX_CUDA(ctx, cudaEventRecord(ev_end, ctx->stream));
+  if (ev_end) PHX_CUDA(ctx, phx_record_event(ev_end, ctx->stream));
   *launches += 2;
   return PHX_OK;
 }
 
 size_t phx_split_smem_bytes(int nr3) { return pair_tc_smem(phx_split_kp(nr3)); }
+
+// Dynamic shared-memory limit of the pair kernel for nT temperatures; called
+// before any launch (and outside graph capture).
+int phx_split_set_attributes(phx_ctx* ctx, int nr3, int nT) {
+  const int smem = (int)pair_tc_smem(phx_split_kp(nr3));
+  switch (nT) {
+    case 1: PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); break;
+    case 2: PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); break;
+    case 3: PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); break;
+    default: PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); break;
+  }
+  return PHX_OK;
+}
 
 extern "C" int phx_diag_tc_gemm(phx_ctx* ctx, int N, int Kp, const float* A, const float* B, float* C) {
   PHX_ARG(ctx, ctx && A && B && C, "phx_diag_tc_gemm: bad arguments");

@@ -215,6 +215,7 @@ extern "C" int phx_v3_create(phx_ctx* ctx, int nat, int nr2, int nr3, const doub
 extern "C" int phx_v3_destroy(phx_v3* v) {
   if (!v) return PHX_OK;
   if (v->ctx) cudaSetDevice(v->ctx->device);
+  phx_builder_release(v);
   cudaFree(v->d_D3w);
   cudaFree(v->d_D3raw);
   cudaFree(v->d_w2);

@@ -256,6 +256,8 @@ def run_ours(args):
             pair_ms.append(st.ms_pair)
             pair_launches += st.pair_launches
             launches += st.kernel_launches
+            plan = {"q2_chunk": st.plan_chunk, "slots": st.plan_slots,
+                    "cuda_graph": ["eager", "captured", "replayed"][st.graph]}
         barrier()
         wall = time.perf_counter() - t0
     total_ms = float(np.sum(dev_ms))
@@ -363,6 +365,7 @@ def run_ours(args):
                "e2e": {"value": e2e_value, "unit": "triplets/s", "h2d_bytes_per_step": int(h2d),
                        "d2h_bytes_per_step": int(d2h)},
                "gpu_launches": launches,
+               "launch_plan": plan,
                "roofline": roof,
                "cpu_baseline": cpu,
                "fp64_path": fp64,

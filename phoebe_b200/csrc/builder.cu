@@ -944,9 +944,11 @@ uint64_t bits(double x) {
 uint64_t bits(const void* p) { return (uint64_t)(uintptr_t)p; }
 
 // Runs `work` (the device work of one call, which records the vertex-loop
-// events and appends its pair events) eagerly, captured into a new graph, or
-// as the replay of a cached one.  On return, *g points at the entry whose
-// events carry this call's timings (`tmp` when eager).
+// events and appends its pair events) eagerly the first time a key is seen,
+// captured into a graph the second time, and as a replay of that graph after
+// that (objects used for a single call never build one).  On return, *g
+// points at the entry whose events carry this call's timings (`tmp` when
+// eager).
 template <class Work>
 int run_device_work(phx_v3* v, const std::vector<uint64_t>& key, Work&& work, phx_builder_graph* tmp,
                     phx_builder_graph** g, int* graph_state) {
@@ -966,14 +968,36 @@ int run_device_work(phx_v3* v, const std::vector<uint64_t>& key, Work&& work, ph
   }
   if (!v->graphs) v->graphs = new phx_builder_graphs;
   auto& es = v->graphs->entries;
+  bool seen = false;
   for (size_t i = 0; i < es.size(); ++i)
     if (es[i].key == key) {
-      PHX_CUDA(ctx, cudaGraphLaunch(es[i].exec, st));
       std::rotate(es.begin() + i, es.begin() + i + 1, es.end());
-      *g = &es.back();
-      *graph_state = 2;
-      return PHX_OK;
+      if (es.back().exec) {
+        PHX_CUDA(ctx, cudaGraphLaunch(es.back().exec, st));
+        *g = &es.back();
+        *graph_state = 2;
+        return PHX_OK;
+      }
+      phx_builder_graph_free(es.back());
+      es.pop_back();
+      seen = true;
+      break;
     }
+  if (!seen) {
+    // first call with this key: eager, remembered for the next one
+    PHX_TRY(make_events(*tmp));
+    PHX_TRY(work(*tmp));
+    if (es.size() >= 4) {
+      phx_builder_graph_free(es.front());
+      es.erase(es.begin());
+    }
+    phx_builder_graph mark;
+    mark.key = key;
+    es.push_back(std::move(mark));
+    *g = tmp;
+    *graph_state = 0;
+    return PHX_OK;
+  }
   phx_builder_graph e;
   e.key = key;
   int rc = make_events(e);
@@ -1026,13 +1050,14 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   // candidate plans; the first is the default
   std::vector<BuilderPlan> cands;
   if (split)
-    cands = {{448, 7}, {448, 14}, {896, 7}, {896, 14}};
+    cands = {{448, 7}, {448, 14}, {896, 14}, {896, 28}, {1792, 14}, {1792, 28}};
   else
-    cands = {{512, 8}, {512, 4}, {512, 16}};
+    cands = {{512, 8}, {512, 4}, {512, 16}, {1024, 16}};
   int max_chunk = 0;
   for (auto& c : cands) max_chunk = std::max(max_chunk, c.chunk);
   max_chunk = std::min(max_chunk, std::max(1, q2e - q2b));
-  const int max_slots = 16;
+  int max_slots = 0;
+  for (auto& c : cands) max_slots = std::max(max_slots, c.slots);
   const size_t nb3 = (size_t)NB * NB * NB;
   const size_t sz_dp = align_up(sizeof(double2) * max_chunk * nr3 * nb3);
   const size_t sz_part = align_up(sizeof(double) * max_slots * nq * NB * nT);

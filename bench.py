@@ -33,9 +33,10 @@ TEMPS_K = (100.0, 300.0, 600.0)
 # FP32 FFMA throughput of a B200 (packed and scalar FFMA stream, all SMs, CUDA
 # events), the denominator of the pair kernel's CUDA-core view
 FFMA_PEAK_TFLOPS = 72.0
-# ncu DRAM bytes (read + write) of one pair-kernel launch (448 q2) per mesh;
-# None where not captured
-PAIR_TRAFFIC_BYTES = {20: 87476992 + 5594112, 16: 85.2e6}
+# ncu DRAM bytes (read + write) of one pair-kernel launch, per (mesh, q2 per
+# launch, slots) of the launch plan; None where not captured
+PAIR_TRAFFIC_BYTES = {(20, 448, 7): 87476992 + 5594112, (20, 1792, 28): 337188096 + 29478400,
+                      (16, 448, 7): 85.2e6}
 
 
 def parse():
@@ -312,9 +313,10 @@ def run_ours(args):
     else:
         pk = peaks.get("bf16_tflops_sustained", 1394.6)
         # DRAM bytes per launch of the pair kernel, ncu dram__bytes_read.sum +
-        # dram__bytes_write.sum of one 20^3 launch (448 q2 x 8000 q1)
+        # dram__bytes_write.sum of one launch of the plan in use
         roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
-                "frac": achieved / pk, "traffic": PAIR_TRAFFIC_BYTES.get(args.mesh),
+                "frac": achieved / pk,
+                "traffic": PAIR_TRAFFIC_BYTES.get((args.mesh, plan["q2_chunk"], plan["slots"])),
                 "peak_source": "measured (sustained)",
                 "simt_view": {"what": "FP32 epilogue (e1, e3 contractions of all 216 triplets) "
                                       "against the measured FFMA rate",

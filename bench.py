@@ -10,7 +10,7 @@ metric: triplets/s, where a triplet is one (q1,q2) pair (q3 fixed by
 momentum); linewidths/s = Nq*nb*nT / step time is reported beside it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--precision fp64|split_bf16|split_tf32] [--mesh 20]
+                  [--precision fp64|split_bf16|split_fp16] [--mesh 20]
 
 Under torchrun each rank processes a contiguous slice of q2 and the
 per-rank partial A_out vectors are summed with one NCCL all-reduce
@@ -50,7 +50,7 @@ def parse():
                          "(8 Wannier functions, 343 x 343 coupling vectors, 40^3 k, 20^3 q)")
     ap.add_argument("--elph-k1", type=int, default=64, help="outer k points timed per elph step")
     ap.add_argument("--precision", default=os.environ.get("PHX_BENCH_PRECISION", "split_bf16"),
-                    choices=["fp64", "split_bf16", "split_tf32"])
+                    choices=["fp64", "split_bf16", "split_fp16"])
     ap.add_argument("--mesh", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-fp64", action="store_true",
@@ -331,6 +331,7 @@ def run_ours(args):
     # the plain FP64 GPU path on the same workload (one step after a one-chunk warm-up)
     fp64 = None
     if args.precision != "fp64" and not args.kernels_only and not args.no_fp64:
+        A_split = A.clone()   # the last timed step's A_out
         v3.setPrecision("fp64")
         p = sm._params(q2b, min(q2e, q2b + 448), finalize=False)
         _abi.check(L.phx_ph_linewidths_d(v3.h, bands.h, ctypes.byref(p), ctypes.c_void_p(A.data_ptr()),
@@ -347,6 +348,17 @@ def run_ours(args):
         v3.setPrecision(args.precision)
         fp64 = {"ms_per_step": ms64, "value": pairs_step / (ms64 / 1000.0), "unit": "triplets/s",
                 "dtype": "f64", "steps": 1, "split_speedup": ms64 / ms_step}
+        if world == 1:
+            # accuracy of the split path on this workload: relative error of the
+            # linewidths (A_out / n(n+1), the same ratio) of non-excluded states
+            # with A_out above 1e-8 of the largest
+            a64 = A.cpu().numpy().reshape(nT, -1)
+            a16 = A_split.cpu().numpy().reshape(nT, -1)
+            Eb = bands.get(velocities=False)[0].reshape(-1)
+            big = (Eb >= C.phExcludeCutoff)[None, :] & (np.abs(a64) > 1e-8 * np.abs(a64).max())
+            rel = np.abs(a16 - a64)[big] / np.abs(a64)[big]
+            fp64["split_linewidth_rel_err"] = {"max": float(rel.max()), "p99": float(np.quantile(rel, 0.99)),
+                                               "median": float(np.median(rel)), "states": int(big.sum())}
 
     out = None
     if rank == 0:
@@ -355,7 +367,7 @@ def run_ours(args):
                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
                "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else
-               ("bf16x3->f32" if args.precision == "split_bf16" else "tf32x3->f32"),
+               ("bf16x3->f32" if args.precision == "split_bf16" else "fp16x3->f32"),
                "data": "synthetic",
                "config": {"workload": "diamond 20x20x20 (8000 q, 64e6 pairs), 400 FC3 pairs "
                                       "(nr3=%d), adaptive smearing, T=100/300/600 K" % nr3,

@@ -249,7 +249,7 @@ class PhononH0 {
 };
 
 // ---------------------------------------------------------------------------
-enum class Precision { fp64 = PHX_PREC_FP64, splitBf16 = PHX_PREC_SPLIT_BF16, splitTf32 = PHX_PREC_SPLIT_TF32 };
+enum class Precision { fp64 = PHX_PREC_FP64, splitBf16 = PHX_PREC_SPLIT_BF16, splitFp16 = PHX_PREC_SPLIT_FP16 };
 enum class Smearing { gaussian = PHX_SMEAR_GAUSSIAN, adaptive = PHX_SMEAR_ADAPTIVE };
 
 class Interaction3Ph {
@@ -330,6 +330,12 @@ class PhScatteringMatrix {
                      Smearing smearing = Smearing::adaptive, double sigma = 0.0)
       : v3_(coupling3Ph), bands_(bands), T_(std::move(temperatures)), smearing_(smearing), sigma_(sigma) {}
 
+  // isotope scattering: per-atom isotope mass variance x mass^2 (the
+  // reference's massVariance); empty disables it
+  void setIsotopeCoupling(std::vector<double> massVariance) { iso_ = std::move(massVariance); }
+  // boundary scattering |v|/L n(n+1); L <= 0 disables it (Bohr)
+  void setBoundaryLength(double L) { boundary_ = L; }
+
   // internalDiagonal A_out (nT, nq*nb) = linewidth * n(n+1); [q2Begin, q2End)
   // restricts the outer loop (one rank's share), finalize = false leaves the
   // degeneracy averaging and exclusions to the caller after summing shares.
@@ -342,6 +348,8 @@ class PhScatteringMatrix {
     p.finalize = finalize ? 1 : 0;
     p.q2_begin = q2Begin;
     p.q2_end = q2End < 0 ? bands_.getNumPoints() : q2End;
+    p.isotope_coupling = iso_.empty() ? nullptr : iso_.data();
+    p.boundary_length = boundary_;
     internalDiagonal_.assign(T_.size() * (size_t)bands_.getNumPoints() * bands_.getNumBands(), 0.0);
     check(phx_ph_linewidths(v3_.get(), bands_.get(), &p, internalDiagonal_.data(), &stats_), v3_.context());
   }
@@ -380,6 +388,8 @@ class PhScatteringMatrix {
   Smearing smearing_;
   double sigma_;
   std::vector<double> internalDiagonal_;
+  std::vector<double> iso_;
+  double boundary_ = 0.0;
   phx_lw_stats stats_{};
 };
 

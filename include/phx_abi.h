@@ -36,8 +36,10 @@ extern "C" {
 #define PHX_SMEAR_ADAPTIVE 1
 
 #define PHX_PREC_FP64 0        /* plain FP64 SIMT path */
-#define PHX_PREC_SPLIT_BF16 1  /* BF16 hi+lo tcgen05 GEMM, FP32 accumulate */
-#define PHX_PREC_SPLIT_TF32 2  /* TF32 hi+lo tcgen05 GEMM, FP32 accumulate */
+#define PHX_PREC_SPLIT_BF16 1  /* BF16 hi+lo tcgen05 GEMM (8+8 mantissa bits), FP32 accumulate */
+#define PHX_PREC_SPLIT_TF32 2  /* reserved: not built (rejected) */
+#define PHX_PREC_SPLIT_FP16 3  /* FP16 hi+lo tcgen05 GEMM (11+11 mantissa bits; the FC3 operand
+                                  scaled by a power of 2 per q2 chunk), FP32 accumulate */
 
 typedef struct phx_ctx phx_ctx;
 typedef struct phx_ph_h0 phx_ph_h0;
@@ -147,6 +149,15 @@ typedef struct phx_lw_params {
    * for every pair.  Runs on the FP64 path. */
   const double* window_energy;
   const double* window_cut;
+  /* Isotope scattering (src/bte/ph_scattering.cpp:616-793): per atom the
+   * reference's massVariance, i.e. the isotope mass variance of the species
+   * times the atom's mass squared (Ry mass units); NULL disables it.  Adaptive
+   * smearing takes the width from v1 and halves the delta, as the reference. */
+  const double* isotope_coupling;
+  /* Boundary scattering |v|/L n(n+1) (src/bte/ph_scattering.cpp:819-860),
+   * added after the degeneracy averaging when finalize = 1; L in Bohr, <= 0
+   * (or NaN) disables it. */
+  double boundary_length;
 } phx_lw_params;
 
 typedef struct phx_lw_stats {

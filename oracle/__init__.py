@@ -48,7 +48,7 @@ def lib():
         L.orc_ph_linewidths.restype = ctypes.c_int
         L.orc_ph_linewidths.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _D, _D, _D, _D, _D,
                                         ctypes.c_int, _D, ctypes.c_int, ctypes.c_double,
-                                        ctypes.c_int, _I, ctypes.c_int, _D, _D, _D]
+                                        ctypes.c_int, _I, ctypes.c_int, _D, _D, _D, _D, ctypes.c_double]
         L.orc_rta_kappa.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, ctypes.c_long,
                                     ctypes.c_double, _D]
         L.orc_el_diag.restype = ctypes.c_int
@@ -172,9 +172,11 @@ class Interaction3Ph:
         return outP, outM
 
     def linewidths(self, mesh, E, ev, vg, qcart, recip, temps_ry, smearing, sigma,
-                   q2_list=None, finalize=True, out=None, window=None):
+                   q2_list=None, finalize=True, out=None, window=None, isotope_coupling=None,
+                   boundary_length=0.0):
         """window: optional (energy (nq), cut (nq)): pair (q1, q2) only when
-        energy[q2] <= cut[q1]."""
+        energy[q2] <= cut[q1].  isotope_coupling: per-atom massVariance (variance x
+        mass^2); boundary_length: Bohr (0: none)."""
         nq, nb = E.shape
         m = np.ascontiguousarray(mesh, dtype=np.int32)
         T = _d(temps_ry)
@@ -188,11 +190,13 @@ class Interaction3Ph:
             ql_arr = np.ascontiguousarray(q2_list, dtype=np.int32)
             nq2, ql = len(ql_arr), ql_arr.ctypes.data_as(_I)
         we, wc = (None, None) if window is None else (_d(window[0]), _d(window[1]))
+        gi = None if isotope_coupling is None else _d(isotope_coupling)
         rc = lib().orc_ph_linewidths(self.h, nq, m.ctypes.data_as(_I), _p(Ed), _p(evd), _p(vgd),
                                      _p(qd), _p(rd), nT, _p(T), 0 if smearing == "gaussian" else 1,
                                      float(sigma), nq2, ql, int(finalize), _p(out),
                                      _p(we) if we is not None else None,
-                                     _p(wc) if wc is not None else None)
+                                     _p(wc) if wc is not None else None,
+                                     _p(gi) if gi is not None else None, float(boundary_length))
         if rc:
             raise RuntimeError("oracle linewidth builder failed: %d" % rc)
         return out

@@ -291,11 +291,13 @@ void orc_symmetrize_coupling(double* c, int nb1, int nb2, int nb3, const double*
 //   win_energy / win_cut (nq) or NULL: the pair (q1, q2) is skipped unless
 //     win_energy[q2] <= win_cut[q1] (per-q1 window of the batched-instance
 //     workload; no counterpart in the reference)
+//   iso (nat) or NULL: isotope scattering with massVariance iso (ph_scattering.cpp:616-793)
+//   boundary_length > 0: boundary scattering after the averaging (ph_scattering.cpp:819-860)
 int orc_ph_linewidths(void* p, int nq, const int* mesh, const double* E, const double* ev,
                       const double* vg, const double* qcart, const double* recip, int nT,
                       const double* Tk_ry, int smearing, double sigma, int nq2,
                       const int* q2_list, int finalize, double* out, const double* win_energy,
-                      const double* win_cut) {
+                      const double* win_cut, const double* iso, double boundary_length) {
   V3& v = *(V3*)p;
   const int nb = v.nb;
   const size_t ns = (size_t)nq * nb;
@@ -445,6 +447,48 @@ int orc_ph_linewidths(void* p, int nq, const int* mesh, const double* E, const d
         }
       }
     }
+    // isotope scattering of the (q1, q2) pairs (ph_scattering.cpp:616-793)
+    if (iso) {
+      const int nat = nb / 3;
+      for (int iq1 = 0; iq1 < nq; ++iq1) {
+        for (int ib1 = 0; ib1 < nb; ++ib1) {
+          const size_t s1 = (size_t)iq1 * nb + ib1;
+          const double en1 = E[s1];
+          if (excluded[s1] || en1 < energyCutoff) continue;
+          for (int ib2 = 0; ib2 < nb; ++ib2) {
+            const size_t s2 = (size_t)iq2 * nb + ib2;
+            const double en2 = E[s2];
+            if (excluded[s2] || en2 < energyCutoff) continue;
+            double deltaIso;
+            if (smearing == 0) {
+              deltaIso = sm.gauss(en1 - en2);
+            } else {
+              // the reference evaluates the v2 width, overwrites it with the v1 one, halves it
+              double v1[3];
+              for (int i = 0; i < 3; ++i) v1[i] = vg[s1 * 3 + i];
+              deltaIso = 0.5 * sm.adaptive(en1 - en2, v1);
+            }
+            double termIso = 0.0;
+            for (int at = 0; at < nat; ++at) {
+              double zr = 0.0, zi = 0.0;
+              for (int k = 0; k < 3; ++k) {
+                const int a = 3 * at + k;
+                const double* u1 = ev + (((size_t)iq1 * nb + a) * nb + ib1) * 2;
+                const double* u2 = ev + (((size_t)iq2 * nb + a) * nb + ib2) * 2;
+                zr += u1[0] * u2[0] + u1[1] * u2[1];   // conj(u1) u2
+                zi += u1[0] * u2[1] - u1[1] * u2[0];
+              }
+              termIso += (zr * zr + zi * zi) * iso[at];
+            }
+            termIso *= pi * 0.5 * norm * en1 * en2 * deltaIso;
+            for (int c = 0; c < nT; ++c) {
+              const double b1 = boseT[c * ns + s1], b2 = boseT[c * ns + s2];
+              out[c * ns + s1] += termIso * (b1 * b2 + 0.5 * (b1 + b2));
+            }
+          }
+        }
+      }
+    }
   }
   if (finalize) {
     // degeneracyAveragingLinewidths, scattering.cpp:1168-1207 (row iCalc=0 only)
@@ -461,6 +505,16 @@ int orc_ph_linewidths(void* p, int nq, const int* mesh, const double* E, const d
         tmp[b1] = t2 / float(n);
       }
       for (int b1 = 0; b1 < nb; ++b1) out[(size_t)iq * nb + b1] = tmp[b1];
+    }
+    // boundary scattering, after the averaging (ph_scattering.cpp:819-860)
+    if (boundary_length > 0.0) {
+      for (int c = 0; c < nT; ++c)
+        for (size_t s = 0; s < ns; ++s) {
+          if (excluded[s]) continue;
+          const double* v = vg + s * 3;
+          const double x = std::sinh(E[s] / 2.0 / Tk_ry[c]);
+          out[c * ns + s] += std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) / boundary_length * (0.25 / x / x);
+        }
     }
     for (int c = 0; c < nT; ++c)
       for (size_t s = 0; s < ns; ++s)

@@ -23,7 +23,8 @@ PHX_SMEAR_GAUSSIAN = 0
 PHX_SMEAR_ADAPTIVE = 1
 PHX_PREC_FP64 = 0
 PHX_PREC_SPLIT_BF16 = 1
-PHX_PREC_SPLIT_TF32 = 2
+PHX_PREC_SPLIT_TF32 = 2   # reserved, rejected
+PHX_PREC_SPLIT_FP16 = 3
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -35,7 +36,8 @@ class LwParams(ctypes.Structure):
     _fields_ = [("num_temperatures", ctypes.c_int), ("temperatures", _D),
                 ("smearing", ctypes.c_int), ("sigma", ctypes.c_double),
                 ("finalize", ctypes.c_int), ("q2_begin", ctypes.c_int), ("q2_end", ctypes.c_int),
-                ("window_energy", _D), ("window_cut", _D)]
+                ("window_energy", _D), ("window_cut", _D),
+                ("isotope_coupling", _D), ("boundary_length", ctypes.c_double)]
 
 
 class LwStats(ctypes.Structure):

@@ -71,10 +71,12 @@ def q2_slice(rank, world, nq):
     return rank * nq // world, (rank + 1) * nq // world
 
 
-def finalize_linewidths(A, E):
+def finalize_linewidths(A, E, vg=None, temperatures=None, boundary_length=0.0):
     """What the builder's finalize step does, for partial results summed over
-    ranks: degeneracy averaging of temperature row 0 (scattering.cpp:1168-1207)
-    and zero for excluded states (scattering.cpp:30-50, ph_scattering.cpp:900-906).
+    ranks: degeneracy averaging of temperature row 0 (scattering.cpp:1168-1207),
+    then boundary scattering |v|/L n(n+1) when boundary_length > 0
+    (ph_scattering.cpp:819-860; needs vg (nq, nb, 3) and the temperatures),
+    then zero for excluded states (scattering.cpp:30-50, ph_scattering.cpp:900-906).
     A (nT, nq*nb) summed over ranks, E (nq, nb); returns a new array."""
     E = np.asarray(E)
     nq, nb = E.shape
@@ -84,8 +86,25 @@ def finalize_linewidths(A, E):
         m = np.abs(E - E[:, b1:b1 + 1]) < C.degeneracyThreshold
         n = m.sum(axis=1).astype(np.float32).astype(np.float64)
         out[0][:, b1] = (row * m).sum(axis=1) / n
+    if boundary_length and boundary_length > 0:
+        speed = np.linalg.norm(np.asarray(vg), axis=-1)
+        ok = E >= C.phExcludeCutoff
+        for c, T in enumerate(np.atleast_1d(temperatures)):
+            with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+                x = np.sinh(E / 2.0 / T)
+                out[c][ok] += (speed / boundary_length * (0.25 / x / x))[ok]
     out[:, E < C.phExcludeCutoff] = 0.0
     return out.reshape(A.shape)
+
+
+def isotope_coupling(crystal, mass_variance):
+    """Per-atom isotope coupling of the builder: the isotope mass variance of
+    each atom's species (dimensionless, e.g. 2.0164e-4 for natural Si) times
+    the atom's mass squared -- the reference's massVariance
+    (ph_scattering.cpp:27-38)."""
+    g = np.asarray(mass_variance, dtype=np.float64)
+    m = np.asarray(crystal.atomic_masses, dtype=np.float64)
+    return g * m * m
 
 
 class PhononH0:
@@ -194,7 +213,7 @@ class BandStructure:
 
 
 PRECISIONS = {"fp64": _abi.PHX_PREC_FP64, "split_bf16": _abi.PHX_PREC_SPLIT_BF16,
-              "split_tf32": _abi.PHX_PREC_SPLIT_TF32}
+              "split_fp16": _abi.PHX_PREC_SPLIT_FP16}
 
 
 class Interaction3Ph:
@@ -281,15 +300,21 @@ class Interaction3Ph:
 class PhScatteringMatrix:
     """RTA phonon scattering rates on a full mesh (linewidth mode of the builder)."""
 
-    def __init__(self, coupling3Ph, bands, temperatures_ry, smearing="adaptive", sigma=0.0, window=None):
+    def __init__(self, coupling3Ph, bands, temperatures_ry, smearing="adaptive", sigma=0.0, window=None,
+                 isotope_coupling=None, boundary_length=0.0):
         """window: optional (energy (nq), cut (nq)) per-q1 q2 window: the pair
-        (q1, q2) counts only when energy[q2] <= cut[q1] (synth.q2_window)."""
+        (q1, q2) counts only when energy[q2] <= cut[q1] (synth.q2_window).
+        isotope_coupling: per-atom coupling (core.isotope_coupling) enables
+        isotope scattering; boundary_length > 0 (Bohr) enables boundary
+        scattering (the reference's withIsotopeScattering / boundaryLength)."""
         self.v3 = coupling3Ph
         self.bands = bands
         self.temperatures = f64(np.atleast_1d(temperatures_ry))
         self.smearing = smearing
         self.sigma = float(sigma)
         self.window = None if window is None else (f64(window[0]), f64(window[1]))
+        self.isotope = None if isotope_coupling is None else f64(isotope_coupling)
+        self.boundary_length = float(boundary_length)
         self.internalDiagonal = None
         self.stats = None
 
@@ -305,6 +330,9 @@ class PhScatteringMatrix:
         if self.window is not None:
             p.window_energy = dptr(self.window[0])
             p.window_cut = dptr(self.window[1])
+        if self.isotope is not None:
+            p.isotope_coupling = dptr(self.isotope)
+        p.boundary_length = self.boundary_length
         return p
 
     def setup(self, q2_begin=0, q2_end=None, finalize=True):

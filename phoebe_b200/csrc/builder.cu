@@ -121,7 +121,8 @@ constexpr int kFoldQ = 8;
 __global__ void __launch_bounds__(256) fold_q2_tiled_kernel(int nb, int nr2, int nr3, const double* __restrict__ D3w,
                                                             const double* __restrict__ R2, const double* __restrict__ R3,
                                                             const double* __restrict__ qcart, const double2* __restrict__ U,
-                                                            int q2_first, int q2_count, double2* __restrict__ Dp) {
+                                                            int q2_first, int q2_count, double2* __restrict__ Dp,
+                                                            unsigned* __restrict__ dmax) {
   extern __shared__ __align__(16) char sraw[];
   const int nbb = nb * nb, nb3 = nbb * nb;
   double2* ph2 = reinterpret_cast<double2*>(sraw);   // [kFoldQ][nr2]
@@ -176,6 +177,7 @@ __global__ void __launch_bounds__(256) fold_q2_tiled_kernel(int nb, int nr2, int
   }
   __syncthreads();
   // Dp[j][r3][a][b2][c] = p3 * sum_b e2(b,b2) Y(a,b,c)
+  float m = 0.f;   // largest |component| written (FP16 operand scale of the split path)
   for (int e = threadIdx.x; e < nj * nb3; e += blockDim.x) {
     const int jl = e / nb3, rest = e % nb3;
     const int a = rest / nbb, b2 = (rest / nb) % nb, c = rest % nb;
@@ -183,7 +185,14 @@ __global__ void __launch_bounds__(256) fold_q2_tiled_kernel(int nb, int nr2, int
     const double2* u = e2 + jl * nbb + b2;
     double2 z = cmk(0.0, 0.0);
     for (int b = 0; b < nb; ++b) cfma(z, u[b * nb], y[b * nb]);
-    Dp[(((size_t)(j0 + jl) * nr3 + r3) * nb + a) * nbb + b2 * nb + c] = cmul(z, p3[jl]);
+    const double2 d = cmul(z, p3[jl]);
+    Dp[(((size_t)(j0 + jl) * nr3 + r3) * nb + a) * nbb + b2 * nb + c] = d;
+    m = fmaxf(m, (float)fmax(fabs(d.x), fabs(d.y)));
+  }
+  if (dmax) {
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    // non-negative floats order like their bit patterns
+    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(dmax, __float_as_uint(m));
   }
 }
 
@@ -191,10 +200,11 @@ size_t fold_tiled_smem(int nb, int nr2) {
   return sizeof(double2) * ((size_t)kFoldQ * (nr2 + nb * nb + nb * nb * nb) + kFoldQ);
 }
 void fold_tiled_launch(int nb, int nr2, int nr3, const phx_v3* v, const phx_bands* b, int c0, int cnt,
-                       double2* Dp, cudaStream_t st) {
+                       double2* Dp, cudaStream_t st, unsigned* dmax = nullptr) {
   dim3 gf(nr3, (cnt + kFoldQ - 1) / kFoldQ);
   fold_q2_tiled_kernel<<<gf, 256, fold_tiled_smem(nb, nr2), st>>>(nb, nr2, nr3, v->d_D3w, v->d_R2, v->d_R3, b->d_q,
-                                                                  reinterpret_cast<const double2*>(b->d_U), c0, cnt, Dp);
+                                                                  reinterpret_cast<const double2*>(b->d_U), c0, cnt, Dp,
+                                                                  dmax);
 }
 
 struct PairArgs {
@@ -680,8 +690,101 @@ __global__ void __launch_bounds__(kGenThreads) pair_generic_kernel(PairArgs P, Q
   }
 }
 
+// Isotope scattering (ph_scattering.cpp:616-793), linewidth mode: one thread
+// per (q1, b1) of a tile of kTile q1, looping over the q2 of its slot;
+//   rate = pi/2 norm w1 w2 delta(w1 - w2) sum_atoms g_a |sum_k conj(U1(3a+k,b1)) U2(3a+k,b2)|^2
+//          (n1 n2 + (n1 + n2)/2),
+// with U mass-scaled and g_a the reference's massVariance (variance x mass^2).
+// Adaptive smearing takes its width from v1 and halves the delta, as the
+// reference does (:684-687).  Rates go to the partial sums of the slot.
+struct IsoArgs {
+  MeshArgs m;
+  int nat;
+  const double* g;      // (nat)
+  int q2_first, q2_count, q2_per_slot;
+  double* partial;      // (S, nq, nb, nT)
+};
+
+inline size_t iso_smem(int nb) { return sizeof(double2) * nb * nb + sizeof(double) * nb; }
+
+__global__ void __launch_bounds__(kTile * kMaxNbGeneric) isotope_kernel(IsoArgs A) {
+  const MeshArgs& M = A.m;
+  extern __shared__ __align__(16) char sraw[];
+  const int nb = M.nb, nbb = nb * nb, nT = M.nT, nq = M.nq;
+  double2* U2 = reinterpret_cast<double2*>(sraw);           // [nb][nb]
+  double* E2 = reinterpret_cast<double*>(U2 + nbb);         // [nb]
+  const int tid = threadIdx.x, ql = tid % kTile, b1 = tid / kTile;
+  const int q1 = blockIdx.x * kTile + ql;
+  const bool active = b1 < nb && q1 < nq;
+  const int q1c = active ? q1 : 0, b1c = active ? b1 : 0;
+  const double en1 = M.E[(size_t)q1c * nb + b1c];
+  const bool ok1 = active && en1 >= phxc::phExcludeCutoff && en1 >= phxc::phEnergyCutoff;
+  double2 u1[kMaxNbGeneric];
+#pragma unroll
+  for (int a = 0; a < kMaxNbGeneric; ++a)
+    u1[a] = a < nb ? M.U[(size_t)q1c * nbb + a * nb + b1c] : cmk(0.0, 0.0);
+  double sg1 = M.sigma;
+  bool vz1 = false;
+  if (M.smearing == PHX_SMEAR_ADAPTIVE && M.vg) {
+    const double* v = M.vg + ((size_t)q1c * nb + b1c) * 3;
+    vz1 = (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) == 0.0;
+    sg1 = floor_sigma(adaptive_sigma(M.qT, v[0], v[1], v[2]));
+  }
+  double n1[kMaxT], acc[kMaxT];
+#pragma unroll
+  for (int c = 0; c < kMaxT; ++c) {
+    n1[c] = c < nT ? M.bose[((size_t)c * nq + q1c) * nb + b1c] : 0.0;
+    acc[c] = 0.0;
+  }
+  const int jbeg = blockIdx.y * A.q2_per_slot;
+  const int jend = min(A.q2_count, jbeg + A.q2_per_slot);
+  for (int j = jbeg; j < jend; ++j) {
+    const int iq2 = A.q2_first + j;
+    __syncthreads();
+    for (int e = tid; e < nbb; e += blockDim.x) U2[e] = M.U[(size_t)iq2 * nbb + e];
+    for (int b = tid; b < nb; b += blockDim.x) E2[b] = M.E[(size_t)iq2 * nb + b];
+    __syncthreads();
+    if (!ok1) continue;
+    for (int b2 = 0; b2 < nb; ++b2) {
+      const double en2 = E2[b2];
+      if (en2 < phxc::phExcludeCutoff || en2 < phxc::phEnergyCutoff) continue;
+      double dl;
+      if (M.smearing == PHX_SMEAR_GAUSSIAN) dl = delta_fn(PHX_SMEAR_GAUSSIAN, M.sigma, en1 - en2, false);
+      else dl = 0.5 * delta_fn(PHX_SMEAR_ADAPTIVE, sg1, en1 - en2, vz1);
+      if (dl == 0.0) continue;
+      // z_atom = sum_k conj(U1(3 atom + k, b1)) U2(3 atom + k, b2)
+      constexpr int kAt = (kMaxNbGeneric + 2) / 3;
+      double2 z[kAt];
+#pragma unroll
+      for (int at = 0; at < kAt; ++at) z[at] = cmk(0.0, 0.0);
+#pragma unroll
+      for (int a = 0; a < kMaxNbGeneric; ++a)
+        if (a < nb) cfmac(z[a / 3], U2[a * nb + b2], u1[a]);
+      double term = 0.0;
+#pragma unroll
+      for (int at = 0; at < kAt; ++at)
+        if (at < A.nat) term += (z[at].x * z[at].x + z[at].y * z[at].y) * A.g[at];
+      term *= phxc::pi * 0.5 * M.norm * en1 * en2 * dl;
+#pragma unroll
+      for (int c = 0; c < kMaxT; ++c)
+        if (c < nT) {
+          const double n2 = M.bose[((size_t)c * nq + iq2) * nb + b2];
+          acc[c] += term * (n1[c] * n2 + 0.5 * (n1[c] + n2));
+        }
+    }
+  }
+  if (active) {
+    double* out = A.partial + (((size_t)blockIdx.y * nq + q1) * nb + b1) * nT;
+    for (int c = 0; c < nT; ++c) out[c] += acc[c];
+  }
+}
+
+// Sums the partial slots into A_out; with finalize: degeneracy averaging of
+// row 0, then boundary scattering |v|/L n(n+1) on every row (added after the
+// averaging, ph_scattering.cpp:819-860), then zero for excluded states.
 __global__ void finalize_kernel(int nq, int nb, int nT, int nslots, const double* __restrict__ partial,
-                                const double* __restrict__ E, int finalize,
+                                const double* __restrict__ E, int finalize, const double* __restrict__ vg,
+                                const double* __restrict__ temps, double boundary_length,
                                 double* __restrict__ Aout) {
   const int iq = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= nq) return;
@@ -708,6 +811,15 @@ __global__ void finalize_kernel(int nq, int nb, int nT, int nslots, const double
       }
       for (int b = 0; b < nb; ++b) lw[b] = tmp[b];
     }
+    if (finalize && boundary_length > 0.0 && vg) {
+      for (int b = 0; b < nb; ++b) {
+        const double e = E[(size_t)iq * nb + b];
+        if (e < phxc::phExcludeCutoff) continue;
+        const double* v = vg + ((size_t)iq * nb + b) * 3;
+        const double x = sinh(e / 2.0 / temps[c]);
+        lw[b] += sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) / boundary_length * (0.25 / x / x);
+      }
+    }
     for (int b = 0; b < nb; ++b) {
       double v = lw[b];
       if (finalize && E[(size_t)iq * nb + b] < phxc::phExcludeCutoff) v = 0.0;
@@ -731,7 +843,10 @@ int phx_split_pack_records(phx_ctx* ctx, const pairc::MeshArgs& M, void* rec, in
 int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v, const phx_bands* b,
                          const double2* Dp, uint8_t* Bimg, const void* rec, double emax, int q2_first,
                          int q2_count, int slots, double* partial, int* launches, cudaEvent_t ev_begin,
-                         cudaEvent_t ev_end);
+                         cudaEvent_t ev_end, int fp16, const unsigned* dmax, void* edges, unsigned* edge_count,
+                         unsigned edge_cap);
+unsigned phx_split_edge_cap();
+size_t phx_split_edge_bytes();
 
 int phx_scratch_reserve(phx_v3* v, size_t bytes) {
   return phx_ctx_reserve(v->ctx, &v->ctx->d_scratch, &v->ctx->scratch_bytes, bytes);
@@ -1065,7 +1180,10 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   const size_t sz_T = align_up(sizeof(double) * 8);
   const size_t sz_img = split ? align_up(phx_split_bimg_bytes(max_chunk, nr3)) : 0;
   const size_t sz_rec = split ? align_up(phx_split_rec_bytes(nq)) : 0;
-  PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_img + sz_rec));
+  const size_t sz_iso = p->isotope_coupling ? align_up(sizeof(double) * v->nat) : 0;
+  const size_t sz_max = align_up(sizeof(unsigned) * 2);
+  const size_t sz_edge = split ? align_up(phx_split_edge_bytes()) : 0;
+  PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_img + sz_rec + sz_iso + sz_max + sz_edge));
   char* base = static_cast<char*>(v->ctx->d_scratch);
   double2* Dp = reinterpret_cast<double2*>(base);
   double* partial = reinterpret_cast<double*>(base + sz_dp);
@@ -1073,6 +1191,14 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   double* temps = reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose);
   uint8_t* Bimg = reinterpret_cast<uint8_t*>(base + sz_dp + sz_part + sz_bose + sz_T);
   void* rec = base + sz_dp + sz_part + sz_bose + sz_T + sz_img;
+  double* giso = p->isotope_coupling ? reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose + sz_T + sz_img +
+                                                                 sz_rec)
+                                     : nullptr;
+  // FP16 operands of the split path: max |Dp| of the current chunk
+  const int fp16 = v->precision == PHX_PREC_SPLIT_FP16 ? 1 : 0;
+  unsigned* dmax = reinterpret_cast<unsigned*>(base + sz_dp + sz_part + sz_bose + sz_T + sz_img + sz_rec + sz_iso);
+  unsigned* edge_count = dmax + 1;
+  void* edges = base + sz_dp + sz_part + sz_bose + sz_T + sz_img + sz_rec + sz_iso + sz_max;
   if (split) {
     PHX_ARG(ctx, NB == 6, "split-precision path supports nb = 6");
     PHX_ARG(ctx, phx_split_smem_bytes(nr3) <= 227 * 1024, "too many R3 vectors for the split path");
@@ -1125,11 +1251,12 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   // one chunk of the q2 loop; pe0/pe1 (may be null) bracket its pair kernel
   auto chunk_work = [&](const BuilderPlan& pl, int c0, int cnt, cudaEvent_t pe0, cudaEvent_t pe1,
                         int* launches) -> int {
-    fold_tiled_launch(NB, nr2, nr3, v, b, c0, cnt, Dp, st);
+    if (fp16) PHX_CUDA(ctx, cudaMemsetAsync(dmax, 0, sizeof(unsigned), st));
+    fold_tiled_launch(NB, nr2, nr3, v, b, c0, cnt, Dp, st, fp16 ? dmax : nullptr);
     ++*launches;
     if (split)
       return phx_split_pair_chunk(ctx, P.m, v, b, Dp, Bimg, rec, emax, c0, cnt, pl.slots, partial, launches,
-                                  pe0, pe1);
+                                  pe0, pe1, fp16, dmax, edges, edge_count, phx_split_edge_cap());
     PairArgs Q = P;
     Q.q2_first = c0;
     Q.q2_count = cnt;
@@ -1143,10 +1270,12 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   };
   PHX_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
   PHX_CUDA(ctx, cudaMemcpyAsync(temps, p->temperatures, sizeof(double) * nT, cudaMemcpyHostToDevice, st));
+  if (giso)
+    PHX_CUDA(ctx, cudaMemcpyAsync(giso, p->isotope_coupling, sizeof(double) * v->nat, cudaMemcpyHostToDevice, st));
   // launch plan: tuned once per problem shape
   int dev = 0;
   cudaGetDevice(&dev);
-  const PlanKey pk{split ? 1 : 0, NB, nq, nr3, nr2, nT, dev};
+  const PlanKey pk{split ? 1 + fp16 : 0, NB, nq, nr3, nr2, nT, dev};
   BuilderPlan plan = cands[0];
   if (!env_off("PHX_TUNE") && q2e - q2b >= 2 * cands[0].chunk && !find_plan(pk, &plan)) {
     int dummy = 0;
@@ -1201,17 +1330,25 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
       PHX_TRY(chunk_work(plan, c0, cnt, pe0, pe1, &launches));
     }
     PHX_CUDA(ctx, phx_record_event(g.vertex_end, st));
-    finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, NB, nT, nslots, partial, b->d_E, p->finalize, Aout_d);
+    if (giso) {
+      IsoArgs I{P.m, v->nat, giso, q2b, q2e - q2b, (q2e - q2b + nslots - 1) / nslots, partial};
+      isotope_kernel<<<dim3(tiles, nslots), kTile * NB, iso_smem(NB), st>>>(I);
+      ++launches;
+      PHX_CUDA(ctx, cudaGetLastError());
+    }
+    finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, NB, nT, nslots, partial, b->d_E, p->finalize, b->d_vg,
+                                                      temps, p->boundary_length, Aout_d);
     ++launches;
     PHX_CUDA(ctx, cudaGetLastError());
     g.launches = launches;
     return PHX_OK;
   };
   const std::vector<uint64_t> key = {
-      (uint64_t)(split ? 1 : 0), (uint64_t)NB, (uint64_t)nq, (uint64_t)nT, (uint64_t)q2b, (uint64_t)q2e,
+      (uint64_t)(split ? 1 + fp16 : 0), (uint64_t)NB, (uint64_t)nq, (uint64_t)nT, (uint64_t)q2b, (uint64_t)q2e,
       (uint64_t)p->smearing, bits(p->sigma), (uint64_t)p->finalize, (uint64_t)plan.chunk, (uint64_t)plan.slots,
       bits(emax), bits(base), bits(Aout_d), bits(b->d_E), bits(b->d_U), bits(b->d_vg), bits(b->d_q),
-      bits(b->d_U32), bits(b->d_q1_order), bits(v->d_D3w), bits(v->d_R2), bits(v->d_R3), bits(ctx->d_status)};
+      bits(b->d_U32), bits(b->d_q1_order), bits(v->d_D3w), bits(v->d_R2), bits(v->d_R3), bits(ctx->d_status),
+      bits(giso), bits(p->boundary_length)};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   PHX_CUDA(ctx, cudaEventCreate(&ev0));
   PHX_CUDA(ctx, cudaEventCreate(&ev1));
@@ -1232,8 +1369,9 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   }
   if (rc == PHX_OK && kst) {
     cudaMemset(ctx->d_status, 0, sizeof(int));
-    phx_set_error(ctx, PHX_ERR_CUDA, "pair kernel gave up waiting on a pipeline barrier (status " +
-                                         std::to_string(kst) + ")");
+    phx_set_error(ctx, PHX_ERR_CUDA, (kst & (1 << 20)) ? std::string("split path: near-cut-off event list overflowed")
+                                                       : "pair kernel gave up waiting on a pipeline barrier (status " +
+                                                             std::to_string(kst) + ")");
     rc = PHX_ERR_CUDA;
   }
   if (rc == PHX_OK && stats) {
@@ -1289,14 +1427,19 @@ int run_builder_generic(phx_v3* v, phx_bands* b, const phx_lw_params* p, double*
   const size_t sz_bose = align_up(sizeof(double) * nT * nq * nb);
   const size_t sz_T = align_up(sizeof(double) * 8);
   const size_t sz_win = windowed ? align_up(sizeof(double) * 2 * nq) : 0;
-  PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_win));
+  const size_t sz_iso = p->isotope_coupling ? align_up(sizeof(double) * v->nat) : 0;
+  PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_win + sz_iso));
   char* base = static_cast<char*>(v->ctx->d_scratch);
   double2* Dp = reinterpret_cast<double2*>(base);
   double* partial = reinterpret_cast<double*>(base + sz_dp);
   double* bose = reinterpret_cast<double*>(base + sz_dp + sz_part);
   double* temps = reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose);
   double* wdev = reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose + sz_T);
+  double* giso = p->isotope_coupling ? reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose + sz_T + sz_win)
+                                     : nullptr;
   PHX_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
+  if (giso)
+    PHX_CUDA(ctx, cudaMemcpyAsync(giso, p->isotope_coupling, sizeof(double) * v->nat, cudaMemcpyHostToDevice, st));
   PHX_CUDA(ctx, cudaMemcpyAsync(temps, p->temperatures, sizeof(double) * nT, cudaMemcpyHostToDevice, st));
   if (windowed) {
     PHX_CUDA(ctx, cudaMemcpyAsync(wdev, p->window_energy, sizeof(double) * nq, cudaMemcpyHostToDevice, st));
@@ -1390,7 +1533,14 @@ int run_builder_generic(phx_v3* v, phx_bands* b, const phx_lw_params* p, double*
     PHX_CUDA(ctx, phx_record_event(g.vertex_begin, st));
     for (int c0 = q2b; c0 < q2e; c0 += chunk) PHX_TRY(chunk_work(c0, std::min(chunk, q2e - c0), slots, &launches));
     PHX_CUDA(ctx, phx_record_event(g.vertex_end, st));
-    finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, nb, nT, slots, partial, b->d_E, p->finalize, Aout_d);
+    if (giso) {
+      IsoArgs I{P.m, v->nat, giso, q2b, q2e - q2b, (q2e - q2b + slots - 1) / slots, partial};
+      isotope_kernel<<<dim3((nq + kTile - 1) / kTile, slots), kTile * nb, iso_smem(nb), st>>>(I);
+      ++launches;
+      PHX_CUDA(ctx, cudaGetLastError());
+    }
+    finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, nb, nT, slots, partial, b->d_E, p->finalize, b->d_vg,
+                                                      temps, p->boundary_length, Aout_d);
     ++launches;
     PHX_CUDA(ctx, cudaGetLastError());
     g.launches = launches;
@@ -1400,7 +1550,7 @@ int run_builder_generic(phx_v3* v, phx_bands* b, const phx_lw_params* p, double*
       (uint64_t)(windowed ? 3 : 2), (uint64_t)nb, (uint64_t)nq, (uint64_t)nT, (uint64_t)q2b, (uint64_t)q2e,
       (uint64_t)p->smearing, bits(p->sigma), (uint64_t)p->finalize, (uint64_t)chunk, (uint64_t)slots, bits(base),
       bits(Aout_d), bits(b->d_E), bits(b->d_U), bits(b->d_vg), bits(b->d_q), bits(v->d_D3w), bits(v->d_R2),
-      bits(v->d_R3), bits(ctx->d_status)};
+      bits(v->d_R3), bits(ctx->d_status), bits(giso), bits(p->boundary_length)};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   PHX_CUDA(ctx, cudaEventCreate(&ev0));
   PHX_CUDA(ctx, cudaEventCreate(&ev1));
@@ -1452,6 +1602,7 @@ extern "C" int phx_ph_linewidths_d(phx_v3* v, phx_bands* b, const phx_lw_params*
   PHX_ARG(ctx, p->smearing != PHX_SMEAR_GAUSSIAN || p->sigma > 0.0, "Gaussian smearing needs sigma > 0");
   PHX_ARG(ctx, p->smearing != PHX_SMEAR_ADAPTIVE || b->d_vg, "adaptive smearing needs velocities");
   PHX_ARG(ctx, 0 <= p->q2_begin && p->q2_begin <= p->q2_end && p->q2_end <= b->nq, "bad q2 range");
+  PHX_ARG(ctx, !(p->boundary_length > 0.0) || b->d_vg, "boundary scattering needs velocities");
   PHX_CUDA(ctx, cudaSetDevice(ctx->device));
   if (p->q2_begin == p->q2_end) {
     PHX_CUDA(ctx, cudaMemsetAsync(Aout_d, 0, sizeof(double) * p->num_temperatures * b->nq * b->nb, ctx->stream));
@@ -1618,7 +1769,8 @@ int run_builder_static(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
     pair_fp64_kernel<NB><<<dim3(tiles, 1), kTile * NB, smem_pair, st>>>(P);
     PHX_CUDA(ctx, cudaGetLastError());
   }
-  finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, NB, nT, 1, partial, b->d_E, p->finalize, Aout_d);
+  finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, NB, nT, 1, partial, b->d_E, p->finalize, nullptr, nullptr,
+                                                    0.0, Aout_d);
   PHX_CUDA(ctx, cudaGetLastError());
   PHX_CUDA(ctx, cudaStreamSynchronize(st));
   return PHX_OK;
@@ -1640,6 +1792,8 @@ extern "C" int phx_ph_linewidths_static(phx_v3* v, phx_bands* b, const phx_lw_pa
   PHX_ARG(ctx, 0 <= p->q2_begin && p->q2_begin <= p->q2_end && p->q2_end <= b->nq, "bad q2 range");
   PHX_ARG(ctx, v->nb == 6, "phx_ph_linewidths_static: this build supports nb = 6");
   PHX_ARG(ctx, !p->window_energy && !p->window_cut, "phx_ph_linewidths_static: no q2 window");
+  PHX_ARG(ctx, !p->isotope_coupling && !(p->boundary_length > 0.0),
+          "phx_ph_linewidths_static: no isotope or boundary scattering");
   PHX_CUDA(ctx, cudaSetDevice(ctx->device));
   if (p->q2_begin == p->q2_end) {
     PHX_CUDA(ctx, cudaMemsetAsync(Aout_d, 0, sizeof(double) * p->num_temperatures * b->nq * b->nb, ctx->stream));

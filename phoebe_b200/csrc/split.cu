@@ -32,6 +32,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <vector>
 
 #include "pair_common.cuh"
@@ -77,7 +78,44 @@ struct TcArgs {
   float tol;                   // margin of the FP32 liveness windows (Ry)
   double* partial;             // (S, nq, nb, nT)
   int* status;
+  int fp16;                    // operands FP16 hi/lo (B scaled by a power of 2) instead of BF16 hi/lo
+  const unsigned* dmax;        // FP16: bits of max |Dp| of the chunk (written by the fold)
+  struct EdgeEvent* edges;     // near-cut-off processes, re-decided in FP64 by edge_fix_kernel
+  unsigned* edge_count;
+  unsigned edge_cap;
 };
+
+// A queued triplet one of whose adaptive deltas sat within 1e-5 of the
+// |E| > 2 sigma cut-off: the queue entry and where it was evaluated.
+struct EdgeEvent {
+  unsigned where;    // tile << 12 | slot << 7 | row
+  int iq2;
+  uint2 entry;       // the queue entry (|V|^2 / n1, meta)
+};
+
+// Power-of-2 scale of the B operand for FP16 hi/lo: max |Dp| * scale in [0.5, 1]
+__device__ __forceinline__ float fp16_scale(unsigned maxbits) {
+  const float m = __uint_as_float(maxbits);
+  if (!(m > 0.f)) return 1.f;
+  int e;
+  frexpf(m, &e);
+  return ldexpf(1.f, -e);
+}
+
+// hi/lo split of v into two 16-bit values of the operand format
+__device__ __forceinline__ void split16(double v, bool fp16, uint16_t* hi, uint16_t* lo) {
+  if (fp16) {
+    const __half h = __double2half(v);
+    const __half l = __double2half(v - (double)__half2float(h));
+    *hi = __half_as_ushort(h);
+    *lo = __half_as_ushort(l);
+  } else {
+    const __nv_bfloat16 h = __double2bfloat16(v);
+    const __nv_bfloat16 l = __double2bfloat16(v - (double)__bfloat162float(h));
+    *hi = __bfloat16_as_ushort(h);
+    *lo = __bfloat16_as_ushort(l);
+  }
+}
 
 // ---------------------------------------------------------------------------
 // degenerate blocks of 6 sorted energies, packed as 3-bit block starts
@@ -106,6 +144,19 @@ __device__ __forceinline__ unsigned blk_mask(unsigned p, int b) {
 // ---------------------------------------------------------------------------
 // records and B images
 // ---------------------------------------------------------------------------
+// A velocity projection p is kept as its FP32 value ph and, in FP16, the
+// residual (p - ph) relative to |ph| 2^-24 (|r| <= 1): together ~35 bits,
+// enough to settle the reference's |E| > 2 sigma cut-off like FP64 does
+// when the FP32 comparison is too close to call.
+__device__ __forceinline__ uint16_t proj_residual(double p, float ph) {
+  if (ph == 0.f) return 0;
+  const double r = (p - (double)ph) / fabs((double)ph) * 16777216.0;
+  return __half_as_ushort(__double2half(r));
+}
+__device__ __forceinline__ double proj_fp64(float ph, unsigned r) {
+  return (double)ph + (double)__half2float(__ushort_as_half((unsigned short)r)) * fabs((double)ph) * 5.9604644775390625e-8;
+}
+
 __global__ void pack_records_kernel(MeshArgs M, uint4* __restrict__ rec) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= M.nq) return;
@@ -124,16 +175,31 @@ __global__ void pack_records_kernel(MeshArgs M, uint4* __restrict__ rec) {
     const unsigned long long eb = (unsigned long long)__double_as_longlong(e[b]);
     o[0] = (uint32_t)eb;
     o[1] = (uint32_t)(eb >> 32);
+    uint16_t plo[3];
     for (int i = 0; i < 3; ++i) {
       double p = 0.0;
       if (M.smearing == PHX_SMEAR_ADAPTIVE && M.vg)
         for (int j = 0; j < 3; ++j) p += M.qT[3 * i + j] * M.vg[((size_t)q * 6 + b) * 3 + j];
-      o[2 + i] = __float_as_uint((float)p);
+      const float ph = (float)p;
+      o[i < 2 ? 2 + i : 4] = __float_as_uint(ph);
+      plo[i] = proj_residual(p, ph);
     }
     o[5] = __float_as_uint(e[b] > 0.0 ? (float)(1.0 / e[b]) : 0.f);
     for (int t = 0; t < kMaxT; ++t)
       o[6 + t] = __float_as_uint(t < M.nT ? (float)M.bose[((size_t)t * M.nq + q) * 6 + b] : 0.f);
-    o[10] = o[11] = 0u;
+    // fingerprint of the FP64 velocity: the reference's adaptive width is zero
+    // only when two velocities are equal in FP64, which FP32 projections
+    // cannot tell from a tiny non-zero difference (then floored at 1e-4 eV)
+    unsigned long long h = 0x9E3779B97F4A7C15ull;
+    if (M.smearing == PHX_SMEAR_ADAPTIVE && M.vg)
+      for (int j = 0; j < 3; ++j) {
+        const double vj = M.vg[((size_t)q * 6 + b) * 3 + j] + 0.0;   // -0 -> +0
+        h ^= (unsigned long long)__double_as_longlong(vj);
+        h *= 0xBF58476D1CE4E5B9ull;
+        h ^= h >> 31;
+      }
+    o[10] = ((uint32_t)(h ^ (h >> 32)) & 0xFFFFu) | ((uint32_t)plo[2] << 16);
+    o[11] = (uint32_t)plo[0] | ((uint32_t)plo[1] << 16);
   }
   w[4 * kChGp] = pack_blocks(e);
   w[4 * kChGp + 1] = w[4 * kChGp + 2] = w[4 * kChGp + 3] = 0u;
@@ -142,10 +208,11 @@ __global__ void pack_records_kernel(MeshArgs M, uint4* __restrict__ rec) {
   for (int c = 0; c < kRecChunks; ++c) dst[c] = make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
 }
 
-// Dp (FP64 complex [j][r3][a][b2][c]) -> BF16 hi/lo K-major tiles
+// Dp (FP64 complex [j][r3][a][b2][c]) -> BF16 (or scaled FP16) hi/lo K-major tiles
 __global__ void convert_b_kernel(const double2* __restrict__ Dp, int nr3, int Kp, int q2_count,
-                                 uint8_t* __restrict__ Bimg) {
+                                 uint8_t* __restrict__ Bimg, int fp16, const unsigned* __restrict__ dmax) {
   const int nkc = Kp / kKC;
+  const double sc = fp16 ? (double)fp16_scale(*dmax) : 1.0;
   const int j = blockIdx.x;
   const int h = blockIdx.y / nkc, kc = blockIdx.y % nkc;
   if (j >= q2_count) return;
@@ -162,13 +229,13 @@ __global__ void convert_b_kernel(const double2* __restrict__ Dp, int nr3, int Kp
       const int part = kg < nr3 ? 0 : 1;
       const int r3 = part ? kg - nr3 : kg;
       const double2 B = D[(size_t)r3 * 216 + a * 36 + b2 * 6 + c];
-      v = ri == 0 ? (part == 0 ? B.x : -B.y) : (part == 0 ? B.y : B.x);
+      v = (ri == 0 ? (part == 0 ? B.x : -B.y) : (part == 0 ? B.y : B.x)) * sc;
     }
-    const __nv_bfloat16 hi = __double2bfloat16(v);
-    const __nv_bfloat16 lo = __double2bfloat16(v - (double)__bfloat162float(hi));
+    uint16_t hi, lo;
+    split16(v, fp16 != 0, &hi, &lo);
     const uint32_t off = tc::core_offset(n, kk, kKC, 2);
-    *reinterpret_cast<__nv_bfloat16*>(img + off) = hi;
-    *reinterpret_cast<__nv_bfloat16*>(img + kPartBytes + off) = lo;
+    *reinterpret_cast<uint16_t*>(img + off) = hi;
+    *reinterpret_cast<uint16_t*>(img + kPartBytes + off) = lo;
   }
 }
 
@@ -183,9 +250,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 struct Band {            // one band of one point
   double E;
-  float P[3];            // qT.v (adaptive smearing)
+  float P[3];            // qT.v (adaptive smearing), FP32
   float iE;              // 1/E
   float N[kMaxT];        // Bose factors
+  unsigned vf;           // 16-bit fingerprint of the FP64 velocity
 };
 
 // c0 points at the band's first chunk, the next two follow at stride st
@@ -200,12 +268,10 @@ __device__ __forceinline__ Band load_band(const uint4* c0, int st) {
   x.iE = __uint_as_float(b.y);
   x.N[0] = __uint_as_float(b.z);
   x.N[1] = __uint_as_float(b.w);
-  x.N[2] = x.N[3] = 0.f;
-  if (NT > 2) {
-    const uint2 c = *reinterpret_cast<const uint2*>(c0 + 2 * st);
-    x.N[2] = __uint_as_float(c.x);
-    x.N[3] = __uint_as_float(c.y);
-  }
+  const uint4 c = c0[2 * st];
+  x.N[2] = NT > 2 ? __uint_as_float(c.x) : 0.f;
+  x.N[3] = NT > 2 ? __uint_as_float(c.y) : 0.f;
+  x.vf = c.z & 0xFFFFu;
   return x;
 }
 
@@ -216,27 +282,55 @@ struct Sig {
 
 // AdaptiveGaussianDeltaFunction::getSmearing (delta_function.cpp:71-83) from
 // the projections P = qT.v: sigma^2 = |P2 - P3|^2 / 6, floored at 1e-4 eV.
-__device__ __forceinline__ Sig sigma_ad(const float* P2, const float* P3) {
+// The width is zero only for velocities equal in FP64 (same fingerprint and
+// same projections); a difference lost in the FP32 projections is below the
+// floor, which is what the FP64 width would be raised to.
+__device__ __forceinline__ Sig sigma_ad(const float* P2, const float* P3, unsigned f2, unsigned f3) {
   const float d0 = P2[0] - P3[0], d1 = P2[1] - P3[1], d2 = P2[2] - P3[2];
   float s2 = fmaf(d0, d0, fmaf(d1, d1, d2 * d2)) * (1.f / 6.f);
   Sig g;
-  g.vz = d0 == 0.f && d1 == 0.f && d2 == 0.f;
+  g.vz = f2 == f3 && d0 == 0.f && d1 == 0.f && d2 == 0.f;
   constexpr float kCut = (float)phxc::adaptiveCutoff;
-  if (s2 != 0.f && s2 < kCut * kCut) s2 = kCut * kCut;
+  if (!g.vz && s2 < kCut * kCut) s2 = kCut * kCut;
   const float r = s2 > 0.f ? rsqrtf(s2) : 0.f;
   g.s = s2 * r;
   g.inv = r;
   return g;
 }
 
-// delta of one process in FP32 from an FP64 energy difference, 0 where the
-// reference's cut-offs make it zero (delta_function.cpp:34-96).  Gaussian:
-// x < -8.5 contributes below 1e-31 of the peak and is dropped.
-__device__ __forceinline__ float delta_ad(const Sig& g, double de) {
+// |de| > 2 sigma decided with the FP64 width of the projections refined by
+// their residuals (floored as the reference does)
+// The bands' records: three consecutive chunks from a and from b.  Word 10
+// (chunk 2 .z) holds the fingerprint and above it the FP16 residual of P[2],
+// word 11 (.w) the residuals of P[0] and P[1].
+__device__ bool beyond_two_sigma(double de, const uint4* a, const uint4* b) {
+  const uint4 a0 = a[0], a1 = a[1], a2 = a[2];
+  const uint4 b0 = b[0], b1 = b[1], b2 = b[2];
+  const float pa[3] = {__uint_as_float(a0.z), __uint_as_float(a0.w), __uint_as_float(a1.x)};
+  const float pb[3] = {__uint_as_float(b0.z), __uint_as_float(b0.w), __uint_as_float(b1.x)};
+  const unsigned ra[3] = {a2.w & 0xFFFFu, a2.w >> 16, a2.z >> 16};
+  const unsigned rb[3] = {b2.w & 0xFFFFu, b2.w >> 16, b2.z >> 16};
+  double s2 = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    const double d = proj_fp64(pa[i], ra[i]) - proj_fp64(pb[i], rb[i]);
+    s2 += d * d;
+  }
+  double sg = sqrt(s2 / 6.0);
+  if (sg != 0.0 && sg < phxc::adaptiveCutoff) sg = phxc::adaptiveCutoff;
+  return fabs(de) > 2.0 * sg;
+}
+
+// Adaptive delta of one process from the FP32 width and the FP64 energy
+// difference, with the reference's cut-offs (delta_function.cpp:65-96).  The
+// cut-off |E| > 2 sigma is discontinuous; `near` is set when the FP32
+// comparison is within 1e-5 of it, and the caller then re-decides in FP64.
+__device__ __forceinline__ float delta_ad(const Sig& g, double de, bool& near) {
   if (g.vz && de == 0.0) return 1.f;
   if (g.s == 0.f) return 0.f;
   const float e = (float)de;
-  if (fabsf(e) > 2.f * g.s) return 0.f;
+  const float two_s = 2.f * g.s;
+  near = fabsf(fabsf(e) - two_s) <= two_s * 1e-5f;
+  if (fabsf(e) > two_s) return 0.f;
   const float x = e * g.inv;
   return __expf(-x * x) * g.inv * (float)(1.0 / (phxc::sqrtPi * phxc::erf2));
 }
@@ -250,21 +344,22 @@ __device__ __forceinline__ float delta_ga(float inv, double de) {
 // of (q1,q2) and the two "-" processes of (q1,-q2), as ph_scattering.cpp:338-380
 // and :466-518 (cut-offs, deltas, Bose factors), times 0.5 (the linewidth
 // convention of :433,:574); multiply by |V|^2.
-template <int NT>
-__device__ __forceinline__ void rate_f(int smearing, float ginv, float pre, double E1, float iE1,
-                                       const float* n1, const Band& x2, const Band& x2m,
-                                       const Band& x3, const Sig& gp, const Sig& gm, float* f) {
-#pragma unroll
-  for (int t = 0; t < NT; ++t) f[t] = 0.f;
-  if (!(x3.E >= phxc::phEnergyCutoff)) return;
+// The three deltas of one triplet; `near` gets a bit per adaptive process
+// whose FP32 cut-off decision was too close to call (+, -1, -2).
+__device__ __forceinline__ void deltas3(int smearing, float ginv, double E1, const Band& x2, const Band& x2m,
+                                        const Band& x3, const Sig& gp, const Sig& gm, float& dp, float& d1,
+                                        float& d2, unsigned& near) {
   const bool ok2 = x2.E >= phxc::phExcludeCutoff, ok2m = x2m.E >= phxc::phExcludeCutoff;
-  float dp = 0.f, d1 = 0.f, d2 = 0.f;
+  dp = d1 = d2 = 0.f;
+  near = 0u;
   if (smearing == PHX_SMEAR_ADAPTIVE) {
-    if (ok2) dp = delta_ad(gp, E1 + x2.E - x3.E);
+    bool np = false, n1 = false, n2 = false;
+    if (ok2) dp = delta_ad(gp, E1 + x2.E - x3.E, np);
     if (ok2m) {
-      d1 = delta_ad(gm, E1 + x3.E - x2m.E);
-      d2 = delta_ad(gm, x2m.E + x3.E - E1);
+      d1 = delta_ad(gm, E1 + x3.E - x2m.E, n1);
+      d2 = delta_ad(gm, x2m.E + x3.E - E1, n2);
     }
+    near = (np ? 1u : 0u) | (n1 ? 2u : 0u) | (n2 ? 4u : 0u);
   } else {
     if (ok2) dp = delta_ga(ginv, E1 + x2.E - x3.E);
     if (ok2m) {
@@ -272,12 +367,32 @@ __device__ __forceinline__ void rate_f(int smearing, float ginv, float pre, doub
       d2 = delta_ga(ginv, x2m.E + x3.E - E1);
     }
   }
+}
+
+template <int NT>
+__device__ __forceinline__ void rate_combine(float pre, float iE1, const float* n1, const Band& x2,
+                                             const Band& x2m, const Band& x3, float dp, float d1, float d2,
+                                             float* f) {
   const float fp = pre * dp * iE1 * x2.iE * x3.iE;
   const float fm = pre * iE1 * x2m.iE * x3.iE;
 #pragma unroll
   for (int t = 0; t < NT; ++t)
     f[t] = fp * n1[t] * x2.N[t] * (x3.N[t] + 1.f) +
            fm * x3.N[t] * (d1 * n1[t] * (x2m.N[t] + 1.f) + d2 * x2m.N[t] * (n1[t] + 1.f));
+}
+
+template <int NT>
+__device__ __forceinline__ void rate_f(int smearing, float ginv, float pre, double E1, float iE1,
+                                       const float* n1, const Band& x2, const Band& x2m,
+                                       const Band& x3, const Sig& gp, const Sig& gm, float* f,
+                                       unsigned& near) {
+#pragma unroll
+  for (int t = 0; t < NT; ++t) f[t] = 0.f;
+  near = 0u;
+  if (!(x3.E >= phxc::phEnergyCutoff)) return;
+  float dp, d1, d2;
+  deltas3(smearing, ginv, E1, x2, x2m, x3, gp, gm, dp, d1, d2, near);
+  rate_combine<NT>(pre, iE1, n1, x2, x2m, x3, dp, d1, d2, f);
 }
 
 // OR a 6-bit b3 mask over the degenerate blocks of q3
@@ -291,12 +406,12 @@ __device__ __noinline__ unsigned expand_b3(unsigned c, unsigned gp3) {
 // Liveness of (b1, b2, b3) for all b1 at one (b2, b3): bit b1 is set when
 // one of the three deltas may be non-zero (FP32 windows widened by tol).
 __device__ __forceinline__ unsigned live6(int smearing, float sg, float tol, const float* E1f,
-                                          float E2f, float E2mf, const float* P2, const float* P2m,
-                                          bool ok2, bool ok2m, float E3f, const float* P3) {
+                                          float E2f, float E2mf, const Band& x2, const Band& x2m,
+                                          bool ok2, bool ok2m, float E3f, const Band& x3) {
   float hp, hm, cp, c1, c2;
   if (smearing == PHX_SMEAR_ADAPTIVE) {
-    hp = 2.f * sigma_ad(P2, P3).s + tol;
-    hm = 2.f * sigma_ad(P2m, P3).s + tol;
+    hp = 2.f * sigma_ad(x2.P, x3.P, x2.vf, x3.vf).s + tol;
+    hm = 2.f * sigma_ad(x2m.P, x3.P, x2m.vf, x3.vf).s + tol;
     cp = E3f - E2f;          // + : E1 + E2 - E3 = E1 - cp
     c1 = E2mf - E3f;         // -1: E1 + E3 - E2m = E1 - c1
     c2 = E2mf + E3f;         // -2: E2m + E3 - E1 = -(E1 - c2)
@@ -388,7 +503,7 @@ template <int NT>
 __device__ __forceinline__ void rate_entry(uint2 e, int qd, const double* En1, const float* iE1s,
                                            const float* N1, const uint4* rec, const uint4* u2,
                                            unsigned gp2, int smearing, float ginv, float pre,
-                                           float* qacc) {
+                                           float* qacc, const TcArgs& P, int iq2) {
   const float wn = __uint_as_float(e.x);
   const int r = e.y & 31, b1 = (e.y >> 5) & 7, b2 = (e.y >> 8) & 7, b3 = (e.y >> 11) & 7;
   const int mm = qd * 32 + r;
@@ -406,6 +521,7 @@ __device__ __forceinline__ void rate_entry(uint2 e, int qd, const double* En1, c
   float g[NT];
 #pragma unroll
   for (int t = 0; t < NT; ++t) g[t] = 0.f;
+  unsigned anynear = 0u;
   for (unsigned m2 = bm2; m2; m2 &= m2 - 1) {
     const int c2 = __ffs(m2) - 1;
     const Band x2 = load_band<NT>(u2 + 3 * c2, 1);
@@ -415,14 +531,21 @@ __device__ __forceinline__ void rate_entry(uint2 e, int qd, const double* En1, c
       const Band x3 = load_band<NT>(srow + (kChBand + 3 * c3) * kM, kM);
       Sig gp, gm;
       if (smearing == PHX_SMEAR_ADAPTIVE) {
-        gp = sigma_ad(x2.P, x3.P);
-        gm = sigma_ad(x2m.P, x3.P);
+        gp = sigma_ad(x2.P, x3.P, x2.vf, x3.vf);
+        gm = sigma_ad(x2m.P, x3.P, x2m.vf, x3.vf);
       }
       float f[NT];
-      rate_f<NT>(smearing, ginv, pre, E1, iE1, n1v, x2, x2m, x3, gp, gm, f);
+      unsigned near;
+      rate_f<NT>(smearing, ginv, pre, E1, iE1, n1v, x2, x2m, x3, gp, gm, f, near);
 #pragma unroll
       for (int t = 0; t < NT; ++t) g[t] += f[t];
+      anynear |= near;
     }
+  }
+  if (anynear) {
+    // a cut-off decision too close for FP32: edge_fix_kernel re-decides the entry in FP64
+    const unsigned i = atomicAdd(P.edge_count, 1u);
+    if (i < P.edge_cap) P.edges[i] = EdgeEvent{(blockIdx.x << 12) | (blockIdx.y << 7) | (unsigned)mm, iq2, e};
   }
   const float scale = wn / (float)(__popc(bm2) * __popc(bm3));
 #pragma unroll
@@ -484,11 +607,11 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
       sincos(-(qc[0] * P.R3[3 * r] + qc[1] * P.R3[3 * r + 1] + qc[2] * P.R3[3 * r + 2]), &sn, &cs);
       v = k < P.nr3 ? cs : sn;
     }
-    const __nv_bfloat16 hi = __double2bfloat16(v);
-    const __nv_bfloat16 lo = __double2bfloat16(v - (double)__bfloat162float(hi));
+    uint16_t hi, lo;
+    split16(v, P.fp16 != 0, &hi, &lo);
     const uint32_t off = tc::core_offset(mm, k, Kp, 2);
-    *reinterpret_cast<__nv_bfloat16*>(S.A + off) = hi;
-    *reinterpret_cast<__nv_bfloat16*>(S.A + S.aPart + off) = lo;
+    *reinterpret_cast<uint16_t*>(S.A + off) = hi;
+    *reinterpret_cast<uint16_t*>(S.A + S.aPart + off) = lo;
   }
   // q1 data of the tile from the records
   for (int e = tid; e < 36 * kM; e += kThreads) {
@@ -535,7 +658,7 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
   } else if (warp == kEpiWarps + 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
-      const uint32_t idesc = tc::idesc_bf16_f32(kM, kNH);
+      const uint32_t idesc = P.fp16 ? tc::idesc_f16_f32(kM, kNH) : tc::idesc_bf16_f32(kM, kNH);
       const uint32_t sbA = (uint32_t)(Kp / 8) * 128;
       const uint32_t aHi = tc::smem_u32(S.A), aLo = tc::smem_u32(S.A + S.aPart);
       int it = 0;
@@ -581,7 +704,12 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
     const unsigned FULL = 0xffffffffu;
     const int smearing = M.smearing;
     const float sg = (float)M.sigma, ginv = M.sigma > 0.0 ? (float)(1.0 / M.sigma) : 0.f;
-    const float pre = (float)(phxc::pi * 0.25 * 0.5) * (float)M.norm;
+    // FP16 operands: |V|^2 carries the square of the B scale, undone here (power of 4)
+    float pre = (float)(phxc::pi * 0.25 * 0.5) * (float)M.norm;
+    if (P.fp16) {
+      const float sc = fp16_scale(*P.dmax);
+      pre *= 1.f / (sc * sc);
+    }
     const unsigned gp1 = P.rec[(size_t)q1c * kRecChunks + kChGp].x;
     const bool deg1 = gp1 != kIdentityBlocks;
     unsigned ok1 = 0;
@@ -656,8 +784,8 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
             for (int b3 = 0; b3 < 6; ++b3) {
               const Band x3 = load_band<1>(srow + (kChBand + 3 * b3) * kM, kM);
               if (!(x3.E >= phxc::phEnergyCutoff)) continue;
-              const unsigned c = live6(smearing, sg, P.tol, E1f, E2f, E2mf, x2.P, x2m.P, ok2, ok2m,
-                                       (float)x3.E, x3.P) & ok1;
+              const unsigned c = live6(smearing, sg, P.tol, E1f, E2f, E2mf, x2, x2m, ok2, ok2m,
+                                       (float)x3.E, x3) & ok1;
               unsigned long long sp = 0;
 #pragma unroll
               for (int b1 = 0; b1 < 6; ++b1) sp |= (unsigned long long)((c >> b1) & 1u) << (6 * b1);
@@ -742,7 +870,8 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
                 qn += __popc(bal);
                 if (qn >= 32) {
                   __syncwarp();
-                  rate_entry<NT>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc);
+                  rate_entry<NT>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc, P,
+                                 iq2);
                   const uint2 rest = lane + 32 < qn ? queue[lane + 32] : make_uint2(0u, 0u);
                   __syncwarp();
                   if (lane + 32 < qn) queue[lane] = rest;
@@ -761,7 +890,7 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
       if (qn) {
         __syncwarp();
         if (lane < qn)
-          rate_entry<NT>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc);
+          rate_entry<NT>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc, P, iq2);
         qn = 0;
       }
       __syncwarp();
@@ -879,6 +1008,88 @@ int launch_pair(phx_ctx* ctx, const TcArgs& A, int tiles, int slots) {
   return PHX_OK;
 }
 
+// Re-decides, on the FP64 widths, the adaptive deltas whose FP32 cut-off
+// test was too close to call (events of the pair kernel), and adds the
+// difference of the two rates, times the event's weight, to the partial sums
+// of the event's row and slot.  One thread per event.
+template <int NT>
+__global__ void edge_fix_kernel(TcArgs P) {
+  const MeshArgs& M = P.m;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && *P.edge_count > P.edge_cap) atomicOr(P.status, 1 << 20);
+  const unsigned n = min(*P.edge_count, P.edge_cap);
+  float pre = (float)(phxc::pi * 0.25 * 0.5) * (float)M.norm;
+  if (P.fp16) {
+    const float sc = fp16_scale(*P.dmax);
+    pre *= 1.f / (sc * sc);
+  }
+  constexpr float kNorm = (float)(1.0 / (phxc::sqrtPi * phxc::erf2));
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const EdgeEvent ev = P.edges[i];
+    const int tile = ev.where >> 12, slot = (ev.where >> 7) & 31, mm = ev.where & 127;
+    const int q1 = P.q1_order[tile * kM + mm];
+    const uint2 e = ev.entry;
+    const float wn = __uint_as_float(e.x);
+    const int b1 = (e.y >> 5) & 7, b2 = (e.y >> 8) & 7, b3 = (e.y >> 11) & 7;
+    const int iq2 = ev.iq2, iq2m = mesh_neg(iq2, M.n0, M.n1, M.n2), iq3 = mesh_add(q1, iq2, M.n0, M.n1, M.n2);
+    const uint4* rq2 = P.rec + (size_t)iq2 * kRecChunks;
+    const uint4* rq2m = P.rec + (size_t)iq2m * kRecChunks;
+    const uint4* rq3 = P.rec + (size_t)iq3 * kRecChunks;
+    unsigned bm2 = 1u << b2, bm3 = 1u << b3;
+    if ((e.y >> 14) & 1) {
+      bm2 = blk_mask(rq2[kChGp].x, b2);
+      bm3 = blk_mask(rq3[kChGp].x, b3);
+    }
+    const Band x1 = load_band<kMaxT>(P.rec + (size_t)q1 * kRecChunks + kChBand + 3 * b1, 1);
+    double corr[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) corr[t] = 0.0;
+    for (unsigned m2 = bm2; m2; m2 &= m2 - 1) {
+      const int c2 = __ffs(m2) - 1;
+      const uint4* r2 = rq2 + kChBand + 3 * c2;
+      const uint4* r2m = rq2m + kChBand + 3 * c2;
+      const Band x2 = load_band<NT>(r2, 1), x2m = load_band<NT>(r2m, 1);
+      for (unsigned m3 = bm3; m3; m3 &= m3 - 1) {
+        const int c3 = __ffs(m3) - 1;
+        const uint4* r3 = rq3 + kChBand + 3 * c3;
+        const Band x3 = load_band<NT>(r3, 1);
+        if (!(x3.E >= phxc::phEnergyCutoff)) continue;
+        const Sig gp = sigma_ad(x2.P, x3.P, x2.vf, x3.vf), gm = sigma_ad(x2m.P, x3.P, x2m.vf, x3.vf);
+        float dp, d1, d2;
+        unsigned near;
+        deltas3(PHX_SMEAR_ADAPTIVE, 0.f, x1.E, x2, x2m, x3, gp, gm, dp, d1, d2, near);
+        if (!near) continue;
+        auto val = [&](double de, float inv) {
+          const float x = (float)de * inv;
+          return __expf(-x * x) * inv * kNorm;
+        };
+        const double ep = x1.E + x2.E - x3.E, e1 = x1.E + x3.E - x2m.E, e2 = x2m.E + x3.E - x1.E;
+        float fdp = dp, fd1 = d1, fd2 = d2;
+        if (near & 1u) fdp = beyond_two_sigma(ep, r2, r3) ? 0.f : val(ep, gp.inv);
+        if (near & 2u) fd1 = beyond_two_sigma(e1, r2m, r3) ? 0.f : val(e1, gm.inv);
+        if (near & 4u) fd2 = beyond_two_sigma(e2, r2m, r3) ? 0.f : val(e2, gm.inv);
+        if (fdp == dp && fd1 == d1 && fd2 == d2) continue;
+        float f0[NT], f1[NT];
+        rate_combine<NT>(pre, x1.iE, x1.N, x2, x2m, x3, dp, d1, d2, f0);
+        rate_combine<NT>(pre, x1.iE, x1.N, x2, x2m, x3, fdp, fd1, fd2, f1);
+#pragma unroll
+        for (int t = 0; t < NT; ++t) corr[t] += (double)f1[t] - (double)f0[t];
+      }
+    }
+    const double scale = (double)(wn / (float)(__popc(bm2) * __popc(bm3)));
+    double* out = P.partial + (((size_t)slot * M.nq + q1) * 6 + b1) * NT;
+#pragma unroll
+    for (int t = 0; t < NT; ++t)
+      if (corr[t] != 0.0) atomicAdd(out + t, scale * corr[t]);
+  }
+}
+
+template <int NT>
+int launch_edge_fix(phx_ctx* ctx, const TcArgs& A) {
+  edge_fix_kernel<NT><<<2 * ctx->num_sms, 128, 0, ctx->stream>>>(A);
+  PHX_CUDA(ctx, cudaGetLastError());
+  return PHX_OK;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -927,10 +1138,12 @@ int phx_split_pack_records(phx_ctx* ctx, const pairc::MeshArgs& M, void* rec, in
 int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v, const phx_bands* b,
                          const double2* Dp, uint8_t* Bimg, const void* rec, double emax, int q2_first,
                          int q2_count, int slots, double* partial, int* launches, cudaEvent_t ev_begin,
-                         cudaEvent_t ev_end) {
+                         cudaEvent_t ev_end, int fp16, const unsigned* dmax, void* edges, unsigned* edge_count,
+                         unsigned edge_cap) {
   const int Kp = phx_split_kp(v->nr3);
   const int nkc = Kp / kKC;
-  convert_b_kernel<<<dim3(q2_count, kParts * nkc), 256, 0, ctx->stream>>>(Dp, v->nr3, Kp, q2_count, Bimg);
+  convert_b_kernel<<<dim3(q2_count, kParts * nkc), 256, 0, ctx->stream>>>(Dp, v->nr3, Kp, q2_count, Bimg, fp16,
+                                                                           dmax);
   PHX_CUDA(ctx, cudaGetLastError());
   TcArgs A;
   A.m = M;
@@ -948,6 +1161,13 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
   A.tol = (float)(32.0 * std::max(emax, 1e-6) * 5.9604644775390625e-8);
   A.partial = partial;
   A.status = ctx->d_status;
+  A.fp16 = fp16;
+  A.dmax = dmax;
+  A.edges = static_cast<EdgeEvent*>(edges);
+  A.edge_count = edge_count;
+  A.edge_cap = edge_cap;
+  PHX_ARG(ctx, slots < 32 && (M.nq + kM - 1) / kM < (1 << 20), "split path: at most 31 slots");
+  PHX_CUDA(ctx, cudaMemsetAsync(edge_count, 0, sizeof(unsigned), ctx->stream));
   const int tiles = (M.nq + kM - 1) / kM;
   int rc = PHX_OK;
   if (ev_begin) PHX_CUDA(ctx, phx_record_event(ev_begin, ctx->stream));
@@ -959,11 +1179,22 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
   }
   if (rc != PHX_OK) return rc;
   if (ev_end) PHX_CUDA(ctx, phx_record_event(ev_end, ctx->stream));
-  *launches += 2;
+  switch (M.nT) {
+    case 1: rc = launch_edge_fix<1>(ctx, A); break;
+    case 2: rc = launch_edge_fix<2>(ctx, A); break;
+    case 3: rc = launch_edge_fix<3>(ctx, A); break;
+    default: rc = launch_edge_fix<4>(ctx, A); break;
+  }
+  if (rc != PHX_OK) return rc;
+  *launches += 3;
   return PHX_OK;
 }
 
 size_t phx_split_smem_bytes(int nr3) { return pair_tc_smem(phx_split_kp(nr3)); }
+
+// capacity of the near-cut-off event list of one pair launch, and its bytes
+unsigned phx_split_edge_cap() { return 1u << 18; }
+size_t phx_split_edge_bytes() { return sizeof(EdgeEvent) * phx_split_edge_cap(); }
 
 // Dynamic shared-memory limit of the pair kernel for nT temperatures; called
 // before any launch (and outside graph capture).

@@ -194,6 +194,12 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
          | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
+// Instruction descriptor, kind::f16 with FP16 A/B (format 0), FP32 D, both K-major.
+__host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N) {
+  return (1u << 4)                  // D format F32
+         | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
 // Byte offset of element (row, k) in a K-major no-swizzle tile whose rows
 // hold Kp elements of esize bytes (core matrix = 8 rows x 16 bytes).
 __host__ __device__ __forceinline__ uint32_t core_offset(int row, int k, int Kp, int esize) {

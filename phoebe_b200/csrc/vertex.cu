@@ -230,7 +230,8 @@ extern "C" int phx_v3_destroy(phx_v3* v) {
 
 extern "C" int phx_v3_set_precision(phx_v3* v, int prec) {
   PHX_ARG(nullptr, v, "null v3 handle");
-  PHX_ARG(v->ctx, prec == PHX_PREC_FP64 || prec == PHX_PREC_SPLIT_BF16 || prec == PHX_PREC_SPLIT_TF32,
+  PHX_ARG(v->ctx, prec != PHX_PREC_SPLIT_TF32, "phx_v3_set_precision: the TF32 split is not built (use PHX_PREC_SPLIT_FP16)");
+  PHX_ARG(v->ctx, prec == PHX_PREC_FP64 || prec == PHX_PREC_SPLIT_BF16 || prec == PHX_PREC_SPLIT_FP16,
           "phx_v3_set_precision: unknown precision");
   v->precision = prec;
   return PHX_OK;

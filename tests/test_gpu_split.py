@@ -45,11 +45,21 @@ def _builder(ctx, diamond, mesh, smearing, temps_k, precision):
     return A, k, E, sm
 
 
-@pytest.mark.parametrize("mesh,smearing,temps", [((8, 8, 8), "gaussian", (300.0,)),
-                                                 ((10, 10, 10), "adaptive", (100.0, 300.0, 600.0))])
-def test_split_linewidths_match_fp64(ctx, diamond, mesh, smearing, temps):
+CASES = [((8, 8, 8), "gaussian", (300.0,)),
+         ((10, 10, 10), "adaptive", (100.0, 300.0, 600.0)),
+         # coarse meshes: pairs whose FP64 velocity difference is non-zero but
+         # lost in FP32 (width floored), and small linewidths built from
+         # triplets with strong cancellation in V (FP16 hi/lo needed for 1e-5)
+         ((6, 6, 6), "adaptive", (300.0, 600.0)),
+         ((8, 8, 8), "adaptive", (300.0,)),
+         ((5, 5, 5), "adaptive", (100.0, 200.0, 300.0, 600.0))]
+
+
+@pytest.mark.parametrize("mesh,smearing,temps,precision",
+                         [c + ("split_fp16",) for c in CASES] + [c + ("split_bf16",) for c in CASES[:3]])
+def test_split_linewidths_match_fp64(ctx, diamond, mesh, smearing, temps, precision):
     A64, k64, E, _ = _builder(ctx, diamond, mesh, smearing, temps, "fp64")
-    A16, k16, _, sm = _builder(ctx, diamond, mesh, smearing, temps, "split_bf16")
+    A16, k16, _, sm = _builder(ctx, diamond, mesh, smearing, temps, precision)
     # linewidths Gamma = A / n(n+1) on non-excluded states
     ok = E.reshape(-1) >= C.phExcludeCutoff
     big = ok[None, :] & (np.abs(A64) > 1e-8 * np.abs(A64).max())

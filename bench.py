@@ -49,7 +49,7 @@ def parse():
                     help="3ph: the headline linewidth builder; elph: electron-phonon linewidths "
                          "(8 Wannier functions, 343 x 343 coupling vectors, 40^3 k, 20^3 q)")
     ap.add_argument("--elph-k1", type=int, default=64, help="outer k points timed per elph step")
-    ap.add_argument("--precision", default=os.environ.get("PHX_BENCH_PRECISION", "split_bf16"),
+    ap.add_argument("--precision", default=os.environ.get("PHX_BENCH_PRECISION", "split_fp16"),
                     choices=["fp64", "split_bf16", "split_fp16"])
     ap.add_argument("--mesh", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)

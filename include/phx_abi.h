@@ -184,6 +184,49 @@ int phx_ph_linewidths(phx_v3* v3, phx_bands* bands, const phx_lw_params* params,
 int phx_ph_linewidths_d(phx_v3* v3, phx_bands* bands, const phx_lw_params* params,
                         double* A_out_d, phx_lw_stats* stats);
 
+/* ---- scattering-matrix modes of the builder (nb = 6, FP64, no q2 window) ----
+ * States are numbered s = iq * nb + ib (the reference's BteIndex without
+ * symmetries).  The rates, cut-offs, exclusions and time-reversal pairing are
+ * those of phx_ph_linewidths; the differences are the reference's: the
+ * diagonal is the linewidth x n(n+1) WITHOUT degeneracy averaging, plus
+ * boundary scattering; off-diagonal elements are the sums over b3 of the "+"
+ * rates minus the two "-" rates (and minus the isotope rates) of each pair of
+ * states.  With finalize = 0 the diagonal is not written and no exclusion is
+ * applied (partial sums of a q2 slice). */
+typedef struct phx_smatrix phx_smatrix;
+
+/* PhScatteringMatrix::builder with switchCase 0 (scatteringMatrixInMemory,
+ * src/bte/ph_scattering.cpp:382-406,520-547,714-738,846-847,864-890,910-933;
+ * src/bte/scattering.cpp:105-160): the whole matrix, ns x ns FP64, kept in
+ * device memory by the handle (18.4 GB for the 20x20x20 diamond mesh).  One
+ * temperature, as the reference requires.  Fails with PHX_ERR_ARG when the
+ * matrix does not fit in free device memory. */
+int phx_ph_smatrix_create(phx_v3* v3, phx_bands* bands, const phx_lw_params* params, phx_smatrix** out,
+                          phx_lw_stats* stats);
+int phx_smatrix_num_states(const phx_smatrix* m);
+/* internalDiagonal (ns) of the stored matrix (ScatteringMatrix::diagonal, scattering.cpp:165-178) */
+int phx_smatrix_diagonal(phx_smatrix* m, double* diag);
+/* rows row0 .. row0+nrows-1 of A, row-major (nrows, ns) host (theMatrix(row, col)) */
+int phx_smatrix_get_rows(phx_smatrix* m, int row0, int nrows, double* out);
+/* ScatteringMatrix::dot (off_diagonal = 0: rows and columns of excluded states
+ * left out, scattering.cpp:266-330) or offDiagonalDot (off_diagonal = 1: the
+ * diagonal left out, :180-232) of the stored matrix: y = A x for nvec vectors,
+ * x and y (nvec, 3, ns) host. */
+int phx_smatrix_dot(phx_smatrix* m, int nvec, const double* x, int off_diagonal, double* y);
+/* Same with device vectors; ms (may be NULL): device time of the product. */
+int phx_smatrix_dot_d(phx_smatrix* m, int nvec, const double* x_d, int off_diagonal, double* y_d, float* ms);
+int phx_smatrix_destroy(phx_smatrix* m);
+
+/* PhScatteringMatrix::builder with switchCase 1 (ScatteringMatrix::dot when the
+ * matrix is not stored, src/bte/ph_scattering.cpp:408-431,549-572,741-759,
+ * 849-855,891-897): y = A x for nvec vectors, one matrix per temperature,
+ * x and y (nvec, nT, 3, ns) host, in one builder pass without storing A. */
+int phx_ph_smatrix_dot(phx_v3* v3, phx_bands* bands, const phx_lw_params* params, int nvec, const double* x,
+                       double* y, phx_lw_stats* stats);
+/* Same with device vectors. */
+int phx_ph_smatrix_dot_d(phx_v3* v3, phx_bands* bands, const phx_lw_params* params, int nvec,
+                         const double* x_d, double* y_d, phx_lw_stats* stats);
+
 /* Allocation-free variant of phx_ph_linewidths_d (no counterpart in the
  * reference).  For callers that cannot allocate device memory when they call
  * the builder -- e.g. an application that has given all free device memory

@@ -49,6 +49,14 @@ def lib():
         L.orc_ph_linewidths.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _D, _D, _D, _D, _D,
                                         ctypes.c_int, _D, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_int, _I, ctypes.c_int, _D, _D, _D, _D, ctypes.c_double]
+        L.orc_ph_smatrix.restype = ctypes.c_int
+        L.orc_ph_smatrix.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _D, _D, _D, _D, _D, _D, ctypes.c_int,
+                                     ctypes.c_double, ctypes.c_int, _I, ctypes.c_int, _D, _D, _D, ctypes.c_double]
+        L.orc_ph_smatrix_dot.restype = ctypes.c_int
+        L.orc_ph_smatrix_dot.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _D, _D, _D, _D, _D, ctypes.c_int, _D,
+                                         ctypes.c_int, ctypes.c_double, ctypes.c_int, _I, ctypes.c_int,
+                                         ctypes.c_int, _D, _D, _D, ctypes.c_double]
+        L.orc_smatrix_dot.argtypes = [ctypes.c_int, _D, _D, ctypes.c_int, _D, ctypes.c_int, _D]
         L.orc_rta_kappa.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, ctypes.c_long,
                                     ctypes.c_double, _D]
         L.orc_el_diag.restype = ctypes.c_int
@@ -200,6 +208,62 @@ class Interaction3Ph:
         if rc:
             raise RuntimeError("oracle linewidth builder failed: %d" % rc)
         return out
+
+    @staticmethod
+    def _q2(q2_list, nq):
+        if q2_list is None:
+            return nq, None
+        ql = np.ascontiguousarray(q2_list, dtype=np.int32)
+        return len(ql), ql
+
+    def scattering_matrix(self, mesh, E, ev, vg, qcart, recip, temp_ry, smearing, sigma, q2_list=None,
+                          finalize=True, isotope_coupling=None, boundary_length=0.0):
+        """switchCase 0 (one temperature): returns (matrix (ns, ns), linewidth row (ns))."""
+        nq, nb = E.shape
+        ns = nq * nb
+        m = np.ascontiguousarray(mesh, dtype=np.int32)
+        T = _d([temp_ry])
+        mat = np.zeros((ns, ns))
+        lw = np.zeros(ns)
+        nq2, ql = self._q2(q2_list, nq)
+        gi = None if isotope_coupling is None else _d(isotope_coupling)
+        rc = lib().orc_ph_smatrix(self.h, nq, m.ctypes.data_as(_I), _p(_d(E)), _p(_c(ev)), _p(_d(vg)),
+                                  _p(_d(qcart)), _p(_d(recip)), _p(T), 0 if smearing == "gaussian" else 1,
+                                  float(sigma), nq2, None if ql is None else ql.ctypes.data_as(_I),
+                                  int(finalize), _p(lw), _p(mat), None if gi is None else _p(gi),
+                                  float(boundary_length))
+        if rc:
+            raise RuntimeError("oracle matrix builder failed: %d" % rc)
+        return mat, lw
+
+    def scattering_dot(self, mesh, E, ev, vg, qcart, recip, temps_ry, smearing, sigma, x, q2_list=None,
+                       finalize=True, isotope_coupling=None, boundary_length=0.0):
+        """switchCase 1: y = A x for x (nvec, nT, 3, ns), without storing A."""
+        nq, nb = E.shape
+        m = np.ascontiguousarray(mesh, dtype=np.int32)
+        T = _d(temps_ry)
+        x = _d(x)
+        assert x.ndim == 4 and x.shape[1:] == (len(T), 3, nq * nb)
+        y = np.zeros_like(x)
+        nq2, ql = self._q2(q2_list, nq)
+        gi = None if isotope_coupling is None else _d(isotope_coupling)
+        rc = lib().orc_ph_smatrix_dot(self.h, nq, m.ctypes.data_as(_I), _p(_d(E)), _p(_c(ev)), _p(_d(vg)),
+                                      _p(_d(qcart)), _p(_d(recip)), len(T), _p(T),
+                                      0 if smearing == "gaussian" else 1, float(sigma), nq2,
+                                      None if ql is None else ql.ctypes.data_as(_I), int(finalize), x.shape[0],
+                                      _p(x), _p(y), None if gi is None else _p(gi), float(boundary_length))
+        if rc:
+            raise RuntimeError("oracle matrix-vector builder failed: %d" % rc)
+        return y
+
+
+def smatrix_dot(mat, E, x, off_diagonal=False):
+    """ScatteringMatrix::dot / offDiagonalDot of a stored matrix; x (nvec, 3, ns)."""
+    ns = mat.shape[0]
+    x = _d(x)
+    y = np.zeros_like(x)
+    lib().orc_smatrix_dot(ns, _p(_d(mat)), _p(_d(E).ravel()), x.shape[0], _p(x), int(off_diagonal), _p(y))
+    return y
 
 
 def symmetrize_coupling(c, e1, e2, e3):

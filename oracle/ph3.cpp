@@ -6,8 +6,13 @@
 //   * Interaction3Ph::getCouplingsSquared (src/interaction/interaction_3ph.cpp:179-405),
 //     including the weights3 factor applied in both stages (:166-169, :284-285)
 //   * ScatteringMatrix::symmetrizeCoupling (src/bte/scattering.cpp:1209-1318)
-//   * PhScatteringMatrix::builder, linewidth mode (src/bte/ph_scattering.cpp:60-613,
-//     795-812, 900-906) with Helper3rdState case 1 (src/bte/helper_3rd_state.cpp:128-170)
+//   * PhScatteringMatrix::builder (src/bte/ph_scattering.cpp:60-935) in its three
+//     modes without symmetries: switchCase 2 (linewidths), 0 (matrix in memory,
+//     :382-406, :520-547, :714-738, :846-847, :864-890, :910-933) and 1 (matrix-vector
+//     product, :408-431, :549-572, :741-759, :849-855, :891-897), with
+//     Helper3rdState case 1 (src/bte/helper_3rd_state.cpp:128-170)
+//   * ScatteringMatrix::dot / offDiagonalDot of a stored matrix (src/bte/scattering.cpp:
+//     180-265, 266-330)
 //   * GaussianDeltaFunction / AdaptiveGaussianDeltaFunction (src/delta_function.cpp:34-96)
 //   * Particle::getPopulation / getPopPopPm1 / getDndt (src/particle.cpp:64-128)
 //   * ScatteringMatrix::degeneracyAveragingLinewidths (src/bte/scattering.cpp:1168-1207),
@@ -236,6 +241,41 @@ struct Smearing {
   }
 };
 
+// Where the builder's rates go (ph_scattering.cpp, the three switchCase branches of
+// each process).  sign: +1 for the "+" process, -1 for the "-" processes and
+// isotope scattering; dfac: the linewidth share (1/2 for 3-phonon rates, 1 for
+// isotope rates).
+struct Sink {
+  int mode = 2;            // 2 linewidths, 0 matrix, 1 matrix-vector product
+  size_t ns = 0;
+  int nT = 0;
+  double* lw = nullptr;    // (nT, ns): modes 2 and 0
+  double* mat = nullptr;   // (ns, ns) row-major: mode 0
+  int nvec = 0;            // mode 1: x, y (nvec, nT, 3, ns)
+  const double* x = nullptr;
+  double* y = nullptr;
+  void add(int c, size_t s1, size_t s2, double rate, double sign, double dfac) const {
+    if (mode == 2) {
+      lw[c * ns + s1] += dfac * rate;
+    } else if (mode == 0) {
+      lw[c * ns + s1] += dfac * rate;
+      mat[s1 * ns + s2] += sign * rate;
+    } else {
+      for (int v = 0; v < nvec; ++v)
+        for (int i = 0; i < 3; ++i) {
+          const size_t o = (((size_t)v * nT + c) * 3 + i) * ns;
+          if (s1 != s2) y[o + s1] += sign * rate * x[o + s2];
+          y[o + s1] += dfac * rate * x[o + s1];
+        }
+    }
+  }
+};
+
+int builder(void* p, int nq, const int* mesh, const double* E, const double* ev, const double* vg,
+            const double* qcart, const double* recip, int nT, const double* Tk_ry, int smearing, double sigma,
+            int nq2, const int* q2_list, int finalize, const Sink& sink, const double* win_energy,
+            const double* win_cut, const double* iso, double boundary_length);
+
 }  // namespace
 
 extern "C" {
@@ -298,6 +338,78 @@ int orc_ph_linewidths(void* p, int nq, const int* mesh, const double* E, const d
                       const double* Tk_ry, int smearing, double sigma, int nq2,
                       const int* q2_list, int finalize, double* out, const double* win_energy,
                       const double* win_cut, const double* iso, double boundary_length) {
+  Sink sk;
+  sk.mode = 2;
+  sk.ns = (size_t)nq * ((V3*)p)->nb;
+  sk.nT = nT;
+  sk.lw = out;
+  return builder(p, nq, mesh, E, ev, vg, qcart, recip, nT, Tk_ry, smearing, sigma, nq2, q2_list, finalize, sk,
+                 win_energy, win_cut, iso, boundary_length);
+}
+
+// switchCase 0: the scattering matrix (ns, ns) row-major and its diagonal
+// linewidth row lw (ns), for one temperature (scattering.cpp:105-111).
+// Accumulates into mat and lw (zero them first).
+int orc_ph_smatrix(void* p, int nq, const int* mesh, const double* E, const double* ev, const double* vg,
+                   const double* qcart, const double* recip, const double* Tk_ry, int smearing, double sigma,
+                   int nq2, const int* q2_list, int finalize, double* lw, double* mat, const double* iso,
+                   double boundary_length) {
+  Sink sk;
+  sk.mode = 0;
+  sk.ns = (size_t)nq * ((V3*)p)->nb;
+  sk.nT = 1;
+  sk.lw = lw;
+  sk.mat = mat;
+  return builder(p, nq, mesh, E, ev, vg, qcart, recip, 1, Tk_ry, smearing, sigma, nq2, q2_list, finalize, sk,
+                 nullptr, nullptr, iso, boundary_length);
+}
+
+// switchCase 1: y += A x for nvec input vectors x (nvec, nT, 3, ns), one matrix
+// per temperature, without storing A.  Accumulates into y (zero it first).
+int orc_ph_smatrix_dot(void* p, int nq, const int* mesh, const double* E, const double* ev, const double* vg,
+                       const double* qcart, const double* recip, int nT, const double* Tk_ry, int smearing,
+                       double sigma, int nq2, const int* q2_list, int finalize, int nvec, const double* x,
+                       double* y, const double* iso, double boundary_length) {
+  Sink sk;
+  sk.mode = 1;
+  sk.ns = (size_t)nq * ((V3*)p)->nb;
+  sk.nT = nT;
+  sk.nvec = nvec;
+  sk.x = x;
+  sk.y = y;
+  return builder(p, nq, mesh, E, ev, vg, qcart, recip, nT, Tk_ry, smearing, sigma, nq2, q2_list, finalize, sk,
+                 nullptr, nullptr, iso, boundary_length);
+}
+
+// ScatteringMatrix::dot (off_diagonal = 0; excluded rows and columns skipped,
+// scattering.cpp:266-330) and offDiagonalDot (off_diagonal = 1; the diagonal
+// skipped, :180-232) of a stored matrix: y (nvec, 3, ns) = A x.
+void orc_smatrix_dot(int ns, const double* mat, const double* E, int nvec, const double* x, int off_diagonal,
+                     double* y) {
+  std::vector<char> excluded(ns, 0);
+  for (int s = 0; s < ns; ++s) excluded[s] = E[s] < 0.1 / ryToCmm1;
+#pragma omp parallel for
+  for (int r = 0; r < ns; ++r)
+    for (int v = 0; v < nvec; ++v)
+      for (int i = 0; i < 3; ++i) {
+        const double* xv = x + ((size_t)v * 3 + i) * ns;
+        double acc = 0.0;
+        for (int c = 0; c < ns; ++c) {
+          if (off_diagonal ? r == c : (excluded[r] || excluded[c])) continue;
+          acc += mat[(size_t)r * ns + c] * xv[c];
+        }
+        y[((size_t)v * 3 + i) * ns + r] = acc;
+      }
+}
+
+}  // extern "C"
+
+namespace {
+
+int builder(void* p, int nq, const int* mesh, const double* E, const double* ev, const double* vg,
+            const double* qcart, const double* recip, int nT, const double* Tk_ry, int smearing, double sigma,
+            int nq2, const int* q2_list, int finalize, const Sink& sink, const double* win_energy,
+            const double* win_cut, const double* iso, double boundary_length) {
   V3& v = *(V3*)p;
   const int nb = v.nb;
   const size_t ns = (size_t)nq * nb;
@@ -415,7 +527,7 @@ int orc_ph_linewidths(void* p, int nq, const int* mesh, const double* E, const d
               double b1 = boseT[c * ns + s1], b2 = boseT[c * ns + s2], b3 = boseT[c * ns + s3];
               double rate = pi * 0.25 * b1 * b2 * (b3 + 1.0) *
                             c_p[((size_t)ib1 * nb + ib2) * nb + ib3] * delta * norm / enProd;
-              out[c * ns + s1] += 0.5 * rate;
+              sink.add(c, s1, s2, rate, 1.0, 0.5);
             }
           }
           for (int ib3 = 0; ib3 < nb; ++ib3) {
@@ -441,7 +553,7 @@ int orc_ph_linewidths(void* p, int nq, const int* mesh, const double* E, const d
               double cm = c_m[((size_t)ib1 * nb + ib2) * nb + ib3];
               double r1 = pi * 0.25 * b3 * b1 * (b2 + 1.0) * cm * d1 * norm / enProd;
               double r2 = pi * 0.25 * b2 * b3 * (b1 + 1.0) * cm * d2 * norm / enProd;
-              out[c * ns + s1] += 0.5 * (r1 + r2);
+              sink.add(c, s1, s2, r1 + r2, -1.0, 0.5);
             }
           }
         }
@@ -483,14 +595,53 @@ int orc_ph_linewidths(void* p, int nq, const int* mesh, const double* E, const d
             termIso *= pi * 0.5 * norm * en1 * en2 * deltaIso;
             for (int c = 0; c < nT; ++c) {
               const double b1 = boseT[c * ns + s1], b2 = boseT[c * ns + s2];
-              out[c * ns + s1] += termIso * (b1 * b2 + 0.5 * (b1 + b2));
+              sink.add(c, s1, s2, termIso * (b1 * b2 + 0.5 * (b1 + b2)), -1.0, 1.0);
             }
           }
         }
       }
     }
   }
-  if (finalize) {
+  if (finalize && sink.mode == 0) {
+    // boundary scattering on the diagonal, exclusions, then the linewidths
+    // placed on the diagonal (ph_scattering.cpp:846-847, :864-890, :910-933)
+    double* lw = sink.lw;
+    if (boundary_length > 0.0)
+      for (size_t s = 0; s < ns; ++s) {
+        if (excluded[s]) continue;
+        const double* u = vg + s * 3;
+        lw[s] += std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) / boundary_length * poppm1(E[s], Tk_ry[0]);
+      }
+    for (size_t s = 0; s < ns; ++s)
+      if (excluded[s]) {
+        lw[s] = 0.0;
+        for (size_t t = 0; t < ns; ++t)
+          if (excluded[t]) sink.mat[s * ns + t] = 0.0;
+      }
+    for (size_t s = 0; s < ns; ++s) sink.mat[s * ns + s] = lw[s];
+  }
+  if (finalize && sink.mode == 1) {
+    // boundary scattering on the diagonal, then excluded rows zeroed (:849-855, :891-897)
+    for (int vv = 0; vv < sink.nvec; ++vv)
+      for (int c = 0; c < nT; ++c)
+        for (int i = 0; i < 3; ++i) {
+          const size_t o = (((size_t)vv * nT + c) * 3 + i) * ns;
+          for (size_t s = 0; s < ns; ++s) {
+            if (excluded[s]) {
+              sink.y[o + s] = 0.0;
+              continue;
+            }
+            if (boundary_length > 0.0) {
+              const double* u = vg + s * 3;
+              const double rate =
+                  std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) / boundary_length * poppm1(E[s], Tk_ry[c]);
+              sink.y[o + s] += rate * sink.x[o + s];
+            }
+          }
+        }
+  }
+  if (finalize && sink.mode == 2) {
+    double* out = sink.lw;
     // degeneracyAveragingLinewidths, scattering.cpp:1168-1207 (row iCalc=0 only)
     for (int iq = 0; iq < nq; ++iq) {
       std::vector<double> tmp(nb);
@@ -522,6 +673,10 @@ int orc_ph_linewidths(void* p, int nq, const int* mesh, const double* E, const d
   }
   return 0;
 }
+
+}  // namespace
+
+extern "C" {
 
 // RTA thermal conductivity from A_out (nT, ns): tau = n(n+1)/A_out,
 // popRTA = dn/dT v tau, kappa_ij = sum n_i v_j E / (Nq V) (atomic units;

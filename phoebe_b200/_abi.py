@@ -82,6 +82,15 @@ SIGNATURES = {
     "phx_ph_linewidths_d": [_VP, _VP, ctypes.POINTER(LwParams), _VP, ctypes.POINTER(LwStats)],
     "phx_ph_rta_kappa": [_VP, _i, _D, _D, ctypes.c_double, _D],
     "phx_ph_linewidths_static": [_VP, _VP, ctypes.POINTER(LwParams), _VP],
+    "phx_ph_smatrix_create": [_VP, _VP, ctypes.POINTER(LwParams), ctypes.POINTER(_VP), ctypes.POINTER(LwStats)],
+    "phx_smatrix_num_states": [_VP],
+    "phx_smatrix_diagonal": [_VP, _D],
+    "phx_smatrix_get_rows": [_VP, _i, _i, _D],
+    "phx_smatrix_dot": [_VP, _i, _D, _i, _D],
+    "phx_smatrix_dot_d": [_VP, _i, _VP, _i, _VP, ctypes.POINTER(ctypes.c_float)],
+    "phx_smatrix_destroy": [_VP],
+    "phx_ph_smatrix_dot": [_VP, _VP, ctypes.POINTER(LwParams), _i, _D, _D, ctypes.POINTER(LwStats)],
+    "phx_ph_smatrix_dot_d": [_VP, _VP, ctypes.POINTER(LwParams), _i, _VP, _VP, ctypes.POINTER(LwStats)],
     "phx_el_h0_create": [_VP, _i, _i, _D, _D, _D, _D, ctypes.POINTER(_VP)],
     "phx_el_h0_destroy": [_VP],
     "phx_el_h0_num_bands": [_VP],

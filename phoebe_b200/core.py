@@ -298,15 +298,23 @@ class Interaction3Ph:
 
 
 class PhScatteringMatrix:
-    """RTA phonon scattering rates on a full mesh (linewidth mode of the builder)."""
+    """Phonon scattering matrix on a full mesh (PhScatteringMatrix / ScatteringMatrix).
+
+    Without in_memory, setup() runs the builder's linewidth mode and dot()
+    its matrix-vector mode (one builder pass per product, nothing stored).
+    With in_memory (the reference's scatteringMatrixInMemory; one
+    temperature), setup() builds the whole matrix into device memory and dot()
+    / offDiagonalDot() multiply with it."""
 
     def __init__(self, coupling3Ph, bands, temperatures_ry, smearing="adaptive", sigma=0.0, window=None,
-                 isotope_coupling=None, boundary_length=0.0):
+                 isotope_coupling=None, boundary_length=0.0, in_memory=False):
         """window: optional (energy (nq), cut (nq)) per-q1 q2 window: the pair
         (q1, q2) counts only when energy[q2] <= cut[q1] (synth.q2_window).
         isotope_coupling: per-atom coupling (core.isotope_coupling) enables
         isotope scattering; boundary_length > 0 (Bohr) enables boundary
         scattering (the reference's withIsotopeScattering / boundaryLength)."""
+        self.in_memory = bool(in_memory)
+        self._m = None
         self.v3 = coupling3Ph
         self.bands = bands
         self.temperatures = f64(np.atleast_1d(temperatures_ry))
@@ -336,7 +344,10 @@ class PhScatteringMatrix:
         return p
 
     def setup(self, q2_begin=0, q2_end=None, finalize=True):
-        """Builds A_out = linewidth * n(n+1) (internalDiagonal), shape (nT, nq*nb)."""
+        """Builds A_out = linewidth * n(n+1) (internalDiagonal), shape (nT, nq*nb).
+        In memory: builds the matrix too; its diagonal is not degeneracy-averaged."""
+        if self.in_memory:
+            return self._setup_matrix(q2_begin, q2_end, finalize)
         nT = len(self.temperatures)
         out = np.zeros((nT, self.bands.nq * self.bands.nb))
         p = self._params(q2_begin, q2_end, finalize)
@@ -346,6 +357,90 @@ class PhScatteringMatrix:
         self.internalDiagonal = out
         self.stats = st
         return out
+
+    def _setup_matrix(self, q2_begin, q2_end, finalize):
+        if len(self.temperatures) != 1:
+            raise ValueError("a stored scattering matrix holds one temperature")
+        self.close()
+        p = self._params(q2_begin, q2_end, finalize)
+        st = _abi.LwStats()
+        h = ctypes.c_void_p()
+        L = _abi.load()
+        check(L.phx_ph_smatrix_create(self.v3.h, self.bands.h, ctypes.byref(p), ctypes.byref(h), ctypes.byref(st)),
+              self.v3.ctx.h)
+        self._m = h
+        ns = L.phx_smatrix_num_states(h)
+        diag = np.zeros((1, ns))
+        check(L.phx_smatrix_diagonal(h, dptr(diag)), self.v3.ctx.h)
+        self.internalDiagonal = diag
+        self.stats = st
+        return diag
+
+    @property
+    def num_states(self):
+        return self.bands.nq * self.bands.nb
+
+    def _vectors(self, x):
+        x = f64(x)
+        single = x.ndim == 3
+        x = x[None] if single else x
+        if x.shape[1:] != (len(self.temperatures), 3, self.num_states):
+            raise ValueError("vectors must be (nT, 3, numStates) or (nvec, nT, 3, numStates)")
+        return x, single
+
+    def dot(self, x, q2_begin=0, q2_end=None, finalize=True):
+        """A x (ScatteringMatrix::dot) for x (nT, 3, ns) or (nvec, nT, 3, ns).
+        In memory: rows and columns of excluded states left out; otherwise one
+        matrix-vector pass of the builder (switchCase 1)."""
+        x, single = self._vectors(x)
+        y = np.zeros_like(x)
+        L = _abi.load()
+        if self.in_memory:
+            if self._m is None:
+                raise RuntimeError("setup() first")
+            check(L.phx_smatrix_dot(self._m, x.shape[0], dptr(x), 0, dptr(y)), self.v3.ctx.h)
+        else:
+            p = self._params(q2_begin, q2_end, finalize)
+            st = _abi.LwStats()
+            check(L.phx_ph_smatrix_dot(self.v3.h, self.bands.h, ctypes.byref(p), x.shape[0], dptr(x), dptr(y),
+                                       ctypes.byref(st)), self.v3.ctx.h)
+            self.stats = st
+        return y[0] if single else y
+
+    def offDiagonalDot(self, x):
+        """ScatteringMatrix::offDiagonalDot (scattering.cpp:180-265).  In memory:
+        A x without the diagonal; otherwise, as the reference, dot(x) minus
+        internalDiagonal * x with the internalDiagonal of setup() (averaged)."""
+        x, single = self._vectors(x)
+        if self.in_memory:
+            if self._m is None:
+                raise RuntimeError("setup() first")
+            y = np.zeros_like(x)
+            check(_abi.load().phx_smatrix_dot(self._m, x.shape[0], dptr(x), 1, dptr(y)), self.v3.ctx.h)
+        else:
+            if self.internalDiagonal is None:
+                raise RuntimeError("setup() first")
+            y = self.dot(x) - self.internalDiagonal[None, :, None, :] * x
+        return y[0] if single else y
+
+    def getMatrixRows(self, row0, nrows):
+        """Rows row0 .. row0+nrows-1 of the stored matrix, (nrows, numStates)."""
+        if self._m is None:
+            raise RuntimeError("the matrix is stored only with in_memory=True, after setup()")
+        out = np.zeros((nrows, self.num_states))
+        check(_abi.load().phx_smatrix_get_rows(self._m, int(row0), int(nrows), dptr(out)), self.v3.ctx.h)
+        return out
+
+    def close(self):
+        if getattr(self, "_m", None) is not None:
+            _abi.load().phx_smatrix_destroy(self._m)
+            self._m = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def getLinewidths(self, E):
         """Gamma = A_out / (n(n+1)) (scattering.cpp:529-568)."""

@@ -214,9 +214,23 @@ struct PairArgs {
   const double2* Dp;
   int q2_first, q2_count, q2_per_slot;
   double* partial;   // (S, nq, nb, nT)
+  // matrix modes (pair_fp64_kernel<NB, true>): column-major blocks of the
+  // scattering matrix, element (row, col) at col * ld + row, row = q1 nb + b1.
+  //   mat_full = 1: matP is the whole matrix (one temperature); the "+" rates
+  //     of (q1 b1, q2 b2) and minus the "-" rates of (q1 b1, -q2 b2) are added
+  //     atomically (each element receives one of each).
+  //   mat_full = 0: slabs of the chunk, column j nb + b2 (j = q2 - q2_first):
+  //     matP the "+" rates of (q1 b1, q2 b2), matM the "-" rates of
+  //     (q1 b1, -q2 b2), each temperature mat_tstride elements further on;
+  //     every element of the slabs is stored.
+  double* matP;
+  double* matM;
+  long long ld;
+  size_t mat_tstride;
+  int mat_full;
 };
 
-template <int NB>
+template <int NB, bool MAT = false>
 __global__ void __launch_bounds__(kTile * NB, 1) pair_fp64_kernel(PairArgs P) {
   const MeshArgs& M = P.m;
   extern __shared__ __align__(16) char sraw[];
@@ -387,7 +401,82 @@ __global__ void __launch_bounds__(kTile * NB, 1) pair_fp64_kernel(PairArgs P) {
         v2m[i] = M.vg[((size_t)iq2m * NB + b2) * 3 + i];
       }
     }
-    if (valid && (ok2 || ok2m)) {
+    if constexpr (MAT) {
+      // one temperature at a time: the sums over b3 of the "+" rates (sp) and
+      // of the two "-" rates (sm) of each b1, which also make the linewidths
+#pragma unroll 1
+      for (int c = 0; c < nT; ++c) {
+        double sp[NB], sm[NB];
+#pragma unroll
+        for (int b1 = 0; b1 < NB; ++b1) sp[b1] = sm[b1] = 0.0;
+        if (valid && (ok2 || ok2m)) {
+          const double n2c = M.bose[((size_t)c * nq + iq2) * NB + b2];
+          const double n2mc = M.bose[((size_t)c * nq + iq2m) * NB + b2];
+#pragma unroll
+          for (int b3 = 0; b3 < NB; ++b3) {
+            const double en3 = E3[b3];
+            if (en3 < phxc::phEnergyCutoff) continue;
+            double sgp = M.sigma, sgm = M.sigma;
+            bool vzp = false, vzm = false;
+            if (M.smearing == PHX_SMEAR_ADAPTIVE) {
+              const double* v3 = M.vg + ((size_t)iq3 * NB + b3) * 3;
+              const double dp0 = v2[0] - v3[0], dp1 = v2[1] - v3[1], dp2 = v2[2] - v3[2];
+              const double dm0 = v2m[0] - v3[0], dm1 = v2m[1] - v3[1], dm2 = v2m[2] - v3[2];
+              vzp = (dp0 * dp0 + dp1 * dp1 + dp2 * dp2) == 0.0;
+              vzm = (dm0 * dm0 + dm1 * dm1 + dm2 * dm2) == 0.0;
+              sgp = floor_sigma(adaptive_sigma(M.qT, dp0, dp1, dp2));
+              sgm = floor_sigma(adaptive_sigma(M.qT, dm0, dm1, dm2));
+            }
+            const double n3c = M.bose[((size_t)c * nq + iq3) * NB + b3];
+#pragma unroll
+            for (int b1 = 0; b1 < NB; ++b1) {
+              const double en1 = E1[b1];
+              if (en1 < phxc::phExcludeCutoff || en1 < phxc::phEnergyCutoff) continue;
+              const double w = W[b1][b3];
+              const double n1 = b1s[(c * NB + b1) * kTile + ql];
+              if (ok2) {
+                const double dlt = delta_fn(M.smearing, sgp, en1 + en2 - en3, vzp);
+                if (dlt > 0.0) sp[b1] += phxc::pi * 0.25 * w * dlt * M.norm / (en1 * en2 * en3) * n1 * n2c * (n3c + 1.0);
+              }
+              if (ok2m) {
+                double d1 = delta_fn(M.smearing, sgm, en1 + en3 - en2m, vzm);
+                double d2 = delta_fn(M.smearing, sgm, en2m + en3 - en1, vzm);
+                if (d1 > 0.0 || d2 > 0.0) {
+                  d1 = fmax(d1, 0.0);
+                  d2 = fmax(d2, 0.0);
+                  const double f = phxc::pi * 0.25 * w * M.norm / (en1 * en2m * en3);
+                  sm[b1] += f * n3c * n1 * (n2mc + 1.0) * d1 + f * n2mc * n3c * (n1 + 1.0) * d2;
+                }
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int b1 = 0; b1 < NB; ++b1)
+#pragma unroll
+          for (int cc = 0; cc < kMaxT; ++cc)
+            if (cc == c) acc[b1][cc] += 0.5 * (sp[b1] + sm[b1]);
+        if (valid) {
+          const size_t row = (size_t)q1 * NB;
+          if (P.mat_full) {
+            double* colp = P.matP + (size_t)(iq2 * NB + b2) * P.ld + row;
+            double* colm = P.matP + (size_t)(iq2m * NB + b2) * P.ld + row;
+#pragma unroll
+            for (int b1 = 0; b1 < NB; ++b1) {
+              if (sp[b1] != 0.0) atomicAdd(colp + b1, sp[b1]);
+              if (sm[b1] != 0.0) atomicAdd(colm + b1, -sm[b1]);
+            }
+          } else {
+            const size_t o = c * P.mat_tstride + (size_t)(j * NB + b2) * P.ld + row;
+#pragma unroll
+            for (int b1 = 0; b1 < NB; ++b1) {
+              P.matP[o + b1] = sp[b1];
+              P.matM[o + b1] = sm[b1];
+            }
+          }
+        }
+      }
+    } else if (valid && (ok2 || ok2m)) {
 #pragma unroll
       for (int b3 = 0; b3 < NB; ++b3) {
         const double en3 = E3[b3];
@@ -696,13 +785,20 @@ __global__ void __launch_bounds__(kGenThreads) pair_generic_kernel(PairArgs P, Q
 //          (n1 n2 + (n1 + n2)/2),
 // with U mass-scaled and g_a the reference's massVariance (variance x mass^2).
 // Adaptive smearing takes its width from v1 and halves the delta, as the
-// reference does (:684-687).  Rates go to the partial sums of the slot.
+// reference does (:684-687).  Rates go to the partial sums of the slot and,
+// in the matrix modes, are subtracted from the element (q1 b1, q2 b2) of the
+// matrix or of the "+" slab (same layouts as PairArgs; this kernel runs after
+// the pair kernels, and each element has one writer).
 struct IsoArgs {
   MeshArgs m;
   int nat;
   const double* g;      // (nat)
   int q2_first, q2_count, q2_per_slot;
   double* partial;      // (S, nq, nb, nT)
+  double* mat = nullptr;
+  long long ld = 0;
+  size_t mat_tstride = 0;
+  int mat_full = 0;
 };
 
 inline size_t iso_smem(int nb) { return sizeof(double2) * nb * nb + sizeof(double) * nb; }
@@ -769,7 +865,14 @@ __global__ void __launch_bounds__(kTile * kMaxNbGeneric) isotope_kernel(IsoArgs 
       for (int c = 0; c < kMaxT; ++c)
         if (c < nT) {
           const double n2 = M.bose[((size_t)c * nq + iq2) * nb + b2];
-          acc[c] += term * (n1[c] * n2 + 0.5 * (n1[c] + n2));
+          const double r = term * (n1[c] * n2 + 0.5 * (n1[c] + n2));
+          acc[c] += r;
+          if (A.mat) {
+            const size_t row = (size_t)q1 * nb + b1;
+            double* dst = A.mat_full ? A.mat + (size_t)(iq2 * nb + b2) * A.ld + row
+                                     : A.mat + c * A.mat_tstride + (size_t)(j * nb + b2) * A.ld + row;
+            *dst -= r;
+          }
         }
     }
   }
@@ -782,10 +885,12 @@ __global__ void __launch_bounds__(kTile * kMaxNbGeneric) isotope_kernel(IsoArgs 
 // Sums the partial slots into A_out; with finalize: degeneracy averaging of
 // row 0, then boundary scattering |v|/L n(n+1) on every row (added after the
 // averaging, ph_scattering.cpp:819-860), then zero for excluded states.
+// The matrix modes pass average = 0: their diagonal is not averaged
+// (ph_scattering.cpp:809-817).
 __global__ void finalize_kernel(int nq, int nb, int nT, int nslots, const double* __restrict__ partial,
                                 const double* __restrict__ E, int finalize, const double* __restrict__ vg,
                                 const double* __restrict__ temps, double boundary_length,
-                                double* __restrict__ Aout) {
+                                double* __restrict__ Aout, int average = 1) {
   const int iq = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= nq) return;
   const size_t ns = (size_t)nq * nb;
@@ -796,7 +901,7 @@ __global__ void finalize_kernel(int nq, int nb, int nT, int nslots, const double
       for (int k = 0; k < nslots; ++k) s += partial[(((size_t)k * nq + iq) * nb + b) * nT + c];
       lw[b] = s;
     }
-    if (finalize && c == 0) {
+    if (finalize && average && c == 0) {
       // degeneracyAveragingLinewidths (scattering.cpp:1168-1207), row 0 only
       double tmp[64];
       for (int b1 = 0; b1 < nb; ++b1) {
@@ -1587,6 +1692,330 @@ int run_builder_generic(phx_v3* v, phx_bands* b, const phx_lw_params* p, double*
   cudaEventDestroy(ev1);
   return rc;
 }
+
+// ---------------------------------------------------------------------------
+// Matrix modes of the builder (ph_scattering.cpp, switchCase 0 and 1, without
+// symmetries), FP64, nb = 6.  The q2 loop is the linewidth builder's: the R2
+// fold of a chunk, then pair_fp64_kernel<6, true>, whose epilogue also keeps,
+// per (q1 b1, q2 b2), the sums over b3 of the "+" and of the "-" rates.
+//   mode 0 (A_full): they go straight into the stored matrix (ns x ns,
+//     column-major; nT = 1), isotope rates after the last chunk, then the
+//     un-averaged linewidths with boundary scattering on the diagonal;
+//   mode 1 (x_d, y_d): they go into two slabs of the chunk's columns, which
+//     are multiplied with x at once (smatrix_dot_kernel) and dropped, so A x
+//     costs one builder pass and slab memory only; then the diagonal term.
+// ---------------------------------------------------------------------------
+template <int NB>
+int run_matrix_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* A_full, double* lw_d, int nvec,
+                       const double* x_d, double* y_d, phx_lw_stats* stats) {
+  phx_ctx* ctx = v->ctx;
+  cudaStream_t st = ctx->stream;
+  const int nq = b->nq, nT = p->num_temperatures, nr3 = v->nr3, nr2 = v->nr2;
+  const int q2b = p->q2_begin, q2e = p->q2_end;
+  const int ns = nq * NB;
+  const bool full = A_full != nullptr;
+  // slab memory of mode 1: at most 4 GiB for the two slabs of all temperatures
+  int chunk = std::min(512, q2e - q2b);
+  if (!full) {
+    const size_t per_q2 = 2 * sizeof(double) * (size_t)nT * ns * NB;
+    chunk = (int)std::max<size_t>(1, std::min<size_t>(chunk, (size_t(4) << 30) / per_q2));
+  }
+  const int slots = std::min(8, chunk);
+  const size_t nb3 = (size_t)NB * NB * NB;
+  const size_t sz_dp = align_up(sizeof(double2) * chunk * nr3 * nb3);
+  const size_t sz_part = align_up(sizeof(double) * slots * nq * NB * nT);
+  const size_t sz_bose = align_up(sizeof(double) * nT * nq * NB);
+  const size_t sz_T = align_up(sizeof(double) * 8);
+  const size_t sz_iso = p->isotope_coupling ? align_up(sizeof(double) * v->nat) : 0;
+  const size_t slab_elems = (size_t)ns * chunk * NB;
+  const size_t sz_slab = full ? 0 : align_up(sizeof(double) * 2 * nT * slab_elems);
+  PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_iso + sz_slab));
+  char* base = static_cast<char*>(v->ctx->d_scratch);
+  double2* Dp = reinterpret_cast<double2*>(base);
+  double* partial = reinterpret_cast<double*>(base + sz_dp);
+  double* bose = reinterpret_cast<double*>(base + sz_dp + sz_part);
+  double* temps = reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose);
+  double* giso =
+      p->isotope_coupling ? reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose + sz_T) : nullptr;
+  double* slabP = full ? nullptr : reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose + sz_T + sz_iso);
+  double* slabM = full ? nullptr : slabP + nT * slab_elems;
+  PairArgs P{};
+  P.m.nq = nq;
+  P.m.nb = NB;
+  P.m.nT = nT;
+  P.m.n0 = b->mesh[0];
+  P.m.n1 = b->mesh[1];
+  P.m.n2 = b->mesh[2];
+  P.m.E = b->d_E;
+  P.m.U = reinterpret_cast<const double2*>(b->d_U);
+  P.m.vg = b->d_vg;
+  P.m.bose = bose;
+  P.m.qcart = b->d_q;
+  P.m.smearing = p->smearing;
+  P.m.sigma = p->sigma;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) P.m.qT[i * 3 + j] = b->recip[i * 3 + j] / b->mesh[i];
+  P.m.norm = 1.0 / (double)nq;
+  P.nr3 = nr3;
+  P.R3 = v->d_R3;
+  P.Dp = Dp;
+  P.partial = partial;
+  P.matP = full ? A_full : slabP;
+  P.matM = slabM;
+  P.ld = ns;
+  P.mat_tstride = slab_elems;
+  P.mat_full = full ? 1 : 0;
+  const size_t smem_pair = sizeof(double2) * ((size_t)nr3 * kTile + 2 * NB * NB * kTile) +
+                           sizeof(double) * ((size_t)NB * NB * NB * kTile + (size_t)kMaxT * NB * kTile);
+  PHX_ARG(ctx, smem_pair <= 227 * 1024, "scattering matrix: too many R3 vectors for the FP64 path");
+  PHX_CUDA(ctx, cudaFuncSetAttribute(pair_fp64_kernel<NB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_pair));
+  const size_t smem_fold = fold_tiled_smem(NB, nr2);
+  PHX_ARG(ctx, smem_fold <= 227 * 1024, "scattering matrix: too many R2 vectors");
+  if (smem_fold > 48 * 1024)
+    PHX_CUDA(ctx, cudaFuncSetAttribute(fold_q2_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_fold));
+  const int tiles = (nq + kTile - 1) / kTile;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evv0 = nullptr, evv1 = nullptr;
+  PHX_CUDA(ctx, cudaEventCreate(&ev0));
+  PHX_CUDA(ctx, cudaEventCreate(&ev1));
+  PHX_CUDA(ctx, cudaEventCreate(&evv0));
+  PHX_CUDA(ctx, cudaEventCreate(&evv1));
+  int launches = 0;
+  auto work = [&]() -> int {
+    PHX_CUDA(ctx, cudaEventRecord(ev0, st));
+    PHX_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
+    PHX_CUDA(ctx, cudaMemcpyAsync(temps, p->temperatures, sizeof(double) * nT, cudaMemcpyHostToDevice, st));
+    if (giso)
+      PHX_CUDA(ctx, cudaMemcpyAsync(giso, p->isotope_coupling, sizeof(double) * v->nat, cudaMemcpyHostToDevice, st));
+    PHX_CUDA(ctx, cudaMemsetAsync(partial, 0, sizeof(double) * slots * nq * NB * nT, st));
+    if (full) PHX_CUDA(ctx, cudaMemsetAsync(A_full, 0, sizeof(double) * ns * (size_t)ns, st));
+    else PHX_CUDA(ctx, cudaMemsetAsync(y_d, 0, sizeof(double) * nvec * nT * 3 * (size_t)ns, st));
+    bose_kernel<<<std::min(1024, (nq * NB * nT + 255) / 256), 256, 0, st>>>(nq, NB, nT, b->d_E, temps, bose);
+    ++launches;
+    PHX_CUDA(ctx, cudaEventRecord(evv0, st));
+    for (int c0 = q2b; c0 < q2e; c0 += chunk) {
+      const int cnt = std::min(chunk, q2e - c0);
+      fold_tiled_launch(NB, nr2, nr3, v, b, c0, cnt, Dp, st);
+      ++launches;
+      PairArgs Q = P;
+      Q.q2_first = c0;
+      Q.q2_count = cnt;
+      Q.q2_per_slot = (cnt + slots - 1) / slots;
+      pair_fp64_kernel<NB, true><<<dim3(tiles, slots), kTile * NB, smem_pair, st>>>(Q);
+      ++launches;
+      PHX_CUDA(ctx, cudaGetLastError());
+      if (!full) {
+        if (giso) {
+          IsoArgs I{P.m, v->nat, giso, c0, cnt, (cnt + slots - 1) / slots, partial, slabP, ns, slab_elems, 0};
+          isotope_kernel<<<dim3(tiles, slots), kTile * NB, iso_smem(NB), st>>>(I);
+          ++launches;
+          PHX_CUDA(ctx, cudaGetLastError());
+        }
+        phx_dot_args a{};
+        a.ns = ns;
+        a.ncols = cnt * NB;
+        a.ld = ns;
+        a.Sp = slabP;
+        a.Sm = slabM;
+        a.tstride = slab_elems;
+        a.slab = 1;
+        a.q2_first = c0;
+        a.nb = NB;
+        a.n0 = b->mesh[0];
+        a.n1 = b->mesh[1];
+        a.n2 = b->mesh[2];
+        a.nT = nT;
+        a.nvec = nvec;
+        a.x = x_d;
+        a.y = y_d;
+        a.skip = 0;
+        a.E = b->d_E;
+        if (phx_smatrix_dot_launch(a, st, &launches) != PHX_OK) {
+          phx_set_error(ctx, PHX_ERR_CUDA, "scattering matrix: slab product launch failed");
+          return PHX_ERR_CUDA;
+        }
+      }
+    }
+    if (full && giso) {
+      IsoArgs I{P.m, v->nat, giso, q2b, q2e - q2b, (q2e - q2b + slots - 1) / slots, partial, A_full, ns, 0, 1};
+      isotope_kernel<<<dim3(tiles, slots), kTile * NB, iso_smem(NB), st>>>(I);
+      ++launches;
+      PHX_CUDA(ctx, cudaGetLastError());
+    }
+    PHX_CUDA(ctx, cudaEventRecord(evv1, st));
+    finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, NB, nT, slots, partial, b->d_E, p->finalize, b->d_vg, temps,
+                                                      p->boundary_length, lw_d, 0);
+    ++launches;
+    PHX_CUDA(ctx, cudaGetLastError());
+    if (full) {
+      if (p->finalize) {
+        PHX_TRY(phx_smatrix_set_diag_launch(ns, ns, lw_d, A_full, st));
+        ++launches;
+      }
+    } else {
+      PHX_TRY(phx_smatrix_diag_term_launch(ns, nT, nvec, lw_d, x_d, y_d, b->d_E, p->finalize, st));
+      ++launches;
+    }
+    PHX_CUDA(ctx, cudaEventRecord(ev1, st));
+    return PHX_OK;
+  };
+  int rc = work();
+  if (rc == PHX_OK) {
+    cudaError_t ce = cudaEventSynchronize(ev1);
+    int kst = 0;
+    if (ce == cudaSuccess) ce = cudaMemcpy(&kst, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) {
+      phx_set_error(ctx, PHX_ERR_CUDA, cudaGetErrorString(ce));
+      rc = PHX_ERR_CUDA;
+    } else if (kst) {
+      cudaMemset(ctx->d_status, 0, sizeof(int));
+      phx_set_error(ctx, PHX_ERR_CUDA, "scattering matrix: kernel status " + std::to_string(kst));
+      rc = PHX_ERR_CUDA;
+    }
+  }
+  if (rc == PHX_OK && stats) {
+    float ms = 0.f, msv = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventElapsedTime(&msv, evv0, evv1);
+    *stats = phx_lw_stats{};
+    stats->ms_total = ms;
+    stats->ms_vertex = msv;
+    stats->pairs = (long long)nq * (q2e - q2b);
+    stats->kernel_launches = launches;
+    stats->plan_chunk = chunk;
+    stats->plan_slots = slots;
+  }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  cudaEventDestroy(evv0);
+  cudaEventDestroy(evv1);
+  return rc;
+}
+
+// argument checks shared by the three builder modes
+int check_builder_args(phx_v3* v, phx_bands* b, const phx_lw_params* p) {
+  PHX_ARG(nullptr, v && b && p, "builder: bad arguments");
+  phx_ctx* ctx = v->ctx;
+  PHX_ARG(ctx, b->ctx == ctx, "v3 and bands belong to different contexts");
+  PHX_ARG(ctx, b->nb == v->nb, "band count of bands and v3 differ");
+  PHX_ARG(ctx, p->num_temperatures >= 1 && p->num_temperatures <= kMaxT && p->temperatures,
+          "1..4 temperatures per call");
+  PHX_ARG(ctx, p->smearing == PHX_SMEAR_GAUSSIAN || p->smearing == PHX_SMEAR_ADAPTIVE, "bad smearing");
+  PHX_ARG(ctx, p->smearing != PHX_SMEAR_GAUSSIAN || p->sigma > 0.0, "Gaussian smearing needs sigma > 0");
+  PHX_ARG(ctx, p->smearing != PHX_SMEAR_ADAPTIVE || b->d_vg, "adaptive smearing needs velocities");
+  PHX_ARG(ctx, 0 <= p->q2_begin && p->q2_begin <= p->q2_end && p->q2_end <= b->nq, "bad q2 range");
+  PHX_ARG(ctx, !(p->boundary_length > 0.0) || b->d_vg, "boundary scattering needs velocities");
+  return PHX_OK;
+}
+
+int check_matrix_args(phx_v3* v, phx_bands* b, const phx_lw_params* p) {
+  PHX_TRY(check_builder_args(v, b, p));
+  phx_ctx* ctx = v->ctx;
+  PHX_ARG(ctx, v->nb == 6, "scattering matrix modes: nb = 6 (the fused FP64 kernels)");
+  PHX_ARG(ctx, v->precision == PHX_PREC_FP64, "scattering matrix modes run in FP64 (set PHX_PREC_FP64)");
+  PHX_ARG(ctx, !p->window_energy && !p->window_cut, "scattering matrix modes take no q2 window");
+  return PHX_OK;
+}
+
+}  // namespace
+
+extern "C" int phx_ph_smatrix_create(phx_v3* v, phx_bands* b, const phx_lw_params* p, phx_smatrix** out,
+                                     phx_lw_stats* stats) {
+  PHX_TRY(check_matrix_args(v, b, p));
+  phx_ctx* ctx = v->ctx;
+  PHX_ARG(ctx, out, "phx_ph_smatrix_create: null output handle");
+  PHX_ARG(ctx, p->num_temperatures == 1,
+          "a stored scattering matrix holds one temperature (scatteringMatrixInMemory)");
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t ns = (size_t)b->nq * b->nb;
+  size_t fr = 0, tot = 0;
+  PHX_CUDA(ctx, cudaMemGetInfo(&fr, &tot));
+  PHX_ARG(ctx, sizeof(double) * ns * ns < fr,
+          "scattering matrix of " + std::to_string(ns) + " states does not fit in free device memory");
+  phx_smatrix* m = new phx_smatrix;
+  m->ctx = ctx;
+  m->nq = b->nq;
+  m->nb = b->nb;
+  m->ns = (int)ns;
+  for (int i = 0; i < 3; ++i) m->mesh[i] = b->mesh[i];
+  cudaError_t e = cudaMalloc(&m->d_A, sizeof(double) * ns * ns);
+  if (e == cudaSuccess) e = cudaMalloc(&m->d_E, sizeof(double) * ns);
+  if (e == cudaSuccess) e = cudaMalloc(&m->d_diag, sizeof(double) * ns);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(m->d_E, b->d_E, sizeof(double) * ns, cudaMemcpyDeviceToDevice, ctx->stream);
+  if (e != cudaSuccess) {
+    phx_set_error(ctx, PHX_ERR_CUDA, std::string("phx_ph_smatrix_create: ") + cudaGetErrorString(e));
+    phx_smatrix_destroy(m);
+    return PHX_ERR_CUDA;
+  }
+  int rc = PHX_OK;
+  if (p->q2_begin == p->q2_end) {
+    if (cudaMemsetAsync(m->d_A, 0, sizeof(double) * ns * ns, ctx->stream) != cudaSuccess ||
+        cudaMemsetAsync(m->d_diag, 0, sizeof(double) * ns, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+      phx_set_error(ctx, PHX_ERR_CUDA, "phx_ph_smatrix_create: memset failed");
+      rc = PHX_ERR_CUDA;
+    }
+  } else {
+    rc = run_matrix_builder<6>(v, b, p, m->d_A, m->d_diag, 0, nullptr, nullptr, stats);
+  }
+  if (rc != PHX_OK) {
+    phx_smatrix_destroy(m);
+    return rc;
+  }
+  *out = m;
+  return PHX_OK;
+}
+
+namespace {
+
+// switchCase 1 with device vectors; lw_d: (nT, ns) device scratch of the diagonal term
+int matrix_dot(phx_v3* v, phx_bands* b, const phx_lw_params* p, int nvec, const double* x_d, double* y_d,
+               double* lw_d, phx_lw_stats* stats) {
+  phx_ctx* ctx = v->ctx;
+  const size_t ns = (size_t)b->nq * b->nb, nT = p->num_temperatures;
+  if (p->q2_begin == p->q2_end) {
+    PHX_CUDA(ctx, cudaMemsetAsync(y_d, 0, sizeof(double) * nvec * nT * 3 * ns, ctx->stream));
+    PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return PHX_OK;
+  }
+  return run_matrix_builder<6>(v, b, p, nullptr, lw_d, nvec, x_d, y_d, stats);
+}
+
+}  // namespace
+
+extern "C" int phx_ph_smatrix_dot_d(phx_v3* v, phx_bands* b, const phx_lw_params* p, int nvec, const double* x_d,
+                                    double* y_d, phx_lw_stats* stats) {
+  PHX_TRY(check_matrix_args(v, b, p));
+  phx_ctx* ctx = v->ctx;
+  PHX_ARG(ctx, nvec >= 1 && x_d && y_d, "phx_ph_smatrix_dot: bad vectors");
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t ns = (size_t)b->nq * b->nb;
+  PHX_TRY(phx_ctx_reserve(ctx, &ctx->d_out, &ctx->out_bytes, sizeof(double) * p->num_temperatures * ns));
+  return matrix_dot(v, b, p, nvec, x_d, y_d, static_cast<double*>(ctx->d_out), stats);
+}
+
+extern "C" int phx_ph_smatrix_dot(phx_v3* v, phx_bands* b, const phx_lw_params* p, int nvec, const double* x,
+                                  double* y, phx_lw_stats* stats) {
+  PHX_TRY(check_matrix_args(v, b, p));
+  phx_ctx* ctx = v->ctx;
+  PHX_ARG(ctx, nvec >= 1 && x && y, "phx_ph_smatrix_dot: bad vectors");
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t ns = (size_t)b->nq * b->nb, nT = p->num_temperatures;
+  const size_t n = (size_t)nvec * nT * 3 * ns;
+  // output staging: the diagonal term's linewidths, x, y
+  PHX_TRY(phx_ctx_reserve(ctx, &ctx->d_out, &ctx->out_bytes, sizeof(double) * (nT * ns + 2 * n)));
+  double* lw = static_cast<double*>(ctx->d_out);
+  double* xd = lw + nT * ns;
+  double* yd = xd + n;
+  PHX_CUDA(ctx, cudaMemcpyAsync(xd, x, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  PHX_TRY(matrix_dot(v, b, p, nvec, xd, yd, lw, stats));
+  PHX_CUDA(ctx, cudaMemcpyAsync(y, yd, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHX_OK;
+}
+
+namespace {
 
 }  // namespace
 

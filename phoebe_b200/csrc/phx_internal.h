@@ -149,6 +149,48 @@ struct phx_elph {
   size_t scratch_bytes = 0;
 };
 
+// ---------------------------------------------------------------------------
+// scattering matrix (smatrix.cu): column-major blocks, element (row, col) at
+// col * ld + row, with row and col the state index iq * nb + ib.
+// ---------------------------------------------------------------------------
+struct phx_smatrix {
+  phx_ctx* ctx = nullptr;
+  int nq = 0, nb = 0, ns = 0;
+  int mesh[3] = {0, 0, 0};
+  double* d_A = nullptr;      // (ns, ns) column-major
+  double* d_E = nullptr;      // (ns) energies (exclusions of the dot product)
+  double* d_diag = nullptr;   // (ns) the diagonal: linewidths x n(n+1), not averaged
+  double* d_xy = nullptr;     // staging of x and y for phx_smatrix_dot
+  size_t xy_bytes = 0;
+};
+
+// y += (block of a scattering matrix) x, for x and y (nvec, nT, 3, ns) on the device.
+struct phx_dot_args {
+  int ns;                  // rows (states)
+  int ncols;               // columns of the block
+  long long ld;
+  const double* Sp;        // the block; temperature c at Sp + c * tstride
+  const double* Sm;        // slab of "-" rates, or null
+  size_t tstride;
+  // slab = 1: column k = j nb + b2 is the state (q2_first + j) nb + b2 in Sp
+  // and (-(q2_first + j)) nb + b2 in Sm; slab = 0: column k is the state k
+  int slab, q2_first, nb, n0, n1, n2;
+  int nT, nvec;
+  const double* x;
+  double* y;
+  // skip = 0: the element whose column state is the row state is left out
+  // (the off-diagonal part); 1: rows and columns of excluded states are left
+  // out (ScatteringMatrix::dot of a stored matrix)
+  int skip;
+  const double* E;         // (ns), for skip = 1
+};
+int phx_smatrix_dot_launch(const phx_dot_args& a, cudaStream_t st, int* launches);
+// y (nvec, nT, 3, ns) += lw (nT, ns) * x; then, with finalize, y = 0 on excluded states
+int phx_smatrix_diag_term_launch(int ns, int nT, int nvec, const double* lw, const double* x, double* y,
+                                 const double* E, int finalize, cudaStream_t st);
+// A(s, s) = diag(s)
+int phx_smatrix_set_diag_launch(int ns, long long ld, const double* diag, double* A, cudaStream_t st);
+
 // kernels implemented in harmonic.cu, used by the ABI layer
 int phx_launch_ph_bands(phx_ph_h0* h0, int nq, const double* d_q, double* d_E, double* d_U,
                         double* d_vg, int mass_scaling);

@@ -1,0 +1,263 @@
+// Scattering matrix in device memory and the matrix-vector products of the
+// builder's matrix modes.
+//
+//   * ScatteringMatrix::dot / offDiagonalDot of a stored matrix
+//     (src/bte/scattering.cpp:180-265, 266-330), for the matrix that
+//     PhScatteringMatrix::builder builds with switchCase 0;
+//   * the product with the rate slabs of one q2 chunk, which is how the
+//     builder's switchCase 1 (src/bte/ph_scattering.cpp:408-431, 549-572) runs
+//     here: A x without storing A, chunk by chunk.
+//
+// Both are reads of FP64 matrix blocks once each, bound by HBM bandwidth: one
+// thread per row (coalesced down a column), a block of columns per CTA with
+// their x values staged in shared memory, 4 input vectors per pass, and one
+// atomic add per row and vector component at the end.
+#include <algorithm>
+#include <cstring>
+
+#include "pair_common.cuh"
+#include "phx_consts.h"
+#include "phx_internal.h"
+
+using pairc::mesh_neg;
+
+namespace {
+
+constexpr int kDotRows = 256;   // rows (threads) per CTA
+constexpr int kDotVec = 4;      // input vectors per pass
+constexpr int kDotV3 = 3 * kDotVec;
+
+__global__ void __launch_bounds__(kDotRows) smatrix_dot_kernel(phx_dot_args A, int cols_per_block) {
+  extern __shared__ __align__(16) double dsm[];
+  double* xp = dsm;                                  // [cols][kDotV3]
+  double* xm = xp + (size_t)cols_per_block * kDotV3; // [cols][kDotV3] (slabs)
+  int* stp = reinterpret_cast<int*>(xm + (A.Sm ? (size_t)cols_per_block * kDotV3 : 0));
+  int* stm = stp + cols_per_block;
+  const int c = blockIdx.z % A.nT, v0 = (blockIdx.z / A.nT) * kDotVec;
+  const int nv = min(kDotVec, A.nvec - v0);
+  const int k0 = blockIdx.y * cols_per_block, kn = min(cols_per_block, A.ncols - k0);
+  for (int t = threadIdx.x; t < cols_per_block; t += blockDim.x) {
+    int sp = 0, sm = 0;
+    if (t < kn) {
+      const int k = k0 + t;
+      if (A.slab) {
+        const int j = k / A.nb, b2 = k - j * A.nb, iq2 = A.q2_first + j;
+        sp = iq2 * A.nb + b2;
+        sm = mesh_neg(iq2, A.n0, A.n1, A.n2) * A.nb + b2;
+      } else {
+        sp = k;
+      }
+    }
+    stp[t] = sp;
+    stm[t] = sm;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < cols_per_block * kDotV3; e += blockDim.x) {
+    const int t = e / kDotV3, vi = e - t * kDotV3, v = vi / 3, i = vi - 3 * v;
+    double a = 0.0, b = 0.0;
+    if (t < kn && v < nv) {
+      const double* xv = A.x + (((size_t)(v0 + v) * A.nT + c) * 3 + i) * A.ns;
+      a = xv[stp[t]];
+      if (A.Sm) b = xv[stm[t]];
+      if (A.skip == 1 && A.E[stp[t]] < phxc::phExcludeCutoff) a = 0.0;
+    }
+    xp[e] = a;
+    if (A.Sm) xm[e] = b;
+  }
+  __syncthreads();
+  const int r = blockIdx.x * kDotRows + threadIdx.x;
+  if (r >= A.ns) return;
+  if (A.skip == 1 && A.E[r] < phxc::phExcludeCutoff) return;
+  double acc[kDotV3];
+#pragma unroll
+  for (int vi = 0; vi < kDotV3; ++vi) acc[vi] = 0.0;
+  const double* P = A.Sp + c * A.tstride + (size_t)k0 * A.ld + r;
+  if (A.Sm) {
+    const double* Q = A.Sm + c * A.tstride + (size_t)k0 * A.ld + r;
+#pragma unroll 4
+    for (int t = 0; t < kn; ++t) {
+      double a = __ldcs(P + (size_t)t * A.ld), b = __ldcs(Q + (size_t)t * A.ld);
+      if (r == stp[t]) a = 0.0;
+      if (r == stm[t]) b = 0.0;
+#pragma unroll
+      for (int vi = 0; vi < kDotV3; ++vi) acc[vi] += a * xp[t * kDotV3 + vi] - b * xm[t * kDotV3 + vi];
+    }
+  } else {
+#pragma unroll 4
+    for (int t = 0; t < kn; ++t) {
+      double a = __ldcs(P + (size_t)t * A.ld);
+      if (A.skip == 0 && r == stp[t]) a = 0.0;
+#pragma unroll
+      for (int vi = 0; vi < kDotV3; ++vi) acc[vi] += a * xp[t * kDotV3 + vi];
+    }
+  }
+  for (int v = 0; v < nv; ++v)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const double s = acc[3 * v + i];
+      if (s != 0.0) atomicAdd(A.y + (((size_t)(v0 + v) * A.nT + c) * 3 + i) * A.ns + r, s);
+    }
+}
+
+__global__ void diag_term_kernel(int ns, int nT, int nvec, const double* __restrict__ lw,
+                                 const double* __restrict__ x, double* __restrict__ y, const double* __restrict__ E,
+                                 int finalize) {
+  const size_t n = (size_t)nvec * nT * 3 * ns;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int s = (int)(e % ns);
+    const int c = (int)((e / ns / 3) % nT);
+    if (finalize && E[s] < phxc::phExcludeCutoff) y[e] = 0.0;
+    else y[e] += lw[(size_t)c * ns + s] * x[e];
+  }
+}
+
+__global__ void set_diag_kernel(int ns, long long ld, const double* __restrict__ diag, double* __restrict__ A) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < ns) A[(size_t)s * ld + s] = diag[s];
+}
+
+// out (nrows, ns) row-major = rows row0.. of the column-major A, through 32x32 tiles
+__global__ void rows_kernel(int ns, long long ld, const double* __restrict__ A, int row0, int nrows,
+                            double* __restrict__ out) {
+  __shared__ double tile[32][33];
+  const int cb = blockIdx.x * 32, rb = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int col = cb + k, r = rb + threadIdx.x;
+    tile[k][threadIdx.x] = (col < ns && r < nrows) ? A[(size_t)col * ld + row0 + r] : 0.0;
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int r = rb + k, col = cb + threadIdx.x;
+    if (r < nrows && col < ns) out[(size_t)r * ns + col] = tile[threadIdx.x][k];
+  }
+}
+
+}  // namespace
+
+int phx_smatrix_dot_launch(const phx_dot_args& a, cudaStream_t st, int* launches) {
+  if (a.ncols <= 0 || a.ns <= 0 || a.nvec <= 0) return PHX_OK;
+  // slabs: two blocks of columns per CTA; a stored matrix: one, longer
+  const int cols = a.Sm ? 64 : 256;
+  const size_t smem = sizeof(double) * cols * kDotV3 * (a.Sm ? 2 : 1) + sizeof(int) * 2 * cols;
+  dim3 grid((a.ns + kDotRows - 1) / kDotRows, (a.ncols + cols - 1) / cols, a.nT * ((a.nvec + kDotVec - 1) / kDotVec));
+  if (smem > 48 * 1024) cudaFuncSetAttribute(smatrix_dot_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  smatrix_dot_kernel<<<grid, kDotRows, smem, st>>>(a, cols);
+  if (launches) ++*launches;
+  return cudaGetLastError() == cudaSuccess ? PHX_OK : PHX_ERR_CUDA;
+}
+
+int phx_smatrix_diag_term_launch(int ns, int nT, int nvec, const double* lw, const double* x, double* y,
+                                 const double* E, int finalize, cudaStream_t st) {
+  const size_t n = (size_t)nvec * nT * 3 * ns;
+  const int blocks = (int)std::min<size_t>(4096, (n + 255) / 256);
+  diag_term_kernel<<<std::max(blocks, 1), 256, 0, st>>>(ns, nT, nvec, lw, x, y, E, finalize);
+  return cudaGetLastError() == cudaSuccess ? PHX_OK : PHX_ERR_CUDA;
+}
+
+int phx_smatrix_set_diag_launch(int ns, long long ld, const double* diag, double* A, cudaStream_t st) {
+  set_diag_kernel<<<(ns + 255) / 256, 256, 0, st>>>(ns, ld, diag, A);
+  return cudaGetLastError() == cudaSuccess ? PHX_OK : PHX_ERR_CUDA;
+}
+
+extern "C" int phx_smatrix_num_states(const phx_smatrix* m) { return m ? m->ns : 0; }
+
+extern "C" int phx_smatrix_diagonal(phx_smatrix* m, double* diag) {
+  PHX_ARG(nullptr, m && diag, "phx_smatrix_diagonal: bad arguments");
+  phx_ctx* ctx = m->ctx;
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  PHX_CUDA(ctx, cudaMemcpyAsync(diag, m->d_diag, sizeof(double) * m->ns, cudaMemcpyDeviceToHost, ctx->stream));
+  PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHX_OK;
+}
+
+extern "C" int phx_smatrix_get_rows(phx_smatrix* m, int row0, int nrows, double* out) {
+  PHX_ARG(nullptr, m && out, "phx_smatrix_get_rows: bad arguments");
+  phx_ctx* ctx = m->ctx;
+  PHX_ARG(ctx, row0 >= 0 && nrows >= 0 && row0 + nrows <= m->ns, "phx_smatrix_get_rows: rows out of range");
+  if (nrows == 0) return PHX_OK;
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t bytes = sizeof(double) * (size_t)nrows * m->ns;
+  PHX_TRY(phx_ctx_reserve(ctx, &ctx->d_out, &ctx->out_bytes, bytes));
+  double* d = static_cast<double*>(ctx->d_out);
+  dim3 grid((m->ns + 31) / 32, (nrows + 31) / 32);
+  rows_kernel<<<grid, dim3(32, 8), 0, ctx->stream>>>(m->ns, m->ns, m->d_A, row0, nrows, d);
+  PHX_CUDA(ctx, cudaGetLastError());
+  PHX_CUDA(ctx, cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHX_OK;
+}
+
+extern "C" int phx_smatrix_dot_d(phx_smatrix* m, int nvec, const double* x_d, int off_diagonal, double* y_d,
+                                 float* ms) {
+  PHX_ARG(nullptr, m && x_d && y_d && nvec >= 1, "phx_smatrix_dot: bad arguments");
+  phx_ctx* ctx = m->ctx;
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ms) {
+    PHX_CUDA(ctx, cudaEventCreate(&e0));
+    PHX_CUDA(ctx, cudaEventCreate(&e1));
+    PHX_CUDA(ctx, cudaEventRecord(e0, st));
+  }
+  PHX_CUDA(ctx, cudaMemsetAsync(y_d, 0, sizeof(double) * nvec * 3 * (size_t)m->ns, st));
+  phx_dot_args a{};
+  a.ns = m->ns;
+  a.ncols = m->ns;
+  a.ld = m->ns;
+  a.Sp = m->d_A;
+  a.Sm = nullptr;
+  a.tstride = 0;
+  a.slab = 0;
+  a.nb = m->nb;
+  a.nT = 1;
+  a.nvec = nvec;
+  a.x = x_d;
+  a.y = y_d;
+  a.skip = off_diagonal ? 0 : 1;
+  a.E = m->d_E;
+  int rc = phx_smatrix_dot_launch(a, st, nullptr);
+  if (rc != PHX_OK) {
+    phx_set_error(ctx, rc, "phx_smatrix_dot: launch failed");
+    return rc;
+  }
+  if (ms) {
+    PHX_CUDA(ctx, cudaEventRecord(e1, st));
+    PHX_CUDA(ctx, cudaEventSynchronize(e1));
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  return PHX_OK;
+}
+
+extern "C" int phx_smatrix_dot(phx_smatrix* m, int nvec, const double* x, int off_diagonal, double* y) {
+  PHX_ARG(nullptr, m && x && y && nvec >= 1, "phx_smatrix_dot: bad arguments");
+  phx_ctx* ctx = m->ctx;
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t n = (size_t)nvec * 3 * m->ns;
+  if (m->xy_bytes < 2 * n * sizeof(double)) {
+    cudaFree(m->d_xy);
+    m->d_xy = nullptr;
+    m->xy_bytes = 0;
+    PHX_CUDA(ctx, cudaMalloc(&m->d_xy, 2 * n * sizeof(double)));
+    m->xy_bytes = 2 * n * sizeof(double);
+  }
+  double* xd = m->d_xy;
+  double* yd = m->d_xy + n;
+  PHX_CUDA(ctx, cudaMemcpyAsync(xd, x, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  PHX_TRY(phx_smatrix_dot_d(m, nvec, xd, off_diagonal, yd, nullptr));
+  PHX_CUDA(ctx, cudaMemcpyAsync(y, yd, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHX_OK;
+}
+
+extern "C" int phx_smatrix_destroy(phx_smatrix* m) {
+  if (!m) return PHX_OK;
+  if (m->ctx) cudaSetDevice(m->ctx->device);
+  cudaFree(m->d_A);
+  cudaFree(m->d_E);
+  cudaFree(m->d_diag);
+  cudaFree(m->d_xy);
+  delete m;
+  return PHX_OK;
+}

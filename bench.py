@@ -45,9 +45,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="3ph", choices=["3ph", "elph"],
+    ap.add_argument("--workload", default="3ph", choices=["3ph", "elph", "smatrix"],
                     help="3ph: the headline linewidth builder; elph: electron-phonon linewidths "
-                         "(8 Wannier functions, 343 x 343 coupling vectors, 40^3 k, 20^3 q)")
+                         "(8 Wannier functions, 343 x 343 coupling vectors, 40^3 k, 20^3 q); smatrix: "
+                         "the scattering matrix of the 3ph workload stored in device memory and its "
+                         "matrix-vector products, beside the matrix-free product")
     ap.add_argument("--elph-k1", type=int, default=64, help="outer k points timed per elph step")
     ap.add_argument("--precision", default=os.environ.get("PHX_BENCH_PRECISION", "split_fp16"),
                     choices=["fp64", "split_bf16", "split_fp16"])
@@ -446,10 +448,74 @@ def run_elph(args):
     print(json.dumps(line), flush=True)
 
 
+def run_smatrix(args):
+    """Scattering-matrix modes on the 3ph workload at one temperature: the stored matrix (FP64,
+    ns x ns in device memory) is built once, then its matrix-vector product A x (3 components) is
+    timed; the matrix-free product (one builder pass) is timed beside it."""
+    import ctypes
+
+    import torch
+    from phoebe_b200 import _abi
+    from phoebe_b200 import constants as C
+    from phoebe_b200.core import Context, Interaction3Ph, PhononH0, PhScatteringMatrix
+    cr, fc2, fc3, mesh = workload(args.mesh)
+    torch.cuda.set_device(0)
+    ctx = Context(0)
+    h0 = PhononH0(ctx, cr, fc2)
+    bands = h0.populate(mesh, withVelocities=True)
+    v3 = Interaction3Ph(ctx, cr, fc3, precision="fp64")
+    T = [C.kelvin_to_ry(300.0)]
+    ns = bands.nq * bands.nb
+    sm = PhScatteringMatrix(v3, bands, T, "adaptive", in_memory=True)
+    sm.setup()
+    ms_build = sm.stats.ms_total
+    L = _abi.load()
+    x = torch.randn(1, 3, ns, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    ms = ctypes.c_float()
+    times = []
+    with Clocks(0) as clk:
+        for i in range(args.warmup + args.steps):
+            _abi.check(L.phx_smatrix_dot_d(sm._m, 1, ctypes.c_void_p(x.data_ptr()), 0,
+                                           ctypes.c_void_p(y.data_ptr()), ctypes.byref(ms)), ctx.h)
+            if i >= args.warmup:
+                times.append(ms.value)
+    ms_dot = float(np.mean(times))
+    # matrix-free product of the same x, one builder pass
+    free = PhScatteringMatrix(v3, bands, T, "adaptive")
+    yf = free.dot(x.cpu().numpy())
+    ms_free = free.stats.ms_total
+    err = float(np.abs(yf - y.cpu().numpy()).max() / np.abs(yf).max())
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    nbytes = 8.0 * ns * ns + 8.0 * 3 * ns * 2
+    achieved = nbytes / (ms_dot / 1000.0) / 1e9
+    line = {"metric": "stored scattering-matrix products A x per second (3 components), diamond 20^3, 48000 states",
+            "value": 1000.0 / ms_dot, "unit": "products/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_dot, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "diamond %dx%dx%d, 400 FC3 pairs, adaptive smearing, 300 K; matrix %d x %d "
+                                   "FP64 (%.1f GB) in device memory, larger than L2" % (*mesh, ns, ns,
+                                                                                         8e-9 * ns * ns)},
+            "matrix_build_ms": ms_build,
+            "matrix_free_product_ms": ms_free,
+            "stored_vs_matrix_free_speedup": ms_free / ms_dot,
+            "stored_vs_matrix_free_rel_err": err,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": None, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    sm.close()
+
+
 def main():
     args = parse()
     if args.workload == "elph":
         run_elph(args)
+        return
+    if args.workload == "smatrix":
+        run_smatrix(args)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -10,8 +10,10 @@
 //
 // Both are reads of FP64 matrix blocks once each, bound by HBM bandwidth: one
 // thread per row (coalesced down a column), a block of columns per CTA with
-// their x values staged in shared memory, 4 input vectors per pass, and one
-// atomic add per row and vector component at the end.
+// their x values staged in shared memory, and one atomic add per row and
+// vector component at the end.  One input vector (the iterative solvers'
+// case) has its own instantiation, whose 3 accumulators leave room for 8
+// loads in flight per thread; more vectors go 4 per pass.
 #include <algorithm>
 #include <cstring>
 
@@ -24,17 +26,18 @@ using pairc::mesh_neg;
 namespace {
 
 constexpr int kDotRows = 256;   // rows (threads) per CTA
-constexpr int kDotVec = 4;      // input vectors per pass
-constexpr int kDotV3 = 3 * kDotVec;
+constexpr int kDotVec = 4;      // input vectors per pass (several vectors)
 
+template <int NV>
 __global__ void __launch_bounds__(kDotRows) smatrix_dot_kernel(phx_dot_args A, int cols_per_block) {
+  constexpr int kDotV3 = 3 * NV;
   extern __shared__ __align__(16) double dsm[];
   double* xp = dsm;                                  // [cols][kDotV3]
   double* xm = xp + (size_t)cols_per_block * kDotV3; // [cols][kDotV3] (slabs)
   int* stp = reinterpret_cast<int*>(xm + (A.Sm ? (size_t)cols_per_block * kDotV3 : 0));
   int* stm = stp + cols_per_block;
-  const int c = blockIdx.z % A.nT, v0 = (blockIdx.z / A.nT) * kDotVec;
-  const int nv = min(kDotVec, A.nvec - v0);
+  const int c = blockIdx.z % A.nT, v0 = (blockIdx.z / A.nT) * NV;
+  const int nv = min(NV, A.nvec - v0);
   const int k0 = blockIdx.y * cols_per_block, kn = min(cols_per_block, A.ncols - k0);
   for (int t = threadIdx.x; t < cols_per_block; t += blockDim.x) {
     int sp = 0, sm = 0;
@@ -83,7 +86,7 @@ __global__ void __launch_bounds__(kDotRows) smatrix_dot_kernel(phx_dot_args A, i
       for (int vi = 0; vi < kDotV3; ++vi) acc[vi] += a * xp[t * kDotV3 + vi] - b * xm[t * kDotV3 + vi];
     }
   } else {
-#pragma unroll 4
+#pragma unroll 8
     for (int t = 0; t < kn; ++t) {
       double a = __ldcs(P + (size_t)t * A.ld);
       if (A.skip == 0 && r == stp[t]) a = 0.0;
@@ -134,16 +137,26 @@ __global__ void rows_kernel(int ns, long long ld, const double* __restrict__ A, 
 
 }  // namespace
 
-int phx_smatrix_dot_launch(const phx_dot_args& a, cudaStream_t st, int* launches) {
-  if (a.ncols <= 0 || a.ns <= 0 || a.nvec <= 0) return PHX_OK;
+namespace {
+
+template <int NV>
+int dot_launch(const phx_dot_args& a, cudaStream_t st) {
   // slabs: two blocks of columns per CTA; a stored matrix: one, longer
   const int cols = a.Sm ? 64 : 256;
-  const size_t smem = sizeof(double) * cols * kDotV3 * (a.Sm ? 2 : 1) + sizeof(int) * 2 * cols;
-  dim3 grid((a.ns + kDotRows - 1) / kDotRows, (a.ncols + cols - 1) / cols, a.nT * ((a.nvec + kDotVec - 1) / kDotVec));
-  if (smem > 48 * 1024) cudaFuncSetAttribute(smatrix_dot_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  smatrix_dot_kernel<<<grid, kDotRows, smem, st>>>(a, cols);
-  if (launches) ++*launches;
+  const size_t smem = sizeof(double) * cols * 3 * NV * (a.Sm ? 2 : 1) + sizeof(int) * 2 * cols;
+  dim3 grid((a.ns + kDotRows - 1) / kDotRows, (a.ncols + cols - 1) / cols, a.nT * ((a.nvec + NV - 1) / NV));
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(smatrix_dot_kernel<NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  smatrix_dot_kernel<NV><<<grid, kDotRows, smem, st>>>(a, cols);
   return cudaGetLastError() == cudaSuccess ? PHX_OK : PHX_ERR_CUDA;
+}
+
+}  // namespace
+
+int phx_smatrix_dot_launch(const phx_dot_args& a, cudaStream_t st, int* launches) {
+  if (a.ncols <= 0 || a.ns <= 0 || a.nvec <= 0) return PHX_OK;
+  if (launches) ++*launches;
+  return a.nvec == 1 ? dot_launch<1>(a, st) : dot_launch<kDotVec>(a, st);
 }
 
 int phx_smatrix_diag_term_launch(int ns, int nT, int nvec, const double* lw, const double* x, double* y,

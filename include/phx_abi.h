@@ -215,6 +215,9 @@ int phx_smatrix_get_rows(phx_smatrix* m, int row0, int nrows, double* out);
 int phx_smatrix_dot(phx_smatrix* m, int nvec, const double* x, int off_diagonal, double* y);
 /* Same with device vectors; ms (may be NULL): device time of the product. */
 int phx_smatrix_dot_d(phx_smatrix* m, int nvec, const double* x_d, int off_diagonal, double* y_d, float* ms);
+/* A -> (A + A^T) / 2 in place (ScatteringMatrix::symmetrize, src/bte/scattering.cpp:1149-1166;
+ * the reference's symmetrizeMatrix option before its exact solvers). */
+int phx_smatrix_symmetrize(phx_smatrix* m);
 int phx_smatrix_destroy(phx_smatrix* m);
 
 /* PhScatteringMatrix::builder with switchCase 1 (ScatteringMatrix::dot when the

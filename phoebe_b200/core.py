@@ -431,6 +431,12 @@ class PhScatteringMatrix:
         check(_abi.load().phx_smatrix_get_rows(self._m, int(row0), int(nrows), dptr(out)), self.v3.ctx.h)
         return out
 
+    def symmetrize(self):
+        """A -> (A + A^T) / 2 for the stored matrix (ScatteringMatrix::symmetrize)."""
+        if self._m is None:
+            raise RuntimeError("the matrix is stored only with in_memory=True, after setup()")
+        check(_abi.load().phx_smatrix_symmetrize(self._m), self.v3.ctx.h)
+
     def close(self):
         if getattr(self, "_m", None) is not None:
             _abi.load().phx_smatrix_destroy(self._m)

@@ -151,7 +151,46 @@ int dot_launch(const phx_dot_args& a, cudaStream_t st) {
   return cudaGetLastError() == cudaSuccess ? PHX_OK : PHX_ERR_CUDA;
 }
 
+// (A + A^T) / 2 in place (SerialMatrix::symmetrize, src/algebra/SMatrix.cpp:124-138):
+// the CTA of tile pair (ti, tj), ti <= tj, stages both 32 x 32 tiles in shared memory
+__global__ void symmetrize_kernel(int ns, long long ld, double* __restrict__ A) {
+  const int ti = blockIdx.y, tj = blockIdx.x;
+  if (ti > tj) return;
+  __shared__ double a[32][33], b[32][33];
+  const int r0 = ti * 32, c0 = tj * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int r = r0 + threadIdx.x, c = c0 + k;        // a[k][x] = A(r0 + x, c0 + k)
+    a[k][threadIdx.x] = (r < ns && c < ns) ? A[(size_t)c * ld + r] : 0.0;
+    const int r2 = c0 + threadIdx.x, c2 = r0 + k;      // b[k][x] = A(c0 + x, r0 + k)
+    b[k][threadIdx.x] = (r2 < ns && c2 < ns) ? A[(size_t)c2 * ld + r2] : 0.0;
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    // A(r0 + x, c0 + k) and A(c0 + k, r0 + x) both become their mean
+    const double m = 0.5 * (a[k][threadIdx.x] + b[threadIdx.x][k]);
+    const int r = r0 + threadIdx.x, c = c0 + k;
+    if (r < ns && c < ns) A[(size_t)c * ld + r] = m;
+  }
+  if (ti == tj) return;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const double m = 0.5 * (b[k][threadIdx.x] + a[threadIdx.x][k]);
+    const int r2 = c0 + threadIdx.x, c2 = r0 + k;
+    if (r2 < ns && c2 < ns) A[(size_t)c2 * ld + r2] = m;
+  }
+}
+
 }  // namespace
+
+extern "C" int phx_smatrix_symmetrize(phx_smatrix* m) {
+  PHX_ARG(nullptr, m, "phx_smatrix_symmetrize: null handle");
+  phx_ctx* ctx = m->ctx;
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int t = (m->ns + 31) / 32;
+  symmetrize_kernel<<<dim3(t, t), dim3(32, 8), 0, ctx->stream>>>(m->ns, m->ns, m->d_A);
+  PHX_CUDA(ctx, cudaGetLastError());
+  PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHX_OK;
+}
 
 int phx_smatrix_dot_launch(const phx_dot_args& a, cudaStream_t st, int* launches) {
   if (a.ncols <= 0 || a.ns <= 0 || a.nvec <= 0) return PHX_OK;

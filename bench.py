@@ -33,10 +33,12 @@ TEMPS_K = (100.0, 300.0, 600.0)
 # FP32 FFMA throughput of a B200 (packed and scalar FFMA stream, all SMs, CUDA
 # events), the denominator of the pair kernel's CUDA-core view
 FFMA_PEAK_TFLOPS = 72.0
-# ncu DRAM bytes (read + write) of one pair-kernel launch, per (mesh, q2 per
-# launch, slots) of the launch plan; None where not captured
-PAIR_TRAFFIC_BYTES = {(20, 448, 7): 87476992 + 5594112, (20, 1792, 28): 337188096 + 29478400,
-                      (16, 448, 7): 85.2e6}
+# ncu DRAM bytes (read + write) of one pair-kernel launch, per (precision,
+# mesh, q2 per launch, slots) of the launch plan; None where not captured
+PAIR_TRAFFIC_BYTES = {("split_bf16", 20, 448, 7): 87476992 + 5594112,
+                      ("split_bf16", 20, 1792, 28): 337188096 + 29478400,
+                      ("split_fp16", 20, 1792, 28): 338063872 + 30249472,
+                      ("split_bf16", 16, 448, 7): 85.2e6}
 
 
 def parse():
@@ -318,7 +320,7 @@ def run_ours(args):
         # dram__bytes_write.sum of one launch of the plan in use
         roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
                 "frac": achieved / pk,
-                "traffic": PAIR_TRAFFIC_BYTES.get((args.mesh, plan["q2_chunk"], plan["slots"])),
+                "traffic": PAIR_TRAFFIC_BYTES.get((args.precision, args.mesh, plan["q2_chunk"], plan["slots"])),
                 "peak_source": "measured (sustained)",
                 "simt_view": {"what": "FP32 epilogue (e1, e3 contractions of all 216 triplets) "
                                       "against the measured FFMA rate",

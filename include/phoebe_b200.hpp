@@ -335,24 +335,76 @@ class PhScatteringMatrix {
   void setIsotopeCoupling(std::vector<double> massVariance) { iso_ = std::move(massVariance); }
   // boundary scattering |v|/L n(n+1); L <= 0 disables it (Bohr)
   void setBoundaryLength(double L) { boundary_ = L; }
+  // the reference's scatteringMatrixInMemory: setup() builds the whole matrix
+  // (one temperature) into device memory, dot() multiplies with it
+  void setMatrixInMemory(bool inMemory) { inMemory_ = inMemory; }
 
   // internalDiagonal A_out (nT, nq*nb) = linewidth * n(n+1); [q2Begin, q2End)
   // restricts the outer loop (one rank's share), finalize = false leaves the
   // degeneracy averaging and exclusions to the caller after summing shares.
+  // In memory: the matrix too, whose diagonal (not degeneracy-averaged) is
+  // then the internalDiagonal.
   void setup(int q2Begin = 0, int q2End = -1, bool finalize = true) {
-    phx_lw_params p{};
-    p.num_temperatures = (int)T_.size();
-    p.temperatures = T_.data();
-    p.smearing = (int)smearing_;
-    p.sigma = sigma_;
-    p.finalize = finalize ? 1 : 0;
-    p.q2_begin = q2Begin;
-    p.q2_end = q2End < 0 ? bands_.getNumPoints() : q2End;
-    p.isotope_coupling = iso_.empty() ? nullptr : iso_.data();
-    p.boundary_length = boundary_;
-    internalDiagonal_.assign(T_.size() * (size_t)bands_.getNumPoints() * bands_.getNumBands(), 0.0);
+    const phx_lw_params p = params(q2Begin, q2End, finalize);
+    internalDiagonal_.assign(T_.size() * numStates(), 0.0);
+    if (inMemory_) {
+      phx_smatrix* m = nullptr;
+      check(phx_ph_smatrix_create(v3_.get(), bands_.get(), &p, &m, &stats_), v3_.context());
+      matrix_ = detail::Handle<phx_smatrix, phx_smatrix_destroy>(m);
+      check(phx_smatrix_diagonal(matrix_.get(), internalDiagonal_.data()), v3_.context());
+      return;
+    }
     check(phx_ph_linewidths(v3_.get(), bands_.get(), &p, internalDiagonal_.data(), &stats_), v3_.context());
   }
+
+  // ScatteringMatrix::dot: A x for nvec vectors x (nvec, nT, 3, numStates);
+  // in memory a product with the stored matrix, otherwise one builder pass
+  std::vector<double> dot(const std::vector<double>& x, int nvec = 1) {
+    std::vector<double> y(x.size(), 0.0);
+    if (x.size() != (size_t)nvec * T_.size() * 3 * numStates()) throw Error(PHX_ERR_ARG, "dot: bad vector size");
+    if (inMemory_) {
+      if (!matrix_.get()) throw Error(PHX_ERR_STATE, "dot: setup() first");
+      check(phx_smatrix_dot(matrix_.get(), nvec, x.data(), 0, y.data()), v3_.context());
+    } else {
+      const phx_lw_params p = params(0, -1, true);
+      check(phx_ph_smatrix_dot(v3_.get(), bands_.get(), &p, nvec, x.data(), y.data(), &stats_), v3_.context());
+    }
+    return y;
+  }
+  // ScatteringMatrix::offDiagonalDot; without a stored matrix, as the
+  // reference, dot(x) - internalDiagonal * x
+  std::vector<double> offDiagonalDot(const std::vector<double>& x, int nvec = 1) {
+    if (inMemory_) {
+      if (!matrix_.get()) throw Error(PHX_ERR_STATE, "offDiagonalDot: setup() first");
+      std::vector<double> y(x.size(), 0.0);
+      if (x.size() != (size_t)nvec * 3 * numStates()) throw Error(PHX_ERR_ARG, "offDiagonalDot: bad vector size");
+      check(phx_smatrix_dot(matrix_.get(), nvec, x.data(), 1, y.data()), v3_.context());
+      return y;
+    }
+    std::vector<double> y = dot(x, nvec);
+    const size_t ns = numStates();
+    for (size_t v = 0; v < (size_t)nvec; ++v)
+      for (size_t t = 0; t < T_.size(); ++t)
+        for (size_t i = 0; i < 3; ++i)
+          for (size_t s = 0; s < ns; ++s) {
+            const size_t o = ((v * T_.size() + t) * 3 + i) * ns + s;
+            y[o] -= internalDiagonal_[t * ns + s] * x[o];
+          }
+    return y;
+  }
+  // rows row0 .. row0+nrows-1 of the stored matrix, row-major (nrows, numStates)
+  std::vector<double> getRows(int row0, int nrows) const {
+    if (!matrix_.get()) throw Error(PHX_ERR_STATE, "getRows: no stored matrix");
+    std::vector<double> out((size_t)nrows * numStates());
+    check(phx_smatrix_get_rows(matrix_.get(), row0, nrows, out.data()), v3_.context());
+    return out;
+  }
+  // A -> (A + A^T) / 2 (ScatteringMatrix::symmetrize)
+  void symmetrize() {
+    if (!matrix_.get()) throw Error(PHX_ERR_STATE, "symmetrize: no stored matrix");
+    check(phx_smatrix_symmetrize(matrix_.get()), v3_.context());
+  }
+  size_t numStates() const { return (size_t)bands_.getNumPoints() * bands_.getNumBands(); }
   const std::vector<double>& internalDiagonal() const { return internalDiagonal_; }
   const phx_lw_stats& stats() const { return stats_; }
 
@@ -369,6 +421,19 @@ class PhScatteringMatrix {
   }
 
  private:
+  phx_lw_params params(int q2Begin, int q2End, bool finalize) const {
+    phx_lw_params p{};
+    p.num_temperatures = (int)T_.size();
+    p.temperatures = T_.data();
+    p.smearing = (int)smearing_;
+    p.sigma = sigma_;
+    p.finalize = finalize ? 1 : 0;
+    p.q2_begin = q2Begin;
+    p.q2_end = q2End < 0 ? bands_.getNumPoints() : q2End;
+    p.isotope_coupling = iso_.empty() ? nullptr : iso_.data();
+    p.boundary_length = boundary_;
+    return p;
+  }
   std::vector<double> divide(bool invert) const {
     const auto E = bands_.getEnergies();
     const size_t ns = E.size();
@@ -390,6 +455,8 @@ class PhScatteringMatrix {
   std::vector<double> internalDiagonal_;
   std::vector<double> iso_;
   double boundary_ = 0.0;
+  bool inMemory_ = false;
+  detail::Handle<phx_smatrix, phx_smatrix_destroy> matrix_;
   phx_lw_stats stats_{};
 };
 

@@ -121,6 +121,24 @@ int main(int argc, char** argv) {
     save("kappa.f64", kappa[0].data(), kappa.size() * 9);
     (void)nT;
 
+    // ---- scattering matrix: stored (first temperature) and matrix-free ------
+    {
+      const auto x = load<double>("smatrix_x.f64");   // (nT, 3, ns)
+      const size_t ns = sm.numStates();
+      std::vector<double> x0(x.begin(), x.begin() + 3 * ns);
+      phx::PhScatteringMatrix mem(v3, bands, {temps[0]}, phx::Smearing::adaptive);
+      mem.setMatrixInMemory(true);
+      mem.setup();
+      save("smatrix_diag.f64", mem.internalDiagonal());
+      save("smatrix_rows.f64", mem.getRows(3, 5));
+      save("smatrix_dot.f64", mem.dot(x0));
+      save("smatrix_offdot.f64", mem.offDiagonalDot(x0));
+      mem.symmetrize();
+      save("smatrix_sym_rows.f64", mem.getRows(3, 5));
+      phx::PhScatteringMatrix freeSm(v3, bands, temps, phx::Smearing::adaptive);
+      save("smatrix_free_dot.f64", freeSm.dot(x));
+    }
+
     // ---- el-ph Wannier path -----------------------------------------------
     const auto edims = load<int>("el_dims.i32");  // nw, nph, kmesh(3), qmesh(3), nk1, nk2
     const int nw = edims[0], nph = edims[1];

@@ -3,8 +3,8 @@ method names, driven by tests/cpp/shim_driver.cpp.
 
 CPU: the header compiles with -Wall -Wextra and the driver links against
 libphx.so (every ABI symbol it uses resolves).  GPU: the driver runs the
-harmonic, 3-phonon, builder, conductivity and el-ph paths through the C++
-classes, and its outputs equal those of the Python mirror (phoebe_b200.core)
+harmonic, 3-phonon, builder (linewidths, stored matrix, matrix-free
+product), conductivity and el-ph paths through the C++ classes, and its outputs equal those of the Python mirror (phoebe_b200.core)
 on the same inputs -- both sit on the same C ABI, whose numerics the other GPU
 tests pin to the oracle -- and a bad argument surfaces as phx::Error with
 PHX_ERR_ARG."""
@@ -123,6 +123,9 @@ def test_shim_matches_python_mirror(ctx, diamond, tmp_path):
     _w(inp, "el_params.f64", [mu, window, T_el], np.float64)
     _w(inp, "el_k1_list.i32", k1_list, np.int32)
 
+    ns_mesh = int(np.prod(mesh)) * nb
+    xs = rng.normal(size=(len(temps), 3, ns_mesh))
+    _w(inp, "smatrix_x.f64", xs, np.float64)
     r = subprocess.run([exe, inp, out], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
 
@@ -158,6 +161,23 @@ def test_shim_matches_python_mirror(ctx, diamond, tmp_path):
     np.testing.assert_allclose(_r(out, "linewidths.f64", np.float64)[ok], lw[ok], rtol=1e-12)
     np.testing.assert_allclose(_r(out, "times.f64", np.float64)[ok], tau[ok], rtol=1e-12)
     kappa = sm.thermalConductivity(lattice.calc_volume(cr.direct_cell))
+    mem = PhScatteringMatrix(v3, bands, temps[:1], "adaptive", in_memory=True)
+    dmem = mem.setup()
+    np.testing.assert_array_equal(_r(out, "smatrix_diag.f64", np.float64), dmem.ravel())
+    np.testing.assert_array_equal(_r(out, "smatrix_rows.f64", np.float64), mem.getMatrixRows(3, 5).ravel())
+    # FP64 atomics: summation order of the products
+    yd = mem.dot(xs[None, :1])[0]
+    np.testing.assert_allclose(_r(out, "smatrix_dot.f64", np.float64), yd.ravel(), rtol=1e-12,
+                               atol=1e-14 * np.abs(yd).max())
+    yo = mem.offDiagonalDot(xs[None, :1])[0]
+    np.testing.assert_allclose(_r(out, "smatrix_offdot.f64", np.float64), yo.ravel(), rtol=1e-12,
+                               atol=1e-14 * np.abs(yo).max())
+    mem.symmetrize()
+    np.testing.assert_array_equal(_r(out, "smatrix_sym_rows.f64", np.float64), mem.getMatrixRows(3, 5).ravel())
+    mem.close()
+    yf = PhScatteringMatrix(v3, bands, temps, "adaptive").dot(xs)
+    np.testing.assert_allclose(_r(out, "smatrix_free_dot.f64", np.float64), yf.ravel(), rtol=1e-12,
+                               atol=1e-14 * np.abs(yf).max())
     np.testing.assert_allclose(_r(out, "kappa.f64", np.float64) * C.thConductivityAuToSi, kappa.ravel(),
                                rtol=1e-10, atol=1e-12 * np.abs(kappa).max())
 

@@ -448,6 +448,16 @@ class PhScatteringMatrix:
         except Exception:
             pass
 
+    def outputToJSON(self, path, crystal):
+        """rta_ph_relaxation_times.json (ScatteringMatrix::outputToJSON, scattering.cpp:639-815)
+        from the internalDiagonal of setup()."""
+        from . import output
+        if self.internalDiagonal is None:
+            raise RuntimeError("setup() first")
+        E, _, vg = self.bands.get()
+        return output.relaxation_times_json(path, crystal, self.bands.mesh, E, vg, self.internalDiagonal,
+                                            self.temperatures)
+
     def getLinewidths(self, E):
         """Gamma = A_out / (n(n+1)) (scattering.cpp:529-568)."""
         T = self.temperatures[:, None]

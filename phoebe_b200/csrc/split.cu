@@ -65,6 +65,9 @@ constexpr int kChBand = 18;
 constexpr int kChGp = 36;
 constexpr int kU2Chunks = kRecChunks - kChBand;   // band blocks + blocks word
 constexpr int kQueue = 64;                        // live-triplet queue entries per warp
+// FP32 rate accumulators of a quarter: one row of 6 b1 x kMaxT per q1, padded
+// to an odd stride so that the rows of a warp fall in distinct banks
+constexpr int kAccRow = 6 * kMaxT + 1;
 
 struct TcArgs {
   MeshArgs m;
@@ -451,7 +454,7 @@ struct Smem {
   uint4* u2;           // [4 quarters][2: q2, -q2][kU2Chunks]
   unsigned long long* need;  // [6 b2][128] bit b1*6+b3
   uint2* queue;        // [12 warps][kQueue] live triplets awaiting their rates
-  float* acc;          // [4 quarters][32 rows][6 b1][kMaxT] rates of the current q2
+  float* acc;          // [4 quarters][32 rows][kAccRow: 6 b1 x kMaxT + pad] rates of the current q2
   uint64_t* bars;
 };
 
@@ -470,7 +473,7 @@ __host__ __device__ inline size_t smem_layout(int Kp, size_t* off) {
   off[7] = o; o += align16(4 * 2 * kU2Chunks * 16);            // q2 bands
   off[8] = o; o += align16(6 * kM * sizeof(unsigned long long));  // masks
   off[9] = o; o += align16(kEpiWarps * kQueue * sizeof(uint2));   // queues
-  off[10] = o; o += align16(4 * 32 * 6 * kMaxT * sizeof(float));  // q2 accumulators
+  off[10] = o; o += align16(4 * 32 * kAccRow * sizeof(float));  // q2 accumulators
   off[11] = o; o += align16(32 * sizeof(uint64_t));            // barriers, tmem slot, flag
   return o;
 }
@@ -549,7 +552,7 @@ __device__ __forceinline__ void rate_entry(uint2 e, int qd, const double* En1, c
   }
   const float scale = wn / (float)(__popc(bm2) * __popc(bm3));
 #pragma unroll
-  for (int t = 0; t < NT; ++t) atomicAdd(&qacc[(r * 6 + b1) * kMaxT + t], scale * g[t]);
+  for (int t = 0; t < NT; ++t) atomicAdd(&qacc[r * kAccRow + b1 * kMaxT + t], scale * g[t]);
 }
 
 template <int NT>
@@ -721,11 +724,11 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
     uint4* u2 = S.u2 + qd * 2 * kU2Chunks;
     const uint4* srow = S.rec + m;
     uint2* queue = S.queue + warp * kQueue;
-    float* qacc = S.acc + qd * 32 * 6 * kMaxT;
+    float* qacc = S.acc + qd * 32 * kAccRow;
 #pragma unroll
     for (int t = 0; t < kMaxT; ++t) {
-      qacc[(lane * 6 + k) * kMaxT + t] = 0.f;
-      qacc[(lane * 6 + k + 3) * kMaxT + t] = 0.f;
+      qacc[lane * kAccRow + k * kMaxT + t] = 0.f;
+      qacc[lane * kAccRow + (k + 3) * kMaxT + t] = 0.f;
     }
     int qn = 0;  // queued live triplets (warp-uniform)
     const unsigned lanemask_lt = (1u << lane) - 1u;
@@ -734,10 +737,10 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
     auto flush = [&]() {
 #pragma unroll
       for (int t = 0; t < NT; ++t) {
-        acc0[t] += (double)qacc[(lane * 6 + k) * kMaxT + t];
-        acc1[t] += (double)qacc[(lane * 6 + k + 3) * kMaxT + t];
-        qacc[(lane * 6 + k) * kMaxT + t] = 0.f;
-        qacc[(lane * 6 + k + 3) * kMaxT + t] = 0.f;
+        acc0[t] += (double)qacc[lane * kAccRow + k * kMaxT + t];
+        acc1[t] += (double)qacc[lane * kAccRow + (k + 3) * kMaxT + t];
+        qacc[lane * kAccRow + k * kMaxT + t] = 0.f;
+        qacc[lane * kAccRow + (k + 3) * kMaxT + t] = 0.f;
       }
     };
     bool failed = false;

@@ -576,10 +576,13 @@ struct Q2Window {
   const double* cut;      // (nq): q2 is paired with q1 iff energy[q2] <= cut[q1]
 };
 
-__host__ __device__ inline size_t generic_smem_bytes(int nb, int nr3) {
+// Shared memory of pair_generic_kernel<Q1>: per q1 of the tile its phases,
+// e1, e3, the b2 slices of T and X, and the coupling W of all (b1, b2, b3).
+__host__ __device__ inline size_t generic_smem_bytes(int nb, int nr3, int q1s) {
   const size_t nbb = (size_t)nb * nb, nb3 = nbb * nb;
-  return sizeof(double2) * ((size_t)nr3 + 2 * nbb + 2 * nb3) + sizeof(double) * ((size_t)nb * kMaxT + 3 * nb) +
-         sizeof(int) * 3 * nb;
+  return (size_t)q1s * (sizeof(double2) * ((size_t)nr3 + 4 * nbb) + sizeof(double) * (nb3 + (size_t)nb * kMaxT + 2 * nb) +
+                        sizeof(int) * (2 * nb + 4)) +
+         sizeof(double) * 2 * nb + sizeof(int) * nb;
 }
 
 // forward-scan degenerate blocks (scattering.cpp:1223,1257,1291): gs[b] = start of b's block
@@ -591,86 +594,135 @@ __device__ inline void scan_blocks(const double* e, int nb, int* gs) {
   }
 }
 
-__global__ void __launch_bounds__(kGenThreads) pair_generic_kernel(PairArgs P, Q2Window win) {
+// Q1 q1 points per block (q1_order[blockIdx.x * Q1 + i]): each element of
+// the q2 slab of the cached vertex is read once per block and used for all Q1
+// (Q1 independent accumulators per thread), one b2 slice at a time:
+//   T(a,c) = sum_r3 e^{-i q1.R3} Dp(q2)[r3][a][b2][c]
+//   X(b1,c) = sum_a e1(a,b1) T(a,c)
+//   W(b1,b2,b3) = |sum_c X(b1,c) conj(e3(c,b3))|^2
+// then the three symmetrisation passes and the rates of each q1 of the tile.
+// With a window, a q2 outside the windows of every q1 of the tile is skipped
+// (the host orders q1 by window so that tiles hold similar windows).
+template <int Q1>
+__global__ void __launch_bounds__(kGenThreads) pair_generic_kernel(PairArgs P, Q2Window win, const int* q1_order) {
   const MeshArgs& M = P.m;
   extern __shared__ __align__(16) char sraw[];
   const int nb = M.nb, nbb = nb * nb, nb3 = nbb * nb, nr3 = P.nr3, nT = M.nT, nq = M.nq;
-  double2* ph = reinterpret_cast<double2*>(sraw);   // [nr3]
-  double2* e1 = ph + nr3;                           // [nb][nb]
-  double2* e3 = e1 + nbb;                           // [nb][nb]
-  double2* T = e3 + nbb;                            // [nb^3]: T(a,b2,c), then W(b1,b2,b3) as doubles
-  double2* X = T + nb3;                             // [nb^3]: X(b1,b2,c)
-  double* W = reinterpret_cast<double*>(T);
-  double* acc = reinterpret_cast<double*>(X + nb3); // [nb][kMaxT]
-  double* E1 = acc + nb * kMaxT;
-  double* E2 = E1 + nb;
-  double* E3 = E2 + nb;
-  int* g1s = reinterpret_cast<int*>(E3 + nb);
-  int* g2s = g1s + nb;
-  int* g3s = g2s + nb;
+  double2* ph = reinterpret_cast<double2*>(sraw);   // [Q1][nr3]
+  double2* e1 = ph + Q1 * nr3;                      // [Q1][nb][nb]
+  double2* e3 = e1 + Q1 * nbb;                      // [Q1][nb][nb]
+  double2* Tb = e3 + Q1 * nbb;                      // [Q1][a][c] of the current b2
+  double2* Xb = Tb + Q1 * nbb;                      // [Q1][b1][c] of the current b2
+  double* W = reinterpret_cast<double*>(Xb + Q1 * nbb);   // [Q1][b1][b2][b3]
+  double* acc = W + Q1 * nb3;                       // [Q1][nb][kMaxT]
+  double* E1 = acc + Q1 * nb * kMaxT;               // [Q1][nb]
+  double* E3 = E1 + Q1 * nb;                        // [Q1][nb]
+  double* E2 = E3 + Q1 * nb;                        // [nb]
+  double* E2m = E2 + nb;                            // [nb]
+  int* g1s = reinterpret_cast<int*>(E2m + nb);      // [Q1][nb]
+  int* g3s = g1s + Q1 * nb;                         // [Q1][nb]
+  int* g2s = g3s + Q1 * nb;                         // [nb]
+  int* q1s = g2s + nb;                              // [Q1] q1 of each slot of the tile, -1: none
+  int* q3s = q1s + Q1;                              // [Q1]
+  int* inw = q3s + Q1;                              // [Q1] bit 0: q2 in the window, bit 1: -q2
   const int tid = threadIdx.x, NT = blockDim.x;
-  const int q1 = blockIdx.x;
   const int n0 = M.n0, n1 = M.n1, n2 = M.n2;
-  for (int r = tid; r < nr3; r += NT) {
+  if (tid < Q1) {
+    const int i = blockIdx.x * Q1 + tid;
+    q1s[tid] = i < nq ? (q1_order ? q1_order[i] : i) : -1;
+  }
+  __syncthreads();
+  for (int e = tid; e < Q1 * nr3; e += NT) {
+    const int t = e / nr3, r = e % nr3;
+    const int q1 = max(q1s[t], 0);
     const double* q = M.qcart + 3 * q1;
     double sn, cs;
     sincos(-(q[0] * P.R3[3 * r] + q[1] * P.R3[3 * r + 1] + q[2] * P.R3[3 * r + 2]), &sn, &cs);
-    ph[r] = cmk(cs, sn);
+    ph[e] = cmk(cs, sn);
   }
-  for (int e = tid; e < nbb; e += NT) e1[e] = M.U[(size_t)q1 * nbb + e];
-  for (int i = tid; i < nb * kMaxT; i += NT) acc[i] = 0.0;
-  for (int b = tid; b < nb; b += NT) E1[b] = M.E[(size_t)q1 * nb + b];
+  for (int e = tid; e < Q1 * nbb; e += NT) e1[e] = M.U[(size_t)max(q1s[e / nbb], 0) * nbb + e % nbb];
+  for (int i = tid; i < Q1 * nb * kMaxT; i += NT) acc[i] = 0.0;
+  for (int e = tid; e < Q1 * nb; e += NT) E1[e] = M.E[(size_t)max(q1s[e / nb], 0) * nb + e % nb];
   __syncthreads();
-  if (tid == 0) scan_blocks(E1, nb, g1s);
+  if (tid < Q1) scan_blocks(E1 + tid * nb, nb, g1s + tid * nb);
   const int jbeg = blockIdx.y * P.q2_per_slot;
   const int jend = min(P.q2_count, jbeg + P.q2_per_slot);
   for (int j = jbeg; j < jend; ++j) {
     const int iq2 = P.q2_first + j;
     const int iq2m = mesh_neg(iq2, n0, n1, n2);
-    const int iq3 = mesh_add(q1, iq2, n0, n1, n2);
-    const bool inP = !win.energy || win.energy[iq2] <= win.cut[q1];
-    const bool inM = !win.energy || win.energy[iq2m] <= win.cut[q1];
-    if (!inP && !inM) continue;   // uniform over the block
-    for (int e = tid; e < nbb; e += NT) e3[e] = M.U[(size_t)iq3 * nbb + e];
+    __syncthreads();   // the previous q2's rates are done with this q2's shared buffers
+    if (tid < Q1) {
+      const int q1 = q1s[tid];
+      int f = 0;
+      if (q1 >= 0) {
+        f |= (!win.energy || win.energy[iq2] <= win.cut[q1]) ? 1 : 0;
+        f |= (!win.energy || win.energy[iq2m] <= win.cut[q1]) ? 2 : 0;
+      }
+      inw[tid] = f;
+      q3s[tid] = mesh_add(max(q1, 0), iq2, n0, n1, n2);
+    }
+    __syncthreads();
+    int any = 0;
+#pragma unroll
+    for (int t = 0; t < Q1; ++t) any |= inw[t];
+    if (!any) continue;   // uniform over the block
+    for (int e = tid; e < Q1 * nbb; e += NT) e3[e] = M.U[(size_t)q3s[e / nbb] * nbb + e % nbb];
+    for (int e = tid; e < Q1 * nb; e += NT) E3[e] = M.E[(size_t)q3s[e / nb] * nb + e % nb];
     for (int b = tid; b < nb; b += NT) {
       E2[b] = M.E[(size_t)iq2 * nb + b];
-      E3[b] = M.E[(size_t)iq3 * nb + b];
+      E2m[b] = M.E[(size_t)iq2m * nb + b];
     }
-    // T(a,b2,c) = sum_r3 e^{-i q1.R3} Dp(q2)[r3][a][b2][c]
+    __syncthreads();
+    if (tid < Q1) scan_blocks(E3 + tid * nb, nb, g3s + tid * nb);
+    if (tid == Q1) scan_blocks(E2, nb, g2s);
     const double2* D = P.Dp + (size_t)j * nr3 * nb3;
-    for (int x = tid; x < nb3; x += NT) {
-      double2 t = cmk(0.0, 0.0);
-      for (int r = 0; r < nr3; ++r) cfma(t, ph[r], __ldg(D + (size_t)r * nb3 + x));
-      T[x] = t;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      scan_blocks(E2, nb, g2s);
-      scan_blocks(E3, nb, g3s);
-    }
-    // X(b1,b2,c) = sum_a e1(a,b1) T(a,b2,c)
-    for (int x = tid; x < nb3; x += NT) {
-      const int b1 = x / nbb, rest = x % nbb;
-      double2 v = cmk(0.0, 0.0);
-      for (int a = 0; a < nb; ++a) cfma(v, e1[a * nb + b1], T[a * nbb + rest]);
-      X[x] = v;
-    }
-    __syncthreads();
-    // W(b1,b2,b3) = |sum_c X(b1,b2,c) conj(e3(c,b3))|^2
-    for (int x = tid; x < nb3; x += NT) {
-      const int row = x / nb, b3 = x % nb;
-      double2 v = cmk(0.0, 0.0);
-      for (int c = 0; c < nb; ++c) cfmac(v, X[row * nb + c], e3[c * nb + b3]);
-      W[x] = v.x * v.x + v.y * v.y;
+    for (int b2 = 0; b2 < nb; ++b2) {
+      // T(a,c) of every q1 of the tile: one read of Dp per element
+      for (int x = tid; x < nbb; x += NT) {
+        const int a = x / nb, c = x % nb;
+        const double2* Dx = D + ((size_t)a * nb + b2) * nb + c;
+        double2 t[Q1];
+#pragma unroll
+        for (int q = 0; q < Q1; ++q) t[q] = cmk(0.0, 0.0);
+#pragma unroll 4
+        for (int r = 0; r < nr3; ++r) {
+          const double2 d = __ldg(Dx + (size_t)r * nb3);
+#pragma unroll
+          for (int q = 0; q < Q1; ++q) cfma(t[q], ph[q * nr3 + r], d);
+        }
+#pragma unroll
+        for (int q = 0; q < Q1; ++q) Tb[q * nbb + x] = t[q];
+      }
+      __syncthreads();
+      for (int y = tid; y < Q1 * nbb; y += NT) {
+        const int q = y / nbb, x = y % nbb, b1 = x / nb, c = x % nb;
+        const double2* eq = e1 + q * nbb;
+        const double2* tq = Tb + q * nbb;
+        double2 v = cmk(0.0, 0.0);
+        for (int a = 0; a < nb; ++a) cfma(v, eq[a * nb + b1], tq[a * nb + c]);
+        Xb[y] = v;
+      }
+      __syncthreads();
+      for (int y = tid; y < Q1 * nbb; y += NT) {
+        const int q = y / nbb, x = y % nbb, b1 = x / nb, b3 = x % nb;
+        const double2* xq = Xb + q * nbb + b1 * nb;
+        const double2* eq = e3 + q * nbb;
+        double2 v = cmk(0.0, 0.0);
+        for (int c = 0; c < nb; ++c) cfmac(v, xq[c], eq[c * nb + b3]);
+        W[(size_t)q * nb3 + ((size_t)b1 * nb + b2) * nb + b3] = v.x * v.x + v.y * v.y;
+      }
+      // the next b2 writes Tb, which nothing reads now; Xb is rewritten after its T barrier
     }
     __syncthreads();
     // symmetrizeCoupling (scattering.cpp:1209-1318): average over the blocks of
     // b3, then b1, then b2 (projections on different indices commute)
-    for (int x = tid; x < nbb; x += NT) {
-      double* w = W + (size_t)x * nb;   // (b1,b2) row over b3
+    for (int y = tid; y < Q1 * nbb; y += NT) {
+      const int q = y / nbb, x = y % nbb;
+      double* w = W + (size_t)q * nb3 + (size_t)x * nb;   // (b1,b2) row over b3
+      const int* g = g3s + q * nb;
       for (int s0 = 0; s0 < nb;) {
         int s1 = s0 + 1;
-        while (s1 < nb && g3s[s1] == s0) ++s1;
+        while (s1 < nb && g[s1] == s0) ++s1;
         if (s1 - s0 > 1) {
           double t = 0.0;
           for (int k = s0; k < s1; ++k) t += w[k];
@@ -680,43 +732,50 @@ __global__ void __launch_bounds__(kGenThreads) pair_generic_kernel(PairArgs P, Q
       }
     }
     __syncthreads();
-    for (int x = tid; x < nbb; x += NT) {
-      const int b2 = x / nb, b3 = x % nb;   // column over b1
+    for (int y = tid; y < Q1 * nbb; y += NT) {
+      const int q = y / nbb, x = y % nbb, b2 = x / nb, b3 = x % nb;   // column over b1
+      double* w = W + (size_t)q * nb3;
+      const int* g = g1s + q * nb;
       for (int s0 = 0; s0 < nb;) {
         int s1 = s0 + 1;
-        while (s1 < nb && g1s[s1] == s0) ++s1;
+        while (s1 < nb && g[s1] == s0) ++s1;
         if (s1 - s0 > 1) {
           double t = 0.0;
-          for (int k = s0; k < s1; ++k) t += W[((size_t)k * nb + b2) * nb + b3];
-          for (int k = s0; k < s1; ++k) W[((size_t)k * nb + b2) * nb + b3] = t / (double)(s1 - s0);
+          for (int k = s0; k < s1; ++k) t += w[((size_t)k * nb + b2) * nb + b3];
+          for (int k = s0; k < s1; ++k) w[((size_t)k * nb + b2) * nb + b3] = t / (double)(s1 - s0);
         }
         s0 = s1;
       }
     }
     __syncthreads();
-    for (int x = tid; x < nbb; x += NT) {
-      const int b1 = x / nb, b3 = x % nb;   // over b2
+    for (int y = tid; y < Q1 * nbb; y += NT) {
+      const int q = y / nbb, x = y % nbb, b1 = x / nb, b3 = x % nb;   // over b2
+      double* w = W + (size_t)q * nb3;
       for (int s0 = 0; s0 < nb;) {
         int s1 = s0 + 1;
         while (s1 < nb && g2s[s1] == s0) ++s1;
         if (s1 - s0 > 1) {
           double t = 0.0;
-          for (int k = s0; k < s1; ++k) t += W[((size_t)b1 * nb + k) * nb + b3];
-          for (int k = s0; k < s1; ++k) W[((size_t)b1 * nb + k) * nb + b3] = t / (double)(s1 - s0);
+          for (int k = s0; k < s1; ++k) t += w[((size_t)b1 * nb + k) * nb + b3];
+          for (int k = s0; k < s1; ++k) w[((size_t)b1 * nb + k) * nb + b3] = t / (double)(s1 - s0);
         }
         s0 = s1;
       }
     }
     __syncthreads();
     // rates: "+" of (q1,q2), "-" of (q1,-q2) (ph_scattering.cpp:338-380, 466-518)
-    for (int x = tid; x < nb3; x += NT) {
+    for (int y = tid; y < Q1 * nb3; y += NT) {
+      const int q = y / nb3, x = y % nb3;
+      const int q1 = q1s[q];
+      if (q1 < 0 || !inw[q]) continue;
+      const int iq3 = q3s[q];
       const int b1 = x / nbb, b2 = (x / nb) % nb, b3 = x % nb;
-      const double en1 = E1[b1], en3 = E3[b3];
+      const double en1 = E1[q * nb + b1], en3 = E3[q * nb + b3];
       if (en1 < phxc::phExcludeCutoff || en1 < phxc::phEnergyCutoff || en3 < phxc::phEnergyCutoff) continue;
-      const double en2 = M.E[(size_t)iq2 * nb + b2];
-      const double en2m = M.E[(size_t)iq2m * nb + b2];
-      const bool ok2 = inP && en2 >= phxc::phExcludeCutoff && en2 >= phxc::phEnergyCutoff;
-      const bool ok2m = inM && en2m >= phxc::phExcludeCutoff && en2m >= phxc::phEnergyCutoff;
+      const double en2 = E2[b2];
+      const double en2m = E2m[b2];
+      const bool ok2 = (inw[q] & 1) && en2 >= phxc::phExcludeCutoff && en2 >= phxc::phEnergyCutoff;
+      const bool ok2m = (inw[q] & 2) && en2m >= phxc::phExcludeCutoff && en2m >= phxc::phEnergyCutoff;
       if (!ok2 && !ok2m) continue;
       double sp = M.sigma, sm = M.sigma;
       bool vzp = false, vzm = false;
@@ -731,7 +790,7 @@ __global__ void __launch_bounds__(kGenThreads) pair_generic_kernel(PairArgs P, Q
         sp = floor_sigma(adaptive_sigma(M.qT, dp0, dp1, dp2));
         sm = floor_sigma(adaptive_sigma(M.qT, dm0, dm1, dm2));
       }
-      const double w = W[x];
+      const double w = W[y];
       double r[kMaxT];
 #pragma unroll
       for (int c = 0; c < kMaxT; ++c) r[c] = 0.0;
@@ -768,14 +827,14 @@ __global__ void __launch_bounds__(kGenThreads) pair_generic_kernel(PairArgs P, Q
       }
 #pragma unroll
       for (int c = 0; c < kMaxT; ++c)
-        if (c < nT && r[c] != 0.0) atomicAdd(&acc[b1 * kMaxT + c], r[c]);
+        if (c < nT && r[c] != 0.0) atomicAdd(&acc[(q * nb + b1) * kMaxT + c], r[c]);
     }
-    __syncthreads();
   }
-  double* out = P.partial + ((size_t)blockIdx.y * nq + q1) * nb * nT;
-  for (int i = tid; i < nb * nT; i += NT) {
-    const int b1 = i / nT, c = i % nT;
-    out[i] += acc[b1 * kMaxT + c];
+  __syncthreads();
+  for (int i = tid; i < Q1 * nb * nT; i += NT) {
+    const int q = i / (nb * nT), rest = i % (nb * nT), b1 = rest / nT, c = rest % nT;
+    const int q1 = q1s[q];
+    if (q1 >= 0) P.partial[((size_t)blockIdx.y * nq + q1) * nb * nT + rest] += acc[(q * nb + b1) * kMaxT + c];
   }
 }
 
@@ -1516,22 +1575,26 @@ int run_builder_generic(phx_v3* v, phx_bands* b, const phx_lw_params* p, double*
   PHX_ARG(ctx, nb <= kMaxNbGeneric, "phx_ph_linewidths: at most 16 branches");
   const bool windowed = p->window_energy != nullptr;
   PHX_ARG(ctx, !windowed || p->window_cut, "phx_ph_linewidths: window_energy without window_cut");
-  const size_t smem_pair = generic_smem_bytes(nb, nr3);
+  // q1 per block: the most that fits in shared memory (each q2 slab element is read once per block)
+  int q1t = 4;
+  while (q1t > 1 && generic_smem_bytes(nb, nr3, q1t) > 227 * 1024) q1t /= 2;
+  const size_t smem_pair = generic_smem_bytes(nb, nr3, q1t);
   PHX_ARG(ctx, smem_pair <= 227 * 1024, "phx_ph_linewidths: too many R3 vectors for this band count");
+  const int tiles = (nq + q1t - 1) / q1t;
   const size_t smem_fold = sizeof(double2) * ((size_t)nr2 + 2 * (size_t)nb * nb);
   PHX_ARG(ctx, smem_fold <= 227 * 1024, "phx_ph_linewidths: too many R2 vectors");
   const size_t nb3 = (size_t)nb * nb * nb, per_q2 = sizeof(double2) * nr3 * nb3;
   // q2 per cached-vertex slab: at most 512 MB of it, at most 512 q2
   const int chunk = (int)std::max<size_t>(1, std::min<size_t>({(size_t)512, (size_t)(q2e - q2b),
                                                                 (size_t(512) << 20) / std::max<size_t>(per_q2, 1)}));
-  // (q1, slot) blocks: the candidates fill the GPU 4, 8 or 16 times over
-  const int fill = std::max(1, (4 * ctx->num_sms + nq - 1) / nq);
+  // (q1 tile, slot) blocks: the candidates fill the GPU 4, 8 or 16 times over
+  const int fill = std::max(1, (4 * ctx->num_sms + tiles - 1) / tiles);
   const int max_slots = std::min(chunk, 4 * fill);
   const size_t sz_dp = align_up(per_q2 * chunk);
   const size_t sz_part = align_up(sizeof(double) * max_slots * nq * nb * nT);
   const size_t sz_bose = align_up(sizeof(double) * nT * nq * nb);
   const size_t sz_T = align_up(sizeof(double) * 8);
-  const size_t sz_win = windowed ? align_up(sizeof(double) * 2 * nq) : 0;
+  const size_t sz_win = windowed ? align_up(sizeof(double) * 2 * nq + sizeof(int) * nq) : 0;
   const size_t sz_iso = p->isotope_coupling ? align_up(sizeof(double) * v->nat) : 0;
   PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_win + sz_iso));
   char* base = static_cast<char*>(v->ctx->d_scratch);
@@ -1546,9 +1609,17 @@ int run_builder_generic(phx_v3* v, phx_bands* b, const phx_lw_params* p, double*
   if (giso)
     PHX_CUDA(ctx, cudaMemcpyAsync(giso, p->isotope_coupling, sizeof(double) * v->nat, cudaMemcpyHostToDevice, st));
   PHX_CUDA(ctx, cudaMemcpyAsync(temps, p->temperatures, sizeof(double) * nT, cudaMemcpyHostToDevice, st));
+  // with a window, q1 in order of their cut: the q1 of a tile keep similar q2 sets
+  int* order = windowed ? reinterpret_cast<int*>(wdev + 2 * nq) : nullptr;
+  std::vector<int> order_h;
   if (windowed) {
     PHX_CUDA(ctx, cudaMemcpyAsync(wdev, p->window_energy, sizeof(double) * nq, cudaMemcpyHostToDevice, st));
     PHX_CUDA(ctx, cudaMemcpyAsync(wdev + nq, p->window_cut, sizeof(double) * nq, cudaMemcpyHostToDevice, st));
+    order_h.resize(nq);
+    for (int i = 0; i < nq; ++i) order_h[i] = i;
+    std::stable_sort(order_h.begin(), order_h.end(),
+                     [&](int a, int c) { return p->window_cut[a] < p->window_cut[c]; });
+    PHX_CUDA(ctx, cudaMemcpyAsync(order, order_h.data(), sizeof(int) * nq, cudaMemcpyHostToDevice, st));
   }
   PairArgs P;
   P.m.nq = nq;
@@ -1572,9 +1643,9 @@ int run_builder_generic(phx_v3* v, phx_bands* b, const phx_lw_params* p, double*
   P.Dp = Dp;
   P.partial = partial;
   Q2Window W{windowed ? wdev : nullptr, windowed ? wdev + nq : nullptr};
+  auto generic_fn = q1t == 4 ? pair_generic_kernel<4> : q1t == 2 ? pair_generic_kernel<2> : pair_generic_kernel<1>;
   if (smem_pair > 48 * 1024)
-    PHX_CUDA(ctx, cudaFuncSetAttribute(pair_generic_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem_pair));
+    PHX_CUDA(ctx, cudaFuncSetAttribute(generic_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pair));
   if (smem_fold > 48 * 1024)
     PHX_CUDA(ctx, cudaFuncSetAttribute(fold_q2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fold));
   auto chunk_work = [&](int c0, int cnt, int slots, int* launches) -> int {
@@ -1588,7 +1659,7 @@ int run_builder_generic(phx_v3* v, phx_bands* b, const phx_lw_params* p, double*
     Q.q2_first = c0;
     Q.q2_count = cnt;
     Q.q2_per_slot = (cnt + slots - 1) / slots;
-    pair_generic_kernel<<<dim3(nq, slots), kGenThreads, smem_pair, st>>>(Q, W);
+    generic_fn<<<dim3(tiles, slots), kGenThreads, smem_pair, st>>>(Q, W, order);
     ++*launches;
     PHX_CUDA(ctx, cudaGetLastError());
     return PHX_OK;

@@ -569,7 +569,8 @@ __global__ void __launch_bounds__(kTile * NB, 1) pair_fp64_kernel(PairArgs P) {
 // inside the window of q1.
 // ---------------------------------------------------------------------------
 constexpr int kMaxNbGeneric = 16;
-constexpr int kGenThreads = 256;
+constexpr int kGenThreads = 512;
+constexpr int kGenRSplit = 2;   // R3 halves of the T phase (threads per T element)
 
 struct Q2Window {
   const double* energy;   // (nq) or null: no window
@@ -580,7 +581,8 @@ struct Q2Window {
 // e1, e3, the b2 slices of T and X, and the coupling W of all (b1, b2, b3).
 __host__ __device__ inline size_t generic_smem_bytes(int nb, int nr3, int q1s) {
   const size_t nbb = (size_t)nb * nb, nb3 = nbb * nb;
-  return (size_t)q1s * (sizeof(double2) * ((size_t)nr3 + 4 * nbb) + sizeof(double) * (nb3 + (size_t)nb * kMaxT + 2 * nb) +
+  return (size_t)q1s * (sizeof(double2) * ((size_t)nr3 + (3 + kGenRSplit) * nbb) +
+                        sizeof(double) * (nb3 + (size_t)nb * kMaxT + 2 * nb) +
                         sizeof(int) * (2 * nb + 4)) +
          sizeof(double) * 2 * nb + sizeof(int) * nb;
 }
@@ -611,8 +613,8 @@ __global__ void __launch_bounds__(kGenThreads) pair_generic_kernel(PairArgs P, Q
   double2* ph = reinterpret_cast<double2*>(sraw);   // [Q1][nr3]
   double2* e1 = ph + Q1 * nr3;                      // [Q1][nb][nb]
   double2* e3 = e1 + Q1 * nbb;                      // [Q1][nb][nb]
-  double2* Tb = e3 + Q1 * nbb;                      // [Q1][a][c] of the current b2
-  double2* Xb = Tb + Q1 * nbb;                      // [Q1][b1][c] of the current b2
+  double2* Tb = e3 + Q1 * nbb;                      // [kGenRSplit][Q1][a][c] partial T of the current b2
+  double2* Xb = Tb + kGenRSplit * Q1 * nbb;         // [Q1][b1][c] of the current b2
   double* W = reinterpret_cast<double*>(Xb + Q1 * nbb);   // [Q1][b1][b2][b3]
   double* acc = W + Q1 * nb3;                       // [Q1][nb][kMaxT]
   double* E1 = acc + Q1 * nb * kMaxT;               // [Q1][nb]
@@ -677,21 +679,23 @@ __global__ void __launch_bounds__(kGenThreads) pair_generic_kernel(PairArgs P, Q
     if (tid == Q1) scan_blocks(E2, nb, g2s);
     const double2* D = P.Dp + (size_t)j * nr3 * nb3;
     for (int b2 = 0; b2 < nb; ++b2) {
-      // T(a,c) of every q1 of the tile: one read of Dp per element
-      for (int x = tid; x < nbb; x += NT) {
-        const int a = x / nb, c = x % nb;
+      // T(a,c) of every q1 of the tile: one read of Dp per element, the R3
+      // sum split in kGenRSplit parts (more loads in flight)
+      for (int y = tid; y < kGenRSplit * nbb; y += NT) {
+        const int h = y / nbb, x = y % nbb, a = x / nb, c = x % nb;
+        const int rb = h * nr3 / kGenRSplit, re = (h + 1) * nr3 / kGenRSplit;
         const double2* Dx = D + ((size_t)a * nb + b2) * nb + c;
         double2 t[Q1];
 #pragma unroll
         for (int q = 0; q < Q1; ++q) t[q] = cmk(0.0, 0.0);
 #pragma unroll 4
-        for (int r = 0; r < nr3; ++r) {
+        for (int r = rb; r < re; ++r) {
           const double2 d = __ldg(Dx + (size_t)r * nb3);
 #pragma unroll
           for (int q = 0; q < Q1; ++q) cfma(t[q], ph[q * nr3 + r], d);
         }
 #pragma unroll
-        for (int q = 0; q < Q1; ++q) Tb[q * nbb + x] = t[q];
+        for (int q = 0; q < Q1; ++q) Tb[(h * Q1 + q) * nbb + x] = t[q];
       }
       __syncthreads();
       for (int y = tid; y < Q1 * nbb; y += NT) {
@@ -699,7 +703,16 @@ __global__ void __launch_bounds__(kGenThreads) pair_generic_kernel(PairArgs P, Q
         const double2* eq = e1 + q * nbb;
         const double2* tq = Tb + q * nbb;
         double2 v = cmk(0.0, 0.0);
-        for (int a = 0; a < nb; ++a) cfma(v, eq[a * nb + b1], tq[a * nb + c]);
+        for (int a = 0; a < nb; ++a) {
+          double2 tt = tq[a * nb + c];
+#pragma unroll
+          for (int h = 1; h < kGenRSplit; ++h) {
+            const double2 u = tq[h * Q1 * nbb + a * nb + c];
+            tt.x += u.x;
+            tt.y += u.y;
+          }
+          cfma(v, eq[a * nb + b1], tt);
+        }
         Xb[y] = v;
       }
       __syncthreads();

@@ -88,7 +88,7 @@ __device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity, 
 }
 
 // ---------------------------------------------------------------------------
-// bulk async copy global -> shared (no tensor map, no multicast)
+// bulk async copy global -> shared of this CTA (no tensor map)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void bulk_g2s(void* smem_dst, const void* gmem_src, uint32_t bytes,
                                          uint64_t* bar) {

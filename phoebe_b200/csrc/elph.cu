@@ -37,10 +37,10 @@ int phx_el_split_g1(phx_ctx* ctx, const uint8_t* gimg, int nRe, long long N, con
 namespace {
 
 constexpr int kB1 = 8;        // k1 points per pass over the coupling tensor
-constexpr int kQT = 4;        // final states per pair block
+constexpr int kQT = 2;        // final states per pair block
 constexpr int kMaxW = 8;      // Wannier orbitals
 constexpr int kMaxPh = 12;    // phonon branches
-constexpr int kPairThreads = 256;
+constexpr int kPairThreads = 128;
 
 // g1[b][e] = sum_Re ph[b][Re] g[Re][e] for the kB1 k1 of the batch (e over nRp*nph*nw*nw)
 __global__ void __launch_bounds__(256) elph_g1_kernel(const float2* __restrict__ g, int nRe, size_t N,
@@ -405,7 +405,10 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
     s.info[4 * tid + 3] = iq;
   }
   __syncthreads();
-  if (!(s.info[0] | s.info[4] | s.info[8] | s.info[12])) return;
+  int any_valid = 0;
+#pragma unroll
+  for (int q = 0; q < kQT; ++q) any_valid |= s.info[4 * q];
+  if (!any_valid) return;
   // phases e^{+i q3.Rp}/deg with q3 = k2 - k1 (helper_el_scattering.cpp:233-234),
   // not needed when g3 comes from the tensor-core GEMM
   for (int i = tid; i < (g3in ? 0 : kQT * nRp); i += NT) {
@@ -487,9 +490,11 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
   pair_couplings(cached, nRp, nph, nw, nb1, s, g3in, A.g3ld);
   pair_symmetrize(E1, nb1, nph, s);
   // rates (el_scattering.cpp:268-327), one thread per (b1, q, b2, nu) with b1
-  // slowest: the kQT * kMaxW * nph entries of one b1 fill whole warps, so a
-  // warp reduces its rates and adds them once
+  // slowest: when the kQT * kMaxW * nph entries of one b1 fill whole warps
+  // (nph even), a warp reduces its rates and adds them once; otherwise every
+  // thread adds its own
   const int per_b1 = kQT * kMaxW * nph;
+  const bool warp_sums = per_b1 % 32 == 0;
   for (int x = tid; x < nb1 * per_b1; x += NT) {
     const int nu = x % nph, b2 = (x / nph) % kMaxW, q = (x / (nph * kMaxW)) % kQT, b1 = x / per_b1;
     double r[pairc::kMaxT];
@@ -518,8 +523,12 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
     for (int t = 0; t < pairc::kMaxT; ++t) {
       if (t < A.nT) {
         double v = r[t];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((tid & 31) == 0 && v != 0.0) atomicAdd(&s.acc[b1 * pairc::kMaxT + t], v);
+        if (warp_sums) {
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if ((tid & 31) == 0 && v != 0.0) atomicAdd(&s.acc[b1 * pairc::kMaxT + t], v);
+        } else if (v != 0.0) {
+          atomicAdd(&s.acc[b1 * pairc::kMaxT + t], v);
+        }
       }
     }
   }

@@ -1061,12 +1061,12 @@ extern "C" int phx_bands_create_mesh(phx_ph_h0* h0, const int* mesh, int with_ve
   std::vector<double> q;
   phx_mesh_cartesian(mesh, h0->recip, q);
   const size_t nq = b->nq, nb = b->nb;
-  cudaError_t e = cudaMalloc(&b->d_E, sizeof(double) * nq * nb);
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_U, sizeof(double) * 2 * nq * nb * nb);
-  if (e == cudaSuccess && with_velocities) e = cudaMalloc(&b->d_vg, sizeof(double) * 3 * nq * nb);
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_q, sizeof(double) * 3 * nq);
+  cudaError_t e = phx_dev_alloc(ctx, (void**)&b->d_E, sizeof(double) * nq * nb);
+  if (e == cudaSuccess) e = phx_dev_alloc(ctx, (void**)&b->d_U, sizeof(double) * 2 * nq * nb * nb);
+  if (e == cudaSuccess && with_velocities) e = phx_dev_alloc(ctx, (void**)&b->d_vg, sizeof(double) * 3 * nq * nb);
+  if (e == cudaSuccess) e = phx_dev_alloc(ctx, (void**)&b->d_q, sizeof(double) * 3 * nq);
   if (e == cudaSuccess)
-    e = cudaMemcpy(b->d_q, q.data(), sizeof(double) * 3 * nq, cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(b->d_q, q.data(), sizeof(double) * 3 * nq, cudaMemcpyHostToDevice, ctx->stream);
   if (e != cudaSuccess) {
     phx_set_error(ctx, PHX_ERR_CUDA, cudaGetErrorString(e));
     phx_bands_destroy(b);
@@ -1096,10 +1096,10 @@ extern "C" int phx_bands_create_from_host(phx_ctx* ctx, const int* mesh,
   std::vector<double> q;
   phx_mesh_cartesian(mesh, reciprocal_cell, q);
   const size_t nq = b->nq;
-  cudaError_t e = cudaMalloc(&b->d_E, sizeof(double) * nq * nb);
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_U, sizeof(double) * 2 * nq * nb * nb);
-  if (e == cudaSuccess && vg) e = cudaMalloc(&b->d_vg, sizeof(double) * 3 * nq * nb);
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_q, sizeof(double) * 3 * nq);
+  cudaError_t e = phx_dev_alloc(ctx, (void**)&b->d_E, sizeof(double) * nq * nb);
+  if (e == cudaSuccess) e = phx_dev_alloc(ctx, (void**)&b->d_U, sizeof(double) * 2 * nq * nb * nb);
+  if (e == cudaSuccess && vg) e = phx_dev_alloc(ctx, (void**)&b->d_vg, sizeof(double) * 3 * nq * nb);
+  if (e == cudaSuccess) e = phx_dev_alloc(ctx, (void**)&b->d_q, sizeof(double) * 3 * nq);
   if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_E, E, sizeof(double) * nq * nb, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b->d_U, U, sizeof(double) * 2 * nq * nb * nb, cudaMemcpyHostToDevice, ctx->stream);
@@ -1119,13 +1119,15 @@ extern "C" int phx_bands_create_from_host(phx_ctx* ctx, const int* mesh,
 
 extern "C" int phx_bands_destroy(phx_bands* b) {
   if (!b) return PHX_OK;
-  if (b->ctx) cudaSetDevice(b->ctx->device);
-  cudaFree(b->d_E);
-  cudaFree(b->d_U);
-  cudaFree(b->d_vg);
-  cudaFree(b->d_q);
-  cudaFree(b->d_U32);
-  cudaFree(b->d_q1_order);
+  if (b->ctx) {
+    cudaSetDevice(b->ctx->device);
+    phx_dev_free(b->ctx, b->d_E);
+    phx_dev_free(b->ctx, b->d_U);
+    phx_dev_free(b->ctx, b->d_vg);
+    phx_dev_free(b->ctx, b->d_q);
+    phx_dev_free(b->ctx, b->d_U32);
+    phx_dev_free(b->ctx, b->d_q1_order);
+  }
   delete b;
   return PHX_OK;
 }

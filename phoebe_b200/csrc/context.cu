@@ -69,6 +69,14 @@ extern "C" int phx_ctx_create(int device, phx_ctx** out) {
   c->device = device;
   c->num_sms = prop.multiProcessorCount;
   cudaError_t e2 = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e2 == cudaSuccess) {
+    // keep freed object memory in this process's pool (phx_dev_alloc)
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = ~uint64_t(0);
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
   if (e2 == cudaSuccess) e2 = cudaMalloc(&c->d_status, 64 * sizeof(int));
   if (e2 == cudaSuccess) e2 = cudaMemset(c->d_status, 0, 64 * sizeof(int));
   if (e2 != cudaSuccess) {
@@ -88,7 +96,12 @@ extern "C" int phx_ctx_destroy(phx_ctx* ctx) {
   cudaFree(ctx->d_scratch);
   cudaFree(ctx->d_out);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
-  delete ctx;
+  // The struct itself stays allocated (a few hundred bytes): objects that
+  // outlive their context free their memory through it, on the default stream.
+  ctx->stream = nullptr;
+  ctx->d_status = nullptr;
+  ctx->d_scratch = ctx->d_out = nullptr;
+  ctx->scratch_bytes = ctx->out_bytes = 0;
   return PHX_OK;
 }
 
@@ -198,6 +211,16 @@ extern "C" int phx_ws_reorder(int nat, const double* cell, const double* pos, co
           }
   *numR = iR;
   return PHX_OK;
+}
+
+cudaError_t phx_dev_alloc(phx_ctx* ctx, void** p, size_t bytes) {
+  return cudaMallocAsync(p, bytes > 0 ? bytes : 1, ctx->stream);
+}
+
+void phx_dev_free(phx_ctx* ctx, void* p) {
+  if (!p) return;
+  if (ctx->stream) cudaFreeAsync(p, ctx->stream);
+  else cudaFree(p);
 }
 
 int phx_ctx_reserve(phx_ctx* ctx, void** buf, size_t* have, size_t bytes) {

@@ -260,18 +260,20 @@ extern "C" int phx_ph_h0_create(phx_ctx* ctx, int nat, const double* cell, const
   for (int a = 0; a < nat; ++a)
     for (int i = 0; i < 3; ++i) h->masses[3 * a + i] = masses[a];
   cudaError_t e = cudaSuccess;
-  e = cudaMalloc(&h->d_R, sizeof(double) * std::max<size_t>(1, Rc.size()));
-  if (e == cudaSuccess) e = cudaMalloc(&h->d_wblk, sizeof(double) * std::max<size_t>(1, wb.size()));
-  if (e == cudaSuccess) e = cudaMalloc(&h->d_pofs, sizeof(int) * pofs.size());
-  if (e == cudaSuccess) e = cudaMalloc(&h->d_masses, sizeof(double) * nb);
+  cudaStream_t st = ctx->stream;
+  e = phx_dev_alloc(ctx, (void**)&h->d_R, sizeof(double) * std::max<size_t>(1, Rc.size()));
+  if (e == cudaSuccess) e = phx_dev_alloc(ctx, (void**)&h->d_wblk, sizeof(double) * std::max<size_t>(1, wb.size()));
+  if (e == cudaSuccess) e = phx_dev_alloc(ctx, (void**)&h->d_pofs, sizeof(int) * pofs.size());
+  if (e == cudaSuccess) e = phx_dev_alloc(ctx, (void**)&h->d_masses, sizeof(double) * nb);
   if (e == cudaSuccess && !Rc.empty())
-    e = cudaMemcpy(h->d_R, Rc.data(), sizeof(double) * Rc.size(), cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(h->d_R, Rc.data(), sizeof(double) * Rc.size(), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && !wb.empty())
-    e = cudaMemcpy(h->d_wblk, wb.data(), sizeof(double) * wb.size(), cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(h->d_wblk, wb.data(), sizeof(double) * wb.size(), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
-    e = cudaMemcpy(h->d_pofs, pofs.data(), sizeof(int) * pofs.size(), cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(h->d_pofs, pofs.data(), sizeof(int) * pofs.size(), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
-    e = cudaMemcpy(h->d_masses, h->masses.data(), sizeof(double) * nb, cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(h->d_masses, h->masses.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     phx_set_error(ctx, PHX_ERR_CUDA, std::string("phx_ph_h0_create: ") + cudaGetErrorString(e));
     phx_ph_h0_destroy(h);
@@ -283,11 +285,13 @@ extern "C" int phx_ph_h0_create(phx_ctx* ctx, int nat, const double* cell, const
 
 extern "C" int phx_ph_h0_destroy(phx_ph_h0* h) {
   if (!h) return PHX_OK;
-  if (h->ctx) cudaSetDevice(h->ctx->device);
-  cudaFree(h->d_R);
-  cudaFree(h->d_pofs);
-  cudaFree(h->d_wblk);
-  cudaFree(h->d_masses);
+  if (h->ctx) {
+    cudaSetDevice(h->ctx->device);
+    phx_dev_free(h->ctx, h->d_R);
+    phx_dev_free(h->ctx, h->d_pofs);
+    phx_dev_free(h->ctx, h->d_wblk);
+    phx_dev_free(h->ctx, h->d_masses);
+  }
   delete h;
   return PHX_OK;
 }

@@ -60,6 +60,14 @@ struct phx_ctx {
 // grow-only device buffers of a context
 int phx_ctx_reserve(phx_ctx* ctx, void** buf, size_t* have, size_t bytes);
 
+// Device memory of the objects (band structures, couplings, Hamiltonians):
+// stream-ordered allocations on the context's stream from the device's default
+// memory pool, whose release threshold phx_ctx_create raises so that freed
+// blocks stay in the pool.  Objects created and destroyed between calls then
+// neither map memory nor synchronise the device.
+cudaError_t phx_dev_alloc(phx_ctx* ctx, void** p, size_t bytes);
+void phx_dev_free(phx_ctx* ctx, void* p);
+
 // Records e on st; while st is being captured into a graph the record becomes
 // an external event node, so that the event times the graph's replays.
 inline cudaError_t phx_record_event(cudaEvent_t e, cudaStream_t st) {

@@ -1121,8 +1121,10 @@ int phx_split_prepare_bands(phx_ctx* ctx, phx_bands* b) {
       order[i] = i;
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return key[a] < key[c]; });
-    PHX_CUDA(ctx, cudaMalloc(&b->d_q1_order, sizeof(int) * b->nq));
-    PHX_CUDA(ctx, cudaMemcpy(b->d_q1_order, order.data(), sizeof(int) * b->nq, cudaMemcpyHostToDevice));
+    PHX_CUDA(ctx, phx_dev_alloc(ctx, (void**)&b->d_q1_order, sizeof(int) * b->nq));
+    PHX_CUDA(ctx, cudaMemcpyAsync(b->d_q1_order, order.data(), sizeof(int) * b->nq, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
   return PHX_OK;
 }

@@ -142,9 +142,9 @@ __global__ void couplings_kernel(int nb, int nat, int nr3, const double2* __rest
 
 template <typename T>
 int dmalloc(phx_ctx* ctx, T** p, size_t n) {
-  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * std::max<size_t>(n, 1));
+  cudaError_t e = phx_dev_alloc(ctx, reinterpret_cast<void**>(p), sizeof(T) * std::max<size_t>(n, 1));
   if (e != cudaSuccess) {
-    phx_set_error(ctx, PHX_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    phx_set_error(ctx, PHX_ERR_CUDA, std::string("device allocation: ") + cudaGetErrorString(e));
     return PHX_ERR_CUDA;
   }
   return PHX_OK;
@@ -194,15 +194,18 @@ extern "C" int phx_v3_create(phx_ctx* ctx, int nat, int nr2, int nr3, const doub
     phx_v3_destroy(v);
     return rc;
   }
-  cudaError_t e = cudaMemcpy(v->d_D3w, d3w.data(), sizeof(double) * d3w.size(), cudaMemcpyHostToDevice);
+  cudaStream_t st = ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(v->d_D3w, d3w.data(), sizeof(double) * d3w.size(), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
-    e = cudaMemcpy(v->d_D3raw, D3, sizeof(double) * nb3 * nr3 * nr2, cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(v->d_D3raw, D3, sizeof(double) * nb3 * nr3 * nr2, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
-    e = cudaMemcpy(v->d_w2, w2, sizeof(double) * nr2 * nat * nat, cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(v->d_w2, w2, sizeof(double) * nr2 * nat * nat, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
-    e = cudaMemcpy(v->d_w3, w3, sizeof(double) * nr3 * nat * nat, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(v->d_R2, R2, sizeof(double) * 3 * nr2, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(v->d_R3, R3, sizeof(double) * 3 * nr3, cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(v->d_w3, w3, sizeof(double) * nr3 * nat * nat, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(v->d_R2, R2, sizeof(double) * 3 * nr2, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(v->d_R3, R3, sizeof(double) * 3 * nr3, cudaMemcpyHostToDevice, st);
+  // the caller may free or reuse its host arrays on return
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     phx_set_error(ctx, PHX_ERR_CUDA, std::string("phx_v3_create: ") + cudaGetErrorString(e));
     phx_v3_destroy(v);
@@ -216,14 +219,16 @@ extern "C" int phx_v3_destroy(phx_v3* v) {
   if (!v) return PHX_OK;
   if (v->ctx) cudaSetDevice(v->ctx->device);
   phx_builder_release(v);
-  cudaFree(v->d_D3w);
-  cudaFree(v->d_D3raw);
-  cudaFree(v->d_w2);
-  cudaFree(v->d_w3);
-  cudaFree(v->d_R2);
-  cudaFree(v->d_R3);
-  cudaFree(v->d_plus);
-  cudaFree(v->d_mins);
+  if (v->ctx) {
+    phx_dev_free(v->ctx, v->d_D3w);
+    phx_dev_free(v->ctx, v->d_D3raw);
+    phx_dev_free(v->ctx, v->d_w2);
+    phx_dev_free(v->ctx, v->d_w3);
+    phx_dev_free(v->ctx, v->d_R2);
+    phx_dev_free(v->ctx, v->d_R3);
+    phx_dev_free(v->ctx, v->d_plus);
+    phx_dev_free(v->ctx, v->d_mins);
+  }
   delete v;
   return PHX_OK;
 }

@@ -64,7 +64,9 @@ def parse():
                     help="skip the plain FP64 GPU step that the split path is compared with")
     ap.add_argument("--kernels-only", action="store_true",
                     help="profiling aid: time the builder only (no e2e leg, no CPU baseline)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    args.precision_given = any(a.startswith("--precision") for a in sys.argv[1:])
+    return args
 
 
 def workload(mesh):
@@ -478,7 +480,8 @@ def run_smatrix(args):
     ctx = Context(0)
     h0 = PhononH0(ctx, cr, fc2)
     bands = h0.populate(mesh, withVelocities=True)
-    v3 = Interaction3Ph(ctx, cr, fc3, precision="fp64")
+    prec = args.precision if args.precision_given else "fp64"
+    v3 = Interaction3Ph(ctx, cr, fc3, precision=prec)
     T = [C.kelvin_to_ry(300.0)]
     ns = bands.nq * bands.nb
     sm = PhScatteringMatrix(v3, bands, T, "adaptive", in_memory=True)
@@ -514,6 +517,7 @@ def run_smatrix(args):
                                    "FP64 (%.1f GB) in device memory, larger than L2" % (*mesh, ns, ns,
                                                                                          8e-9 * ns * ns)},
             "matrix_build_ms": ms_build,
+            "build_precision": prec,
             "matrix_free_product_ms": ms_free,
             "stored_vs_matrix_free_speedup": ms_free / ms_dot,
             "stored_vs_matrix_free_rel_err": err,

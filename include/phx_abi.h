@@ -184,7 +184,10 @@ int phx_ph_linewidths(phx_v3* v3, phx_bands* bands, const phx_lw_params* params,
 int phx_ph_linewidths_d(phx_v3* v3, phx_bands* bands, const phx_lw_params* params,
                         double* A_out_d, phx_lw_stats* stats);
 
-/* ---- scattering-matrix modes of the builder (nb = 6, FP64, no q2 window) ----
+/* ---- scattering-matrix modes of the builder (nb = 6, no q2 window) ----
+ * Both precisions of the coupling object: PHX_PREC_FP64, or the split paths,
+ * whose matrix elements are within 1e-6 of the largest FP64 element (their
+ * sums over q2 within the linewidths' 1e-5).  The stored matrix is FP64.
  * States are numbered s = iq * nb + ib (the reference's BteIndex without
  * symmetries).  The rates, cut-offs, exclusions and time-reversal pairing are
  * those of phx_ph_linewidths; the differences are the reference's: the

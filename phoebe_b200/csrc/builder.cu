@@ -1021,7 +1021,7 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
                          const double2* Dp, uint8_t* Bimg, const void* rec, double emax, int q2_first,
                          int q2_count, int slots, double* partial, int* launches, cudaEvent_t ev_begin,
                          cudaEvent_t ev_end, int fp16, const unsigned* dmax, void* edges, unsigned* edge_count,
-                         unsigned edge_cap);
+                         unsigned edge_cap, const phx_split_matrix* mat = nullptr);
 unsigned phx_split_edge_cap();
 size_t phx_split_edge_bytes();
 
@@ -1800,13 +1800,17 @@ int run_matrix_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
   const int q2b = p->q2_begin, q2e = p->q2_end;
   const int ns = nq * NB;
   const bool full = A_full != nullptr;
+  const bool split = v->precision != PHX_PREC_FP64;
+  const int fp16 = v->precision == PHX_PREC_SPLIT_FP16 ? 1 : 0;
+  // plan: the FP64 kernel's default, or the split kernel's large plan (the
+  // matrix-free mode takes its small one: the slabs are zeroed per chunk);
   // slab memory of mode 1: at most 4 GiB for the two slabs of all temperatures
-  int chunk = std::min(512, q2e - q2b);
+  int chunk = std::min(split ? (full ? 1792 : 448) : 512, q2e - q2b);
   if (!full) {
     const size_t per_q2 = 2 * sizeof(double) * (size_t)nT * ns * NB;
     chunk = (int)std::max<size_t>(1, std::min<size_t>(chunk, (size_t(4) << 30) / per_q2));
   }
-  const int slots = std::min(8, chunk);
+  const int slots = std::min(split ? (full ? 28 : 7) : 8, chunk);
   const size_t nb3 = (size_t)NB * NB * NB;
   const size_t sz_dp = align_up(sizeof(double2) * chunk * nr3 * nb3);
   const size_t sz_part = align_up(sizeof(double) * slots * nq * NB * nT);
@@ -1815,7 +1819,12 @@ int run_matrix_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
   const size_t sz_iso = p->isotope_coupling ? align_up(sizeof(double) * v->nat) : 0;
   const size_t slab_elems = (size_t)ns * chunk * NB;
   const size_t sz_slab = full ? 0 : align_up(sizeof(double) * 2 * nT * slab_elems);
-  PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_iso + sz_slab));
+  const size_t sz_img = split ? align_up(phx_split_bimg_bytes(chunk, nr3)) : 0;
+  const size_t sz_rec = split ? align_up(phx_split_rec_bytes(nq)) : 0;
+  const size_t sz_max = split ? align_up(sizeof(unsigned) * 2) : 0;
+  const size_t sz_edge = split ? align_up(phx_split_edge_bytes()) : 0;
+  PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_iso + sz_slab + sz_img + sz_rec + sz_max +
+                                     sz_edge));
   char* base = static_cast<char*>(v->ctx->d_scratch);
   double2* Dp = reinterpret_cast<double2*>(base);
   double* partial = reinterpret_cast<double*>(base + sz_dp);
@@ -1825,6 +1834,24 @@ int run_matrix_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
       p->isotope_coupling ? reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose + sz_T) : nullptr;
   double* slabP = full ? nullptr : reinterpret_cast<double*>(base + sz_dp + sz_part + sz_bose + sz_T + sz_iso);
   double* slabM = full ? nullptr : slabP + nT * slab_elems;
+  char* sbase = base + sz_dp + sz_part + sz_bose + sz_T + sz_iso + sz_slab;
+  uint8_t* Bimg = reinterpret_cast<uint8_t*>(sbase);
+  void* rec = sbase + sz_img;
+  unsigned* dmax = reinterpret_cast<unsigned*>(sbase + sz_img + sz_rec);
+  unsigned* edge_count = dmax + 1;
+  void* edges = sbase + sz_img + sz_rec + sz_max;
+  if (split) {
+    PHX_ARG(ctx, phx_split_smem_bytes(nr3) <= 227 * 1024, "too many R3 vectors for the split path");
+    PHX_TRY(phx_split_prepare_bands(ctx, b));
+    if (b->emax < 0.0) {
+      std::vector<double> Eh((size_t)nq * NB);
+      PHX_CUDA(ctx, cudaMemcpy(Eh.data(), b->d_E, sizeof(double) * Eh.size(), cudaMemcpyDeviceToHost));
+      double m = 0.0;
+      for (double e : Eh) m = std::max(m, std::fabs(e));
+      b->emax = m;
+    }
+    PHX_TRY(phx_split_set_attributes(ctx, nr3, nT));
+  }
   PairArgs P{};
   P.m.nq = nq;
   P.m.nb = NB;
@@ -1879,18 +1906,30 @@ int run_matrix_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
     else PHX_CUDA(ctx, cudaMemsetAsync(y_d, 0, sizeof(double) * nvec * nT * 3 * (size_t)ns, st));
     bose_kernel<<<std::min(1024, (nq * NB * nT + 255) / 256), 256, 0, st>>>(nq, NB, nT, b->d_E, temps, bose);
     ++launches;
+    if (split) PHX_TRY(phx_split_pack_records(ctx, P.m, rec, &launches));
     PHX_CUDA(ctx, cudaEventRecord(evv0, st));
     for (int c0 = q2b; c0 < q2e; c0 += chunk) {
       const int cnt = std::min(chunk, q2e - c0);
-      fold_tiled_launch(NB, nr2, nr3, v, b, c0, cnt, Dp, st);
-      ++launches;
-      PairArgs Q = P;
-      Q.q2_first = c0;
-      Q.q2_count = cnt;
-      Q.q2_per_slot = (cnt + slots - 1) / slots;
-      pair_fp64_kernel<NB, true><<<dim3(tiles, slots), kTile * NB, smem_pair, st>>>(Q);
-      ++launches;
-      PHX_CUDA(ctx, cudaGetLastError());
+      if (split) {
+        // tensor-core pair kernel: its matrix sums go in by atomics, onto zeroed slabs
+        if (!full) PHX_CUDA(ctx, cudaMemsetAsync(slabP, 0, sizeof(double) * 2 * nT * slab_elems, st));
+        if (fp16) PHX_CUDA(ctx, cudaMemsetAsync(dmax, 0, sizeof(unsigned), st));
+        fold_tiled_launch(NB, nr2, nr3, v, b, c0, cnt, Dp, st, fp16 ? dmax : nullptr);
+        ++launches;
+        const phx_split_matrix mo{full ? A_full : slabP, slabM, (long long)ns, slab_elems, full ? 1 : 0};
+        PHX_TRY(phx_split_pair_chunk(ctx, P.m, v, b, Dp, Bimg, rec, b->emax, c0, cnt, slots, partial, &launches,
+                                     nullptr, nullptr, fp16, dmax, edges, edge_count, phx_split_edge_cap(), &mo));
+      } else {
+        fold_tiled_launch(NB, nr2, nr3, v, b, c0, cnt, Dp, st);
+        ++launches;
+        PairArgs Q = P;
+        Q.q2_first = c0;
+        Q.q2_count = cnt;
+        Q.q2_per_slot = (cnt + slots - 1) / slots;
+        pair_fp64_kernel<NB, true><<<dim3(tiles, slots), kTile * NB, smem_pair, st>>>(Q);
+        ++launches;
+        PHX_CUDA(ctx, cudaGetLastError());
+      }
       if (!full) {
         if (giso) {
           IsoArgs I{P.m, v->nat, giso, c0, cnt, (cnt + slots - 1) / slots, partial, slabP, ns, slab_elems, 0};
@@ -1956,7 +1995,8 @@ int run_matrix_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
       rc = PHX_ERR_CUDA;
     } else if (kst) {
       cudaMemset(ctx->d_status, 0, sizeof(int));
-      phx_set_error(ctx, PHX_ERR_CUDA, "scattering matrix: kernel status " + std::to_string(kst));
+      phx_set_error(ctx, PHX_ERR_CUDA, (kst & (1 << 20)) ? std::string("split path: near-cut-off event list overflowed")
+                                                         : "scattering matrix: kernel status " + std::to_string(kst));
       rc = PHX_ERR_CUDA;
     }
   }
@@ -1998,8 +2038,7 @@ int check_builder_args(phx_v3* v, phx_bands* b, const phx_lw_params* p) {
 int check_matrix_args(phx_v3* v, phx_bands* b, const phx_lw_params* p) {
   PHX_TRY(check_builder_args(v, b, p));
   phx_ctx* ctx = v->ctx;
-  PHX_ARG(ctx, v->nb == 6, "scattering matrix modes: nb = 6 (the fused FP64 kernels)");
-  PHX_ARG(ctx, v->precision == PHX_PREC_FP64, "scattering matrix modes run in FP64 (set PHX_PREC_FP64)");
+  PHX_ARG(ctx, v->nb == 6, "scattering matrix modes: nb = 6 (the fused kernels)");
   PHX_ARG(ctx, !p->window_energy && !p->window_cut, "scattering matrix modes take no q2 window");
   return PHX_OK;
 }

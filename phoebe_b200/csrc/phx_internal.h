@@ -193,6 +193,17 @@ struct phx_dot_args {
   const double* E;         // (ns), for skip = 1
 };
 int phx_smatrix_dot_launch(const phx_dot_args& a, cudaStream_t st, int* launches);
+// Matrix output of the split pair kernel, in the layouts of the FP64 matrix
+// modes: full = 1, `plus` is the whole matrix (one temperature); full = 0,
+// `plus` and `minus` are the two slabs of the chunk, columns j nb + b2 with
+// j = q2 - q2_first, temperature t at t * tstride.
+struct phx_split_matrix {
+  double* plus;
+  double* minus;
+  long long ld;
+  size_t tstride;
+  int full;
+};
 // y (nvec, nT, 3, ns) += lw (nT, ns) * x; then, with finalize, y = 0 on excluded states
 int phx_smatrix_diag_term_launch(int ns, int nT, int nvec, const double* lw, const double* x, double* y,
                                  const double* E, int finalize, cudaStream_t st);

@@ -86,6 +86,7 @@ struct TcArgs {
   struct EdgeEvent* edges;     // near-cut-off processes, re-decided in FP64 by edge_fix_kernel
   unsigned* edge_count;
   unsigned edge_cap;
+  phx_split_matrix mat;        // matrix modes: mat.plus != null
 };
 
 // A queued triplet one of whose adaptive deltas sat within 1e-5 of the
@@ -384,6 +385,43 @@ __device__ __forceinline__ void rate_combine(float pre, float iE1, const float* 
            fm * x3.N[t] * (d1 * n1[t] * (x2m.N[t] + 1.f) + d2 * x2m.N[t] * (n1[t] + 1.f));
 }
 
+// The "+" and "-" parts of rate_combine separately (matrix modes: the "+"
+// process goes to the column of q2, the "-" ones to the column of -q2).
+template <int NT>
+__device__ __forceinline__ void rate_combine2(float pre, float iE1, const float* n1, const Band& x2,
+                                              const Band& x2m, const Band& x3, float dp, float d1, float d2,
+                                              float* fplus, float* fminus) {
+  const float fp = pre * dp * iE1 * x2.iE * x3.iE;
+  const float fm = pre * iE1 * x2m.iE * x3.iE;
+#pragma unroll
+  for (int t = 0; t < NT; ++t) {
+    fplus[t] = fp * n1[t] * x2.N[t] * (x3.N[t] + 1.f);
+    fminus[t] = fm * x3.N[t] * (d1 * n1[t] * (x2m.N[t] + 1.f) + d2 * x2m.N[t] * (n1[t] + 1.f));
+  }
+}
+
+// Adds the matrix elements of one row (q1 b1) and one c2: the "+" sums to
+// column (q2, c2), minus the "-" sums to column (-q2, c2) (the full matrix),
+// or to the two slabs of the chunk.  The rates carry the linewidth's 1/2.
+template <int NT>
+__device__ __forceinline__ void add_matrix(const TcArgs& P, int q1, int b1, int iq2, int c2, double scale,
+                                           const float* gp, const float* gm) {
+  const phx_split_matrix& X = P.mat;
+  const size_t row = (size_t)q1 * 6 + b1;
+  if (X.full) {
+    const int iq2m = mesh_neg(iq2, P.m.n0, P.m.n1, P.m.n2);
+    if (gp[0] != 0.f) atomicAdd(X.plus + (size_t)(iq2 * 6 + c2) * X.ld + row, 2.0 * scale * (double)gp[0]);
+    if (gm[0] != 0.f) atomicAdd(X.plus + (size_t)(iq2m * 6 + c2) * X.ld + row, -2.0 * scale * (double)gm[0]);
+    return;
+  }
+  const size_t col = (size_t)((iq2 - P.q2_first) * 6 + c2) * X.ld + row;
+#pragma unroll
+  for (int t = 0; t < NT; ++t) {
+    if (gp[t] != 0.f) atomicAdd(X.plus + t * X.tstride + col, 2.0 * scale * (double)gp[t]);
+    if (gm[t] != 0.f) atomicAdd(X.minus + t * X.tstride + col, 2.0 * scale * (double)gm[t]);
+  }
+}
+
 template <int NT>
 __device__ __forceinline__ void rate_f(int smearing, float ginv, float pre, double E1, float iE1,
                                        const float* n1, const Band& x2, const Band& x2m,
@@ -504,7 +542,7 @@ __device__ __forceinline__ Smem carve(uint8_t* base, int Kp) {
 // the hot loop within the instruction cache (14% faster than inlined).  Entry: x = |V|^2 / n1, y = lane of the q1 row | b1 << 5 | b2 << 8 |
 // b3 << 11 | degenerate flag << 14.  Flagged entries average the rate factors
 // over the degenerate blocks of b2 and b3 (one band each otherwise).
-template <int NT>
+template <int NT, bool MAT>
 __device__ __noinline__ void rate_entry(uint2 e, int qd, const double* En1, const float* iE1s,
                                            const float* N1, const uint4* rec, const uint4* u2,
                                            unsigned gp2, int smearing, float ginv, float pre,
@@ -527,10 +565,15 @@ __device__ __noinline__ void rate_entry(uint2 e, int qd, const double* En1, cons
 #pragma unroll
   for (int t = 0; t < NT; ++t) g[t] = 0.f;
   unsigned anynear = 0u;
+  constexpr bool matm = MAT;   // matrix modes: their own instantiation
+  const double mscale = (double)(wn / (float)(__popc(bm2) * __popc(bm3)));
   for (unsigned m2 = bm2; m2; m2 &= m2 - 1) {
     const int c2 = __ffs(m2) - 1;
     const Band x2 = load_band<NT>(u2 + 3 * c2, 1);
     const Band x2m = load_band<NT>(u2 + kU2Chunks + 3 * c2, 1);
+    float gpl[NT], gmi[NT];   // matrix modes: the "+" and "-" sums of this c2
+#pragma unroll
+    for (int t = 0; t < NT; ++t) gpl[t] = gmi[t] = 0.f;
     for (unsigned m3 = bm3; m3; m3 &= m3 - 1) {
       const int c3 = __ffs(m3) - 1;
       const Band x3 = load_band<NT>(srow + (kChBand + 3 * c3) * kM, kM);
@@ -540,12 +583,29 @@ __device__ __noinline__ void rate_entry(uint2 e, int qd, const double* En1, cons
         gm = sigma_ad(x2m.P, x3.P, x2m.vf, x3.vf);
       }
       float f[NT];
-      unsigned near;
-      rate_f<NT>(smearing, ginv, pre, E1, iE1, n1v, x2, x2m, x3, gp, gm, f, near);
+      unsigned near = 0u;
+      if constexpr (matm) {
+#pragma unroll
+        for (int t = 0; t < NT; ++t) f[t] = 0.f;
+        if (x3.E >= phxc::phEnergyCutoff) {
+          float dp, d1, d2, fpv[NT], fmv[NT];
+          deltas3(smearing, ginv, E1, x2, x2m, x3, gp, gm, dp, d1, d2, near);
+          rate_combine2<NT>(pre, iE1, n1v, x2, x2m, x3, dp, d1, d2, fpv, fmv);
+#pragma unroll
+          for (int t = 0; t < NT; ++t) {
+            gpl[t] += fpv[t];
+            gmi[t] += fmv[t];
+            f[t] = fpv[t] + fmv[t];
+          }
+        }
+      } else {
+        rate_f<NT>(smearing, ginv, pre, E1, iE1, n1v, x2, x2m, x3, gp, gm, f, near);
+      }
 #pragma unroll
       for (int t = 0; t < NT; ++t) g[t] += f[t];
       anynear |= near;
     }
+    if constexpr (matm) add_matrix<NT>(P, P.q1_order[blockIdx.x * kM + mm], b1, iq2, c2, mscale, gpl, gmi);
   }
   if (anynear) {
     // a cut-off decision too close for FP32: edge_fix_kernel re-decides the entry in FP64
@@ -557,7 +617,7 @@ __device__ __noinline__ void rate_entry(uint2 e, int qd, const double* En1, cons
   for (int t = 0; t < NT; ++t) atomicAdd(&qacc[r * kAccRow + b1 * kMaxT + t], scale * g[t]);
 }
 
-template <int NT>
+template <int NT, bool MAT>
 __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
   const MeshArgs& M = P.m;
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -875,7 +935,7 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
                 qn += __popc(bal);
                 if (qn >= 32) {
                   __syncwarp();
-                  rate_entry<NT>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc, P,
+                  rate_entry<NT, MAT>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc, P,
                                  iq2);
                   const uint2 rest = lane + 32 < qn ? queue[lane + 32] : make_uint2(0u, 0u);
                   __syncwarp();
@@ -895,7 +955,7 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
       if (qn) {
         __syncwarp();
         if (lane < qn)
-          rate_entry<NT>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc, P, iq2);
+          rate_entry<NT, MAT>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc, P, iq2);
         qn = 0;
       }
       __syncwarp();
@@ -1008,7 +1068,8 @@ size_t pair_tc_smem(int Kp) {
 template <int NT>
 int launch_pair(phx_ctx* ctx, const TcArgs& A, int tiles, int slots) {
   const size_t smem = pair_tc_smem(A.Kp);   // attribute set by phx_split_set_attributes
-  pair_tc_kernel<NT><<<dim3(tiles, slots), kThreads, smem, ctx->stream>>>(A);
+  if (A.mat.plus) pair_tc_kernel<NT, true><<<dim3(tiles, slots), kThreads, smem, ctx->stream>>>(A);
+  else pair_tc_kernel<NT, false><<<dim3(tiles, slots), kThreads, smem, ctx->stream>>>(A);
   PHX_CUDA(ctx, cudaGetLastError());
   return PHX_OK;
 }
@@ -1048,11 +1109,15 @@ __global__ void edge_fix_kernel(TcArgs P) {
     double corr[NT];
 #pragma unroll
     for (int t = 0; t < NT; ++t) corr[t] = 0.0;
+    const double scale = (double)(wn / (float)(__popc(bm2) * __popc(bm3)));
     for (unsigned m2 = bm2; m2; m2 &= m2 - 1) {
       const int c2 = __ffs(m2) - 1;
       const uint4* r2 = rq2 + kChBand + 3 * c2;
       const uint4* r2m = rq2m + kChBand + 3 * c2;
       const Band x2 = load_band<NT>(r2, 1), x2m = load_band<NT>(r2m, 1);
+      float cp[NT], cm[NT];   // matrix modes: corrections of the "+" and "-" sums of this c2
+#pragma unroll
+      for (int t = 0; t < NT; ++t) cp[t] = cm[t] = 0.f;
       for (unsigned m3 = bm3; m3; m3 &= m3 - 1) {
         const int c3 = __ffs(m3) - 1;
         const uint4* r3 = rq3 + kChBand + 3 * c3;
@@ -1078,9 +1143,19 @@ __global__ void edge_fix_kernel(TcArgs P) {
         rate_combine<NT>(pre, x1.iE, x1.N, x2, x2m, x3, fdp, fd1, fd2, f1);
 #pragma unroll
         for (int t = 0; t < NT; ++t) corr[t] += (double)f1[t] - (double)f0[t];
+        if (P.mat.plus) {
+          float p0[NT], m0[NT], p1[NT], m1[NT];
+          rate_combine2<NT>(pre, x1.iE, x1.N, x2, x2m, x3, dp, d1, d2, p0, m0);
+          rate_combine2<NT>(pre, x1.iE, x1.N, x2, x2m, x3, fdp, fd1, fd2, p1, m1);
+#pragma unroll
+          for (int t = 0; t < NT; ++t) {
+            cp[t] += p1[t] - p0[t];
+            cm[t] += m1[t] - m0[t];
+          }
+        }
       }
+      if (P.mat.plus) add_matrix<NT>(P, q1, b1, iq2, c2, scale, cp, cm);
     }
-    const double scale = (double)(wn / (float)(__popc(bm2) * __popc(bm3)));
     double* out = P.partial + (((size_t)slot * M.nq + q1) * 6 + b1) * NT;
 #pragma unroll
     for (int t = 0; t < NT; ++t)
@@ -1146,7 +1221,7 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
                          const double2* Dp, uint8_t* Bimg, const void* rec, double emax, int q2_first,
                          int q2_count, int slots, double* partial, int* launches, cudaEvent_t ev_begin,
                          cudaEvent_t ev_end, int fp16, const unsigned* dmax, void* edges, unsigned* edge_count,
-                         unsigned edge_cap) {
+                         unsigned edge_cap, const phx_split_matrix* mat) {
   const int Kp = phx_split_kp(v->nr3);
   const int nkc = Kp / kKC;
   convert_b_kernel<<<dim3(q2_count, kParts * nkc), 256, 0, ctx->stream>>>(Dp, v->nr3, Kp, q2_count, Bimg, fp16,
@@ -1173,6 +1248,7 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
   A.edges = static_cast<EdgeEvent*>(edges);
   A.edge_count = edge_count;
   A.edge_cap = edge_cap;
+  A.mat = mat ? *mat : phx_split_matrix{nullptr, nullptr, 0, 0, 0};
   PHX_ARG(ctx, slots < 32 && (M.nq + kM - 1) / kM < (1 << 20), "split path: at most 31 slots");
   PHX_CUDA(ctx, cudaMemsetAsync(edge_count, 0, sizeof(unsigned), ctx->stream));
   const int tiles = (M.nq + kM - 1) / kM;
@@ -1207,11 +1283,24 @@ size_t phx_split_edge_bytes() { return sizeof(EdgeEvent) * phx_split_edge_cap();
 // before any launch (and outside graph capture).
 int phx_split_set_attributes(phx_ctx* ctx, int nr3, int nT) {
   const int smem = (int)pair_tc_smem(phx_split_kp(nr3));
+  const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
   switch (nT) {
-    case 1: PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); break;
-    case 2: PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); break;
-    case 3: PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); break;
-    default: PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); break;
+    case 1:
+      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<1, false>, a, smem));
+      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<1, true>, a, smem));
+      break;
+    case 2:
+      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<2, false>, a, smem));
+      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<2, true>, a, smem));
+      break;
+    case 3:
+      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<3, false>, a, smem));
+      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<3, true>, a, smem));
+      break;
+    default:
+      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<4, false>, a, smem));
+      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<4, true>, a, smem));
+      break;
   }
   return PHX_OK;
 }

@@ -37,10 +37,10 @@ int phx_el_split_g1(phx_ctx* ctx, const uint8_t* gimg, int nRe, long long N, con
 namespace {
 
 constexpr int kB1 = 8;        // k1 points per pass over the coupling tensor
-constexpr int kQT = 2;        // final states per pair block
+constexpr int kQT = 1;        // final states per pair block
 constexpr int kMaxW = 8;      // Wannier orbitals
 constexpr int kMaxPh = 12;    // phonon branches
-constexpr int kPairThreads = 128;
+constexpr int kPairThreads = 64;
 
 // g1[b][e] = sum_Re ph[b][Re] g[Re][e] for the kB1 k1 of the batch (e over nRp*nph*nw*nw)
 __global__ void __launch_bounds__(256) elph_g1_kernel(const float2* __restrict__ g, int nRe, size_t N,

@@ -35,7 +35,7 @@ constexpr uint32_t kABytes = kM * kKC * 2 * 2;   // hi + lo
 constexpr uint32_t kBBytes = kN * kKC * 2 * 2;
 constexpr uint32_t kStageBytes = kABytes + kBBytes;
 constexpr int kThreads = 192;  // producer, MMA, 4 epilogue warps
-constexpr int kMaxBatch = 8;
+constexpr int kMaxBatch = 16;
 
 __device__ __forceinline__ void split8(const double* v, uint4& hi, uint4& lo) {
   uint32_t h[4], l[4];
@@ -274,16 +274,17 @@ __global__ void __launch_bounds__(kThreads, 1) el_gemm_kernel(GemmArgs P) {
 //   g1(k1; x) = sum_Re e^{+i k1.Re}/deg_Re g(Re; x),   x = (Rp, nu, w1, w2)
 // as D[x][n] = sum_k A[x][k] B[n][k] with A[x][k] = [Re g | Im g](Re; x)
 // (the coupling tensor itself, split once into a BF16 hi/lo image) and
-// B[2j] = [cos ; -sin], B[2j+1] = [sin ; cos] of k1 j (16 columns, 8 k1).
+// B[2j] = [cos ; -sin], B[2j+1] = [sin ; cos] of k1 j (32 columns, 16 k1: each
+// pass over the 371 MB image of g serves 16 k1).
 // The tensor core's FP32 accumulation rounds toward zero, which biases long
 // sums; here every 64-deep K chunk goes to its own TMEM buffer (one of
 // kG1Bufs in turn) and the epilogue adds the chunk sums in FP64 registers.
 // ---------------------------------------------------------------------------
 constexpr int kKC1 = 64;
-constexpr int kG1Stages = 4;
-constexpr int kG1N = 2 * kMaxBatch;                       // 16 real columns
+constexpr int kG1Stages = 3;
+constexpr int kG1N = 2 * kMaxBatch;                       // 32 real columns
 constexpr uint32_t kA1Bytes = kM * kKC1 * 2 * 2;          // 32 KB per (tile, chunk)
-constexpr uint32_t kB1Bytes = kG1N * kKC1 * 2 * 2;        // 4 KB per chunk
+constexpr uint32_t kB1Bytes = kG1N * kKC1 * 2 * 2;        // 8 KB per chunk
 constexpr int kG1Bufs = 8;
 constexpr int kG1MaxKC = 16;                              // nRe <= 512
 
@@ -318,7 +319,7 @@ __global__ void el_g_image_kernel(const float2* __restrict__ g, int nRe, long lo
   *reinterpret_cast<uint4*>(tile + kA1Bytes / 2 + off) = lo;
 }
 
-// B image of a batch: chunk kc = [hi 16 x kKC1 | lo 16 x kKC1]
+// B image of a batch: chunk kc = [hi kG1N x kKC1 | lo kG1N x kKC1]
 __global__ void el_k1_phase_image_kernel(const double* __restrict__ k1s, int nb, int nRe,
                                          const double* __restrict__ Re, const double* __restrict__ degE, int nKC,
                                          uint8_t* __restrict__ img) {
@@ -466,8 +467,8 @@ __global__ void __launch_bounds__(kThreads, 1) el_g1_gemm_kernel(G1Args P) {
         }
         tc::tc_fence_after();
         float v[kG1N];
-        tc::tmem_ld8(tmem + lanes + buf * kG1N, v);
-        tc::tmem_ld8(tmem + lanes + buf * kG1N + 8, v + 8);
+#pragma unroll
+        for (int i = 0; i < kG1N; i += 8) tc::tmem_ld8(tmem + lanes + buf * kG1N + i, v + i);
         tc::tmem_wait_ld();
         tc::tc_fence_before();
         __syncwarp();
@@ -533,7 +534,7 @@ int phx_el_split_phases(phx_ctx* ctx, int nq, const double* qcart, int nRp, cons
 int phx_el_split_g3_batch(phx_ctx* ctx, const uint8_t* Aimg, uint8_t* Bimg, const double2* cached, size_t per,
                           int nRp, int nph, int nw, int nq, int nb, const int* nb1, float2* g3T, int* ldq_out,
                           int* xoff_out) {
-  PHX_ARG(ctx, nb >= 1 && nb <= kMaxBatch, "split el-ph GEMM: batch of 1..8 k1");
+  PHX_ARG(ctx, nb >= 1 && nb <= kMaxBatch, "split el-ph GEMM: batch of 1..16 k1");
   BatchCols cols;
   cols.nb = nb;
   cols.xoff[0] = 0;
@@ -595,12 +596,12 @@ int phx_el_split_g_image(phx_ctx* ctx, const float* g, int nRe, long long N, uin
   return PHX_OK;
 }
 
-// g1 (nb, N) of a batch of nb <= 8 k1 (Cartesian coordinates k1s on the device)
+// g1 (nb, N) of a batch of nb <= 16 k1 (Cartesian coordinates k1s on the device)
 // from the split image of g; kimg is scratch of phx_el_split_k1_image_bytes().  Two launches.
 int phx_el_split_g1(phx_ctx* ctx, const uint8_t* gimg, int nRe, long long N, const double* Re, const double* degE,
                     int nb, const double* k1s, uint8_t* kimg, double2* g1) {
   const int nKC = (2 * nRe + kKC1 - 1) / kKC1;
-  PHX_ARG(ctx, nKC <= kG1MaxKC && nb >= 1 && nb <= kMaxBatch, "split el-ph g1: nRe <= 512 and 1..8 k1");
+  PHX_ARG(ctx, nKC <= kG1MaxKC && nb >= 1 && nb <= kMaxBatch, "split el-ph g1: nRe <= 512 and 1..16 k1");
   const int nMT = (int)((N + kM - 1) / kM);
   const int tb = nKC * kG1N * (kKC1 / 8);
   el_k1_phase_image_kernel<<<(tb + 255) / 256, 256, 0, ctx->stream>>>(k1s, nb, nRe, Re, degE, nKC, kimg);

@@ -1,7 +1,7 @@
 // Electron-phonon Wannier path on the GPU, plain FP64:
 //   * cacheElPh (interaction_elph.cpp:492-701): g1 = sum_Re e^{+i k1.Re}/deg g(Re, Rp, nu, w1, w2)
 //     and cached(Rp, nu, b1, w2) = sum_w1 U1[w1][b1] g1.  The coupling tensor is
-//     read from HBM once per 8 k1 (a batched GEMV), FP32 elements, FP64 sums.
+//     read from HBM once per 16 k1 (a batched GEMV), FP32 elements, FP64 sums.
 //   * calcCouplingSquared (:229-448, no polar term): g3 = sum_Rp e^{+i q3.Rp}/deg cached,
 //     g4 = sum_nu g3 ev3[nu][nu2], g = sum_w2 conj(U2[w2][b2]) g4, |g|^2.
 //   * ElScatteringMatrix::builder, linewidth mode (el_scattering.cpp:38-405) with
@@ -36,7 +36,7 @@ int phx_el_split_g1(phx_ctx* ctx, const uint8_t* gimg, int nRe, long long N, con
 
 namespace {
 
-constexpr int kB1 = 8;        // k1 points per pass over the coupling tensor
+constexpr int kB1 = 16;       // k1 points per pass over the coupling tensor
 constexpr int kQT = 1;        // final states per pair block
 constexpr int kMaxW = 8;      // Wannier orbitals
 constexpr int kMaxPh = 12;    // phonon branches

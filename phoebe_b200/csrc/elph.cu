@@ -164,12 +164,16 @@ __device__ inline PairSmem pair_carve(char* base, int nRp, int nph, int nw) {
 }
 
 // |g|^2 of the kQT final states whose phases, U2 (nb2 columns) and ev3 are staged;
-// cached is (nRp, nph, nw(b1), nw) of one k1 with nb1 active bands.
+// cached is (nRp, nph, nw(b1), nw) of one k1 with nb1 active bands.  G3IN:
+// g3 comes from the tensor-core GEMM (split path) instead of the FP64 Rp
+// transform; each path is its own instantiation, so that each kernel holds
+// only its code (the pair kernel is bound by instruction fetch otherwise).
+template <bool G3IN>
 __device__ void pair_couplings(const double2* __restrict__ cached, int nRp, int nph, int nw, int nb1,
                                const PairSmem& s, const float2* __restrict__ g3in = nullptr, int g3ld = 0) {
   const int tid = threadIdx.x, NT = blockDim.x;
   const int nx = nph * nb1 * nw;
-  if (g3in) {
+  if constexpr (G3IN) {
     // g3 from the tensor-core GEMM, stored g3in[x * g3ld + q] (q = phonon mesh index)
     for (int i = tid; i < kQT * nx; i += NT) {
       const int q = i % kQT, x = i / kQT;
@@ -183,7 +187,7 @@ __device__ void pair_couplings(const double2* __restrict__ cached, int nRp, int 
     }
   }
   // g3[q][nu][b1][w2] = sum_Rp ph[q][Rp] cached[Rp][nu][b1][w2]
-  for (int x = tid; x < (g3in ? 0 : nx); x += NT) {
+  for (int x = tid; x < (G3IN ? 0 : nx); x += NT) {
     const int w2 = x % nw, b1 = (x / nw) % nb1, nu = x / (nw * nb1);
     const size_t cx = ((size_t)nu * nw + b1) * nw + w2;
     double2 acc[kQT];
@@ -373,17 +377,18 @@ __device__ __forceinline__ double el_delta(const ElArgs& A, double e, const ElWi
   return exp(-x * x) / phxc::sqrtPi / sg / phxc::erf2;
 }
 
+template <bool G3IN>
 __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
   extern __shared__ __align__(16) char sraw[];
   const int nw = A.nw, nph = A.nph, nRp = A.nRp;
   // no phase buffer when g3 comes from the tensor-core GEMM
-  const PairSmem s = pair_carve(sraw, A.g3in ? 0 : nRp, nph, nw);
+  const PairSmem s = pair_carve(sraw, G3IN ? 0 : nRp, nph, nw);
   const int tid = threadIdx.x, NT = blockDim.x;
   const int nq = A.qmesh[0] * A.qmesh[1] * A.qmesh[2];
   const int jb = blockIdx.y;
   const int ik1 = A.ik1s[jb], i1 = A.i1s[jb], lo1 = A.lo[ik1], nb1 = A.hi[ik1] - lo1;
   const double2* cached = A.cached + (size_t)jb * A.cper;
-  const float2* g3in = A.g3in ? A.g3in + A.g3offs[jb] : nullptr;
+  const float2* g3in = G3IN ? A.g3in + A.g3offs[jb] : nullptr;
   const int x1 = ik1 % A.kmesh[0], y1 = (ik1 / A.kmesh[0]) % A.kmesh[1], z1 = ik1 / (A.kmesh[0] * A.kmesh[1]);
   const int f0 = A.kmesh[0] / A.qmesh[0], f1 = A.kmesh[1] / A.qmesh[1], f2 = A.kmesh[2] / A.qmesh[2];
   const double* E1 = A.Ek + (size_t)ik1 * nw + lo1;
@@ -411,7 +416,7 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
   if (!any_valid) return;
   // phases e^{+i q3.Rp}/deg with q3 = k2 - k1 (helper_el_scattering.cpp:233-234),
   // not needed when g3 comes from the tensor-core GEMM
-  for (int i = tid; i < (g3in ? 0 : kQT * nRp); i += NT) {
+  for (int i = tid; i < (G3IN ? 0 : kQT * nRp); i += NT) {
     const int q = i / nRp, r = i % nRp;
     double2 v = cmk(0.0, 0.0);
     if (s.info[4 * q]) {
@@ -487,7 +492,7 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
     s.wd[x] = wv;
   }
   __syncthreads();
-  pair_couplings(cached, nRp, nph, nw, nb1, s, g3in, A.g3ld);
+  pair_couplings<G3IN>(cached, nRp, nph, nw, nb1, s, g3in, A.g3ld);
   pair_symmetrize(E1, nb1, nph, s);
   // rates (el_scattering.cpp:268-327), one thread per (b1, q, b2, nu) with b1
   // slowest: when the kQT * kMaxW * nph entries of one b1 fill whole warps
@@ -576,7 +581,7 @@ __global__ void __launch_bounds__(kPairThreads) elph_api_pair_kernel(
     s.ev3[i] = j < nk2 ? ev3s[(size_t)j * nph * nph + i % (nph * nph)] : cmk(0.0, 0.0);
   }
   __syncthreads();
-  pair_couplings(cached, nRp, nph, nw, nb1, s);
+  pair_couplings<false>(cached, nRp, nph, nw, nb1, s);
   for (int x = tid; x < kQT * nb1 * nb2max * nph; x += NT) {
     const int nu = x % nph, b2 = (x / nph) % nb2max, b1 = (x / (nph * nb2max)) % nb1, q = x / (nph * nb2max * nb1);
     const int j = blockIdx.x * kQT + q;
@@ -943,7 +948,8 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
   size_t soff[13];
   const size_t smem = pair_smem_layout(split ? 0 : e->nRp, nph, nw, soff);
   PHX_ARG(ctx, smem <= 227 * 1024, "phx_el_linewidths: too many phonon Bravais vectors");
-  PHX_CUDA(ctx, cudaFuncSetAttribute(el_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  PHX_CUDA(ctx, cudaFuncSetAttribute(el_pair_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  PHX_CUDA(ctx, cudaFuncSetAttribute(el_pair_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int nq = ph->nq;
   const int qblocks = (nq + kQT - 1) / kQT;
   const size_t per = N;
@@ -980,7 +986,8 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
       A.g3in = dg3;
       A.g3ld = g3ld;
     }
-    el_pair_kernel<<<dim3(qblocks, nb), kPairThreads, smem, st>>>(A);
+    if (A.g3in) el_pair_kernel<true><<<dim3(qblocks, nb), kPairThreads, smem, st>>>(A);
+    else el_pair_kernel<false><<<dim3(qblocks, nb), kPairThreads, smem, st>>>(A);
     ++launches;
     pairs += (long long)nq * nb;
     PHX_CUDA(ctx, cudaGetLastError());

@@ -896,15 +896,22 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
             float2 Y[6];
 #pragma unroll
             for (int c = 0; c < 6; ++c) Y[c] = make_float2(0.f, 0.f);
+            // two rows a of X per TMEM wait
 #pragma unroll
-            for (int a = 0; a < 6; ++a) {
-              float t[12];
+            for (int a = 0; a < 6; a += 2) {
+              float t[24];
               tc::tmem_ld8(col0 + a * 12, t);
               tc::tmem_ld4(col0 + a * 12 + 8, t + 8);
+              tc::tmem_ld8(col0 + a * 12 + 12, t + 12);
+              tc::tmem_ld4(col0 + a * 12 + 20, t + 20);
+              const float2 e0 = S.E1v[(a * 6 + row) * kM + m];
+              const float2 e1 = S.E1v[((a + 1) * 6 + row) * kM + m];
               tc::tmem_wait_ld();
-              const float2 e = S.E1v[(a * 6 + row) * kM + m];
 #pragma unroll
-              for (int c = 0; c < 6; ++c) cfmaf(Y[c], e, make_float2(t[2 * c], t[2 * c + 1]));
+              for (int c = 0; c < 6; ++c) {
+                cfmaf(Y[c], e0, make_float2(t[2 * c], t[2 * c + 1]));
+                cfmaf(Y[c], e1, make_float2(t[12 + 2 * c], t[12 + 2 * c + 1]));
+              }
             }
             const unsigned cols = (((bmO0 >> row) & 1u) ? nO0 : 0u) | (((bmO1 >> row) & 1u) ? nO1 : 0u);
             unsigned UC = __reduce_or_sync(FULL, cols);

@@ -542,11 +542,12 @@ __device__ __forceinline__ Smem carve(uint8_t* base, int Kp) {
 // the hot loop within the instruction cache (14% faster than inlined).  Entry: x = |V|^2 / n1, y = lane of the q1 row | b1 << 5 | b2 << 8 |
 // b3 << 11 | degenerate flag << 14.  Flagged entries average the rate factors
 // over the degenerate blocks of b2 and b3 (one band each otherwise).
-template <int NT, bool MAT>
+template <int NT, bool MAT, int SM>
 __device__ __noinline__ void rate_entry(uint2 e, int qd, const double* En1, const float* iE1s,
                                            const float* N1, const uint4* rec, const uint4* u2,
-                                           unsigned gp2, int smearing, float ginv, float pre,
+                                           unsigned gp2, int /*smearing: SM*/, float ginv, float pre,
                                            float* qacc, const TcArgs& P, int iq2) {
+  constexpr int smearing = SM;   // each smearing has its own instantiation
   const float wn = __uint_as_float(e.x);
   const int r = e.y & 31, b1 = (e.y >> 5) & 7, b2 = (e.y >> 8) & 7, b3 = (e.y >> 11) & 7;
   const int mm = qd * 32 + r;
@@ -617,7 +618,7 @@ __device__ __noinline__ void rate_entry(uint2 e, int qd, const double* En1, cons
   for (int t = 0; t < NT; ++t) atomicAdd(&qacc[r * kAccRow + b1 * kMaxT + t], scale * g[t]);
 }
 
-template <int NT, bool MAT>
+template <int NT, bool MAT, int SM>
 __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
   const MeshArgs& M = P.m;
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -767,7 +768,7 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
     const bool valid = tile0 + m < nq;
     const int q1c = P.q1_order[min(tile0 + m, nq - 1)];
     const unsigned FULL = 0xffffffffu;
-    const int smearing = M.smearing;
+    constexpr int smearing = SM;   // one instantiation per smearing keeps the loop small
     const float sg = (float)M.sigma, ginv = M.sigma > 0.0 ? (float)(1.0 / M.sigma) : 0.f;
     // FP16 operands: |V|^2 carries the square of the B scale, undone here (power of 4)
     float pre = (float)(phxc::pi * 0.25 * 0.5) * (float)M.norm;
@@ -942,7 +943,7 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
                 qn += __popc(bal);
                 if (qn >= 32) {
                   __syncwarp();
-                  rate_entry<NT, MAT>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc, P,
+                  rate_entry<NT, MAT, SM>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc, P,
                                  iq2);
                   const uint2 rest = lane + 32 < qn ? queue[lane + 32] : make_uint2(0u, 0u);
                   __syncwarp();
@@ -962,7 +963,7 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
       if (qn) {
         __syncwarp();
         if (lane < qn)
-          rate_entry<NT, MAT>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc, P, iq2);
+          rate_entry<NT, MAT, SM>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc, P, iq2);
         qn = 0;
       }
       __syncwarp();
@@ -1075,8 +1076,16 @@ size_t pair_tc_smem(int Kp) {
 template <int NT>
 int launch_pair(phx_ctx* ctx, const TcArgs& A, int tiles, int slots) {
   const size_t smem = pair_tc_smem(A.Kp);   // attribute set by phx_split_set_attributes
-  if (A.mat.plus) pair_tc_kernel<NT, true><<<dim3(tiles, slots), kThreads, smem, ctx->stream>>>(A);
-  else pair_tc_kernel<NT, false><<<dim3(tiles, slots), kThreads, smem, ctx->stream>>>(A);
+  constexpr int ad = PHX_SMEAR_ADAPTIVE, ga = PHX_SMEAR_GAUSSIAN;
+  const bool adaptive = A.m.smearing == PHX_SMEAR_ADAPTIVE;
+  const dim3 grid(tiles, slots);
+  if (A.mat.plus) {
+    if (adaptive) pair_tc_kernel<NT, true, ad><<<grid, kThreads, smem, ctx->stream>>>(A);
+    else pair_tc_kernel<NT, true, ga><<<grid, kThreads, smem, ctx->stream>>>(A);
+  } else {
+    if (adaptive) pair_tc_kernel<NT, false, ad><<<grid, kThreads, smem, ctx->stream>>>(A);
+    else pair_tc_kernel<NT, false, ga><<<grid, kThreads, smem, ctx->stream>>>(A);
+  }
   PHX_CUDA(ctx, cudaGetLastError());
   return PHX_OK;
 }
@@ -1286,28 +1295,28 @@ size_t phx_split_smem_bytes(int nr3) { return pair_tc_smem(phx_split_kp(nr3)); }
 unsigned phx_split_edge_cap() { return 1u << 18; }
 size_t phx_split_edge_bytes() { return sizeof(EdgeEvent) * phx_split_edge_cap(); }
 
+namespace {
+template <int NT>
+int set_pair_attributes(phx_ctx* ctx, int smem) {
+  const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  constexpr int ad = PHX_SMEAR_ADAPTIVE, ga = PHX_SMEAR_GAUSSIAN;
+  PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<NT, false, ad>, a, smem));
+  PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<NT, false, ga>, a, smem));
+  PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<NT, true, ad>, a, smem));
+  PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<NT, true, ga>, a, smem));
+  return PHX_OK;
+}
+}  // namespace
+
 // Dynamic shared-memory limit of the pair kernel for nT temperatures; called
 // before any launch (and outside graph capture).
 int phx_split_set_attributes(phx_ctx* ctx, int nr3, int nT) {
   const int smem = (int)pair_tc_smem(phx_split_kp(nr3));
-  const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
   switch (nT) {
-    case 1:
-      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<1, false>, a, smem));
-      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<1, true>, a, smem));
-      break;
-    case 2:
-      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<2, false>, a, smem));
-      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<2, true>, a, smem));
-      break;
-    case 3:
-      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<3, false>, a, smem));
-      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<3, true>, a, smem));
-      break;
-    default:
-      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<4, false>, a, smem));
-      PHX_CUDA(ctx, cudaFuncSetAttribute(pair_tc_kernel<4, true>, a, smem));
-      break;
+    case 1: PHX_TRY(set_pair_attributes<1>(ctx, smem)); break;
+    case 2: PHX_TRY(set_pair_attributes<2>(ctx, smem)); break;
+    case 3: PHX_TRY(set_pair_attributes<3>(ctx, smem)); break;
+    default: PHX_TRY(set_pair_attributes<4>(ctx, smem)); break;
   }
   return PHX_OK;
 }

@@ -56,8 +56,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 // Bounded wait: polls for at most kWaitNs (checking a global abort bit every
 // 256 polls); on timeout sets *status |= code | abort bit and returns false.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status, int code) {
-  if (mbar_try_wait(bar, parity)) return true;
+// the bounded poll of mbar_wait, out of line: the waits' call sites stay a
+// few instructions each in the hot loops that use them
+static __device__ __noinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity, int* status, int code) {
   const unsigned long long t0 = globaltimer();
   for (unsigned i = 1;; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
@@ -68,6 +69,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* s
   }
   atomicOr(status, code | 0x40000000);
   return false;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status, int code) {
+  if (mbar_try_wait(bar, parity)) return true;
+  return mbar_wait_slow(bar, parity, status, code);
 }
 
 // Same bound, with a short sleep between polls: for warps whose waiting must

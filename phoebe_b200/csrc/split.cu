@@ -818,9 +818,8 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
       const int iq3 = mesh_add(q1c, iq2, n0, n1, n2);
       {
         const uint4* src = P.rec + (size_t)iq3 * kRecChunks;
-#pragma unroll
-        for (int i = 0; i < 13; ++i)
-          if (k + 3 * i < kRecChunks) cp_async16(&S.rec[(k + 3 * i) * kM + m], src + k + 3 * i);
+#pragma unroll 1
+        for (int c = k; c < kRecChunks; c += 3) cp_async16(&S.rec[c * kM + m], src + c);
         if (k == 2 && lane < kU2Chunks) {
           cp_async16(&u2[lane], P.rec + (size_t)iq2 * kRecChunks + kChBand + lane);
           cp_async16(&u2[kU2Chunks + lane], P.rec + (size_t)iq2m * kRecChunks + kChBand + lane);

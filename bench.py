@@ -37,7 +37,7 @@ FFMA_PEAK_TFLOPS = 72.0
 # mesh, q2 per launch, slots) of the launch plan; None where not captured
 PAIR_TRAFFIC_BYTES = {("split_bf16", 20, 448, 7): 87476992 + 5594112,
                       ("split_bf16", 20, 1792, 28): 337188096 + 29478400,
-                      ("split_fp16", 20, 1792, 28): 339106304 + 142633728,
+                      ("split_fp16", 20, 1792, 28): 339287552 + 177198336,
                       ("split_bf16", 16, 448, 7): 85.2e6}
 
 

@@ -50,7 +50,13 @@ typedef struct phx_elph phx_elph;
 typedef struct phx_mlp phx_mlp;
 
 /* ---- context ---------------------------------------------------------- */
-/* Replaces initKokkos / DeviceManager (src/common_kokkos.cpp:104-134,182-190). */
+/* Replaces initKokkos / DeviceManager (src/common_kokkos.cpp:104-134,182-190).
+ * One CUDA stream per context; every call on a context runs on it.  Objects
+ * (band structures, couplings, Hamiltonians) take their device memory from the
+ * device's stream-ordered pool, whose release threshold phx_ctx_create raises
+ * for this process.  phx_ctx_destroy releases the stream and the context's
+ * buffers; objects created on it may still be destroyed afterwards, but no
+ * other call may use it or them. */
 int phx_ctx_create(int device, phx_ctx** out);
 int phx_ctx_destroy(phx_ctx* ctx);
 int phx_ctx_synchronize(phx_ctx* ctx);

@@ -360,8 +360,9 @@ __device__ __forceinline__ ElWidth el_width(const ElArgs& A, const double v[3]) 
   return w;
 }
 
+template <int SM>
 __device__ __forceinline__ double el_delta(const ElArgs& A, double e, const ElWidth& w) {
-  if (A.smearing == PHX_SMEAR_GAUSSIAN) {
+  if constexpr (SM == PHX_SMEAR_GAUSSIAN) {
     const double x = e / A.sigma;
     if (x > 6.0) return 0.0;
     return 1.0 / A.sigma / phxc::sqrtPi * exp(-x * x);
@@ -377,7 +378,9 @@ __device__ __forceinline__ double el_delta(const ElArgs& A, double e, const ElWi
   return exp(-x * x) / phxc::sqrtPi / sg / phxc::erf2;
 }
 
-template <bool G3IN>
+// G3IN: g3 from the tensor-core GEMM (split path); SM: the smearing.  Each
+// combination is its own instantiation, which keeps the kernel's code small.
+template <bool G3IN, int SM>
 __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
   extern __shared__ __align__(16) char sraw[];
   const int nw = A.nw, nph = A.nph, nRp = A.nRp;
@@ -478,7 +481,7 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
     s.n3[(q * kMaxPh + nu) * pairc::kMaxT + t] = n;
   }
   // adaptive widths of the (b1, b2) pairs (delta_function.cpp:65-88)
-  for (int x = tid; x < (A.smearing == PHX_SMEAR_ADAPTIVE ? kQT * kMaxW * kMaxW : 0); x += NT) {
+  for (int x = tid; x < (SM == PHX_SMEAR_ADAPTIVE ? kQT * kMaxW * kMaxW : 0); x += NT) {
     const int b2 = x % kMaxW, b1 = (x / kMaxW) % kMaxW, q = x / (kMaxW * kMaxW);
     double2 wv = make_double2(0.0, 0.0);
     if (s.info[4 * q] && b1 < nb1 && b2 < s.info[4 * q + 1]) {
@@ -510,8 +513,8 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
       const double en1 = E1[b1], en2 = s.E2[q * kMaxW + b2];
       const double2 wv = s.wd[(q * kMaxW + b1) * kMaxW + b2];
       const ElWidth w{wv.x, wv.y != 0.0};
-      const double d1 = el_delta(A, en1 - en2 + en3, w);
-      const double d2 = el_delta(A, en1 - en2 - en3, w);
+      const double d1 = el_delta<SM>(A, en1 - en2 + en3, w);
+      const double d2 = el_delta<SM>(A, en1 - en2 - en3, w);
       if (d1 > 0.0 || d2 > 0.0) {
         const double c = s.cs[((q * kMaxW + b1) * kMaxW + b2) * nph + nu];
 #pragma unroll
@@ -948,8 +951,12 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
   size_t soff[13];
   const size_t smem = pair_smem_layout(split ? 0 : e->nRp, nph, nw, soff);
   PHX_ARG(ctx, smem <= 227 * 1024, "phx_el_linewidths: too many phonon Bravais vectors");
-  PHX_CUDA(ctx, cudaFuncSetAttribute(el_pair_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  PHX_CUDA(ctx, cudaFuncSetAttribute(el_pair_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  constexpr int ad = PHX_SMEAR_ADAPTIVE, ga = PHX_SMEAR_GAUSSIAN;
+  const cudaFuncAttribute fa = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  PHX_CUDA(ctx, cudaFuncSetAttribute(el_pair_kernel<false, ad>, fa, (int)smem));
+  PHX_CUDA(ctx, cudaFuncSetAttribute(el_pair_kernel<false, ga>, fa, (int)smem));
+  PHX_CUDA(ctx, cudaFuncSetAttribute(el_pair_kernel<true, ad>, fa, (int)smem));
+  PHX_CUDA(ctx, cudaFuncSetAttribute(el_pair_kernel<true, ga>, fa, (int)smem));
   const int nq = ph->nq;
   const int qblocks = (nq + kQT - 1) / kQT;
   const size_t per = N;
@@ -986,8 +993,15 @@ extern "C" int phx_el_linewidths(phx_elph* e, phx_bands* el, phx_bands* ph, cons
       A.g3in = dg3;
       A.g3ld = g3ld;
     }
-    if (A.g3in) el_pair_kernel<true><<<dim3(qblocks, nb), kPairThreads, smem, st>>>(A);
-    else el_pair_kernel<false><<<dim3(qblocks, nb), kPairThreads, smem, st>>>(A);
+    const dim3 grid(qblocks, nb);
+    const bool adaptive = A.smearing == PHX_SMEAR_ADAPTIVE;
+    if (A.g3in) {
+      if (adaptive) el_pair_kernel<true, ad><<<grid, kPairThreads, smem, st>>>(A);
+      else el_pair_kernel<true, ga><<<grid, kPairThreads, smem, st>>>(A);
+    } else {
+      if (adaptive) el_pair_kernel<false, ad><<<grid, kPairThreads, smem, st>>>(A);
+      else el_pair_kernel<false, ga><<<grid, kPairThreads, smem, st>>>(A);
+    }
     ++launches;
     pairs += (long long)nq * nb;
     PHX_CUDA(ctx, cudaGetLastError());

@@ -404,6 +404,32 @@ class PhScatteringMatrix {
     if (!matrix_.get()) throw Error(PHX_ERR_STATE, "symmetrize: no stored matrix");
     check(phx_smatrix_symmetrize(matrix_.get()), v3_.context());
   }
+  // ScatteringMatrix::a2Omega (src/bte/scattering.cpp:366-434); internalDiagonal / n(n+1)
+  void a2Omega() {
+    if (!matrix_.get()) throw Error(PHX_ERR_STATE, "a2Omega: no stored matrix");
+    check(phx_smatrix_a2omega(matrix_.get()), v3_.context());
+    check(phx_smatrix_diagonal(matrix_.get(), internalDiagonal_.data()), v3_.context());
+  }
+  // ScatteringMatrix::diagonalize (scattering.cpp:872-910): eigenvalues of the
+  // upper triangle, ascending; all (numEigenvalues <= 0) or the smallest
+  // numEigenvalues.  The eigenvectors replace the matrix (getRows).
+  std::vector<double> diagonalize(int numEigenvalues = 0) {
+    if (!matrix_.get()) throw Error(PHX_ERR_STATE, "diagonalize: no stored matrix");
+    std::vector<double> ev(numStates());
+    int found = 0;
+    check(phx_smatrix_diagonalize(matrix_.get(), numEigenvalues, ev.data(), &found), v3_.context());
+    ev.resize((size_t)found);
+    return ev;
+  }
+  // Theta diag(1/lambda, lambda > 0) Theta^T x, x (nvec, 3, numStates)
+  // (calcFromRelaxons, src/observable/phonon_thermal_cond.cpp:316-380)
+  std::vector<double> relaxonSolve(const std::vector<double>& x, int nvec = 1) {
+    if (!matrix_.get()) throw Error(PHX_ERR_STATE, "relaxonSolve: no stored matrix");
+    if (x.size() != (size_t)nvec * 3 * numStates()) throw Error(PHX_ERR_ARG, "relaxonSolve: bad vector size");
+    std::vector<double> y(x.size(), 0.0);
+    check(phx_smatrix_relaxon_solve(matrix_.get(), nvec, x.data(), y.data()), v3_.context());
+    return y;
+  }
   size_t numStates() const { return (size_t)bands_.getNumPoints() * bands_.getNumBands(); }
   const std::vector<double>& internalDiagonal() const { return internalDiagonal_; }
   const phx_lw_stats& stats() const { return stats_; }

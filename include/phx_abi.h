@@ -227,6 +227,29 @@ int phx_smatrix_dot_d(phx_smatrix* m, int nvec, const double* x_d, int off_diago
 /* A -> (A + A^T) / 2 in place (ScatteringMatrix::symmetrize, src/bte/scattering.cpp:1149-1166;
  * the reference's symmetrizeMatrix option before its exact solvers). */
 int phx_smatrix_symmetrize(phx_smatrix* m);
+/* Relaxons (src/apps/phonon_transport_app.cpp:386-420).
+ * ScatteringMatrix::a2Omega (src/bte/scattering.cpp:366-434): in place,
+ * A(i, j) /= sqrt(n_i(n_i+1) n_j(n_j+1)) for included states i, j, and the
+ * diagonal returned by phx_smatrix_diagonal /= n_i(n_i+1).  A second call does
+ * nothing.  Products (phx_smatrix_dot) are refused afterwards (PHX_ERR_STATE). */
+int phx_smatrix_a2omega(phx_smatrix* m);
+/* ScatteringMatrix::diagonalize (scattering.cpp:872-910; ParallelMatrix
+ * ::diagonalize, src/algebra/PMatrix.cpp:99-160 and 266-404): eigenvalues and
+ * eigenvectors of the symmetric matrix read from its UPPER triangle (uplo 'U'),
+ * computed in place: as in the reference, the matrix is destroyed.
+ * num_eigenvalues <= 0 or = ns: all of them; else the smallest num_eigenvalues.
+ * eigenvalues: (ns) host, ascending; *num_found: how many were computed.
+ * Afterwards phx_smatrix_get_rows returns rows of the eigenvector matrix
+ * Theta(s, alpha), columns alpha < *num_found.  More eigenvalues than states:
+ * PHX_ERR_ARG; a solver failure to converge: PHX_ERR_NOCONV. */
+int phx_smatrix_diagonalize(phx_smatrix* m, int num_eigenvalues, double* eigenvalues, int* num_found);
+/* The relaxon-basis solve of PhononThermalConductivity::calcFromRelaxons
+ * without symmetries (src/observable/phonon_thermal_cond.cpp:316-380):
+ * y = Theta diag(g) Theta^T x, g_alpha = 1/lambda_alpha for the computed
+ * eigenvalues lambda_alpha > 0 and 0 otherwise; x and y (nvec, 3, ns) host.
+ * With x = dn/dT v / sqrt(n(n+1)) this gives the relaxon population before
+ * the reference's final sqrt(n(n+1)) rescaling. */
+int phx_smatrix_relaxon_solve(phx_smatrix* m, int nvec, const double* x, double* y);
 int phx_smatrix_destroy(phx_smatrix* m);
 
 /* PhScatteringMatrix::builder with switchCase 1 (ScatteringMatrix::dot when the

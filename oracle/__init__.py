@@ -266,6 +266,66 @@ def smatrix_dot(mat, E, x, off_diagonal=False):
     return y
 
 
+# src/constants/constants.h: 0.1 cm^-1 in Ry, the phonon exclusion cut-off (scattering.cpp:37)
+_TERAHERTZ_AU = 6.62607015e-34 / (2.0 * np.pi) / 4.359744650e-18 * 1.0e12
+_RY_TO_CMM1 = 1.0e10 * (1.0 / _TERAHERTZ_AU / 2.0 / (2.0 * np.pi)) / 299792458.0
+_PH_EXCLUDE_CUTOFF = 0.1 / _RY_TO_CMM1
+
+
+def _poppm1(E, T):
+    x = np.sinh(np.asarray(E, dtype=np.float64) / 2.0 / T)
+    return 0.25 / x / x
+
+
+def a2omega(mat, diag, E, T):
+    """ScatteringMatrix::a2Omega (src/bte/scattering.cpp:366-434), without
+    symmetries: for states i, j both outside excludeIndices (E < 0.1 cm^-1,
+    :30-41), mat[i, j] /= sqrt(term_i term_j) and diag[i] /= term_i, term the
+    n(n+1) of Particle::getPopPopPm1.  Returns copies."""
+    mat = np.array(mat, dtype=np.float64, copy=True)
+    diag = np.array(diag, dtype=np.float64, copy=True).ravel()
+    E = np.asarray(E, dtype=np.float64).ravel()
+    keep = E >= _PH_EXCLUDE_CUTOFF
+    with np.errstate(divide="ignore", over="ignore", invalid="ignore"):
+        term = _poppm1(E, T)
+    idx = np.flatnonzero(keep)
+    mat[np.ix_(idx, idx)] /= np.sqrt(np.outer(term[idx], term[idx]))
+    diag[idx] /= term[idx]
+    return mat, diag
+
+
+def relaxons(mat, E, vg, T, num_q, volume, num_eigenvalues=0):
+    """The relaxon solver without symmetries (src/apps/phonon_transport_app.cpp:
+    386-420) on a stored matrix A (already a2omega'd): eigenvalues of the upper
+    triangle, all or the smallest num_eigenvalues (ParallelMatrix::diagonalize,
+    src/algebra/PMatrix.cpp:99-160, 266-404, uplo 'U'; LAPACK here), then
+    PhononThermalConductivity::calcFromRelaxons (src/observable/
+    phonon_thermal_cond.cpp:316-445):
+        relaxonsPopulation(a, i) = sum_s [lambda_a > 0, E_s > 0]
+                                   dndt_s / sqrt(term_s) v_si theta(s, a) / lambda_a
+        population(i, s) = sum_a theta(s, a) relaxonsPopulation(a, i),
+        times sqrt(term_s) where E_s > 0, then calcFromPopulation
+    (:64-113; excluded states left out).  Returns (eigenvalues, eigenvectors, kappa (3, 3))."""
+    E = np.asarray(E, dtype=np.float64).ravel()
+    vg = np.asarray(vg, dtype=np.float64).reshape(-1, 3)
+    lam, theta = np.linalg.eigh(np.asarray(mat, dtype=np.float64), UPLO="U")
+    if 0 < num_eigenvalues < E.size:
+        lam, theta = lam[:num_eigenvalues], theta[:, :num_eigenvalues]
+    with np.errstate(divide="ignore", over="ignore", invalid="ignore"):
+        term = _poppm1(E, T)
+        dndt = term * E / T / T
+        w = np.where((E > 0.0)[:, None], (dndt / np.sqrt(term))[:, None] * vg, 0.0)    # (ns, 3)
+    good = lam > 0.0
+    rpop = np.zeros((lam.size, 3))
+    rpop[good] = (theta[:, good].T @ w) / lam[good][:, None]
+    pop = theta[:, good] @ rpop[good]                                               # (ns, 3)
+    with np.errstate(invalid="ignore"):
+        pop = np.where((E > 0.0)[:, None], pop * np.sqrt(np.where(E > 0.0, term, 1.0))[:, None], pop)
+    keep = E >= _PH_EXCLUDE_CUTOFF
+    kappa = np.einsum("si,sj,s->ij", pop[keep], vg[keep], E[keep]) / float(num_q) / float(volume)
+    return lam, theta, kappa
+
+
 def symmetrize_coupling(c, e1, e2, e3):
     c = _d(c).copy()
     nb1, nb2, nb3 = c.shape

@@ -90,6 +90,9 @@ SIGNATURES = {
     "phx_smatrix_dot_d": [_VP, _i, _VP, _i, _VP, ctypes.POINTER(ctypes.c_float)],
     "phx_smatrix_destroy": [_VP],
     "phx_smatrix_symmetrize": [_VP],
+    "phx_smatrix_a2omega": [_VP],
+    "phx_smatrix_diagonalize": [_VP, _i, _D, ctypes.POINTER(_i)],
+    "phx_smatrix_relaxon_solve": [_VP, _i, _D, _D],
     "phx_ph_smatrix_dot": [_VP, _VP, ctypes.POINTER(LwParams), _i, _D, _D, ctypes.POINTER(LwStats)],
     "phx_ph_smatrix_dot_d": [_VP, _VP, ctypes.POINTER(LwParams), _i, _VP, _VP, ctypes.POINTER(LwStats)],
     "phx_el_h0_create": [_VP, _i, _i, _D, _D, _D, _D, ctypes.POINTER(_VP)],

@@ -437,6 +437,45 @@ class PhScatteringMatrix:
             raise RuntimeError("the matrix is stored only with in_memory=True, after setup()")
         check(_abi.load().phx_smatrix_symmetrize(self._m), self.v3.ctx.h)
 
+    def _stored(self):
+        if self._m is None:
+            raise RuntimeError("the matrix is stored only with in_memory=True, after setup()")
+        return self._m
+
+    def a2Omega(self):
+        """ScatteringMatrix::a2Omega (scattering.cpp:366-434) in device memory:
+        A(i, j) / sqrt(n_i(n_i+1) n_j(n_j+1)); internalDiagonal / n(n+1)."""
+        L = _abi.load()
+        check(L.phx_smatrix_a2omega(self._stored()), self.v3.ctx.h)
+        diag = np.zeros((1, self.num_states))
+        check(L.phx_smatrix_diagonal(self._m, dptr(diag)), self.v3.ctx.h)
+        self.internalDiagonal = diag
+
+    def diagonalize(self, numEigenvalues=0):
+        """ScatteringMatrix::diagonalize (scattering.cpp:872-910): eigenvalues
+        (ascending) of the matrix's upper triangle, all of them or the
+        smallest numEigenvalues; the eigenvectors replace the matrix in device
+        memory (getMatrixRows then returns their rows)."""
+        ev = np.zeros(self.num_states)
+        found = ctypes.c_int(0)
+        check(_abi.load().phx_smatrix_diagonalize(self._stored(), int(numEigenvalues), dptr(ev),
+                                                  ctypes.byref(found)), self.v3.ctx.h)
+        self.eigenvalues = ev[:found.value].copy()
+        return self.eigenvalues
+
+    def relaxonSolve(self, x):
+        """Theta diag(1/lambda, lambda > 0) Theta^T x for x (3, ns) or
+        (nvec, 3, ns), after diagonalize() (calcFromRelaxons,
+        phonon_thermal_cond.cpp:316-380)."""
+        x = f64(x)
+        single = x.ndim == 2
+        x = x[None] if single else x
+        if x.shape[1:] != (3, self.num_states):
+            raise ValueError("vectors must be (3, numStates) or (nvec, 3, numStates)")
+        y = np.zeros_like(x)
+        check(_abi.load().phx_smatrix_relaxon_solve(self._stored(), x.shape[0], dptr(x), dptr(y)), self.v3.ctx.h)
+        return y[0] if single else y
+
     def close(self):
         if getattr(self, "_m", None) is not None:
             _abi.load().phx_smatrix_destroy(self._m)

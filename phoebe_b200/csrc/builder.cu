@@ -2064,6 +2064,7 @@ extern "C" int phx_ph_smatrix_create(phx_v3* v, phx_bands* b, const phx_lw_param
   m->nb = b->nb;
   m->ns = (int)ns;
   for (int i = 0; i < 3; ++i) m->mesh[i] = b->mesh[i];
+  m->temperature = p->temperatures[0];
   cudaError_t e = cudaMalloc(&m->d_A, sizeof(double) * ns * ns);
   if (e == cudaSuccess) e = cudaMalloc(&m->d_E, sizeof(double) * ns);
   if (e == cudaSuccess) e = cudaMalloc(&m->d_diag, sizeof(double) * ns);

@@ -170,6 +170,10 @@ struct phx_smatrix {
   double* d_diag = nullptr;   // (ns) the diagonal: linewidths x n(n+1), not averaged
   double* d_xy = nullptr;     // staging of x and y for phx_smatrix_dot
   size_t xy_bytes = 0;
+  double temperature = 0.0;   // Ry, the matrix's one temperature
+  int omega = 0;              // 1: scaled to Omega (phx_smatrix_a2omega)
+  int num_eig = -1;           // >= 0: d_A holds that many eigenvectors (phx_smatrix_diagonalize)
+  double* d_W = nullptr;      // (ns) eigenvalues, ascending
 };
 
 // y += (block of a scattering matrix) x, for x and y (nvec, nT, 3, ns) on the device.
@@ -188,7 +192,7 @@ struct phx_dot_args {
   double* y;
   // skip = 0: the element whose column state is the row state is left out
   // (the off-diagonal part); 1: rows and columns of excluded states are left
-  // out (ScatteringMatrix::dot of a stored matrix)
+  // out (ScatteringMatrix::dot of a stored matrix); 2: nothing left out
   int skip;
   const double* E;         // (ns), for skip = 1
 };

@@ -14,7 +14,10 @@
 // vector component at the end.  One input vector (the iterative solvers'
 // case) has its own instantiation, whose 3 accumulators leave room for 8
 // loads in flight per thread; more vectors go 4 per pass.
+#include <cusolverDn.h>
+
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "pair_common.cuh"
@@ -179,11 +182,104 @@ __global__ void symmetrize_kernel(int ns, long long ld, double* __restrict__ A) 
   }
 }
 
+// n(n+1) of each state at temperature T (Particle::getPopPopPm1 for phonons,
+// src/particle.cpp), 0 for the excluded states (E < 0.1 cm^-1)
+__global__ void poppm1_kernel(int ns, const double* __restrict__ E, double T, double* __restrict__ term) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  const double e = E[s];
+  if (e < phxc::phExcludeCutoff) {
+    term[s] = 0.0;
+    return;
+  }
+  const double x = sinh(e / (2.0 * T));
+  term[s] = 0.25 / (x * x);
+}
+
+// ScatteringMatrix::a2Omega (src/bte/scattering.cpp:366-434): A(i, j) /=
+// sqrt(n_i(n_i+1) n_j(n_j+1)) unless i or j is excluded, and the diagonal
+// (the linewidths) /= n_i(n_i+1).  Threads down a column (coalesced), CTAs
+// over row blocks x a stride of columns.
+__global__ void __launch_bounds__(256) a2omega_kernel(int ns, long long ld, const double* __restrict__ term,
+                                                       double* __restrict__ A, double* __restrict__ diag) {
+  const int r = blockIdx.x * 256 + threadIdx.x;
+  if (r >= ns) return;
+  const double tr = term[r];
+  if (blockIdx.y == 0 && tr != 0.0) diag[r] /= tr;
+  if (tr == 0.0) return;
+  for (int c = blockIdx.y; c < ns; c += gridDim.y) {
+    const double tc = term[c];
+    if (tc != 0.0) A[(size_t)c * ld + r] /= sqrt(tr * tc);
+  }
+}
+
+// The relaxon populations of calcFromRelaxons (src/observable/
+// phonon_thermal_cond.cpp:316-347): r(v, i, a) = g_a sum_s Theta(s, a) x(v, i, s),
+// g_a = 1/lambda_a for lambda_a > 0, else 0.  One CTA per eigenvector a (a
+// coalesced read of its column), x (nvec, 3, ns) from L2.
+__global__ void __launch_bounds__(256) relaxon_project_kernel(int ns, long long ld, const double* __restrict__ Th,
+                                                               const double* __restrict__ W, int nvec,
+                                                               const double* __restrict__ x, double* __restrict__ r) {
+  const int a = blockIdx.x;
+  const double lam = W[a];
+  const double* col = Th + (size_t)a * ld;
+  __shared__ double red[8][3];
+  for (int v = 0; v < nvec; ++v) {
+    const double* xv = x + (size_t)v * 3 * ns;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int s = threadIdx.x; s < ns; s += 256) {
+      const double t = col[s];
+      s0 += t * xv[s];
+      s1 += t * xv[ns + s];
+      s2 += t * xv[2 * ns + s];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+      red[w][0] = s0;
+      red[w][1] = s1;
+      red[w][2] = s2;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+      double t = 0.0;
+      for (int k = 0; k < 8; ++k) t += red[k][threadIdx.x];
+      r[((size_t)v * 3 + threadIdx.x) * ns + a] = lam > 0.0 ? t / lam : 0.0;
+    }
+    __syncthreads();
+  }
+}
+
+// cuSOLVER objects and buffers of one eigensolve, released on every path
+struct EigScratch {
+  cusolverDnHandle_t h = nullptr;
+  cusolverDnParams_t prm = nullptr;
+  void* dwork = nullptr;
+  void* hwork = nullptr;
+  int* dinfo = nullptr;
+  ~EigScratch() {
+    cudaFree(dwork);
+    cudaFree(dinfo);
+    std::free(hwork);
+    if (prm) cusolverDnDestroyParams(prm);
+    if (h) cusolverDnDestroy(h);
+  }
+};
+
 }  // namespace
 
 extern "C" int phx_smatrix_symmetrize(phx_smatrix* m) {
   PHX_ARG(nullptr, m, "phx_smatrix_symmetrize: null handle");
   phx_ctx* ctx = m->ctx;
+  if (m->num_eig >= 0) {
+    phx_set_error(ctx, PHX_ERR_STATE, "phx_smatrix_symmetrize: the matrix was diagonalized in place");
+    return PHX_ERR_STATE;
+  }
   PHX_CUDA(ctx, cudaSetDevice(ctx->device));
   const int t = (m->ns + 31) / 32;
   symmetrize_kernel<<<dim3(t, t), dim3(32, 8), 0, ctx->stream>>>(m->ns, m->ns, m->d_A);
@@ -243,6 +339,12 @@ extern "C" int phx_smatrix_dot_d(phx_smatrix* m, int nvec, const double* x_d, in
                                  float* ms) {
   PHX_ARG(nullptr, m && x_d && y_d && nvec >= 1, "phx_smatrix_dot: bad arguments");
   phx_ctx* ctx = m->ctx;
+  if (m->num_eig >= 0 || m->omega) {
+    phx_set_error(ctx, PHX_ERR_STATE,
+                  m->num_eig >= 0 ? "phx_smatrix_dot: the matrix was diagonalized in place"
+                                  : "phx_smatrix_dot: the matrix is scaled to Omega");
+    return PHX_ERR_STATE;
+  }
   PHX_CUDA(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -303,9 +405,148 @@ extern "C" int phx_smatrix_dot(phx_smatrix* m, int nvec, const double* x, int of
   return PHX_OK;
 }
 
+extern "C" int phx_smatrix_a2omega(phx_smatrix* m) {
+  PHX_ARG(nullptr, m, "phx_smatrix_a2omega: null handle");
+  phx_ctx* ctx = m->ctx;
+  if (m->num_eig >= 0) {
+    phx_set_error(ctx, PHX_ERR_STATE, "phx_smatrix_a2omega: the matrix was diagonalized in place");
+    return PHX_ERR_STATE;
+  }
+  if (m->omega) return PHX_OK;   // already scaled, as the reference's isMatrixOmega
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const int ns = m->ns;
+  double* term = nullptr;
+  PHX_CUDA(ctx, phx_dev_alloc(ctx, (void**)&term, sizeof(double) * ns));
+  poppm1_kernel<<<(ns + 255) / 256, 256, 0, st>>>(ns, m->d_E, m->temperature, term);
+  a2omega_kernel<<<dim3((ns + 255) / 256, std::min(ns, 2048)), 256, 0, st>>>(ns, ns, term, m->d_A, m->d_diag);
+  const cudaError_t e = cudaGetLastError();
+  phx_dev_free(ctx, term);
+  PHX_CUDA(ctx, e);
+  PHX_CUDA(ctx, cudaStreamSynchronize(st));
+  m->omega = 1;
+  return PHX_OK;
+}
+
+extern "C" int phx_smatrix_diagonalize(phx_smatrix* m, int num_eigenvalues, double* eigenvalues, int* num_found) {
+  PHX_ARG(nullptr, m && eigenvalues && num_found, "phx_smatrix_diagonalize: bad arguments");
+  phx_ctx* ctx = m->ctx;
+  const int ns = m->ns;
+  PHX_ARG(ctx, num_eigenvalues <= ns,
+          "You have requested to calculate more relaxons eigenvalues than your number of particle states.");
+  if (m->num_eig >= 0) {
+    phx_set_error(ctx, PHX_ERR_STATE, "phx_smatrix_diagonalize: the matrix was diagonalized already");
+    return PHX_ERR_STATE;
+  }
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  if (!m->d_W) PHX_CUDA(ctx, cudaMalloc(&m->d_W, sizeof(double) * ns));
+  PHX_CUDA(ctx, cudaMemsetAsync(m->d_W, 0, sizeof(double) * ns, st));
+  EigScratch z;
+  auto solver = [&](cusolverStatus_t s, const char* what) {
+    if (s == CUSOLVER_STATUS_SUCCESS) return PHX_OK;
+    phx_set_error(ctx, PHX_ERR_CUDA, std::string("phx_smatrix_diagonalize: ") + what + " failed (cusolver status " +
+                                         std::to_string((int)s) + ")");
+    return PHX_ERR_CUDA;
+  };
+  PHX_TRY(solver(cusolverDnCreate(&z.h), "cusolverDnCreate"));
+  PHX_TRY(solver(cusolverDnSetStream(z.h, st), "cusolverDnSetStream"));
+  PHX_TRY(solver(cusolverDnCreateParams(&z.prm), "cusolverDnCreateParams"));
+  // the upper triangle, as the reference's pdsyevd / pdsyevr with uplo = 'U'
+  const cublasFillMode_t uplo = CUBLAS_FILL_MODE_UPPER;
+  const cusolverEigMode_t jobz = CUSOLVER_EIG_MODE_VECTOR;
+  const bool some = num_eigenvalues > 0 && num_eigenvalues != ns;
+  double vl = -1.0, vu = 0.0;
+  int64_t meig = ns;
+  size_t dws = 0, hws = 0;
+  if (some)
+    PHX_TRY(solver(cusolverDnXsyevdx_bufferSize(z.h, z.prm, jobz, CUSOLVER_EIG_RANGE_I, uplo, ns, CUDA_R_64F, m->d_A,
+                                                ns, &vl, &vu, 1, num_eigenvalues, &meig, CUDA_R_64F, m->d_W,
+                                                CUDA_R_64F, &dws, &hws),
+                   "cusolverDnXsyevdx_bufferSize"));
+  else
+    PHX_TRY(solver(cusolverDnXsyevd_bufferSize(z.h, z.prm, jobz, uplo, ns, CUDA_R_64F, m->d_A, ns, CUDA_R_64F, m->d_W,
+                                               CUDA_R_64F, &dws, &hws),
+                   "cusolverDnXsyevd_bufferSize"));
+  PHX_CUDA(ctx, cudaMalloc(&z.dwork, std::max<size_t>(dws, 8)));
+  PHX_CUDA(ctx, cudaMalloc(&z.dinfo, sizeof(int)));
+  z.hwork = std::malloc(std::max<size_t>(hws, 8));
+  PHX_ARG(ctx, z.hwork, "phx_smatrix_diagonalize: host workspace allocation failed");
+  if (some)
+    PHX_TRY(solver(cusolverDnXsyevdx(z.h, z.prm, jobz, CUSOLVER_EIG_RANGE_I, uplo, ns, CUDA_R_64F, m->d_A, ns, &vl, &vu,
+                                     1, num_eigenvalues, &meig, CUDA_R_64F, m->d_W, CUDA_R_64F, z.dwork, dws, z.hwork,
+                                     hws, z.dinfo),
+                   "cusolverDnXsyevdx"));
+  else
+    PHX_TRY(solver(cusolverDnXsyevd(z.h, z.prm, jobz, uplo, ns, CUDA_R_64F, m->d_A, ns, CUDA_R_64F, m->d_W,
+                                    CUDA_R_64F, z.dwork, dws, z.hwork, hws, z.dinfo),
+                   "cusolverDnXsyevd"));
+  int info = 0;
+  PHX_CUDA(ctx, cudaMemcpyAsync(&info, z.dinfo, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PHX_CUDA(ctx, cudaStreamSynchronize(st));
+  // the matrix is overwritten from here on, whatever the outcome
+  m->num_eig = 0;
+  if (info != 0) {
+    phx_set_error(ctx, info > 0 ? PHX_ERR_NOCONV : PHX_ERR_ARG,
+                  "phx_smatrix_diagonalize: eigensolver info = " + std::to_string(info));
+    return info > 0 ? PHX_ERR_NOCONV : PHX_ERR_ARG;
+  }
+  m->num_eig = (int)meig;
+  PHX_CUDA(ctx, cudaMemcpyAsync(eigenvalues, m->d_W, sizeof(double) * meig, cudaMemcpyDeviceToHost, st));
+  PHX_CUDA(ctx, cudaStreamSynchronize(st));
+  *num_found = (int)meig;
+  return PHX_OK;
+}
+
+extern "C" int phx_smatrix_relaxon_solve(phx_smatrix* m, int nvec, const double* x, double* y) {
+  PHX_ARG(nullptr, m && x && y && nvec >= 1, "phx_smatrix_relaxon_solve: bad arguments");
+  phx_ctx* ctx = m->ctx;
+  if (m->num_eig < 0) {
+    phx_set_error(ctx, PHX_ERR_STATE, "phx_smatrix_relaxon_solve called before phx_smatrix_diagonalize");
+    return PHX_ERR_STATE;
+  }
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const int ns = m->ns;
+  const size_t n = (size_t)nvec * 3 * ns;
+  double* d = nullptr;   // x, the relaxon populations, y
+  PHX_CUDA(ctx, phx_dev_alloc(ctx, (void**)&d, 3 * n * sizeof(double)));
+  double *xd = d, *rd = d + n, *yd = d + 2 * n;
+  cudaError_t e = cudaMemcpyAsync(xd, x, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(rd, 0, 2 * n * sizeof(double), st);
+  int rc = PHX_OK;
+  if (e == cudaSuccess && m->num_eig > 0) {
+    relaxon_project_kernel<<<m->num_eig, 256, 0, st>>>(ns, ns, m->d_A, m->d_W, nvec, xd, rd);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) {
+      // back to the states: y = Theta r over the computed eigenvectors (:350-380)
+      phx_dot_args a{};
+      a.ns = ns;
+      a.ncols = m->num_eig;
+      a.ld = ns;
+      a.Sp = m->d_A;
+      a.nb = m->nb;
+      a.nT = 1;
+      a.nvec = nvec;
+      a.x = rd;
+      a.y = yd;
+      a.skip = 2;
+      a.E = m->d_E;
+      rc = phx_smatrix_dot_launch(a, st, nullptr);
+    }
+  }
+  if (e == cudaSuccess && rc == PHX_OK) e = cudaMemcpyAsync(y, yd, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  phx_dev_free(ctx, d);
+  PHX_CUDA(ctx, e);
+  if (rc != PHX_OK) phx_set_error(ctx, rc, "phx_smatrix_relaxon_solve: launch failed");
+  return rc;
+}
+
 extern "C" int phx_smatrix_destroy(phx_smatrix* m) {
   if (!m) return PHX_OK;
   if (m->ctx) cudaSetDevice(m->ctx->device);
+  cudaFree(m->d_W);
   cudaFree(m->d_A);
   cudaFree(m->d_E);
   cudaFree(m->d_diag);

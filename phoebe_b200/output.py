@@ -7,8 +7,10 @@
     the temperatures (K), the wavevectors in lattice coordinates;
   * thermal_conductivity_json: PhononThermalConductivity::outputToJSON
     (src/observable/phonon_thermal_cond.cpp:475-505), the files
-    rta_phonon_thermal_cond.json, omini_phonon_thermal_cond.json and
-    variational_phonon_thermal_cond.json.
+    rta_phonon_thermal_cond.json, omini_phonon_thermal_cond.json,
+    variational_phonon_thermal_cond.json and relaxons_phonon_thermal_cond.json;
+  * relaxons_relaxation_times_json: ScatteringMatrix::relaxonsToJSON
+    (src/bte/scattering.cpp:816-870), relaxons_relaxation_times.json.
 
 Non-finite numbers (the relaxation time of an excluded state is n(n+1)/0)
 are written as null, as nlohmann::json does; the layout is indented by 3 like
@@ -62,6 +64,29 @@ def relaxation_times_json(path, crystal, mesh, E, vg, A_out, temperatures_ry):
         "energyUnit": "meV",
         "wavevectorCoordinates": _clean(coords.tolist()),
         "coordsType": "lattice",
+        "particleType": "phonon",
+    }
+    with open(path, "w") as f:
+        json.dump(out, f, indent=3, sort_keys=True, allow_nan=False)
+        f.write("\n")
+    return out
+
+
+def relaxons_relaxation_times_json(path, eigenvalues, temperatures_ry):
+    """ScatteringMatrix::relaxonsToJSON (src/bte/scattering.cpp:816-870), the
+    file relaxons_relaxation_times.json: the relaxon times 1/lambda of every
+    eigenvalue, in fs, once per temperature (the reference writes the same
+    list for each; a zero eigenvalue gives null)."""
+    T = np.atleast_1d(np.asarray(temperatures_ry, dtype=np.float64))
+    lam = np.asarray(eigenvalues, dtype=np.float64).ravel()
+    with np.errstate(divide="ignore"):
+        times = (1.0 / lam) * C.energyRyToFs
+    out = {
+        "temperatures": [float(t * C.temperatureAuToSi) for t in T],
+        "temperatureUnit": "K",
+        "chemicalPotentials": [0.0] * len(T),
+        "relaxationTimes": _clean([times.tolist() for _ in T]),
+        "relaxationTimeUnit": "fs",
         "particleType": "phonon",
     }
     with open(path, "w") as f:

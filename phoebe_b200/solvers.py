@@ -154,6 +154,27 @@ def variational(problem, diagonal, dot, threshold=1e-5, max_iter=50):
     raise BteNotConverged("Reached max BTE iterations without convergence", history)
 
 
+def relaxons(problem, relaxon_solve):
+    """Relaxon conductivity without symmetries (PhononThermalConductivity::
+    calcFromRelaxons, phonon_thermal_cond.cpp:242-445; the reference allows
+    one temperature, the first).  relaxon_solve(x) = Theta diag(1/lambda+)
+    Theta^T x for x (3, ns), Theta and lambda the eigenvectors and eigenvalues
+    of Omega = a2Omega(A).  States with E > 0 take part, as in the reference:
+    x = dn/dT v / sqrt(n(n+1)), and the result is rescaled by sqrt(n(n+1)) before
+    calcFromPopulation.  Returns kappa (1, 3, 3)."""
+    P = problem
+    T = P.T[0]
+    term = P.popterm[0]
+    pos = P.E > 0.0
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        root = np.sqrt(term)
+        dndt = term * P.E / T / T                                        # Particle::getDndt
+        x = np.where(pos[None, :], (dndt / root)[None, :] * P.vg.T, 0.0)  # (3, ns)
+    pop = relaxon_solve(x)
+    pop = np.where(pos[None, :], pop * np.where(pos, root, 1.0)[None, :], pop)
+    return P.kappa_from_population(pop[None])
+
+
 def exact(problem, matrix):
     """Direct solve of A f = b on the included states (no reference
     counterpart; the fixed point both solvers approach), kappa from f."""

@@ -135,6 +135,10 @@ int main(int argc, char** argv) {
       save("smatrix_offdot.f64", mem.offDiagonalDot(x0));
       mem.symmetrize();
       save("smatrix_sym_rows.f64", mem.getRows(3, 5));
+      mem.a2Omega();
+      save("omega_diag.f64", mem.internalDiagonal());
+      save("relaxon_eigenvalues.f64", mem.diagonalize());
+      save("relaxon_solve.f64", mem.relaxonSolve(x0));
       phx::PhScatteringMatrix freeSm(v3, bands, temps, phx::Smearing::adaptive);
       save("smatrix_free_dot.f64", freeSm.dot(x));
     }

@@ -174,6 +174,14 @@ def test_shim_matches_python_mirror(ctx, diamond, tmp_path):
                                atol=1e-14 * np.abs(yo).max())
     mem.symmetrize()
     np.testing.assert_array_equal(_r(out, "smatrix_sym_rows.f64", np.float64), mem.getMatrixRows(3, 5).ravel())
+    mem.a2Omega()
+    np.testing.assert_array_equal(_r(out, "omega_diag.f64", np.float64), mem.internalDiagonal.ravel())
+    lam = mem.diagonalize()
+    np.testing.assert_allclose(_r(out, "relaxon_eigenvalues.f64", np.float64), lam, rtol=0,
+                               atol=1e-12 * np.abs(lam).max())
+    yr = mem.relaxonSolve(xs[0])
+    np.testing.assert_allclose(_r(out, "relaxon_solve.f64", np.float64), yr.ravel(), rtol=0,
+                               atol=1e-10 * np.abs(yr).max())
     mem.close()
     yf = PhScatteringMatrix(v3, bands, temps, "adaptive").dot(xs)
     np.testing.assert_allclose(_r(out, "smatrix_free_dot.f64", np.float64), yf.ravel(), rtol=1e-12,

@@ -47,13 +47,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="3ph", choices=["3ph", "elph", "smatrix", "perovskite"],
+    ap.add_argument("--workload", default="3ph", choices=["3ph", "elph", "smatrix", "perovskite", "relaxons"],
                     help="3ph: the headline linewidth builder; elph: electron-phonon linewidths "
                          "(8 Wannier functions, 343 x 343 coupling vectors, 40^3 k, 20^3 q); smatrix: "
                          "the scattering matrix of the 3ph workload stored in device memory and its "
                          "matrix-vector products, beside the matrix-free product; perovskite: the batched "
                          "uneven instances (5-atom cell, 15 branches, 24^3 mesh, per-q1 q2 window) on a q2 "
-                         "slice of --q2-slice points per step")
+                         "slice of --q2-slice points per step; relaxons: the relaxon solver (a2Omega, full "
+                         "eigensolve, relaxon conductivity) on the stored matrix of the 3ph workload at --mesh")
     ap.add_argument("--q2-slice", type=int, default=256, help="q2 points per perovskite step")
     ap.add_argument("--elph-k1", type=int, default=64, help="outer k points timed per elph step")
     ap.add_argument("--precision", default=os.environ.get("PHX_BENCH_PRECISION", "split_fp16"),
@@ -528,6 +529,51 @@ def run_smatrix(args):
     sm.close()
 
 
+def run_relaxons(args):
+    """Relaxon solver on the stored FP64 matrix of the 3ph workload (one temperature, boundary
+    scattering of 3e4 Bohr): a2Omega in device memory, the eigensolve of all ns x ns
+    (cuSOLVER, in place), then the relaxon conductivity.  One pass (the eigensolve destroys the
+    matrix); each stage is a synchronous library call, timed by the host clock around it."""
+    import torch
+    from phoebe_b200 import constants as C
+    from phoebe_b200 import lattice, solvers
+    from phoebe_b200.core import Context, Interaction3Ph, PhononH0, PhScatteringMatrix
+    cr, fc2, fc3, mesh = workload(args.mesh)
+    torch.cuda.set_device(0)
+    ctx = Context(0)
+    h0 = PhononH0(ctx, cr, fc2)
+    bands = h0.populate(mesh, withVelocities=True)
+    E, _, vg = bands.get()
+    v3 = Interaction3Ph(ctx, cr, fc3)
+    T = C.kelvin_to_ry(300.0)
+    ns = bands.nq * bands.nb
+    P = solvers.BteProblem(E, vg, [T], int(np.prod(mesh)), lattice.calc_volume(cr.direct_cell))
+    sm = PhScatteringMatrix(v3, bands, [T], "adaptive", boundary_length=3.0e4, in_memory=True)
+    with Clocks(0) as clk:
+        sm.setup()
+        ms_build = sm.stats.ms_total
+        t0 = time.perf_counter()
+        sm.a2Omega()
+        t1 = time.perf_counter()
+        lam = sm.diagonalize(0)
+        t2 = time.perf_counter()
+        kappa = solvers.relaxons(P, sm.relaxonSolve)[0]
+        t3 = time.perf_counter()
+    total = t3 - t0
+    line = {"metric": "relaxon solver wall time after the matrix build, diamond %d^3, %d states" % (args.mesh, ns),
+            "value": total, "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": 1000.0 * total,
+            "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "diamond %dx%dx%d, 400 FC3 pairs, adaptive smearing, boundary 3e4 Bohr, 300 K; "
+                                   "matrix %d x %d FP64 (%.2f GB) in device memory" % (*mesh, ns, ns,
+                                                                                        8e-9 * ns * ns)},
+            "matrix_build_ms": ms_build, "a2omega_s": t1 - t0, "eigensolve_s": t2 - t1,
+            "relaxon_kappa_s": t3 - t2, "positive_eigenvalues": int((lam > 0).sum()),
+            "kappa_diag_au": np.diagonal(kappa).tolist(), "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    sm.close()
+
+
 def run_perovskite(args):
     """Batched uneven instances (the 15-branch perovskite cell on the 24^3 mesh with per-q1 q2
     windows): the band structure of all 13 824 points in one launch, then the windowed FP64
@@ -587,6 +633,9 @@ def main():
         return
     if args.workload == "smatrix":
         run_smatrix(args)
+        return
+    if args.workload == "relaxons":
+        run_relaxons(args)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -10,8 +10,9 @@ GPU (8x8x8 diamond, adaptive smearing, boundary scattering): a2Omega in
 device memory equals the oracle's; the eigenvalues equal LAPACK's on the
 oracle's Omega; the eigenvectors satisfy S theta = theta lambda, S the
 symmetric matrix of Omega's upper triangle; the
-relaxon conductivity equals the oracle's, with all eigenvalues and with the
-smallest half; products and a second eigensolve are refused afterwards."""
+relaxon conductivity equals the oracle's, with all eigenvalues (k = 0 and
+k = ns) and with the smallest half; a relaxon solve before the eigensolve,
+products and a second eigensolve afterwards are refused."""
 import json
 
 import numpy as np
@@ -102,7 +103,7 @@ def test_gpu_relaxons_match_oracle(ctx, diamond):
     vol = lattice.calc_volume(cr.direct_cell)
     ns = E.size
     scale = np.abs(Om).max()
-    for k in (0, ns // 2):
+    for k in (0, ns // 2, ns):
         A = PhScatteringMatrix(v3, bands, [T], "adaptive", boundary_length=L, in_memory=True)
         A.setup()
         A.a2Omega()
@@ -113,9 +114,11 @@ def test_gpu_relaxons_match_oracle(ctx, diamond):
             A.dot(P.drift)
         with pytest.raises(PhxError):
             A.diagonalize(ns + 1)
+        with pytest.raises(PhxError):
+            A.relaxonSolve(P.drift[0])   # before the eigensolve
         lam = A.diagonalize(k)
         lam_ref, theta_ref, k_ref = oracle.relaxons(Om, E, vg, T, int(np.prod(mesh)), vol, num_eigenvalues=k)
-        assert lam.size == lam_ref.size == (k or ns)
+        assert lam.size == lam_ref.size == (k or ns)   # k = ns: all of them, as the reference
         np.testing.assert_allclose(lam, lam_ref, rtol=0, atol=1e-9 * np.abs(lam_ref).max())
         theta = A.getMatrixRows(0, ns)[:, :lam.size]
         # eigenpairs of the symmetric matrix of Omega's upper triangle
@@ -123,7 +126,7 @@ def test_gpu_relaxons_match_oracle(ctx, diamond):
         assert np.abs(res).max() < 1e-9 * np.abs(lam_ref).max()
         kappa = solvers.relaxons(P, A.relaxonSolve)[0]
         np.testing.assert_allclose(kappa, k_ref, rtol=0, atol=1e-8 * np.abs(k_ref).max())
-        if k == 0:
+        if k in (0, ns):
             k_exact = solvers.exact(P, np.triu(M) + np.triu(M, 1).T)[0]
             np.testing.assert_allclose(kappa, k_exact, rtol=0, atol=1e-8 * np.abs(k_exact).max())
         with pytest.raises(PhxError):

@@ -33,6 +33,8 @@ TEMPS_K = (100.0, 300.0, 600.0)
 # FP32 FFMA throughput of a B200 (packed and scalar FFMA stream, all SMs, CUDA
 # events), the denominator of the pair kernel's CUDA-core view
 FFMA_PEAK_TFLOPS = 72.0
+# nominal FP64 rate of a B200 (no measured FP64 peak exists for this pool)
+FP64_PEAK_TFLOPS = 37.0
 # ncu DRAM bytes (read + write) of one pair-kernel launch, per (precision,
 # mesh, q2 per launch, slots) of the launch plan; None where not captured
 PAIR_TRAFFIC_BYTES = {("split_bf16", 20, 448, 7): 87476992 + 5594112,
@@ -144,6 +146,32 @@ def flops_per_pair_reference(nb, nr3):
     return 16 * nb ** 3 * nr3 + 16 * nb ** 4 + 16 * nb ** 4 + 8 * nb ** 4 * 2 + 3 * nb ** 3 * 2
 
 
+def host_cpu():
+    """CPU model, hardware threads and physical cores of this host (/proc/cpuinfo)."""
+    model, cores = None, set()
+    phys = core = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                k, _, v = line.partition(":")
+                k, v = k.strip(), v.strip()
+                if k == "model name" and model is None:
+                    model = v
+                elif k == "physical id":
+                    phys = v
+                elif k == "core id":
+                    core = v
+                elif not k and phys is not None:
+                    cores.add((phys, core))
+                    phys = core = None
+        if phys is not None:
+            cores.add((phys, core))
+    except OSError:
+        pass
+    return {"cpu_model": model, "hardware_threads": os.cpu_count(),
+            "physical_cores": len(cores) or None}
+
+
 def cpu_baseline(cr, fc2, fc3, mesh, budget_s, q2_hint=None):
     """Oracle (restatement of the reference CPU path) on a q2 sample."""
     import oracle
@@ -172,9 +200,10 @@ def cpu_baseline(cr, fc2, fc3, mesh, budget_s, q2_hint=None):
     dt = time.perf_counter() - t0
     pairs = n * nq
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": pairs / dt, "unit": "triplets/s", "cores": threads, "kind": "port",
-            "sample": "%d q2 points x all %d q1 of the %s mesh (%d pairs, %.1f s), OpenMP oracle"
-                      % (n, nq, "x".join(map(str, mesh)), pairs, dt)}
+    return dict({"value": pairs / dt, "unit": "triplets/s", "cores": threads, "kind": "port",
+                 "sample": "%d q2 points x all %d q1 of the %s mesh (%d pairs, %.1f s), OpenMP oracle"
+                           % (n, nq, "x".join(map(str, mesh)), pairs, dt),
+                 "sample_wall_s": t1 + dt}, **host_cpu())
 
 
 def run_reference(args):
@@ -191,9 +220,12 @@ def run_reference(args):
             vals.append(b["value"])
     v = float(np.median(vals))
     nq = int(np.prod(mesh))
+    # a step is the whole builder (nq^2 pairs); each step here times a bounded
+    # q2 sample, so the step time is projected from the measured rate
     line = {"impl": "reference", "metric": "3ph triplets/s @20^3 mesh", "value": v,
             "unit": "triplets/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 * nq * nq / v, "higher_is_better": True, "scaling": "strong",
+            "ms_per_step": 1000.0 * nq * nq / v, "projected_from_sample": True,
+            "sample_wall_s_per_step": b["sample_wall_s"], "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "diamond 20x20x20, 400 FC3 pairs, adaptive smearing, "
                                    "100/300/600 K (CPU sample per step)"},
@@ -328,8 +360,8 @@ def run_ours(args):
     except Exception:
         pass
     if args.precision == "fp64":
-        roof = {"bound": "fp64", "achieved": achieved, "peak": 37.0, "unit": "TFLOP/s",
-                "frac": achieved / 37.0, "traffic": None,
+        roof = {"bound": "fp64", "achieved": achieved, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
+                "frac": achieved / FP64_PEAK_TFLOPS, "traffic": None,
                 "note": "plain FP64 SIMT path; peak is the nominal B200 FP64 rate (no measured "
                         "FP64 peak available)"}
     else:
@@ -350,30 +382,44 @@ def run_ours(args):
     roof["ms_per_pair_launch"] = float(np.sum(pair_ms)) / max(1, pair_launches)
     roof["flops_per_pair_reference_formulation"] = flops_per_pair_reference(nb, nr3)
 
-    # the plain FP64 GPU path on the same workload (one step after a one-chunk warm-up)
+    # the plain FP64 GPU path on the same workload, timed like the split path:
+    # two untimed calls (eager, then captured into a CUDA graph), then replays
     fp64 = None
+    edge_peak = int(st.edge_events_peak)
     if args.precision != "fp64" and not args.kernels_only and not args.no_fp64:
         A_split = A.clone()   # the last timed step's A_out
         v3.setPrecision("fp64")
-        p = sm._params(q2b, min(q2e, q2b + 448), finalize=False)
-        _abi.check(L.phx_ph_linewidths_d(v3.h, bands.h, ctypes.byref(p), ctypes.c_void_p(A.data_ptr()),
-                                         None), ctx.h)
+        for _ in range(2):
+            step()
         flush.zero_()
         barrier()
-        st64 = step()
+        ms64s, pms64, pl64 = [], [], 0
+        for _ in range(3):
+            flush.zero_()
+            torch.cuda.synchronize()
+            st64 = step()
+            ms64s.append(st64.ms_total)
+            pms64.append(st64.ms_pair)
+            pl64 += st64.pair_launches
         barrier()
-        ms64 = float(st64.ms_total)
+        ms64 = float(np.mean(ms64s))
         if dist:
             t = torch.tensor([ms64], dtype=torch.float64, device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms64 = float(t.item())
         v3.setPrecision(args.precision)
+        ach64 = fl * (q2e - q2b) * nq * 3 / (float(np.sum(pms64)) / 1000.0) / 1e12
         fp64 = {"ms_per_step": ms64, "value": pairs_step / (ms64 / 1000.0), "unit": "triplets/s",
-                "dtype": "f64", "steps": 1, "split_speedup": ms64 / ms_step}
+                "dtype": "f64", "steps": 3, "timing": "CUDA graph replays after an eager and a captured call",
+                "split_speedup": ms64 / ms_step,
+                "roofline": {"bound": "fp64", "achieved": ach64, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
+                             "frac": ach64 / FP64_PEAK_TFLOPS, "flops_per_pair": fl,
+                             "ms_per_pair_launch": float(np.sum(pms64)) / max(1, pl64),
+                             "peak_source": "fallback: nominal B200 FP64 rate (no measured FP64 peak)"}}
         if world == 1:
             # accuracy of the split path on this workload: relative error of the
             # linewidths (A_out / n(n+1), the same ratio) of non-excluded states
-            # with A_out above 1e-8 of the largest
+            # with A_out above 1e-8 of the largest, and of the RTA conductivity
             a64 = A.cpu().numpy().reshape(nT, -1)
             a16 = A_split.cpu().numpy().reshape(nT, -1)
             Eb = bands.get(velocities=False)[0].reshape(-1)
@@ -381,6 +427,21 @@ def run_ours(args):
             rel = np.abs(a16 - a64)[big] / np.abs(a64)[big]
             fp64["split_linewidth_rel_err"] = {"max": float(rel.max()), "p99": float(np.quantile(rel, 0.99)),
                                                "median": float(np.median(rel)), "states": int(big.sum())}
+
+            def kappa(a):
+                k = np.zeros((nT, 3, 3))
+                _abi.check(L.phx_ph_rta_kappa(bands.h, nT, T.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                              np.ascontiguousarray(a).ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                              float(cr.volume), k.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                           ctx.h)
+                return k
+            k64, k16 = kappa(a64), kappa(a16)
+            d64 = np.array([np.diagonal(k) for k in k64])
+            d16 = np.array([np.diagonal(k) for k in k16])
+            fp64["split_kappa_rel_err"] = {"max": float(np.abs(d16 - d64).max() / np.abs(d64).max()),
+                                           "per_temperature": [float(np.abs(d16[t] - d64[t]).max() /
+                                                                     np.abs(d64[t]).max()) for t in range(nT)],
+                                           "what": "diagonal RTA conductivity, each temperature"}
 
     out = None
     if rank == 0:
@@ -402,6 +463,8 @@ def run_ours(args):
                        "d2h_bytes_per_step": int(d2h)},
                "gpu_launches": launches,
                "launch_plan": plan,
+               "near_cutoff_events": {"peak_per_pair_launch": edge_peak,
+                                      "capacity": int(st.edge_events_cap)},
                "roofline": roof,
                "cpu_baseline": cpu,
                "fp64_path": fp64,

@@ -175,6 +175,12 @@ typedef struct phx_lw_stats {
   double ms_pair;             /* device time of those launches alone (CUDA events) */
   int plan_chunk, plan_slots; /* launch plan used (q2 per chunk, partial-sum slots) */
   int graph;                  /* 0 eager launches, 1 captured into a CUDA graph, 2 graph replayed */
+  /* split path: the most near-cut-off events one pair launch recorded (their
+   * adaptive deltas re-decided in FP64) and the capacity of the event list;
+   * chunks of q2 with more events than that apply none of them and are re-run
+   * in smaller pieces with the rates off (edge_overflow_chunks counts them) */
+  long long edge_events_peak, edge_events_cap;
+  int edge_overflow_chunks;
 } phx_lw_stats;
 
 /* Whole PhScatteringMatrix::builder, switchCase 2 (linewidths), on the GPU:
@@ -273,12 +279,14 @@ int phx_ph_smatrix_dot_d(phx_v3* v3, phx_bands* bands, const phx_lw_params* para
  * device output A_out_d (nT*nq*nb doubles).  Limit: Bose table and partial
  * sums, 16*nq*nb*nT bytes, plus one q2 slab of the cached vertex,
  * 16*nr3*nb^3 bytes, must fit in 16 MiB; larger problems are rejected with
- * PHX_ERR_ARG.  The first call on a device looks up the array's address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * All calls share the array and leave their contents in it (the call clears
- * what must start at zero): calls that overlap on the same GPU race.  The
- * precision setting of v3 is ignored (FP64).  Returns after the stream has
- * drained. */
+ * PHX_ERR_ARG.  The first call on a device (and in each new CUDA context of
+ * it) looks up the array's address with cudaGetSymbolAddress.  Never call
+ * this function inside a stream capture: every call sets kernel attributes,
+ * copies the temperatures from pageable host memory and synchronises the
+ * stream before it returns.  All calls share the array and leave their
+ * contents in it (the call clears what must start at zero): calls that
+ * overlap on the same GPU race.  The precision setting of v3 is ignored
+ * (FP64).  Returns after the stream has drained. */
 int phx_ph_linewidths_static(phx_v3* v3, phx_bands* bands, const phx_lw_params* params,
                              double* A_out_d);
 
@@ -389,6 +397,13 @@ int phx_mlp_train(phx_mlp* net, int n, const float* X, const float* t, int epoch
  * tcgen05.mma with the builder's shared-memory layouts.  No reference
  * counterpart (validates this library's own tensor-core building block). */
 int phx_diag_tc_gemm(phx_ctx* ctx, int N, int Kp, const float* A, const float* B, float* C);
+
+/* Test hook (no reference counterpart): capacity of the split path's
+ * near-cut-off event list per pair launch, for this process (0: the default,
+ * 2^18).  A linewidth chunk with more events is re-run in pieces whose events
+ * fit, so the results do not depend on it; a small capacity exercises that
+ * path.  The matrix modes fail with PHX_ERR_ARG on an overflow. */
+int phx_debug_set_split_edge_cap(unsigned cap);
 
 #ifdef __cplusplus
 }

@@ -44,7 +44,9 @@ class LwStats(ctypes.Structure):
     _fields_ = [("ms_total", ctypes.c_double), ("ms_vertex", ctypes.c_double),
                 ("pairs", ctypes.c_longlong), ("kernel_launches", ctypes.c_int),
                 ("pair_launches", ctypes.c_int), ("ms_pair", ctypes.c_double),
-                ("plan_chunk", ctypes.c_int), ("plan_slots", ctypes.c_int), ("graph", ctypes.c_int)]
+                ("plan_chunk", ctypes.c_int), ("plan_slots", ctypes.c_int), ("graph", ctypes.c_int),
+                ("edge_events_peak", ctypes.c_longlong), ("edge_events_cap", ctypes.c_longlong),
+                ("edge_overflow_chunks", ctypes.c_int)]
 
 
 class ElParams(ctypes.Structure):
@@ -119,6 +121,7 @@ SIGNATURES = {
                       ctypes.c_float, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_float)],
     "phx_diag_tc_gemm": [_VP, _i, _i, ctypes.POINTER(ctypes.c_float),
                          ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)],
+    "phx_debug_set_split_edge_cap": [ctypes.c_uint],
 }
 _RESTYPE = {"phx_version": ctypes.c_char_p, "phx_mlp_num_params": ctypes.c_longlong}
 

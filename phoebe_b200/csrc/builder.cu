@@ -35,11 +35,14 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+
 #include "cplx.cuh"
 #include "phx_consts.h"
 #include "phx_internal.h"
 
 #include "pair_common.cuh"
+#include "wide.cuh"
 
 using namespace pairc;
 
@@ -1021,7 +1024,8 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
                          const double2* Dp, uint8_t* Bimg, const void* rec, double emax, int q2_first,
                          int q2_count, int slots, double* partial, int* launches, cudaEvent_t ev_begin,
                          cudaEvent_t ev_end, int fp16, const unsigned* dmax, void* edges, unsigned* edge_count,
-                         unsigned edge_cap, const phx_split_matrix* mat = nullptr);
+                         unsigned edge_cap, unsigned* edge_peak, unsigned* edge_overflow, int edge_only,
+                         const phx_split_matrix* mat = nullptr);
 unsigned phx_split_edge_cap();
 size_t phx_split_edge_bytes();
 
@@ -1177,6 +1181,10 @@ struct BuilderPlan {
 bool env_off(const char* name) {
   const char* e = std::getenv(name);
   return e && e[0] == '0';
+}
+bool env_on(const char* name) {
+  const char* e = std::getenv(name);
+  return e && e[0] == '1';
 }
 
 struct PlanKey {
@@ -1360,7 +1368,9 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   const size_t sz_img = split ? align_up(phx_split_bimg_bytes(max_chunk, nr3)) : 0;
   const size_t sz_rec = split ? align_up(phx_split_rec_bytes(nq)) : 0;
   const size_t sz_iso = p->isotope_coupling ? align_up(sizeof(double) * v->nat) : 0;
-  const size_t sz_max = align_up(sizeof(unsigned) * 2);
+  // per chunk: flag of a near-cut-off event list that overflowed (the smallest candidate chunk is 448 q2)
+  const int max_chunks = (q2e - q2b + 447) / 448 + 1;
+  const size_t sz_max = align_up(sizeof(unsigned) * (4 + max_chunks + 1));
   const size_t sz_edge = split ? align_up(phx_split_edge_bytes()) : 0;
   PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_img + sz_rec + sz_iso + sz_max + sz_edge));
   char* base = static_cast<char*>(v->ctx->d_scratch);
@@ -1377,6 +1387,9 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   const int fp16 = v->precision == PHX_PREC_SPLIT_FP16 ? 1 : 0;
   unsigned* dmax = reinterpret_cast<unsigned*>(base + sz_dp + sz_part + sz_bose + sz_T + sz_img + sz_rec + sz_iso);
   unsigned* edge_count = dmax + 1;
+  unsigned* edge_peak = dmax + 2;   // largest near-cut-off event count of the call's pair launches
+  unsigned* edge_flags = dmax + 4;  // [max_chunks] overflow flag of each chunk, then one for re-runs
+  const unsigned edge_cap = phx_split_edge_cap();
   void* edges = base + sz_dp + sz_part + sz_bose + sz_T + sz_img + sz_rec + sz_iso + sz_max;
   if (split) {
     PHX_ARG(ctx, NB == 6, "split-precision path supports nb = 6");
@@ -1392,7 +1405,7 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
     }
   }
   const double emax = split ? b->emax : 0.0;
-  PairArgs P;
+  PairArgs P{};
   P.m.nq = nq;
   P.m.nb = NB;
   P.m.nT = nT;
@@ -1429,13 +1442,14 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   const int tiles = (nq + kTile - 1) / kTile;
   // one chunk of the q2 loop; pe0/pe1 (may be null) bracket its pair kernel
   auto chunk_work = [&](const BuilderPlan& pl, int c0, int cnt, cudaEvent_t pe0, cudaEvent_t pe1,
-                        int* launches) -> int {
+                        int* launches, unsigned* overflow = nullptr, int edge_only = 0) -> int {
     if (fp16) PHX_CUDA(ctx, cudaMemsetAsync(dmax, 0, sizeof(unsigned), st));
     fold_tiled_launch(NB, nr2, nr3, v, b, c0, cnt, Dp, st, fp16 ? dmax : nullptr);
     ++*launches;
     if (split)
       return phx_split_pair_chunk(ctx, P.m, v, b, Dp, Bimg, rec, emax, c0, cnt, pl.slots, partial, launches,
-                                  pe0, pe1, fp16, dmax, edges, edge_count, phx_split_edge_cap());
+                                  pe0, pe1, fp16, dmax, edges, edge_count, edge_cap, edge_peak, overflow,
+                                  edge_only);
     PairArgs Q = P;
     Q.q2_first = c0;
     Q.q2_count = cnt;
@@ -1495,6 +1509,7 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   auto work = [&](phx_builder_graph& g) -> int {
     int launches = 0;
     PHX_CUDA(ctx, cudaMemsetAsync(partial, 0, sizeof(double) * nslots * nq * NB * nT, st));
+    if (split) PHX_CUDA(ctx, cudaMemsetAsync(edge_peak, 0, sizeof(unsigned) * (3 + max_chunks), st));
     bose_kernel<<<std::min(1024, (nq * NB * nT + 255) / 256), 256, 0, st>>>(nq, NB, nT, b->d_E, temps, bose);
     ++launches;
     if (split) PHX_TRY(phx_split_pack_records(ctx, P.m, rec, &launches));
@@ -1506,7 +1521,7 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
       g.pair_events.push_back(pe0);
       PHX_CUDA(ctx, cudaEventCreate(&pe1));
       g.pair_events.push_back(pe1);
-      PHX_TRY(chunk_work(plan, c0, cnt, pe0, pe1, &launches));
+      PHX_TRY(chunk_work(plan, c0, cnt, pe0, pe1, &launches, split ? edge_flags + (c0 - q2b) / plan.chunk : nullptr));
     }
     PHX_CUDA(ctx, phx_record_event(g.vertex_end, st));
     if (giso) {
@@ -1527,7 +1542,7 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
       (uint64_t)p->smearing, bits(p->sigma), (uint64_t)p->finalize, (uint64_t)plan.chunk, (uint64_t)plan.slots,
       bits(emax), bits(base), bits(Aout_d), bits(b->d_E), bits(b->d_U), bits(b->d_vg), bits(b->d_q),
       bits(b->d_U32), bits(b->d_q1_order), bits(v->d_D3w), bits(v->d_R2), bits(v->d_R3), bits(ctx->d_status),
-      bits(giso), bits(p->boundary_length)};
+      bits(giso), bits(p->boundary_length), (uint64_t)edge_cap};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   PHX_CUDA(ctx, cudaEventCreate(&ev0));
   PHX_CUDA(ctx, cudaEventCreate(&ev1));
@@ -1537,10 +1552,12 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   int graph_state = 0;
   int rc = run_device_work(v, key, work, &eager, &g, &graph_state);
   int kst = 0;
+  unsigned epeak = 0;
   if (rc == PHX_OK) {
     cudaError_t ce = cudaEventRecord(ev1, st);
     if (ce == cudaSuccess) ce = cudaEventSynchronize(ev1);
     if (ce == cudaSuccess) ce = cudaMemcpy(&kst, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (ce == cudaSuccess && split) ce = cudaMemcpy(&epeak, edge_peak, sizeof(unsigned), cudaMemcpyDeviceToHost);
     if (ce != cudaSuccess) {
       phx_set_error(ctx, PHX_ERR_CUDA, cudaGetErrorString(ce));
       rc = PHX_ERR_CUDA;
@@ -1548,10 +1565,65 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   }
   if (rc == PHX_OK && kst) {
     cudaMemset(ctx->d_status, 0, sizeof(int));
-    phx_set_error(ctx, PHX_ERR_CUDA, (kst & (1 << 20)) ? std::string("split path: near-cut-off event list overflowed")
-                                                       : "pair kernel gave up waiting on a pipeline barrier (status " +
-                                                             std::to_string(kst) + ")");
+    phx_set_error(ctx, PHX_ERR_CUDA,
+                  "pair kernel gave up waiting on a pipeline barrier (status " + std::to_string(kst) + ")");
     rc = PHX_ERR_CUDA;
+  }
+  // Chunks whose near-cut-off events overflowed the list applied none of
+  // them: re-run their q2 with the rates off, in pieces whose events fit,
+  // then finalise again.  Eager launches, outside any graph.
+  int overflowed = 0;
+  if (rc == PHX_OK && split) {
+    const int nchunks = (q2e - q2b + plan.chunk - 1) / plan.chunk;
+    std::vector<unsigned> fl(nchunks, 0u);
+    if (cudaMemcpy(fl.data(), edge_flags, sizeof(unsigned) * nchunks, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      phx_set_error(ctx, PHX_ERR_CUDA, "reading the near-cut-off overflow flags failed");
+      rc = PHX_ERR_CUDA;
+    }
+    unsigned* piece_flag = edge_flags + max_chunks;
+    int dummy = 0;
+    for (int ci = 0; ci < nchunks && rc == PHX_OK; ++ci) {
+      if (!fl[ci]) continue;
+      ++overflowed;
+      std::vector<std::pair<int, int>> todo = {{q2b + ci * plan.chunk, std::min(plan.chunk, q2e - (q2b + ci * plan.chunk))}};
+      while (!todo.empty() && rc == PHX_OK) {
+        const std::pair<int, int> pc = todo.back();
+        todo.pop_back();
+        const BuilderPlan pp{pc.second, std::min(plan.slots, pc.second)};
+        unsigned f = 0;
+        rc = [&]() -> int {
+          PHX_CUDA(ctx, cudaMemsetAsync(piece_flag, 0, sizeof(unsigned), st));
+          PHX_TRY(chunk_work(pp, pc.first, pc.second, nullptr, nullptr, &dummy, piece_flag, 1));
+          PHX_CUDA(ctx, cudaMemcpyAsync(&f, piece_flag, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+          PHX_CUDA(ctx, cudaStreamSynchronize(st));
+          return PHX_OK;
+        }();
+        if (rc == PHX_OK && f) {
+          if (pc.second == 1) {
+            phx_set_error(ctx, PHX_ERR_ARG, "split path: the near-cut-off events of one q2 exceed the event list");
+            rc = PHX_ERR_ARG;
+          } else {
+            const int h = pc.second / 2;
+            todo.push_back({pc.first, h});
+            todo.push_back({pc.first + h, pc.second - h});
+          }
+        }
+      }
+    }
+    if (rc == PHX_OK && overflowed) {
+      finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, NB, nT, nslots, partial, b->d_E, p->finalize, b->d_vg,
+                                                        temps, p->boundary_length, Aout_d);
+      cudaError_t ce = cudaGetLastError();
+      if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+      if (ce == cudaSuccess) ce = cudaMemcpy(&kst, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+      if (ce != cudaSuccess || kst) {
+        cudaMemset(ctx->d_status, 0, sizeof(int));
+        phx_set_error(ctx, PHX_ERR_CUDA, ce != cudaSuccess ? std::string(cudaGetErrorString(ce))
+                                                           : "re-run of an overflowed chunk: kernel status " +
+                                                                 std::to_string(kst));
+        rc = PHX_ERR_CUDA;
+      }
+    }
   }
   if (rc == PHX_OK && stats) {
     float ms = 0, msv = 0;
@@ -1572,6 +1644,9 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
     stats->plan_chunk = plan.chunk;
     stats->plan_slots = plan.slots;
     stats->graph = graph_state;
+    stats->edge_events_peak = (long long)epeak;
+    stats->edge_events_cap = split ? (long long)edge_cap : 0;
+    stats->edge_overflow_chunks = overflowed;
     cudaGetLastError();   // an elapsed-time query that failed must not leak into the next call
   }
   phx_builder_graph_free(eager);
@@ -1636,7 +1711,7 @@ int run_builder_generic(phx_v3* v, phx_bands* b, const phx_lw_params* p, double*
                      [&](int a, int c) { return p->window_cut[a] < p->window_cut[c]; });
     PHX_CUDA(ctx, cudaMemcpyAsync(order, order_h.data(), sizeof(int) * nq, cudaMemcpyHostToDevice, st));
   }
-  PairArgs P;
+  PairArgs P{};
   P.m.nq = nq;
   P.m.nb = nb;
   P.m.nT = nT;
@@ -1821,7 +1896,7 @@ int run_matrix_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
   const size_t sz_slab = full ? 0 : align_up(sizeof(double) * 2 * nT * slab_elems);
   const size_t sz_img = split ? align_up(phx_split_bimg_bytes(chunk, nr3)) : 0;
   const size_t sz_rec = split ? align_up(phx_split_rec_bytes(nq)) : 0;
-  const size_t sz_max = split ? align_up(sizeof(unsigned) * 2) : 0;
+  const size_t sz_max = split ? align_up(sizeof(unsigned) * 4) : 0;
   const size_t sz_edge = split ? align_up(phx_split_edge_bytes()) : 0;
   PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_part + sz_bose + sz_T + sz_iso + sz_slab + sz_img + sz_rec + sz_max +
                                      sz_edge));
@@ -1839,6 +1914,8 @@ int run_matrix_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
   void* rec = sbase + sz_img;
   unsigned* dmax = reinterpret_cast<unsigned*>(sbase + sz_img + sz_rec);
   unsigned* edge_count = dmax + 1;
+  unsigned* edge_peak = dmax + 2;
+  unsigned* edge_over = dmax + 3;   // the matrix modes fail on an overflow
   void* edges = sbase + sz_img + sz_rec + sz_max;
   if (split) {
     PHX_ARG(ctx, phx_split_smem_bytes(nr3) <= 227 * 1024, "too many R3 vectors for the split path");
@@ -1907,6 +1984,7 @@ int run_matrix_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
     bose_kernel<<<std::min(1024, (nq * NB * nT + 255) / 256), 256, 0, st>>>(nq, NB, nT, b->d_E, temps, bose);
     ++launches;
     if (split) PHX_TRY(phx_split_pack_records(ctx, P.m, rec, &launches));
+    if (split) PHX_CUDA(ctx, cudaMemsetAsync(edge_peak, 0, sizeof(unsigned) * 2, st));
     PHX_CUDA(ctx, cudaEventRecord(evv0, st));
     for (int c0 = q2b; c0 < q2e; c0 += chunk) {
       const int cnt = std::min(chunk, q2e - c0);
@@ -1918,7 +1996,8 @@ int run_matrix_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
         ++launches;
         const phx_split_matrix mo{full ? A_full : slabP, slabM, (long long)ns, slab_elems, full ? 1 : 0};
         PHX_TRY(phx_split_pair_chunk(ctx, P.m, v, b, Dp, Bimg, rec, b->emax, c0, cnt, slots, partial, &launches,
-                                     nullptr, nullptr, fp16, dmax, edges, edge_count, phx_split_edge_cap(), &mo));
+                                     nullptr, nullptr, fp16, dmax, edges, edge_count, phx_split_edge_cap(),
+                                     edge_peak, edge_over, 0, &mo));
       } else {
         fold_tiled_launch(NB, nr2, nr3, v, b, c0, cnt, Dp, st);
         ++launches;
@@ -1989,15 +2068,21 @@ int run_matrix_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
   if (rc == PHX_OK) {
     cudaError_t ce = cudaEventSynchronize(ev1);
     int kst = 0;
+    unsigned over = 0;
     if (ce == cudaSuccess) ce = cudaMemcpy(&kst, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (ce == cudaSuccess && split) ce = cudaMemcpy(&over, edge_over, sizeof(unsigned), cudaMemcpyDeviceToHost);
     if (ce != cudaSuccess) {
       phx_set_error(ctx, PHX_ERR_CUDA, cudaGetErrorString(ce));
       rc = PHX_ERR_CUDA;
     } else if (kst) {
       cudaMemset(ctx->d_status, 0, sizeof(int));
-      phx_set_error(ctx, PHX_ERR_CUDA, (kst & (1 << 20)) ? std::string("split path: near-cut-off event list overflowed")
-                                                         : "scattering matrix: kernel status " + std::to_string(kst));
+      phx_set_error(ctx, PHX_ERR_CUDA, "scattering matrix: kernel status " + std::to_string(kst));
       rc = PHX_ERR_CUDA;
+    } else if (over) {
+      phx_set_error(ctx, PHX_ERR_ARG,
+                    "scattering matrix (split path): a pair launch had more near-cut-off events than the event "
+                    "list holds; use PHX_PREC_FP64 or a smaller mesh");
+      rc = PHX_ERR_ARG;
     }
   }
   if (rc == PHX_OK && stats) {
@@ -2145,6 +2230,258 @@ namespace {
 
 }  // namespace
 
+namespace {
+
+// Non-zero (r3, r2) blocks of the folded vertex, once per coupling object:
+// the many-branch fold sums over them only.
+int wide_prepare_blocks(phx_v3* v) {
+  if (v->d_r2_ofs) return PHX_OK;
+  phx_ctx* ctx = v->ctx;
+  cudaStream_t st = ctx->stream;
+  const int nr3 = v->nr3, nr2 = v->nr2;
+  int* d_flags = nullptr;
+  PHX_CUDA(ctx, phx_dev_alloc(ctx, (void**)&d_flags, sizeof(int) * (size_t)nr3 * nr2));
+  std::vector<int> flags((size_t)nr3 * nr2);
+  cudaError_t e = wide::launch_nonzero_blocks(v->nb, nr3, nr2, v->d_D3w, d_flags, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(flags.data(), d_flags, sizeof(int) * flags.size(), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  phx_dev_free(ctx, d_flags);
+  PHX_CUDA(ctx, e);
+  std::vector<int> ofs(nr3 + 1, 0), list;
+  int maxl = 1;
+  for (int r3 = 0; r3 < nr3; ++r3) {
+    for (int r2 = 0; r2 < nr2; ++r2)
+      if (flags[(size_t)r3 * nr2 + r2]) list.push_back(r2);
+    ofs[r3 + 1] = (int)list.size();
+    maxl = std::max(maxl, ofs[r3 + 1] - ofs[r3]);
+  }
+  if (list.empty()) list.push_back(0);
+  PHX_CUDA(ctx, phx_dev_alloc(ctx, (void**)&v->d_r2_ofs, sizeof(int) * ofs.size()));
+  PHX_CUDA(ctx, phx_dev_alloc(ctx, (void**)&v->d_r2_list, sizeof(int) * list.size()));
+  PHX_CUDA(ctx, cudaMemcpyAsync(v->d_r2_ofs, ofs.data(), sizeof(int) * ofs.size(), cudaMemcpyHostToDevice, st));
+  PHX_CUDA(ctx, cudaMemcpyAsync(v->d_r2_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, st));
+  PHX_CUDA(ctx, cudaStreamSynchronize(st));
+  v->r2_max_list = maxl;
+  return PHX_OK;
+}
+
+// Builder for cells with many branches (wide.cu), both precisions, with an
+// optional per-q1 q2 window: per chunk of q2 the sparse R2 fold, for the
+// split path the FP16/BF16 hi/lo image of the folded vertex, then one
+// persistent pair kernel over (q2, q1 tile) items from a work queue.
+int run_builder_wide(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d, phx_lw_stats* stats) {
+  phx_ctx* ctx = v->ctx;
+  cudaStream_t st = ctx->stream;
+  const int nq = b->nq, nT = p->num_temperatures, nr3 = v->nr3, nr2 = v->nr2, nb = v->nb;
+  const int q2b = p->q2_begin, q2e = p->q2_end;
+  const bool split = v->precision != PHX_PREC_FP64;
+  const int fp16 = v->precision == PHX_PREC_SPLIT_FP16 ? 1 : 0;
+  const bool windowed = p->window_energy != nullptr;
+  PHX_ARG(ctx, nb <= wide::kMaxNb, "phx_ph_linewidths: at most 48 branches (16 atoms)");
+  PHX_ARG(ctx, !p->isotope_coupling || nb <= 32, "phx_ph_linewidths: isotope scattering supports nb <= 32");
+  const int Kp = wide::split_kp(nr3);
+  int nq1 = wide::kQ1;
+  if (split) {
+    PHX_ARG(ctx, wide::split_smem(nb, Kp) <= 227 * 1024,
+            "phx_ph_linewidths: too many branches or R3 vectors for the split path");
+  } else {
+    nq1 = wide::fp64_q1(nb, nr3);
+    PHX_ARG(ctx, nq1 > 0, "phx_ph_linewidths: too many branches or R3 vectors for the FP64 path");
+  }
+  PHX_TRY(wide_prepare_blocks(v));
+  PHX_ARG(ctx, wide::fold_smem(nb, v->r2_max_list) <= 227 * 1024, "phx_ph_linewidths: too many R2 vectors");
+  const size_t nb3 = (size_t)nb * nb * nb;
+  const size_t per_q2 = sizeof(double2) * nr3 * nb3 + (split ? wide::split_img_bytes(nb, Kp) : 0);
+  // q2 per chunk: at most 2 GiB of folded vertex (and its image), at most 512 q2
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>({(size_t)512, (size_t)(q2e - q2b),
+                                                                (size_t(2) << 30) / per_q2}));
+  const int nchunks = (q2e - q2b + chunk - 1) / chunk;
+  const size_t sz_dp = align_up(sizeof(double2) * nr3 * nb3 * chunk);
+  const size_t sz_img = split ? align_up(wide::split_img_bytes(nb, Kp) * chunk) : 0;
+  const size_t sz_lw = align_up(sizeof(double) * (size_t)nq * nb * nT);
+  const size_t sz_bose = align_up(sizeof(double) * (size_t)nT * nq * nb);
+  const size_t sz_T = align_up(sizeof(double) * 8);
+  const size_t sz_win = align_up(sizeof(double) * 2 * nq);
+  const size_t sz_ord = align_up(sizeof(int) * nq);
+  const size_t sz_iso = p->isotope_coupling ? align_up(sizeof(double) * v->nat) : 0;
+  const size_t sz_cnt = align_up(sizeof(unsigned) * (nchunks + 1));
+  const size_t sz_u32 = split && !b->d_U32 ? 0 : 0;
+  (void)sz_u32;
+  PHX_TRY(phx_scratch_reserve(v, sz_dp + sz_img + sz_lw + sz_bose + sz_T + sz_win + sz_ord + sz_iso + sz_cnt));
+  char* base = static_cast<char*>(v->ctx->d_scratch);
+  size_t o = 0;
+  double2* Dp = reinterpret_cast<double2*>(base + o); o += sz_dp;
+  uint8_t* img = reinterpret_cast<uint8_t*>(base + o); o += sz_img;
+  double* lw = reinterpret_cast<double*>(base + o); o += sz_lw;
+  double* bose = reinterpret_cast<double*>(base + o); o += sz_bose;
+  double* temps = reinterpret_cast<double*>(base + o); o += sz_T;
+  double* wdev = reinterpret_cast<double*>(base + o); o += sz_win;
+  int* order = reinterpret_cast<int*>(base + o); o += sz_ord;
+  double* giso = p->isotope_coupling ? reinterpret_cast<double*>(base + o) : nullptr; o += sz_iso;
+  unsigned* counters = reinterpret_cast<unsigned*>(base + o);   // [nchunks] work queues, then dmax
+  unsigned* dmax = counters + nchunks;
+  if (split && !b->d_U32) {
+    const size_t n = (size_t)nq * nb * nb;
+    PHX_CUDA(ctx, phx_dev_alloc(ctx, (void**)&b->d_U32, sizeof(float2) * n));
+    PHX_CUDA(ctx, wide::launch_u32(reinterpret_cast<const double2*>(b->d_U), reinterpret_cast<float2*>(b->d_U32), n,
+                                   st));
+  }
+  PHX_CUDA(ctx, wide::set_attributes(nb, nr3, split));
+  // q1 order: by window cut with a window (tiles of similar q2 sets), else the mesh order
+  std::vector<int> order_h(nq);
+  for (int i = 0; i < nq; ++i) order_h[i] = i;
+  if (windowed)
+    std::stable_sort(order_h.begin(), order_h.end(), [&](int a, int c) { return p->window_cut[a] < p->window_cut[c]; });
+  PHX_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
+  PHX_CUDA(ctx, cudaMemcpyAsync(temps, p->temperatures, sizeof(double) * nT, cudaMemcpyHostToDevice, st));
+  PHX_CUDA(ctx, cudaMemcpyAsync(order, order_h.data(), sizeof(int) * nq, cudaMemcpyHostToDevice, st));
+  if (windowed) {
+    PHX_CUDA(ctx, cudaMemcpyAsync(wdev, p->window_energy, sizeof(double) * nq, cudaMemcpyHostToDevice, st));
+    PHX_CUDA(ctx, cudaMemcpyAsync(wdev + nq, p->window_cut, sizeof(double) * nq, cudaMemcpyHostToDevice, st));
+  }
+  if (giso)
+    PHX_CUDA(ctx, cudaMemcpyAsync(giso, p->isotope_coupling, sizeof(double) * v->nat, cudaMemcpyHostToDevice, st));
+  wide::Args A{};
+  A.m.nq = nq;
+  A.m.nb = nb;
+  A.m.nT = nT;
+  A.m.n0 = b->mesh[0];
+  A.m.n1 = b->mesh[1];
+  A.m.n2 = b->mesh[2];
+  A.m.E = b->d_E;
+  A.m.U = reinterpret_cast<const double2*>(b->d_U);
+  A.m.vg = b->d_vg;
+  A.m.bose = bose;
+  A.m.qcart = b->d_q;
+  A.m.smearing = p->smearing;
+  A.m.sigma = p->sigma;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) A.m.qT[i * 3 + j] = b->recip[i * 3 + j] / b->mesh[i];
+  A.m.norm = 1.0 / (double)nq;
+  A.nr3 = nr3;
+  A.R3 = v->d_R3;
+  A.Dp = Dp;
+  A.q1_order = order;
+  A.nq1 = nq1;
+  A.ntiles = (nq + nq1 - 1) / nq1;
+  A.win_energy = windowed ? wdev : nullptr;
+  A.win_cut = windowed ? wdev + nq : nullptr;
+  A.lw = lw;
+  A.status = ctx->d_status;
+  A.img = img;
+  A.U32 = reinterpret_cast<const float2*>(b->d_U32);
+  A.Kp = Kp;
+  A.mtiles = wide::split_mtiles(nb);
+  A.fp16 = fp16;
+  A.dmax = dmax;
+  const int grid = ctx->num_sms * wide::blocks_per_sm(nb, nr3, split);
+  long long pairs = 0;
+  for (int c0 = q2b; c0 < q2e; c0 += chunk) pairs += (long long)nq * std::min(chunk, q2e - c0);
+  auto work = [&](phx_builder_graph& g) -> int {
+    int launches = 0;
+    PHX_CUDA(ctx, cudaMemsetAsync(lw, 0, sizeof(double) * (size_t)nq * nb * nT, st));
+    PHX_CUDA(ctx, cudaMemsetAsync(counters, 0, sizeof(unsigned) * (nchunks + 1), st));
+    bose_kernel<<<std::min(1024, (nq * nb * nT + 255) / 256), 256, 0, st>>>(nq, nb, nT, b->d_E, temps, bose);
+    ++launches;
+    PHX_CUDA(ctx, phx_record_event(g.vertex_begin, st));
+    for (int ci = 0; ci < nchunks; ++ci) {
+      const int c0 = q2b + ci * chunk, cnt = std::min(chunk, q2e - c0);
+      if (fp16) PHX_CUDA(ctx, cudaMemsetAsync(dmax, 0, sizeof(unsigned), st));
+      PHX_CUDA(ctx, wide::launch_fold(nb, nr2, nr3, v->d_D3w, v->d_r2_ofs, v->d_r2_list, v->r2_max_list, v->d_R2,
+                                      v->d_R3, b->d_q, reinterpret_cast<const double2*>(b->d_U), c0, cnt, Dp,
+                                      fp16 ? dmax : nullptr, st));
+      ++launches;
+      if (split) {
+        PHX_CUDA(ctx, wide::launch_convert(nb, nr3, Kp, cnt, Dp, img, fp16, dmax, st));
+        ++launches;
+      }
+      wide::Args Ac = A;
+      Ac.q2_first = c0;
+      Ac.q2_count = cnt;
+      Ac.counter = counters + ci;
+      cudaEvent_t pe0 = nullptr, pe1 = nullptr;
+      PHX_CUDA(ctx, cudaEventCreate(&pe0));
+      g.pair_events.push_back(pe0);
+      PHX_CUDA(ctx, cudaEventCreate(&pe1));
+      g.pair_events.push_back(pe1);
+      PHX_CUDA(ctx, phx_record_event(pe0, st));
+      PHX_CUDA(ctx, split ? wide::launch_split(Ac, grid, st) : wide::launch_fp64(Ac, grid, st));
+      PHX_CUDA(ctx, phx_record_event(pe1, st));
+      ++launches;
+    }
+    PHX_CUDA(ctx, phx_record_event(g.vertex_end, st));
+    if (giso) {
+      IsoArgs I{A.m, v->nat, giso, q2b, q2e - q2b, q2e - q2b, lw};
+      isotope_kernel<<<dim3((nq + kTile - 1) / kTile, 1), kTile * nb, iso_smem(nb), st>>>(I);
+      ++launches;
+      PHX_CUDA(ctx, cudaGetLastError());
+    }
+    finalize_kernel<<<(nq + 127) / 128, 128, 0, st>>>(nq, nb, nT, 1, lw, b->d_E, p->finalize, b->d_vg, temps,
+                                                      p->boundary_length, Aout_d);
+    ++launches;
+    PHX_CUDA(ctx, cudaGetLastError());
+    g.launches = launches;
+    return PHX_OK;
+  };
+  const std::vector<uint64_t> key = {
+      (uint64_t)(split ? 10 + fp16 : 9), (uint64_t)nb, (uint64_t)nq, (uint64_t)nT, (uint64_t)q2b, (uint64_t)q2e,
+      (uint64_t)p->smearing, bits(p->sigma), (uint64_t)p->finalize, (uint64_t)chunk, (uint64_t)windowed, bits(base),
+      bits(Aout_d), bits(b->d_E), bits(b->d_U), bits(b->d_vg), bits(b->d_q), bits(b->d_U32), bits(v->d_D3w),
+      bits(v->d_R2), bits(v->d_R3), bits(ctx->d_status), bits(giso), bits(p->boundary_length), (uint64_t)grid};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  PHX_CUDA(ctx, cudaEventCreate(&ev0));
+  PHX_CUDA(ctx, cudaEventCreate(&ev1));
+  PHX_CUDA(ctx, cudaEventRecord(ev0, st));
+  phx_builder_graph eager;
+  phx_builder_graph* g = nullptr;
+  int graph_state = 0;
+  int rc = run_device_work(v, key, work, &eager, &g, &graph_state);
+  int kst = 0;
+  if (rc == PHX_OK) {
+    cudaError_t ce = cudaEventRecord(ev1, st);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(ev1);
+    if (ce == cudaSuccess) ce = cudaMemcpy(&kst, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) {
+      phx_set_error(ctx, PHX_ERR_CUDA, cudaGetErrorString(ce));
+      rc = PHX_ERR_CUDA;
+    }
+  }
+  if (rc == PHX_OK && kst) {
+    cudaMemset(ctx->d_status, 0, sizeof(int));
+    phx_set_error(ctx, PHX_ERR_CUDA,
+                  "many-branch pair kernel gave up waiting on a pipeline barrier (status " + std::to_string(kst) + ")");
+    rc = PHX_ERR_CUDA;
+  }
+  if (rc == PHX_OK && stats) {
+    float ms = 0, msv = 0;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventElapsedTime(&msv, g->vertex_begin, g->vertex_end);
+    *stats = phx_lw_stats{};
+    stats->ms_total = ms;
+    stats->ms_vertex = msv;
+    stats->pairs = pairs;
+    stats->kernel_launches = g->launches;
+    stats->pair_launches = (int)(g->pair_events.size() / 2);
+    double msp = 0.0;
+    for (size_t i = 0; i + 1 < g->pair_events.size(); i += 2) {
+      float x = 0.f;
+      cudaEventElapsedTime(&x, g->pair_events[i], g->pair_events[i + 1]);
+      msp += x;
+    }
+    stats->ms_pair = msp;
+    stats->plan_chunk = chunk;
+    stats->plan_slots = grid;
+    stats->graph = graph_state;
+    cudaGetLastError();
+  }
+  phx_builder_graph_free(eager);
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  return rc;
+}
+
+}  // namespace
+
 extern "C" int phx_ph_linewidths_d(phx_v3* v, phx_bands* b, const phx_lw_params* p,
                                    double* Aout_d, phx_lw_stats* stats) {
   PHX_ARG(nullptr, v && b && p && Aout_d, "phx_ph_linewidths: bad arguments");
@@ -2163,7 +2500,13 @@ extern "C" int phx_ph_linewidths_d(phx_v3* v, phx_bands* b, const phx_lw_params*
     PHX_CUDA(ctx, cudaMemsetAsync(Aout_d, 0, sizeof(double) * p->num_temperatures * b->nq * b->nb, ctx->stream));
     return PHX_OK;
   }
+  // PHX_WIDE=1: every problem on the many-branch builder (its cross-check
+  // against the nb = 6 kernels)
+  if (env_on("PHX_WIDE")) return run_builder_wide(v, b, p, Aout_d, stats);
   if (v->nb == 6 && !p->window_energy) return run_builder<6>(v, b, p, Aout_d, stats);
+  // the split precisions and cells beyond 16 branches run on the many-branch
+  // builder; FP64 up to 16 branches (or with a window) on the shared-memory one
+  if (v->precision != PHX_PREC_FP64 || v->nb > kMaxNbGeneric) return run_builder_wide(v, b, p, Aout_d, stats);
   return run_builder_generic(v, b, p, Aout_d, stats);
 }
 
@@ -2231,14 +2574,41 @@ constexpr size_t kStaticScratchBytes = size_t(16) << 20;  // 16 MiB per GPU
 __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
 std::mutex g_static_mutex;
-void* g_static_addr[64] = {nullptr};  // device address of g_static_scratch, per device
+// device address of g_static_scratch, per device, with the CUDA context it was
+// looked up in: a new context on the device (after cudaDeviceReset, say) is
+// looked up again
+struct StaticAddr {
+  CUcontext cu = nullptr;
+  void* addr = nullptr;
+};
+StaticAddr g_static_addr[64];
 
-// Looks the array up once per device (the device must be current).  This is
-// the one CUDA call of the variant that must not run inside a stream capture.
+// The current CUDA context, through the driver entry point the runtime hands
+// out (no link-time dependency on the driver library); null if unavailable.
+CUcontext current_cu_context() {
+  using Fn = CUresult (*)(CUcontext*);
+  static Fn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<Fn>(p);
+  }();
+  CUcontext c = nullptr;
+  if (!fn || fn(&c) != CUDA_SUCCESS) c = nullptr;
+  return c;
+}
+
+// Looks the array up once per device and context (the device must be current).
+// This lookup is one reason the entry point is never called inside a stream
+// capture.
 int static_scratch_address(phx_ctx* ctx, void** out) {
   std::lock_guard<std::mutex> lk(g_static_mutex);
   PHX_ARG(ctx, ctx->device >= 0 && ctx->device < 64, "device index out of range");
-  if (!g_static_addr[ctx->device]) {
+  CUcontext cur = current_cu_context();
+  StaticAddr& s = g_static_addr[ctx->device];
+  if (!s.addr || s.cu != cur) {
     void* addr = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&addr, g_static_scratch);
     if (e != cudaSuccess || !addr) {
@@ -2246,9 +2616,12 @@ int static_scratch_address(phx_ctx* ctx, void** out) {
                     std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
       return PHX_ERR_CUDA;
     }
-    g_static_addr[ctx->device] = addr;
+    // the runtime call makes the primary context current when none was
+    cur = current_cu_context();
+    s.cu = cur;
+    s.addr = addr;
   }
-  *out = g_static_addr[ctx->device];
+  *out = s.addr;
   return PHX_OK;
 }
 
@@ -2264,6 +2637,7 @@ int run_builder_static(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
   const size_t sz_T = align_up(sizeof(double) * 8);
   const size_t per_q2 = sizeof(double2) * (size_t)nr3 * nb3;
   const size_t fixed = sz_part + sz_bose + sz_T;
+  // every argument-only check comes before the first call that touches the device
   if (fixed + align_up(per_q2) > kStaticScratchBytes) {
     phx_set_error(ctx, PHX_ERR_ARG,
                   "phx_ph_linewidths_static: this problem needs " + std::to_string(fixed + align_up(per_q2)) +
@@ -2271,8 +2645,18 @@ int run_builder_static(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
                       std::to_string(kStaticScratchBytes) + " bytes (reduce mesh points or temperatures)");
     return PHX_ERR_ARG;
   }
+  const size_t smem_pair = sizeof(double2) * ((size_t)nr3 * kTile + 2 * NB * NB * kTile) +
+                           sizeof(double) * ((size_t)NB * NB * NB * kTile + (size_t)kMaxT * NB * kTile);
+  PHX_ARG(ctx, smem_pair <= 227 * 1024, "phx_ph_linewidths_static: too many R3 vectors");
+  const size_t smem_fold = sizeof(double2) * ((size_t)nr2 + 2 * NB * NB);
+  PHX_ARG(ctx, smem_fold <= 227 * 1024, "phx_ph_linewidths_static: too many R2 vectors");
   const int chunk = (int)std::min<size_t>({(kStaticScratchBytes - fixed) / per_q2, (size_t)512,
                                            (size_t)(q2e - q2b)});
+  PHX_CUDA(ctx, cudaFuncSetAttribute(pair_fp64_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_pair));
+  if (smem_fold > 48 * 1024)
+    PHX_CUDA(ctx, cudaFuncSetAttribute(fold_q2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_fold));
   void* base_v = nullptr;
   PHX_TRY(static_scratch_address(ctx, &base_v));
   char* base = static_cast<char*>(base_v);
@@ -2284,7 +2668,7 @@ int run_builder_static(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
   PHX_CUDA(ctx, cudaMemcpyAsync(temps, p->temperatures, sizeof(double) * nT, cudaMemcpyHostToDevice, st));
   PHX_CUDA(ctx, cudaMemsetAsync(partial, 0, sizeof(double) * (size_t)nq * NB * nT, st));
   bose_kernel<<<std::min(1024, (nq * NB * nT + 255) / 256), 256, 0, st>>>(nq, NB, nT, b->d_E, temps, bose);
-  PairArgs P;
+  PairArgs P{};
   P.m.nq = nq;
   P.m.nb = NB;
   P.m.nT = nT;
@@ -2305,12 +2689,6 @@ int run_builder_static(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
   P.R3 = v->d_R3;
   P.Dp = Dp;
   P.partial = partial;
-  const size_t smem_pair = sizeof(double2) * ((size_t)nr3 * kTile + 2 * NB * NB * kTile) +
-                           sizeof(double) * ((size_t)NB * NB * NB * kTile + (size_t)kMaxT * NB * kTile);
-  PHX_ARG(ctx, smem_pair <= 227 * 1024, "phx_ph_linewidths_static: too many R3 vectors");
-  PHX_CUDA(ctx, cudaFuncSetAttribute(pair_fp64_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem_pair));
-  const size_t smem_fold = sizeof(double2) * (nr2 + 2 * NB * NB);
   const int tiles = (nq + kTile - 1) / kTile;
   for (int c0 = q2b; c0 < q2e; c0 += chunk) {
     const int cnt = std::min(chunk, q2e - c0);

@@ -123,6 +123,11 @@ struct phx_v3 {
   bool cached = false;
   double q2_cached[3];
   phx_builder_graphs* graphs = nullptr;
+  // non-zero (r3, r2) blocks of d_D3w (many-branch builder): for r3, the r2 in
+  // d_r2_list[d_r2_ofs[r3] .. d_r2_ofs[r3+1]); built on first use
+  int* d_r2_ofs = nullptr;
+  int* d_r2_list = nullptr;
+  int r2_max_list = 0;
 };
 
 int phx_scratch_reserve(phx_v3* v3, size_t bytes);

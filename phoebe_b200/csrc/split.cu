@@ -30,6 +30,7 @@
 // owner therefore contracts the rows of its b1 block and averages F, and the
 // triplets whose delta is zero by the reference's own cut-offs are skipped.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -86,6 +87,9 @@ struct TcArgs {
   struct EdgeEvent* edges;     // near-cut-off processes, re-decided in FP64 by edge_fix_kernel
   unsigned* edge_count;
   unsigned edge_cap;
+  unsigned* edge_peak;         // largest event count of the call's launches
+  unsigned* edge_overflow;     // set when this launch's events exceeded edge_cap (none applied)
+  int edge_only;               // 1: rates off, only the near-cut-off events (re-run of an overflowed chunk)
   phx_split_matrix mat;        // matrix modes: mat.plus != null
 };
 
@@ -771,7 +775,7 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
     constexpr int smearing = SM;   // one instantiation per smearing keeps the loop small
     const float sg = (float)M.sigma, ginv = M.sigma > 0.0 ? (float)(1.0 / M.sigma) : 0.f;
     // FP16 operands: |V|^2 carries the square of the B scale, undone here (power of 4)
-    float pre = (float)(phxc::pi * 0.25 * 0.5) * (float)M.norm;
+    float pre = P.edge_only ? 0.f : (float)(phxc::pi * 0.25 * 0.5) * (float)M.norm;
     if (P.fp16) {
       const float sc = fp16_scale(*P.dmax);
       pre *= 1.f / (sc * sc);
@@ -1089,92 +1093,112 @@ int launch_pair(phx_ctx* ctx, const TcArgs& A, int tiles, int slots) {
   return PHX_OK;
 }
 
-// Re-decides, on the FP64 widths, the adaptive deltas whose FP32 cut-off
-// test was too close to call (events of the pair kernel), and adds the
-// difference of the two rates, times the event's weight, to the partial sums
-// of the event's row and slot.  One thread per event.
+// FP64 re-decision of the adaptive deltas of one queued triplet (q1, q2 and
+// its queue entry) whose FP32 cut-off test was too close to call: returns in
+// corr[t] the difference of the two rates, times the entry's weight, for the
+// partial sum of its row (q1, b1); the matrix modes also correct their
+// elements here.
 template <int NT>
-__global__ void edge_fix_kernel(TcArgs P) {
+__device__ __forceinline__ void edge_correction(const TcArgs& P, int q1, int iq2, uint2 e, double* corr) {
   const MeshArgs& M = P.m;
-  if (blockIdx.x == 0 && threadIdx.x == 0 && *P.edge_count > P.edge_cap) atomicOr(P.status, 1 << 20);
-  const unsigned n = min(*P.edge_count, P.edge_cap);
   float pre = (float)(phxc::pi * 0.25 * 0.5) * (float)M.norm;
   if (P.fp16) {
     const float sc = fp16_scale(*P.dmax);
     pre *= 1.f / (sc * sc);
   }
   constexpr float kNorm = (float)(1.0 / (phxc::sqrtPi * phxc::erf2));
+  const float wn = __uint_as_float(e.x);
+  const int b1 = (e.y >> 5) & 7, b2 = (e.y >> 8) & 7, b3 = (e.y >> 11) & 7;
+  const int iq2m = mesh_neg(iq2, M.n0, M.n1, M.n2), iq3 = mesh_add(q1, iq2, M.n0, M.n1, M.n2);
+  const uint4* rq2 = P.rec + (size_t)iq2 * kRecChunks;
+  const uint4* rq2m = P.rec + (size_t)iq2m * kRecChunks;
+  const uint4* rq3 = P.rec + (size_t)iq3 * kRecChunks;
+  unsigned bm2 = 1u << b2, bm3 = 1u << b3;
+  if ((e.y >> 14) & 1) {
+    bm2 = blk_mask(rq2[kChGp].x, b2);
+    bm3 = blk_mask(rq3[kChGp].x, b3);
+  }
+  const Band x1 = load_band<kMaxT>(P.rec + (size_t)q1 * kRecChunks + kChBand + 3 * b1, 1);
+  double c[NT];
+#pragma unroll
+  for (int t = 0; t < NT; ++t) c[t] = 0.0;
+  const double scale = (double)(wn / (float)(__popc(bm2) * __popc(bm3)));
+  for (unsigned m2 = bm2; m2; m2 &= m2 - 1) {
+    const int c2 = __ffs(m2) - 1;
+    const uint4* r2 = rq2 + kChBand + 3 * c2;
+    const uint4* r2m = rq2m + kChBand + 3 * c2;
+    const Band x2 = load_band<NT>(r2, 1), x2m = load_band<NT>(r2m, 1);
+    float cp[NT], cm[NT];   // matrix modes: corrections of the "+" and "-" sums of this c2
+#pragma unroll
+    for (int t = 0; t < NT; ++t) cp[t] = cm[t] = 0.f;
+    for (unsigned m3 = bm3; m3; m3 &= m3 - 1) {
+      const int c3 = __ffs(m3) - 1;
+      const uint4* r3 = rq3 + kChBand + 3 * c3;
+      const Band x3 = load_band<NT>(r3, 1);
+      if (!(x3.E >= phxc::phEnergyCutoff)) continue;
+      const Sig gp = sigma_ad(x2.P, x3.P, x2.vf, x3.vf), gm = sigma_ad(x2m.P, x3.P, x2m.vf, x3.vf);
+      float dp, d1, d2;
+      unsigned near;
+      deltas3(PHX_SMEAR_ADAPTIVE, 0.f, x1.E, x2, x2m, x3, gp, gm, dp, d1, d2, near);
+      if (!near) continue;
+      auto val = [&](double de, float inv) {
+        const float x = (float)de * inv;
+        return __expf(-x * x) * inv * kNorm;
+      };
+      const double ep = x1.E + x2.E - x3.E, e1 = x1.E + x3.E - x2m.E, e2 = x2m.E + x3.E - x1.E;
+      float fdp = dp, fd1 = d1, fd2 = d2;
+      if (near & 1u) fdp = beyond_two_sigma(ep, r2, r3) ? 0.f : val(ep, gp.inv);
+      if (near & 2u) fd1 = beyond_two_sigma(e1, r2m, r3) ? 0.f : val(e1, gm.inv);
+      if (near & 4u) fd2 = beyond_two_sigma(e2, r2m, r3) ? 0.f : val(e2, gm.inv);
+      if (fdp == dp && fd1 == d1 && fd2 == d2) continue;
+      float f0[NT], f1[NT];
+      rate_combine<NT>(pre, x1.iE, x1.N, x2, x2m, x3, dp, d1, d2, f0);
+      rate_combine<NT>(pre, x1.iE, x1.N, x2, x2m, x3, fdp, fd1, fd2, f1);
+#pragma unroll
+      for (int t = 0; t < NT; ++t) c[t] += (double)f1[t] - (double)f0[t];
+      if (P.mat.plus) {
+        float p0[NT], m0[NT], p1[NT], m1[NT];
+        rate_combine2<NT>(pre, x1.iE, x1.N, x2, x2m, x3, dp, d1, d2, p0, m0);
+        rate_combine2<NT>(pre, x1.iE, x1.N, x2, x2m, x3, fdp, fd1, fd2, p1, m1);
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+          cp[t] += p1[t] - p0[t];
+          cm[t] += m1[t] - m0[t];
+        }
+      }
+    }
+    if (P.mat.plus) add_matrix<NT>(P, q1, b1, iq2, c2, scale, cp, cm);
+  }
+#pragma unroll
+  for (int t = 0; t < NT; ++t) corr[t] = scale * c[t];
+}
+
+// Re-decides the recorded near-cut-off events of one pair launch (one thread
+// per event) and adds their corrections to the partial sums of the event's
+// row and slot; records the largest event count of the call.  When the
+// launch had more events than the list holds, none is applied and the
+// launch is flagged: the host re-runs its q2 in pieces whose events fit
+// (events only, rates off) and applies them all there.
+template <int NT>
+__global__ void edge_fix_kernel(TcArgs P) {
+  const unsigned cnt = *P.edge_count;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    atomicMax(P.edge_peak, cnt);
+    if (cnt > P.edge_cap && P.edge_overflow) *P.edge_overflow = 1u;
+  }
+  if (cnt > P.edge_cap) return;
+  const unsigned n = cnt;
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const EdgeEvent ev = P.edges[i];
     const int tile = ev.where >> 12, slot = (ev.where >> 7) & 31, mm = ev.where & 127;
     const int q1 = P.q1_order[tile * kM + mm];
-    const uint2 e = ev.entry;
-    const float wn = __uint_as_float(e.x);
-    const int b1 = (e.y >> 5) & 7, b2 = (e.y >> 8) & 7, b3 = (e.y >> 11) & 7;
-    const int iq2 = ev.iq2, iq2m = mesh_neg(iq2, M.n0, M.n1, M.n2), iq3 = mesh_add(q1, iq2, M.n0, M.n1, M.n2);
-    const uint4* rq2 = P.rec + (size_t)iq2 * kRecChunks;
-    const uint4* rq2m = P.rec + (size_t)iq2m * kRecChunks;
-    const uint4* rq3 = P.rec + (size_t)iq3 * kRecChunks;
-    unsigned bm2 = 1u << b2, bm3 = 1u << b3;
-    if ((e.y >> 14) & 1) {
-      bm2 = blk_mask(rq2[kChGp].x, b2);
-      bm3 = blk_mask(rq3[kChGp].x, b3);
-    }
-    const Band x1 = load_band<kMaxT>(P.rec + (size_t)q1 * kRecChunks + kChBand + 3 * b1, 1);
+    const int b1 = (ev.entry.y >> 5) & 7;
     double corr[NT];
-#pragma unroll
-    for (int t = 0; t < NT; ++t) corr[t] = 0.0;
-    const double scale = (double)(wn / (float)(__popc(bm2) * __popc(bm3)));
-    for (unsigned m2 = bm2; m2; m2 &= m2 - 1) {
-      const int c2 = __ffs(m2) - 1;
-      const uint4* r2 = rq2 + kChBand + 3 * c2;
-      const uint4* r2m = rq2m + kChBand + 3 * c2;
-      const Band x2 = load_band<NT>(r2, 1), x2m = load_band<NT>(r2m, 1);
-      float cp[NT], cm[NT];   // matrix modes: corrections of the "+" and "-" sums of this c2
-#pragma unroll
-      for (int t = 0; t < NT; ++t) cp[t] = cm[t] = 0.f;
-      for (unsigned m3 = bm3; m3; m3 &= m3 - 1) {
-        const int c3 = __ffs(m3) - 1;
-        const uint4* r3 = rq3 + kChBand + 3 * c3;
-        const Band x3 = load_band<NT>(r3, 1);
-        if (!(x3.E >= phxc::phEnergyCutoff)) continue;
-        const Sig gp = sigma_ad(x2.P, x3.P, x2.vf, x3.vf), gm = sigma_ad(x2m.P, x3.P, x2m.vf, x3.vf);
-        float dp, d1, d2;
-        unsigned near;
-        deltas3(PHX_SMEAR_ADAPTIVE, 0.f, x1.E, x2, x2m, x3, gp, gm, dp, d1, d2, near);
-        if (!near) continue;
-        auto val = [&](double de, float inv) {
-          const float x = (float)de * inv;
-          return __expf(-x * x) * inv * kNorm;
-        };
-        const double ep = x1.E + x2.E - x3.E, e1 = x1.E + x3.E - x2m.E, e2 = x2m.E + x3.E - x1.E;
-        float fdp = dp, fd1 = d1, fd2 = d2;
-        if (near & 1u) fdp = beyond_two_sigma(ep, r2, r3) ? 0.f : val(ep, gp.inv);
-        if (near & 2u) fd1 = beyond_two_sigma(e1, r2m, r3) ? 0.f : val(e1, gm.inv);
-        if (near & 4u) fd2 = beyond_two_sigma(e2, r2m, r3) ? 0.f : val(e2, gm.inv);
-        if (fdp == dp && fd1 == d1 && fd2 == d2) continue;
-        float f0[NT], f1[NT];
-        rate_combine<NT>(pre, x1.iE, x1.N, x2, x2m, x3, dp, d1, d2, f0);
-        rate_combine<NT>(pre, x1.iE, x1.N, x2, x2m, x3, fdp, fd1, fd2, f1);
-#pragma unroll
-        for (int t = 0; t < NT; ++t) corr[t] += (double)f1[t] - (double)f0[t];
-        if (P.mat.plus) {
-          float p0[NT], m0[NT], p1[NT], m1[NT];
-          rate_combine2<NT>(pre, x1.iE, x1.N, x2, x2m, x3, dp, d1, d2, p0, m0);
-          rate_combine2<NT>(pre, x1.iE, x1.N, x2, x2m, x3, fdp, fd1, fd2, p1, m1);
-#pragma unroll
-          for (int t = 0; t < NT; ++t) {
-            cp[t] += p1[t] - p0[t];
-            cm[t] += m1[t] - m0[t];
-          }
-        }
-      }
-      if (P.mat.plus) add_matrix<NT>(P, q1, b1, iq2, c2, scale, cp, cm);
-    }
-    double* out = P.partial + (((size_t)slot * M.nq + q1) * 6 + b1) * NT;
+    edge_correction<NT>(P, q1, ev.iq2, ev.entry, corr);
+    double* out = P.partial + (((size_t)slot * P.m.nq + q1) * 6 + b1) * NT;
 #pragma unroll
     for (int t = 0; t < NT; ++t)
-      if (corr[t] != 0.0) atomicAdd(out + t, scale * corr[t]);
+      if (corr[t] != 0.0) atomicAdd(out + t, corr[t]);
   }
 }
 
@@ -1236,7 +1260,8 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
                          const double2* Dp, uint8_t* Bimg, const void* rec, double emax, int q2_first,
                          int q2_count, int slots, double* partial, int* launches, cudaEvent_t ev_begin,
                          cudaEvent_t ev_end, int fp16, const unsigned* dmax, void* edges, unsigned* edge_count,
-                         unsigned edge_cap, const phx_split_matrix* mat) {
+                         unsigned edge_cap, unsigned* edge_peak, unsigned* edge_overflow, int edge_only,
+                         const phx_split_matrix* mat) {
   const int Kp = phx_split_kp(v->nr3);
   const int nkc = Kp / kKC;
   convert_b_kernel<<<dim3(q2_count, kParts * nkc), 256, 0, ctx->stream>>>(Dp, v->nr3, Kp, q2_count, Bimg, fp16,
@@ -1263,6 +1288,9 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
   A.edges = static_cast<EdgeEvent*>(edges);
   A.edge_count = edge_count;
   A.edge_cap = edge_cap;
+  A.edge_peak = edge_peak;
+  A.edge_overflow = edge_overflow;
+  A.edge_only = edge_only;
   A.mat = mat ? *mat : phx_split_matrix{nullptr, nullptr, 0, 0, 0};
   PHX_ARG(ctx, slots < 32 && (M.nq + kM - 1) / kM < (1 << 20), "split path: at most 31 slots");
   PHX_CUDA(ctx, cudaMemsetAsync(edge_count, 0, sizeof(unsigned), ctx->stream));
@@ -1290,9 +1318,19 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
 
 size_t phx_split_smem_bytes(int nr3) { return pair_tc_smem(phx_split_kp(nr3)); }
 
-// capacity of the near-cut-off event list of one pair launch, and its bytes
-unsigned phx_split_edge_cap() { return 1u << 18; }
-size_t phx_split_edge_bytes() { return sizeof(EdgeEvent) * phx_split_edge_cap(); }
+// capacity of the near-cut-off event list of one pair launch (a smaller one
+// may be set for tests: a launch with more events is re-run in pieces), and
+// the bytes of the list
+namespace {
+constexpr unsigned kEdgeCapMax = 1u << 18;
+std::atomic<unsigned> g_edge_cap{kEdgeCapMax};
+}  // namespace
+unsigned phx_split_edge_cap() { return g_edge_cap.load(); }
+size_t phx_split_edge_bytes() { return sizeof(EdgeEvent) * kEdgeCapMax; }
+extern "C" int phx_debug_set_split_edge_cap(unsigned cap) {
+  g_edge_cap.store(cap == 0 || cap > kEdgeCapMax ? kEdgeCapMax : cap);
+  return PHX_OK;
+}
 
 namespace {
 template <int NT>

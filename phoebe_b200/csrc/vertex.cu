@@ -150,6 +150,24 @@ int dmalloc(phx_ctx* ctx, T** p, size_t n) {
   return PHX_OK;
 }
 
+// D3w[r3][r2][a][b][c] = D3(a,b,c,r3,r2) w2(r2,at_a,at_b) w3(r3,at_a,at_c)^2:
+// the reference applies w3 in cacheD3 and again in the R3 sum
+// (interaction_3ph.cpp:166-169,284-285), folded here once with w2.
+__global__ void fold_weights_kernel(int nat, int nr2, int nr3, const double* __restrict__ D3,
+                                    const double* __restrict__ w2, const double* __restrict__ w3,
+                                    double* __restrict__ D3w) {
+  const int nb = 3 * nat;
+  const size_t nb3 = (size_t)nb * nb * nb, n = nb3 * nr3 * nr2;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t abc = i % nb3, rr = i / nb3;
+    const int r2 = (int)(rr % nr2), r3 = (int)(rr / nr2);
+    const int i3 = (int)(abc % nb), i2 = (int)((abc / nb) % nb), i1 = (int)(abc / ((size_t)nb * nb));
+    const int at1 = i1 / 3, at2 = i2 / 3, at3 = i3 / 3;
+    const double ww3 = w3[((size_t)r3 * nat + at1) * nat + at3];
+    D3w[i] = D3[(abc * nr3 + r3) * nr2 + r2] * w2[((size_t)r2 * nat + at1) * nat + at2] * ww3 * ww3;
+  }
+}
+
 }  // namespace
 
 extern "C" int phx_v3_create(phx_ctx* ctx, int nat, int nr2, int nr3, const double* D3,
@@ -169,20 +187,8 @@ extern "C" int phx_v3_create(phx_ctx* ctx, int nat, int nr2, int nr3, const doub
   v->R3.assign(R3, R3 + 3 * (size_t)nr3);
   const int nb = v->nb;
   const size_t nb3 = (size_t)nb * nb * nb;
-  // weights folded once: w2(r2,a,b) * w3(r3,a,c) [cacheD3] * w3(r3,a,c) [tmploop]
-  std::vector<double> d3w(nb3 * nr3 * nr2);
-  for (size_t abc = 0; abc < nb3; ++abc) {
-    const int i3 = abc % nb, i2 = (abc / nb) % nb, i1 = abc / (nb * nb);
-    const int at1 = i1 / 3, at2 = i2 / 3, at3 = i3 / 3;
-    for (int r3 = 0; r3 < nr3; ++r3)
-      for (int r2 = 0; r2 < nr2; ++r2) {
-        const double ww3 = w3[((size_t)r3 * nat + at1) * nat + at3];
-        d3w[((size_t)r3 * nr2 + r2) * nb3 + abc] =
-            D3[(abc * nr3 + r3) * nr2 + r2] * w2[((size_t)r2 * nat + at1) * nat + at2] * ww3 * ww3;
-      }
-  }
   int rc = PHX_OK;
-  if (rc == PHX_OK) rc = dmalloc(ctx, &v->d_D3w, d3w.size());
+  if (rc == PHX_OK) rc = dmalloc(ctx, &v->d_D3w, nb3 * nr3 * nr2);
   if (rc == PHX_OK) rc = dmalloc(ctx, &v->d_D3raw, nb3 * nr3 * nr2);
   if (rc == PHX_OK) rc = dmalloc(ctx, &v->d_w2, (size_t)nr2 * nat * nat);
   if (rc == PHX_OK) rc = dmalloc(ctx, &v->d_w3, (size_t)nr3 * nat * nat);
@@ -195,15 +201,19 @@ extern "C" int phx_v3_create(phx_ctx* ctx, int nat, int nr2, int nr3, const doub
     return rc;
   }
   cudaStream_t st = ctx->stream;
-  cudaError_t e = cudaMemcpyAsync(v->d_D3w, d3w.data(), sizeof(double) * d3w.size(), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(v->d_D3raw, D3, sizeof(double) * nb3 * nr3 * nr2, cudaMemcpyHostToDevice, st);
+  cudaError_t e = cudaMemcpyAsync(v->d_D3raw, D3, sizeof(double) * nb3 * nr3 * nr2, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(v->d_w2, w2, sizeof(double) * nr2 * nat * nat, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(v->d_w3, w3, sizeof(double) * nr3 * nat * nat, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(v->d_R2, R2, sizeof(double) * 3 * nr2, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(v->d_R3, R3, sizeof(double) * 3 * nr3, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    const size_t n = nb3 * nr3 * nr2;
+    fold_weights_kernel<<<(unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 64), 256, 0, st>>>(
+        nat, nr2, nr3, v->d_D3raw, v->d_w2, v->d_w3, v->d_D3w);
+    e = cudaGetLastError();
+  }
   // the caller may free or reuse its host arrays on return
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
@@ -228,6 +238,8 @@ extern "C" int phx_v3_destroy(phx_v3* v) {
     phx_dev_free(v->ctx, v->d_R3);
     phx_dev_free(v->ctx, v->d_plus);
     phx_dev_free(v->ctx, v->d_mins);
+    phx_dev_free(v->ctx, v->d_r2_ofs);
+    phx_dev_free(v->ctx, v->d_r2_list);
   }
   delete v;
   return PHX_OK;

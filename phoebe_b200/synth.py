@@ -281,12 +281,17 @@ def random_fc3(crystal, num_pairs, seed, amp_ev=3.0, decay_ang=4.0,
             r = max(r, np.abs(blk.sum(axis=(0, 3))).max())
         return r
 
-    for it in range(max_iter):
-        B = asr_project(symmetrise(B))
-        ref = np.abs(B).max()
-        res = max(np.abs(symmetrise(B) - B).max(), asr_residual(B)) / ref
-        if res < tol:
-            break
+    if nb >= 24:
+        # large cells (the 36-branch one): the same alternating projections,
+        # vectorised with torch on a GPU when one is present
+        B, it, res = _project_torch(B, jmap, axes, R2s, pairs, nat, nb, tol, max_iter)
+    else:
+        for it in range(max_iter):
+            B = asr_project(symmetrise(B))
+            ref = np.abs(B).max()
+            res = max(np.abs(symmetrise(B) - B).max(), asr_residual(B)) / ref
+            if res < tol:
+                break
     # dense ShengBTE-style layout
     Rvecs = sorted(set(p[0] for p in pairs) | set(p[1] for p in pairs))
     ridx = {v: i for i, v in enumerate(Rvecs)}
@@ -297,6 +302,50 @@ def random_fc3(crystal, num_pairs, seed, amp_ev=3.0, decay_ang=4.0,
     Rcart = np.array([A @ np.array(v, dtype=np.float64) for v in Rvecs])
     w = np.ones((nr, nat, nat))
     return FC3(D3, Rcart.copy(), Rcart.copy(), w, w.copy(), num_pairs, it + 1, res)
+
+
+def _project_torch(B, jmap, axes, R2s, pairs, nat, nb, tol, max_iter):
+    """random_fc3's alternating projections (index-permutation symmetrisation,
+    then the acoustic sum rule per R2 group) for large blocks, with torch
+    index_add_ instead of numpy loops.  Returns (B, iterations, residual)."""
+    import torch
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    n = B.shape[0]
+    gidx = {R2: g for g, R2 in enumerate(R2s)}
+    gid = torch.tensor([gidx[p[0]] for p in pairs], dtype=torch.int64, device=dev)
+    cnt = torch.bincount(gid, minlength=len(R2s)).to(torch.float64) * nat
+    jm = torch.from_numpy(np.ascontiguousarray(jmap)).to(dev)
+    X = torch.from_numpy(B).to(dev)
+
+    def sym(Y):
+        S = torch.zeros_like(Y)
+        for k, ax in enumerate(axes):
+            S.index_add_(0, jm[:, k], Y.permute((0,) + tuple(1 + a for a in ax)))
+        return S / 6.0
+
+    def group_sums(Y):
+        ps = Y.reshape(n, nb, nb, nat, 3).sum(dim=3)
+        return torch.zeros((len(R2s), nb, nb, 3), dtype=Y.dtype, device=dev).index_add_(0, gid, ps)
+
+    def asr(Y):
+        corr = (group_sums(Y) / cnt[:, None, None, None])[gid]
+        return (Y.reshape(n, nb, nb, nat, 3) - corr[:, :, :, None, :]).reshape(n, nb, nb, nb)
+
+    S = sym(X)
+    res = float("inf")
+    it = 0
+    for it in range(max_iter):
+        X = asr(S)
+        S = sym(X)
+        ref = X.abs().max()
+        res = float(torch.maximum((S - X).abs().max(), group_sums(X).abs().max()) / ref)
+        if res < tol:
+            break
+    out = X.cpu().numpy()
+    del X, S
+    if dev == "cuda":
+        torch.cuda.empty_cache()
+    return out, it, res
 
 
 # ---------------------------------------------------------------------------

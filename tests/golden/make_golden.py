@@ -9,7 +9,8 @@ them follow test/interaction3phTest.cpp:9-127 (Gamma,Gamma,Gamma; sum over the
 optical manifold) and :129-350 (q-indices 10, 210, 200 on a 20^3 mesh; sum
 over b1 < 2 after symmetrizeCoupling).
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference]
+Usage:  python tests/golden/make_golden.py /path/to/reference
+(the root of a mir-group/phoebe checkout; required)
 """
 import os
 import sys
@@ -41,4 +42,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py /path/to/reference")
+    main(sys.argv[1])

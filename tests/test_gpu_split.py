@@ -67,3 +67,34 @@ def test_split_linewidths_match_fp64(ctx, diamond, mesh, smearing, temps, precis
     assert rel.max() < 1e-5, rel.max()
     np.testing.assert_allclose(k16, k64, rtol=1e-4)
     assert sm.stats.kernel_launches > 0
+
+
+def test_near_cutoff_events_beyond_the_list_capacity(ctx, diamond):
+    """The split path records triplets whose adaptive-delta cut-off test is
+    too close for FP32 and re-decides them in FP64 after each pair launch.
+    With the event list capped below what a chunk produces, the chunk applies
+    none of its events and is re-run in smaller q2 pieces with the rates off;
+    the linewidths must not change (beyond rounding)."""
+    from phoebe_b200 import _abi
+    L = _abi.load()
+    mesh, temps = (8, 8, 8), (300.0,)
+    A0, k0, E, sm0 = _builder(ctx, diamond, mesh, "adaptive", temps, "split_fp16")
+    assert sm0.stats.edge_events_cap == 2 ** 18
+    assert sm0.stats.edge_overflow_chunks == 0
+    peak = sm0.stats.edge_events_peak
+    assert peak > 4      # this mesh has near-cut-off events
+    try:
+        _abi.check(L.phx_debug_set_split_edge_cap(peak // 3), ctx.h)
+        A1, k1, _, sm1 = _builder(ctx, diamond, mesh, "adaptive", temps, "split_fp16")
+        assert sm1.stats.edge_events_cap == peak // 3
+        assert sm1.stats.edge_overflow_chunks >= 1
+    finally:
+        _abi.check(L.phx_debug_set_split_edge_cap(0), ctx.h)
+    ok = E.reshape(-1) >= C.phExcludeCutoff
+    big = ok[None, :] & (np.abs(A0) > 1e-8 * np.abs(A0).max())
+    rel = np.abs(A1 - A0)[big] / np.abs(A0)[big]
+    assert rel.max() < 1e-6, rel.max()
+    # and the capped run still matches the FP64 path at the split bar
+    A64, _, _, _ = _builder(ctx, diamond, mesh, "adaptive", temps, "fp64")
+    rel64 = np.abs(A1 - A64)[big] / np.abs(A64)[big]
+    assert rel64.max() < 1e-5, rel64.max()

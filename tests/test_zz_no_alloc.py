@@ -100,3 +100,53 @@ def test_static_scratch_rejects_problems_beyond_its_size():
     rc = L.phx_ph_linewidths_static(v3.h, bands.h, ctypes.byref(p), ctypes.c_void_p(out.data_ptr()))
     assert rc == _abi.PHX_ERR_ARG
     assert "static scratch" in _abi.last_error(ctx.h)
+
+
+def test_static_scratch_q2_slices_match_regular_entry_point():
+    """A q2 slice (what one rank of a multi-GPU run computes, finalize = 0) over
+    more than one chunk of the 16 MiB array, and an empty slice."""
+    import torch
+
+    from phoebe_b200 import _abi, synth
+    from phoebe_b200.core import Context, Interaction3Ph, PhononH0
+
+    ctx = Context(0)
+    cr = synth.diamond_crystal()
+    fc3 = synth.random_fc3(cr, 400, synth.SEED_BASE)
+    mesh = (6, 6, 6)
+    T = np.array([C.kelvin_to_ry(t) for t in (100.0, 300.0, 600.0)])
+    h0 = PhononH0(ctx, cr, synth.diamond_fc2(cr))
+    bands = h0.populate(mesh, withVelocities=True)
+    v3 = Interaction3Ph(ctx, cr, fc3, precision="fp64")
+    nq, nb = bands.nq, bands.nb
+    n = len(T) * nq * nb
+    # q2 per chunk of the static path: what is left of 16 MiB after the Bose
+    # table and the partial sums, over one q2 slab of the cached vertex
+    align = lambda x: (x + 255) // 256 * 256
+    fixed = 2 * align(8 * nq * nb * len(T)) + align(64)
+    chunk = (16 * 2 ** 20 - fixed) // (16 * v3.nr3 * nb ** 3)
+    q2b, q2e = 30, 190
+    assert q2e - q2b > chunk, "the slice must span more than one chunk"
+    L = _abi.load()
+    p = _params(T, nq, "adaptive", 0.0)
+    p.finalize = 0
+    p.q2_begin, p.q2_end = q2b, q2e
+    ref = torch.zeros(n, dtype=torch.float64, device="cuda")
+    _abi.check(L.phx_ph_linewidths_d(v3.h, bands.h, ctypes.byref(p), ctypes.c_void_p(ref.data_ptr()), None),
+               ctx.h)
+    out = torch.full((n,), np.nan, dtype=torch.float64, device="cuda")
+    _abi.check(L.phx_ph_linewidths_static(v3.h, bands.h, ctypes.byref(p), ctypes.c_void_p(out.data_ptr())),
+               ctx.h)
+    A, B = ref.cpu().numpy(), out.cpu().numpy()
+    assert np.abs(A).max() > 0 and np.all(np.isfinite(B))
+    big = np.abs(A) > 1e-6 * np.abs(A).max()
+    assert (np.abs(B - A)[big] / np.abs(A)[big]).max() < 1e-10
+    assert np.abs(B - A)[~big].max(initial=0.0) < 1e-16 * np.abs(A).max()
+    # an empty slice writes zeros
+    p.q2_begin = p.q2_end = 50
+    _abi.check(L.phx_ph_linewidths_static(v3.h, bands.h, ctypes.byref(p), ctypes.c_void_p(out.data_ptr())),
+               ctx.h)
+    assert np.all(out.cpu().numpy() == 0.0)
+    v3.close()
+    bands.close()
+    h0.close()

@@ -49,14 +49,19 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="3ph", choices=["3ph", "elph", "smatrix", "perovskite", "relaxons"],
+    ap.add_argument("--workload", default="3ph", choices=["3ph", "elph", "smatrix", "perovskite", "relaxons", "twelve", "screening"],
                     help="3ph: the headline linewidth builder; elph: electron-phonon linewidths "
                          "(8 Wannier functions, 343 x 343 coupling vectors, 40^3 k, 20^3 q); smatrix: "
                          "the scattering matrix of the 3ph workload stored in device memory and its "
                          "matrix-vector products, beside the matrix-free product; perovskite: the batched "
                          "uneven instances (5-atom cell, 15 branches, 24^3 mesh, per-q1 q2 window) on a q2 "
                          "slice of --q2-slice points per step; relaxons: the relaxon solver (a2Omega, full "
-                         "eigensolve, relaxon conductivity) on the stored matrix of the 3ph workload at --mesh")
+                         "eigensolve, relaxon conductivity) on the stored matrix of the 3ph workload at --mesh; "
+                         "twelve: the 12-atom cell (36 branches, 4000 FC3 pairs, 16^3 mesh) of the learned-screening "
+                         "workload, split and FP64 on q2 slices of --q2-slice points; screening: learned screening "
+                         "on the 12-atom cell at 16^3 (exact split run, training pairs from the exact builder, "
+                         "screened run, errors)")
+    ap.add_argument("--train-q2", type=int, default=512, help="screening: q2 points whose vertices train the network")
     ap.add_argument("--q2-slice", type=int, default=256, help="q2 points per perovskite step")
     ap.add_argument("--elph-k1", type=int, default=64, help="outer k points timed per elph step")
     ap.add_argument("--precision", default=os.environ.get("PHX_BENCH_PRECISION", "split_fp16"),
@@ -675,6 +680,18 @@ def run_perovskite(args):
     ms_step = float(np.mean(ms))
     rate = float(np.sum(pairs) / (np.sum(ms) / 1000.0))
     total = int(keep.sum())
+    # the split path (many-branch builder, tcgen05 R3 transform) on the same slices
+    prec = args.precision if args.precision != "fp64" else "split_fp16"
+    v3.setPrecision(prec)
+    rng = np.random.default_rng(0)
+    ms16, pairs16 = [], []
+    for i in range(args.warmup + args.steps):
+        q0 = int(rng.integers(0, nq - args.q2_slice))
+        sm.setup(q0, q0 + args.q2_slice, finalize=False)
+        if i >= args.warmup:
+            ms16.append(sm.stats.ms_total)
+            pairs16.append(int(per_q2[q0:q0 + args.q2_slice].sum()))
+    rate16 = float(np.sum(pairs16) / (np.sum(ms16) / 1000.0))
     line = {"metric": "windowed (q1,q2) pairs/s, 15 branches, 24^3 mesh, per-q1 q2 window",
             "value": rate, "unit": "pairs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
@@ -685,12 +702,203 @@ def run_perovskite(args):
                        "windowed_pairs_total": total, "window_fill": total / float(nq * nq)},
             "bands_s_13824_points": bands_s,
             "projected_full_run_s": total / rate,
+            "split_path": {"precision": prec, "value": rate16, "unit": "pairs/s", "ms_per_step": float(np.mean(ms16)),
+                           "speedup_over_fp64": rate16 / rate, "projected_full_run_s": total / rate16},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def run_twelve(args):
+    """The 12-atom cell (36 branches, 4000 FC3 pairs, 16^3 mesh, adaptive smearing, 300 K) on the
+    many-branch builder: the split path and the FP64 path on the same random q2 slices (every q1),
+    their linewidth partial sums compared; the full run is projected from the rates."""
+    import torch
+    from phoebe_b200 import constants as C
+    from phoebe_b200 import synth
+    from phoebe_b200.core import Context, Interaction3Ph, PhononH0, PhScatteringMatrix
+    t0 = time.perf_counter()
+    w = synth.twelve_atom_workload()
+    gen_s = time.perf_counter() - t0
+    torch.cuda.set_device(0)
+    ctx = Context(0)
+    h0 = PhononH0(ctx, w.crystal, w.fc2)
+    t0 = time.perf_counter()
+    bands = h0.populate(w.mesh, withVelocities=True)
+    bands_s = time.perf_counter() - t0
+    prec = args.precision if args.precision != "fp64" else "split_fp16"
+    v3 = Interaction3Ph(ctx, w.crystal, w.fc3, precision=prec)
+    T = np.array([C.kelvin_to_ry(t) for t in w.temperatures_k])
+    sm = PhScatteringMatrix(v3, bands, T, "adaptive")
+    nq, nb, nr3 = bands.nq, bands.nb, v3.nr3
+    rng = np.random.default_rng(0)
+    starts = [int(rng.integers(0, nq - args.q2_slice)) for _ in range(args.warmup + args.steps)]
+    ms, parts, pms, plaunch = [], [], [], 0
+    with Clocks(0) as clk:
+        for i, q0 in enumerate(starts):
+            A = sm.setup(q0, q0 + args.q2_slice, finalize=False)
+            if i >= args.warmup:
+                ms.append(sm.stats.ms_total)
+                pms.append(sm.stats.ms_pair)
+                plaunch += sm.stats.pair_launches
+                parts.append(A)
+    ms_step = float(np.mean(ms))
+    pairs_step = nq * args.q2_slice
+    rate = pairs_step / (ms_step / 1000.0)
+    # FP64 on the same slices (the first two timed ones)
+    v3.setPrecision("fp64")
+    ms64, rel = [], []
+    for i, q0 in enumerate(starts[args.warmup:args.warmup + 2]):
+        A64 = sm.setup(q0, q0 + args.q2_slice, finalize=False)
+        ms64.append(sm.stats.ms_total)
+        big = np.abs(A64) > 1e-8 * np.abs(A64).max()
+        rel.append(float((np.abs(parts[i] - A64)[big] / np.abs(A64)[big]).max()))
+    rate64 = pairs_step / (float(np.mean(ms64)) / 1000.0)
+    fl_tc = 8 * nb ** 3 * nr3            # R3 transform per pair (tensor cores)
+    fl_simt = 16 * nb ** 4               # e1 and e3 contractions per pair (CUDA cores, FP32)
+    ach = fl_tc * pairs_step * len(pms) / (float(np.sum(pms)) / 1000.0) / 1e12
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    pk = peaks.get("bf16_tflops_sustained", 1346.1)
+    ach_simt = fl_simt * pairs_step * len(pms) / (float(np.sum(pms)) / 1000.0) / 1e12
+    line = {"metric": "3ph (q1,q2) pairs/s, 12-atom cell (36 branches), 16^3 mesh",
+            "value": rate, "unit": "pairs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "fp16x3->f32" if prec == "split_fp16" else "bf16x3->f32", "data": "synthetic",
+            "config": {"workload": "12-atom cell, 36 branches, 4000 FC3 pairs (nr3=%d), 16x16x16 mesh, adaptive "
+                                   "smearing, 300 K; %d q2 x all %d q1 per step (random slice)"
+                                   % (nr3, args.q2_slice, nq), "fc3_generation_s": gen_s},
+            "bands_s_4096_points": bands_s,
+            "projected_full_run_s": nq * nq / rate,
+            "fp64_path": {"value": rate64, "unit": "pairs/s", "ms_per_step": float(np.mean(ms64)),
+                          "split_speedup": rate / rate64, "projected_full_run_s": nq * nq / rate64,
+                          "split_partial_linewidth_rel_err_max": max(rel)},
+            "roofline": {"bound": "tensor", "achieved": ach, "peak": pk, "unit": "TFLOP/s", "frac": ach / pk,
+                         "traffic": None, "flops_per_pair": fl_tc, "peak_source": "measured (sustained)",
+                         "ms_per_pair_launch": float(np.sum(pms)) / max(1, plaunch),
+                         "simt_view": {"what": "FP32 e1/e3 contractions on CUDA cores", "flops_per_pair": fl_simt,
+                                       "achieved": ach_simt, "peak": FFMA_PEAK_TFLOPS,
+                                       "frac": ach_simt / FFMA_PEAK_TFLOPS}},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def run_screening(args):
+    """Learned screening on the 12-atom cell (36 branches, 4000 FC3 pairs, 16^3 mesh, adaptive
+    smearing, 300 K).  The exact split builder over every (q1, q2) vertex; the network
+    (12 -> 256 -> 256 -> 256 -> 1, tensor-core kernels) trained on the exact contributions of the
+    vertices of --train-q2 q2 points (every q1), each from a one-q2 call of the builder; the
+    threshold calibrated on those; then the screened builder over every vertex.  FP64 is timed on a
+    q2 slice for the three-way comparison."""
+    import torch
+    from phoebe_b200 import constants as C
+    from phoebe_b200 import screening, synth
+    from phoebe_b200.core import Context, Interaction3Ph, PhononH0, PhScatteringMatrix
+    w = synth.twelve_atom_workload()
+    torch.cuda.set_device(0)
+    ctx = Context(0)
+    h0 = PhononH0(ctx, w.crystal, w.fc2)
+    bands = h0.populate(w.mesh, withVelocities=True)
+    E = bands.get(velocities=False)[0]
+    prec = args.precision if args.precision != "fp64" else "split_fp16"
+    v3 = Interaction3Ph(ctx, w.crystal, w.fc3, precision=prec)
+    T = np.array([C.kelvin_to_ry(t) for t in w.temperatures_k])
+    sm = PhScatteringMatrix(v3, bands, T, "adaptive")
+    nq, nb = bands.nq, bands.nb
+    with Clocks(0) as clk:
+        A_exact = sm.setup()
+        ms_exact = sm.stats.ms_total
+        k_exact = sm.thermalConductivity(w.crystal.volume)
+        # training pairs from the exact builder, one q2 at a time
+        rng = np.random.default_rng(4)
+        q2_train = np.sort(rng.choice(nq, size=min(args.train_q2, nq), replace=False))
+        t0 = time.perf_counter()
+        u = screening.pair_contributions(sm, q2_train)                  # (nt, nq, nb)
+        gen_s = time.perf_counter() - t0
+        A0 = A_exact[0].reshape(nq, nb)
+        X = screening.pair_features(w.mesh, E, q2_train).reshape(-1, screening.NIN)
+        y = screening.pair_targets(u, A0).reshape(-1)
+        net = screening.ScreeningMLP(ctx, seed=7)
+        t0 = time.perf_counter()
+        epochs = 6
+        losses = net.train(X, y, epochs=epochs, batch=4096, lr=1e-3)
+        train_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        pred = net.infer(X).reshape(len(q2_train), nq)
+        infer_s = time.perf_counter() - t0
+        # threshold: the largest whose drops, scaled from the training q2 to the whole mesh,
+        # move no training linewidth by more than 5e-4
+        frac = u / np.where(A0 > 0, A0, np.inf)[None]
+        scale = nq / float(len(q2_train))
+        thr = None
+        for cand in np.arange(-3.0, -12.01, -0.25):
+            drop = pred < cand
+            err = (np.where(drop[:, :, None], frac, 0.0).sum(axis=0) * scale).max()
+            if err <= 5e-4:
+                thr = float(cand)
+                break
+        # perfect screen on the training vertices: the most vertices of each q1 that can go
+        # (smallest largest-fraction first) with the scaled drop <= 1e-3 for every mode
+        fmax = frac.max(axis=2)                                        # (nt, nq)
+        perfect = 0
+        for q1 in range(nq):
+            order = np.argsort(fmax[:, q1])
+            cum = np.cumsum(frac[order, q1, :], axis=0) * scale          # (nt, nb)
+            ok = np.nonzero(cum.max(axis=1) <= 1e-3)[0]
+            perfect += 0 if ok.size == 0 else ok[-1] + 1
+        perfect_frac = perfect / float(fmax.size)
+        A_scr = sm.setup_screened(net, thr if thr is not None else -np.inf)
+        ms_scr = sm.stats.ms_total
+        skipped = int(sm.stats.pairs_screened_out)
+        k_scr = sm.thermalConductivity(w.crystal.volume)
+    ok = (E.reshape(-1) >= C.phExcludeCutoff)[None, :]
+    big = ok & (np.abs(A_exact) > 1e-8 * np.abs(A_exact).max())
+    lw_err = float((np.abs(A_scr - A_exact)[big] / np.abs(A_exact)[big]).max())
+    d0, d1 = np.diagonal(k_exact[0]), np.diagonal(k_scr[0])
+    kappa_err = float(np.abs(d1 - d0).max() / np.abs(d0).max())
+    # FP64 on a q2 slice
+    v3.setPrecision("fp64")
+    sl = min(args.q2_slice, nq)
+    sm.setup(0, sl, finalize=False)
+    ms64 = sm.stats.ms_total
+    rate64 = nq * sl / (ms64 / 1000.0)
+    pairs = nq * nq
+    line = {"metric": "3ph (q1,q2) pairs/s with learned screening, 12-atom cell (36 branches), 16^3 mesh",
+            "value": pairs / (ms_scr / 1000.0), "unit": "pairs/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "ms_per_step": ms_scr, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "fp16x3->f32" if prec == "split_fp16" else "bf16x3->f32", "data": "synthetic",
+            "config": {"workload": "12-atom cell, 36 branches, 4000 FC3 pairs (nr3=%d), 16x16x16 mesh (%d vertices), "
+                                   "adaptive smearing, 300 K" % (v3.nr3, pairs),
+                       "network": "12-256-256-256-1 GELU, BF16 weights, FP32 accumulation, tcgen05 GEMMs"},
+            "exact_split": {"value": pairs / (ms_exact / 1000.0), "ms": ms_exact},
+            "exact_fp64": {"value": rate64, "ms_per_%d_q2" % sl: ms64, "projected_full_run_s": pairs / rate64},
+            "screened_split": {"value": pairs / (ms_scr / 1000.0), "ms": ms_scr, "vertices_dropped": skipped,
+                               "fraction_dropped": skipped / float(pairs),
+                               "speedup_over_exact_split": ms_exact / ms_scr,
+                               "speedup_over_fp64": (pairs / (ms_scr / 1000.0)) / rate64,
+                               "log10_threshold": thr, "linewidth_rel_err_max": lw_err,
+                               "kappa_rel_err": kappa_err},
+            "training": {"vertices": int(X.shape[0]), "q2_points": int(len(q2_train)), "epochs": epochs,
+                         "data_generation_s": gen_s, "train_s": train_s,
+                         "train_samples_per_s": X.shape[0] * epochs / train_s,
+                         "loss_first_last": [float(losses[0]), float(losses[-1])],
+                         "inference_ns_per_vertex": 1e9 * infer_s / X.shape[0]},
+            "perfect_screen_bound": {"fraction_of_training_vertices": perfect_frac,
+                                     "what": "vertices a perfect screen could drop with every linewidth within 1e-3"},
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
 
 
 def main():
     args = parse()
+    if args.workload == "screening":
+        run_screening(args)
+        return
+    if args.workload == "twelve":
+        run_twelve(args)
+        return
     if args.workload == "perovskite":
         run_perovskite(args)
         return

@@ -181,6 +181,8 @@ typedef struct phx_lw_stats {
    * in smaller pieces with the rates off (edge_overflow_chunks counts them) */
   long long edge_events_peak, edge_events_cap;
   int edge_overflow_chunks;
+  /* phx_ph_linewidths_screened: vertices (q1, q2) the network dropped */
+  long long pairs_screened_out;
 } phx_lw_stats;
 
 /* Whole PhScatteringMatrix::builder, switchCase 2 (linewidths), on the GPU:
@@ -195,6 +197,20 @@ int phx_ph_linewidths(phx_v3* v3, phx_bands* bands, const phx_lw_params* params,
 /* Same with a device output buffer (nT*nq*nb doubles). */
 int phx_ph_linewidths_d(phx_v3* v3, phx_bands* bands, const phx_lw_params* params,
                         double* A_out_d, phx_lw_stats* stats);
+
+/* Linewidths with learned screening (no counterpart in the reference; the
+ * screened builder that the north star's learned part asks for).  The
+ * network net (phx_mlp_create with 12 inputs) predicts, for every vertex
+ * (q1, q2) of the q2 range, log10 of the largest fraction that the vertex
+ * adds to the linewidth of any mode of q1 (its "+" process of (q1, q2) and
+ * "-" process of (q1, -q2), the builder's unit of work).  Vertices predicted
+ * below log10_threshold are dropped; every other one is evaluated exactly on
+ * the many-branch builder in the precision of v3.  Inputs of a vertex: the
+ * fractional coordinates of q1, q2 and q3 = q1 + q2, and the lowest phonon
+ * energy of each over the largest of the mesh (screening.pair_features).
+ * stats->pairs_screened_out counts the dropped vertices.  A_out host. */
+int phx_ph_linewidths_screened(phx_v3* v3, phx_bands* bands, const phx_lw_params* params, phx_mlp* net,
+                               double log10_threshold, double* A_out, phx_lw_stats* stats);
 
 /* ---- scattering-matrix modes of the builder (nb = 6, no q2 window) ----
  * Both precisions of the coupling object: PHX_PREC_FP64, or the split paths,

@@ -46,7 +46,7 @@ class LwStats(ctypes.Structure):
                 ("pair_launches", ctypes.c_int), ("ms_pair", ctypes.c_double),
                 ("plan_chunk", ctypes.c_int), ("plan_slots", ctypes.c_int), ("graph", ctypes.c_int),
                 ("edge_events_peak", ctypes.c_longlong), ("edge_events_cap", ctypes.c_longlong),
-                ("edge_overflow_chunks", ctypes.c_int)]
+                ("edge_overflow_chunks", ctypes.c_int), ("pairs_screened_out", ctypes.c_longlong)]
 
 
 class ElParams(ctypes.Structure):
@@ -81,6 +81,8 @@ SIGNATURES = {
     "phx_v3_couplings_sq": [_VP, _i, _D, _D, _I, _D, _i, _D, _I, _D, _I, _D, _D],
     "phx_v3_estimate_num_batches": [_VP, _i, _i, _I],
     "phx_ph_linewidths": [_VP, _VP, ctypes.POINTER(LwParams), _D, ctypes.POINTER(LwStats)],
+    "phx_ph_linewidths_screened": [_VP, _VP, ctypes.POINTER(LwParams), _VP, ctypes.c_double, _D,
+                                   ctypes.POINTER(LwStats)],
     "phx_ph_linewidths_d": [_VP, _VP, ctypes.POINTER(LwParams), _VP, ctypes.POINTER(LwStats)],
     "phx_ph_rta_kappa": [_VP, _i, _D, _D, ctypes.c_double, _D],
     "phx_ph_linewidths_static": [_VP, _VP, ctypes.POINTER(LwParams), _VP],

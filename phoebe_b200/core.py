@@ -358,6 +358,22 @@ class PhScatteringMatrix:
         self.stats = st
         return out
 
+    def setup_screened(self, net, log10_threshold, q2_begin=0, q2_end=None, finalize=True):
+        """setup() with learned screening (phx_ph_linewidths_screened): the vertices
+        (q1, q2) that the network net (screening.ScreeningMLP with 12 pair inputs)
+        predicts below log10_threshold are dropped; the rest are exact.
+        self.stats.pairs_screened_out counts the dropped vertices."""
+        nT = len(self.temperatures)
+        out = np.zeros((nT, self.bands.nq * self.bands.nb))
+        p = self._params(q2_begin, q2_end, finalize)
+        st = _abi.LwStats()
+        check(_abi.load().phx_ph_linewidths_screened(self.v3.h, self.bands.h, ctypes.byref(p), net.h,
+                                                     float(log10_threshold), dptr(out), ctypes.byref(st)),
+              self.v3.ctx.h)
+        self.internalDiagonal = out
+        self.stats = st
+        return out
+
     def _setup_matrix(self, q2_begin, q2_end, finalize):
         if len(self.temperatures) != 1:
             raise ValueError("a stored scattering matrix holds one temperature")

@@ -2269,7 +2269,8 @@ int wide_prepare_blocks(phx_v3* v) {
 // optional per-q1 q2 window: per chunk of q2 the sparse R2 fold, for the
 // split path the FP16/BF16 hi/lo image of the folded vertex, then one
 // persistent pair kernel over (q2, q1 tile) items from a work queue.
-int run_builder_wide(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d, phx_lw_stats* stats) {
+int run_builder_wide(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d, phx_lw_stats* stats,
+                     const uint8_t* skip = nullptr) {
   phx_ctx* ctx = v->ctx;
   cudaStream_t st = ctx->stream;
   const int nq = b->nq, nT = p->num_temperatures, nr3 = v->nr3, nr2 = v->nr2, nb = v->nb;
@@ -2374,6 +2375,8 @@ int run_builder_wide(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Ao
   A.mtiles = wide::split_mtiles(nb);
   A.fp16 = fp16;
   A.dmax = dmax;
+  A.skip = skip;
+  A.skip_base = q2b;
   const int grid = ctx->num_sms * wide::blocks_per_sm(nb, nr3, split);
   long long pairs = 0;
   for (int c0 = q2b; c0 < q2e; c0 += chunk) pairs += (long long)nq * std::min(chunk, q2e - c0);
@@ -2427,7 +2430,8 @@ int run_builder_wide(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Ao
       (uint64_t)(split ? 10 + fp16 : 9), (uint64_t)nb, (uint64_t)nq, (uint64_t)nT, (uint64_t)q2b, (uint64_t)q2e,
       (uint64_t)p->smearing, bits(p->sigma), (uint64_t)p->finalize, (uint64_t)chunk, (uint64_t)windowed, bits(base),
       bits(Aout_d), bits(b->d_E), bits(b->d_U), bits(b->d_vg), bits(b->d_q), bits(b->d_U32), bits(v->d_D3w),
-      bits(v->d_R2), bits(v->d_R3), bits(ctx->d_status), bits(giso), bits(p->boundary_length), (uint64_t)grid};
+      bits(v->d_R2), bits(v->d_R3), bits(ctx->d_status), bits(giso), bits(p->boundary_length), (uint64_t)grid,
+      bits(skip)};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   PHX_CUDA(ctx, cudaEventCreate(&ev0));
   PHX_CUDA(ctx, cudaEventCreate(&ev1));
@@ -2508,6 +2512,109 @@ extern "C" int phx_ph_linewidths_d(phx_v3* v, phx_bands* b, const phx_lw_params*
   // builder; FP64 up to 16 branches (or with a window) on the shared-memory one
   if (v->precision != PHX_PREC_FP64 || v->nb > kMaxNbGeneric) return run_builder_wide(v, b, p, Aout_d, stats);
   return run_builder_generic(v, b, p, Aout_d, stats);
+}
+
+// Shared argument checks of the linewidth entry points.
+int check_lw_args(phx_v3* v, phx_bands* b, const phx_lw_params* p) {
+  phx_ctx* ctx = v->ctx;
+  PHX_ARG(ctx, b->ctx == ctx, "v3 and bands belong to different contexts");
+  PHX_ARG(ctx, b->nb == v->nb, "band count of bands and v3 differ");
+  PHX_ARG(ctx, p->num_temperatures >= 1 && p->num_temperatures <= kMaxT && p->temperatures,
+          "1..4 temperatures per call");
+  PHX_ARG(ctx, p->smearing == PHX_SMEAR_GAUSSIAN || p->smearing == PHX_SMEAR_ADAPTIVE, "bad smearing");
+  PHX_ARG(ctx, p->smearing != PHX_SMEAR_GAUSSIAN || p->sigma > 0.0, "Gaussian smearing needs sigma > 0");
+  PHX_ARG(ctx, p->smearing != PHX_SMEAR_ADAPTIVE || b->d_vg, "adaptive smearing needs velocities");
+  PHX_ARG(ctx, 0 <= p->q2_begin && p->q2_begin <= p->q2_end && p->q2_end <= b->nq, "bad q2 range");
+  PHX_ARG(ctx, !(p->boundary_length > 0.0) || b->d_vg, "boundary scattering needs velocities");
+  return PHX_OK;
+}
+
+extern "C" int phx_ph_linewidths_screened(phx_v3* v, phx_bands* b, const phx_lw_params* p, phx_mlp* net,
+                                          double log10_threshold, double* Aout, phx_lw_stats* stats) {
+  PHX_ARG(nullptr, v && b && p && Aout && net, "phx_ph_linewidths_screened: bad arguments");
+  phx_ctx* ctx = v->ctx;
+  PHX_TRY(check_lw_args(v, b, p));
+  PHX_ARG(ctx, phx_mlp_context(net) == ctx, "screening network and v3 belong to different contexts");
+  PHX_ARG(ctx, phx_mlp_num_inputs(net) == wide::kPairFeatures, "screening network: 12 inputs expected");
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const int nq = b->nq, nb = b->nb, q2b = p->q2_begin, q2e = p->q2_end;
+  const size_t n_out = (size_t)p->num_temperatures * nq * nb;
+  PHX_TRY(phx_ctx_reserve(ctx, &ctx->d_out, &ctx->out_bytes, sizeof(double) * std::max<size_t>(n_out, 1)));
+  double* Aout_d = static_cast<double*>(ctx->d_out);
+  if (q2b == q2e) {
+    std::fill(Aout, Aout + n_out, 0.0);
+    if (stats) *stats = phx_lw_stats{};
+    return PHX_OK;
+  }
+  if (b->emax < 0.0) {
+    std::vector<double> Eh((size_t)nq * nb);
+    PHX_CUDA(ctx, cudaMemcpy(Eh.data(), b->d_E, sizeof(double) * Eh.size(), cudaMemcpyDeviceToHost));
+    double m = 0.0;
+    for (double e : Eh) m = std::max(m, std::fabs(e));
+    b->emax = m;
+  }
+  // the network's verdict on every vertex (q1, q2) of the range, in chunks of q2
+  const size_t npairs = (size_t)(q2e - q2b) * nq;
+  const int qc = std::max(1, std::min(q2e - q2b, (int)(((size_t)1 << 20) / std::max(nq, 1)) + 1));
+  uint8_t* skip = nullptr;
+  float *X = nullptr, *y = nullptr;
+  unsigned long long* nskip = nullptr;
+  int rc = PHX_OK;
+  auto dev = [&](void** ptr, size_t bytes) {
+    if (rc == PHX_OK && phx_dev_alloc(ctx, ptr, bytes) != cudaSuccess) {
+      phx_set_error(ctx, PHX_ERR_CUDA, "phx_ph_linewidths_screened: device allocation failed");
+      rc = PHX_ERR_CUDA;
+    }
+  };
+  dev((void**)&skip, npairs);
+  dev((void**)&X, sizeof(float) * wide::kPairFeatures * (size_t)qc * nq);
+  dev((void**)&y, sizeof(float) * (size_t)qc * nq);
+  dev((void**)&nskip, sizeof(unsigned long long));
+  if (rc == PHX_OK && cudaMemsetAsync(nskip, 0, sizeof(unsigned long long), st) != cudaSuccess) rc = PHX_ERR_CUDA;
+  for (int c0 = q2b; c0 < q2e && rc == PHX_OK; c0 += qc) {
+    const int cnt = std::min(qc, q2e - c0);
+    const size_t n = (size_t)cnt * nq;
+    cudaError_t e = wide::launch_pair_features(nq, nb, b->mesh[0], b->mesh[1], b->mesh[2], b->d_E, b->emax, c0, cnt,
+                                               X, st);
+    if (e != cudaSuccess) {
+      phx_set_error(ctx, PHX_ERR_CUDA, cudaGetErrorString(e));
+      rc = PHX_ERR_CUDA;
+      break;
+    }
+    rc = phx_mlp_forward_device(net, (long long)n, X, y);
+    if (rc != PHX_OK) break;
+    e = wide::launch_screen_mask(n, y, (float)log10_threshold, skip + (size_t)(c0 - q2b) * nq, nskip, st);
+    if (e != cudaSuccess) {
+      phx_set_error(ctx, PHX_ERR_CUDA, cudaGetErrorString(e));
+      rc = PHX_ERR_CUDA;
+    }
+  }
+  unsigned long long skipped = 0;
+  if (rc == PHX_OK && (cudaMemcpyAsync(&skipped, nskip, sizeof(skipped), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                       cudaStreamSynchronize(st) != cudaSuccess)) {
+    phx_set_error(ctx, PHX_ERR_CUDA, "phx_ph_linewidths_screened: screening pass failed");
+    rc = PHX_ERR_CUDA;
+  }
+  phx_lw_stats st_local{};
+  if (rc == PHX_OK) rc = run_builder_wide(v, b, p, Aout_d, &st_local, skip);
+  if (rc == PHX_OK) {
+    cudaError_t e = cudaMemcpyAsync(Aout, Aout_d, sizeof(double) * n_out, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      phx_set_error(ctx, PHX_ERR_CUDA, cudaGetErrorString(e));
+      rc = PHX_ERR_CUDA;
+    }
+  }
+  phx_dev_free(ctx, skip);
+  phx_dev_free(ctx, X);
+  phx_dev_free(ctx, y);
+  phx_dev_free(ctx, nskip);
+  if (rc == PHX_OK && stats) {
+    *stats = st_local;
+    stats->pairs_screened_out = (long long)skipped;
+  }
+  return rc;
 }
 
 extern "C" int phx_ph_linewidths(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout,

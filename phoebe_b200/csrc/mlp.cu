@@ -4,11 +4,19 @@
 // product, with FP32 accumulation ("BF16 weights, FP32 accumulation").
 // No counterpart in the reference (phoebe has no learned screening).
 //
-// Kernels: one tiled GEMM (64 x 64 output tile per 256-thread block, 16-deep
-// K slices in shared memory, 4 x 4 outputs per thread) used for the forward
-// products X W^T, the weight gradients dY^T X and the input gradients dY W;
-// element-wise bias + GELU and its derivative; a mean-squared-error head;
-// Adam.  GELU is the tanh form 0.5 x (1 + tanh(sqrt(2/pi)(x + 0.044715 x^3))).
+// Kernels: one tensor-core GEMM (tcgen05, 128 x 64 output tile per CTA)
+// used for the forward products X W^T, the weight gradients dY^T X and the
+// input gradients dY W; element-wise bias + GELU and its derivative; a
+// mean-squared-error head; Adam.  GELU is the tanh form
+// 0.5 x (1 + tanh(sqrt(2/pi)(x + 0.044715 x^3))).
+//
+// GEMM numerics: operands are staged in shared memory as BF16 hi + lo pairs.
+// A weight operand keeps its hi part only (BF16 weights, exactly as rounded
+// for the forward pass), so the product is A_hi W + A_lo W; two activation /
+// gradient operands take hi*hi + hi*lo + lo*hi.  K is processed in 64-deep
+// chunks, each accumulated in FP32 in tensor memory and added to FP32
+// registers, so the tensor core's FP32 accumulation runs over 64 terms at a
+// time.
 #include <algorithm>
 #include <cmath>
 #include <cuda_bf16.h>
@@ -16,6 +24,8 @@
 #include <vector>
 
 #include "phx_internal.h"
+#include "tc.cuh"
+#include "tcgemm.cuh"
 
 struct phx_mlp {
   phx_ctx* ctx = nullptr;
@@ -34,68 +44,7 @@ struct phx_mlp {
 
 namespace {
 
-constexpr int kTM = 64, kTN = 64, kTK = 16;
-
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
-
-// C[M,N] (ldc) = sum_k A(m,k) B(k,n) (+ beta*C), where
-//   A(m,k) = TA ? A[k*lda + m] : A[m*lda + k]
-//   B(k,n) = TB ? B[n*ldb + k] : B[k*ldb + n]
-// RB: values of B rounded to BF16 on load (weights).  accumulate: C += result.
-template <bool TA, bool TB, bool RB>
-__global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const float* __restrict__ A, int lda,
-                                                   const float* __restrict__ B, int ldb, float* __restrict__ C,
-                                                   int ldc, int accumulate) {
-  __shared__ float sA[kTK][kTM + 4];
-  __shared__ float sB[kTK][kTN + 4];
-  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-  const int m0 = blockIdx.y * kTM, n0 = blockIdx.x * kTN;
-  float acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
-  for (int k0 = 0; k0 < K; k0 += kTK) {
-    for (int e = tid; e < kTK * kTM; e += 256) {
-      const int kk = e / kTM, mm = e % kTM;
-      const int m = m0 + mm, k = k0 + kk;
-      float v = 0.f;
-      if (m < M && k < K) v = TA ? A[(size_t)k * lda + m] : A[(size_t)m * lda + k];
-      sA[kk][mm] = v;
-    }
-    for (int e = tid; e < kTK * kTN; e += 256) {
-      const int kk = e / kTN, nn = e % kTN;
-      const int n = n0 + nn, k = k0 + kk;
-      float v = 0.f;
-      if (n < N && k < K) v = TB ? B[(size_t)n * ldb + k] : B[(size_t)k * ldb + n];
-      sB[kk][nn] = RB ? bf16r(v) : v;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < kTK; ++kk) {
-      float a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = sA[kk][ty * 4 + i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = sB[kk][tx * 4 + j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int m = m0 + ty * 4 + i, n = n0 + tx * 4 + j;
-      if (m < M && n < N) {
-        float* c = C + (size_t)m * ldc + n;
-        *c = accumulate ? *c + acc[i][j] : acc[i][j];
-      }
-    }
-}
 
 __device__ __forceinline__ float gelu(float x) {
   const float k = 0.7978845608028654f;  // sqrt(2/pi)
@@ -162,9 +111,21 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
 template <bool TA, bool TB, bool RB>
 int gemm(phx_ctx* ctx, int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C, int ldc,
          int accumulate) {
-  dim3 grid((N + kTN - 1) / kTN, (M + kTM - 1) / kTM);
-  gemm_kernel<TA, TB, RB><<<grid, 256, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc, accumulate);
-  PHX_CUDA(ctx, cudaGetLastError());
+  PHX_CUDA(ctx, (tcgemm::launch<TA, TB, RB, false>(M, N, K, A, lda, B, ldb, C, ldc, accumulate, 1.f, ctx->d_status,
+                                                   ctx->stream)));
+  return PHX_OK;
+}
+
+// a tensor-core GEMM that gave up waiting for its MMAs leaves a status bit
+int check_status(phx_ctx* ctx) {
+  int st = 0;
+  PHX_CUDA(ctx, cudaMemcpy(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st) {
+    cudaMemset(ctx->d_status, 0, sizeof(int));
+    phx_set_error(ctx, PHX_ERR_CUDA, "screening network: a tensor-core GEMM gave up waiting (status " +
+                                         std::to_string(st) + ")");
+    return PHX_ERR_CUDA;
+  }
   return PHX_OK;
 }
 
@@ -250,6 +211,24 @@ int backward(phx_mlp* net, int B, const float* dT, Acts& acts, float* dA0, float
 }
 
 }  // namespace
+
+// Forward pass of B samples already on the device (dX (B, nin) -> dY (B)),
+// in chunks of 65536 samples, on the network's stream (screened builder).
+int phx_mlp_forward_device(phx_mlp* net, long long B, const float* dX, float* dY) {
+  const long long chunk = 65536;
+  for (long long b0 = 0; b0 < B; b0 += chunk) {
+    const int nb = (int)std::min(chunk, B - b0);
+    Acts acts;
+    float *dA0, *dA1, *dl;
+    PHX_TRY(reserve(net, nb, acts, &dA0, &dA1, &dl));
+    PHX_TRY(forward(net, nb, dX + b0 * net->nin, acts));
+    PHX_CUDA(net->ctx, cudaMemcpyAsync(dY + b0, acts.A.back(), sizeof(float) * nb, cudaMemcpyDeviceToDevice,
+                                       net->ctx->stream));
+  }
+  return PHX_OK;
+}
+int phx_mlp_num_inputs(const phx_mlp* net) { return net ? net->nin : 0; }
+phx_ctx* phx_mlp_context(const phx_mlp* net) { return net ? net->ctx : nullptr; }
 
 extern "C" int phx_mlp_create(phx_ctx* ctx, int nin, int hidden, int depth, const float* params, phx_mlp** out) {
   PHX_ARG(ctx, ctx && out && nin > 0 && hidden > 0 && depth >= 1, "phx_mlp_create: bad arguments");
@@ -341,6 +320,7 @@ extern "C" int phx_mlp_infer(phx_mlp* net, int B, const float* X, float* y) {
     }
   }
   cudaFree(dX);
+  if (rc == PHX_OK) rc = check_status(ctx);
   return rc;
 }
 
@@ -377,6 +357,7 @@ extern "C" int phx_mlp_grad(phx_mlp* net, int B, const float* X, const float* t,
   }
   cudaFree(dX);
   cudaFree(dT);
+  if (rc == PHX_OK) rc = check_status(ctx);
   return rc;
 }
 
@@ -453,5 +434,6 @@ extern "C" int phx_mlp_train(phx_mlp* net, int n, const float* X, const float* t
   cudaFree(dT);
   cudaFree(dXb);
   cudaFree(dTb);
+  if (rc == PHX_OK) rc = check_status(ctx);
   return rc;
 }

@@ -132,6 +132,11 @@ struct phx_v3 {
 
 int phx_scratch_reserve(phx_v3* v3, size_t bytes);
 
+// screening network (mlp.cu): forward pass of device inputs, on the context's stream
+int phx_mlp_forward_device(phx_mlp* net, long long B, const float* dX, float* dY);
+int phx_mlp_num_inputs(const phx_mlp* net);
+phx_ctx* phx_mlp_context(const phx_mlp* net);
+
 // Cartesian coordinates (n,3) of a Gamma-centred mesh (recip: columns = b vectors)
 void phx_mesh_cartesian(const int* mesh, const double* recip, std::vector<double>& q);
 

@@ -92,21 +92,24 @@ struct Tile {
 
 // Stages 2 and 3 for one b2 of every q1 of the item, on CUDA cores: T (a, c)
 // -> X (b1, c) -> W (b1, b3) = |V|^2, W written over T (as R).  Register
-// tiles of RT x RT outputs per thread; e1 and e3 read through L1.
+// tiles of RT x RT outputs per thread.
 //   The q1 planes q0 .. q0+nq1-1 are contracted in this call, X holds nq1
-// planes (X[q - q0]); W plane q lands in the first half of T's plane q / 2
-// (R is half of C), i.e. on planes already consumed when calls run in
-// increasing q0.
+// planes (X[q - q0], rows of ldx >= nb elements: an odd stride keeps the
+// stage-3 row reads of a warp in distinct banks); W plane q lands in the
+// first half of T's plane q / 2 (R is half of C), i.e. on planes already
+// consumed when calls run in increasing q0.  e1 and e3 come from E1s / E3s
+// (the caller's shared-memory copies [q - q0][row][col], rows of nb) when
+// given, else from the global table U through L1.
 template <class R, class C, int RT>
-__device__ void wide_contract(const Tile& t, int q0, int nq1, int nb, const C* __restrict__ U, C* T, C* X, int tid,
-                              int nthreads, int bar_id) {
+__device__ void wide_contract(const Tile& t, int q0, int nq1, int nb, const C* __restrict__ U, const C* E1s,
+                              const C* E3s, C* T, C* X, int ldx, int tid, int nthreads, int bar_id) {
   const int nt = (nb + RT - 1) / RT, per_q = nt * nt, nbb = nb * nb;
   // stage 2: X[q][b1][c] = sum_a e1(a, b1) T[q][a][c]
   for (int u = tid; u < nq1 * per_q; u += nthreads) {
     const int q = q0 + u / per_q, r = u % per_q, b10 = (r / nt) * RT, c0 = (r % nt) * RT;
     const int q1 = t.q1s[q];
-    if (q1 < 0) continue;
-    const C* e1 = U + (size_t)q1 * nbb;
+    if (q1 < 0 || !t.inw[q]) continue;
+    const C* e1 = E1s ? E1s + (size_t)(q - q0) * nbb : U + (size_t)q1 * nbb;
     const C* Tq = T + (size_t)q * nbb;
     C acc[RT][RT];
 #pragma unroll
@@ -116,7 +119,7 @@ __device__ void wide_contract(const Tile& t, int q0, int nq1, int nb, const C* _
     for (int a = 0; a < nb; ++a) {
       C ev[RT], tv[RT];
 #pragma unroll
-      for (int i = 0; i < RT; ++i) ev[i] = b10 + i < nb ? ld_eig(e1, (size_t)a * nb + b10 + i) : czero<C>();
+      for (int i = 0; i < RT; ++i) ev[i] = b10 + i < nb ? e1[a * nb + b10 + i] : czero<C>();
 #pragma unroll
       for (int k = 0; k < RT; ++k) tv[k] = c0 + k < nb ? Tq[a * nb + c0 + k] : czero<C>();
 #pragma unroll
@@ -124,21 +127,21 @@ __device__ void wide_contract(const Tile& t, int q0, int nq1, int nb, const C* _
 #pragma unroll
         for (int k = 0; k < RT; ++k) cfma_t(acc[i][k], ev[i], tv[k]);
     }
-    C* Xq = X + (size_t)(q - q0) * nbb;
+    C* Xq = X + (size_t)(q - q0) * nb * ldx;
 #pragma unroll
     for (int i = 0; i < RT; ++i)
 #pragma unroll
       for (int k = 0; k < RT; ++k)
-        if (b10 + i < nb && c0 + k < nb) Xq[(b10 + i) * nb + c0 + k] = acc[i][k];
+        if (b10 + i < nb && c0 + k < nb) Xq[(b10 + i) * ldx + c0 + k] = acc[i][k];
   }
   asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
   // stage 3: W[q][b1][b3] = |sum_c X[q][b1][c] conj(e3(c, b3))|^2, over T
   R* W = reinterpret_cast<R*>(T);
   for (int u = tid; u < nq1 * per_q; u += nthreads) {
     const int q = q0 + u / per_q, r = u % per_q, b10 = (r / nt) * RT, b30 = (r % nt) * RT;
-    if (t.q1s[q] < 0) continue;
-    const C* e3 = U + (size_t)t.q3s[q] * nbb;
-    const C* Xq = X + (size_t)(q - q0) * nbb;
+    if (t.q1s[q] < 0 || !t.inw[q]) continue;
+    const C* e3 = E3s ? E3s + (size_t)(q - q0) * nbb : U + (size_t)t.q3s[q] * nbb;
+    const C* Xq = X + (size_t)(q - q0) * nb * ldx;
     C acc[RT][RT];
 #pragma unroll
     for (int i = 0; i < RT; ++i)
@@ -147,9 +150,9 @@ __device__ void wide_contract(const Tile& t, int q0, int nq1, int nb, const C* _
     for (int c = 0; c < nb; ++c) {
       C xv[RT], ev[RT];
 #pragma unroll
-      for (int i = 0; i < RT; ++i) xv[i] = b10 + i < nb ? Xq[(b10 + i) * nb + c] : czero<C>();
+      for (int i = 0; i < RT; ++i) xv[i] = b10 + i < nb ? Xq[(b10 + i) * ldx + c] : czero<C>();
 #pragma unroll
-      for (int k = 0; k < RT; ++k) ev[k] = b30 + k < nb ? ld_eig(e3, (size_t)c * nb + b30 + k) : czero<C>();
+      for (int k = 0; k < RT; ++k) ev[k] = b30 + k < nb ? e3[c * nb + b30 + k] : czero<C>();
 #pragma unroll
       for (int i = 0; i < RT; ++i)
 #pragma unroll
@@ -167,7 +170,7 @@ __device__ void wide_contract(const Tile& t, int q0, int nq1, int nb, const C* _
   // over the blocks of b3 (rows), then of b1 (columns); b2 enters the rates
   for (int u = tid; u < nq1 * nb; u += nthreads) {
     const int q = q0 + u / nb, b1 = u % nb;
-    if (t.q1s[q] < 0) continue;
+    if (t.q1s[q] < 0 || !t.inw[q]) continue;
     R* w = W + (size_t)q * nbb + (size_t)b1 * nb;
     const int* g = t.g3s + q * nb;
     for (int s0 = 0; s0 < nb;) {
@@ -183,7 +186,7 @@ __device__ void wide_contract(const Tile& t, int q0, int nq1, int nb, const C* _
   asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
   for (int u = tid; u < nq1 * nb; u += nthreads) {
     const int q = q0 + u / nb, b3 = u % nb;
-    if (t.q1s[q] < 0) continue;
+    if (t.q1s[q] < 0 || !t.inw[q]) continue;
     R* w = W + (size_t)q * nbb + b3;
     const int* g = t.g1s + q * nb;
     for (int s0 = 0; s0 < nb;) {
@@ -295,7 +298,7 @@ __device__ bool wide_load_tile(const Tile& t, const WideArgs& P, int tile, int i
     const int i = tile * nq1 + tid;
     const int q1 = i < M.nq ? P.q1_order[i] : -1;
     int f = 0;
-    if (q1 >= 0) {
+    if (q1 >= 0 && !(P.skip && P.skip[(size_t)(iq2 - P.skip_base) * M.nq + q1])) {
       f |= (!P.win_energy || P.win_energy[iq2] <= P.win_cut[q1]) ? 1 : 0;
       f |= (!P.win_energy || P.win_energy[iq2m] <= P.win_cut[q1]) ? 2 : 0;
     }
@@ -349,9 +352,11 @@ __device__ inline Tile carve_tile(char* p, int nq1, int nb) {
 // accumulates them for every q1 of the tile: one read of the folded vertex per
 // tile), T / X / W in FP64 shared memory.
 // ---------------------------------------------------------------------------
+__host__ __device__ inline int wide_ldx(int nb) { return nb | 1; }   // odd row stride of X
 __host__ __device__ inline size_t wide_fp64_smem(int nq1, int nb, int nr3) {
   const size_t nbb = (size_t)nb * nb;
-  return sizeof(double2) * ((size_t)nq1 * nr3 + 2 * (size_t)nq1 * nbb) + wide_tile_bytes(nq1, nb) + 16;
+  return sizeof(double2) * ((size_t)nq1 * nr3 + (size_t)nq1 * nbb + (size_t)nq1 * nb * wide_ldx(nb)) +
+         wide_tile_bytes(nq1, nb) + 16;
 }
 
 template <int NQ1, int RT>
@@ -361,9 +366,10 @@ __global__ void __launch_bounds__(kWideThreads) wide_fp64_kernel(WideArgs P) {
   const int nb = M.nb, nbb = nb * nb, nr3 = P.nr3;
   double2* ph = reinterpret_cast<double2*>(sraw);    // [NQ1][nr3]
   double2* T = ph + NQ1 * nr3;                       // [NQ1][nb][nb]: T (a, c), then W (b1, b3)
-  double2* X = T + NQ1 * nbb;                        // [NQ1][nb][nb]
-  const Tile t = carve_tile(reinterpret_cast<char*>(X + NQ1 * nbb), NQ1, nb);
-  int* item_s = reinterpret_cast<int*>(reinterpret_cast<char*>(X + NQ1 * nbb) + wide_tile_bytes(NQ1, nb));
+  double2* X = T + NQ1 * nbb;                        // [NQ1][nb][ldx]
+  double2* Xend = X + (size_t)NQ1 * nb * wide_ldx(nb);
+  const Tile t = carve_tile(reinterpret_cast<char*>(Xend), NQ1, nb);
+  int* item_s = reinterpret_cast<int*>(reinterpret_cast<char*>(Xend) + wide_tile_bytes(NQ1, nb));
   const int tid = threadIdx.x;
   const unsigned total = (unsigned)P.q2_count * P.ntiles;
   for (;;) {
@@ -401,7 +407,8 @@ __global__ void __launch_bounds__(kWideThreads) wide_fp64_kernel(WideArgs P) {
         for (int q = 0; q < NQ1; ++q) T[(size_t)q * nbb + col] = acc[q];
       }
       __syncthreads();
-      wide_contract<double, double2, RT>(t, 0, NQ1, nb, M.U, T, X, tid, kWideThreads, 1);
+      wide_contract<double, double2, RT>(t, 0, NQ1, nb, M.U, nullptr, nullptr, T, X, wide_ldx(nb), tid, kWideThreads,
+                                         1);
       wide_rates<double>(t, M, NQ1, b2, iq2, iq2m, reinterpret_cast<const double*>(T), 1.0, tid, kWideThreads);
       __syncthreads();
     }
@@ -519,14 +526,14 @@ __global__ void nonzero_blocks_kernel(int nb3, int nblocks, const double* __rest
 constexpr int kSplitEpiWarps = 8;
 constexpr int kSplitThreads = (kSplitEpiWarps + 2) * 32;
 constexpr int kAKC = 16;                                // K per A stage (one MMA K-step)
-constexpr int kAStages = 3;
+constexpr int kAStages = 2;
 constexpr uint32_t kAPart = 128 * kAKC * 2;             // one of hi / lo: 4096 B
 constexpr uint32_t kAStage = 2 * kAPart;                // hi + lo
 constexpr int kN = 2 * kWideQ1;                         // MMA N
 constexpr int kItemSlots = 4;
 
 __host__ __device__ inline int split_nt(int nb) { return (nb * nb + 127) / 128; }
-__host__ __device__ inline int split_qp(int nb) { return nb > 24 ? kWideQ1 / 2 : kWideQ1; }
+__host__ __device__ inline int split_qp(int nb) { return nb > 24 ? 2 : kWideQ1; }
 __host__ __device__ inline uint32_t split_tmem_cols(int nb) {
   const uint32_t need = 2u * split_nt(nb) * kN;
   uint32_t c = 32;
@@ -538,7 +545,9 @@ struct SplitSmem {
   uint8_t* A;        // [kAStages][hi, lo]
   uint8_t* B;        // [2][hi, lo] x kN rows x Kp
   float2* T;         // [kWideQ1][nb][nb]
-  float2* X;         // [qp][nb][nb]
+  float2* X;         // [qp][nb][ldx]
+  float2* E1s;       // [qp][nb][nb] e1 of the planes of a pass
+  float2* E3s;       // [qp][nb][nb] e3 of the planes of a pass
   char* tile;
   uint64_t* bars;
   int* items;        // [kItemSlots]
@@ -552,7 +561,8 @@ __host__ __device__ inline size_t split_offsets(int nb, int Kp, size_t* o) {
   o[0] = x; x += (size_t)kAStages * kAStage;                       // A ring (1024-aligned start)
   o[1] = x; x += 2 * (size_t)kN * Kp * 2 * 2;                      // B: 2 buffers x hi/lo
   o[2] = x; x += sizeof(float2) * kWideQ1 * nbb;                   // T
-  o[3] = x; x += sizeof(float2) * split_qp(nb) * nbb;              // X
+  o[3] = x; x += sizeof(float2) * split_qp(nb) * nb * wide_ldx(nb); // X
+  o[7] = x; x += sizeof(float2) * split_qp(nb) * nbb * 2;          // E1s, E3s
   x = (x + 15) & ~size_t(15);
   o[4] = x; x += wide_tile_bytes(kWideQ1, nb);
   x = (x + 7) & ~size_t(7);
@@ -561,13 +571,15 @@ __host__ __device__ inline size_t split_offsets(int nb, int Kp, size_t* o) {
   return x;
 }
 __device__ inline SplitSmem carve_split(uint8_t* base, int nb, int Kp) {
-  size_t o[7];
+  size_t o[8];
   split_offsets(nb, Kp, o);
   SplitSmem s;
   s.A = base + o[0];
   s.B = base + o[1];
   s.T = reinterpret_cast<float2*>(base + o[2]);
   s.X = reinterpret_cast<float2*>(base + o[3]);
+  s.E1s = reinterpret_cast<float2*>(base + o[7]);
+  s.E3s = s.E1s + (size_t)split_qp(nb) * nb * nb;
   s.tile = reinterpret_cast<char*>(base + o[4]);
   s.bars = reinterpret_cast<uint64_t*>(base + o[5]);
   s.items = reinterpret_cast<int*>(base + o[6]);
@@ -601,12 +613,13 @@ __device__ __forceinline__ void wide_split16(double v, bool fp16, uint16_t* hi, 
 
 // is any q1 of tile t paired with q2 or -q2 (the producer's item filter)
 __device__ bool tile_live(const WideArgs& P, int tile, int iq2, int iq2m) {
-  if (!P.win_energy) return true;
+  if (!P.win_energy && !P.skip) return true;
   for (int i = 0; i < P.nq1; ++i) {
     const int k = tile * P.nq1 + i;
     if (k >= P.m.nq) break;
     const int q1 = P.q1_order[k];
-    if (P.win_energy[iq2] <= P.win_cut[q1] || P.win_energy[iq2m] <= P.win_cut[q1]) return true;
+    if (P.skip && P.skip[(size_t)(iq2 - P.skip_base) * P.m.nq + q1]) continue;
+    if (!P.win_energy || P.win_energy[iq2] <= P.win_cut[q1] || P.win_energy[iq2m] <= P.win_cut[q1]) return true;
   }
   return false;
 }
@@ -832,8 +845,17 @@ __global__ void __launch_bounds__(kSplitThreads, 1) wide_split_kernel(WideArgs P
         tc::tc_fence_before();
         asm volatile("bar.sync 1, %0;" ::"r"(nth) : "memory");
         if (tid == 0) tc::mbar_arrive(&tfree[buf]);
-        for (int q0 = 0; q0 < kWideQ1; q0 += qp)
-          wide_contract<float, float2, RT>(t, q0, qp, nb, P.U32, S.T, S.X, tid, nth, 1);
+        for (int q0 = 0; q0 < kWideQ1; q0 += qp) {
+          // e1 and e3 of the pass's planes into shared memory (FP32)
+          for (int e = tid; e < qp * nbb; e += nth) {
+            const int q = q0 + e / nbb, x = e % nbb;
+            const int q1 = max(t.q1s[q], 0);
+            S.E1s[e] = P.U32[(size_t)q1 * nbb + x];
+            S.E3s[e] = P.U32[(size_t)t.q3s[q] * nbb + x];
+          }
+          asm volatile("bar.sync 1, %0;" ::"r"(nth) : "memory");
+          wide_contract<float, float2, RT>(t, q0, qp, nb, P.U32, S.E1s, S.E3s, S.T, S.X, wide_ldx(nb), tid, nth, 1);
+        }
         wide_rates<float>(t, M, kWideQ1, b2, iq2, iq2m, reinterpret_cast<const float*>(S.T), wscale, tid, nth);
         asm volatile("bar.sync 1, %0;" ::"r"(nth) : "memory");
       }
@@ -888,6 +910,42 @@ __global__ void convert_wide_kernel(int nb, int nr3, int Kp, int q2_count, const
   }
 }
 
+// Screening features of the pairs (q1, q2) of a q2 range, 12 per pair: the
+// fractional coordinates of q1, q2 and q3 = q1 + q2, and the lowest phonon
+// energy at each of the three over the largest of the mesh.
+__global__ void pair_features_kernel(int nq, int nb, int n0, int n1, int n2, const double* __restrict__ E,
+                                     double emax, int q2_first, int q2_count, float* __restrict__ X) {
+  const size_t n = (size_t)q2_count * nq;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int q1 = (int)(i % nq), iq2 = q2_first + (int)(i / nq);
+    const int iq3 = mesh_add(q1, iq2, n0, n1, n2);
+    float* x = X + i * wide::kPairFeatures;
+    const int qs[3] = {q1, iq2, iq3};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int q = qs[k];
+      x[3 * k] = (float)(q % n0) / n0;
+      x[3 * k + 1] = (float)((q / n0) % n1) / n1;
+      x[3 * k + 2] = (float)(q / (n0 * n1)) / n2;
+      double e = E[(size_t)q * nb];
+      for (int b = 1; b < nb; ++b) e = fmin(e, E[(size_t)q * nb + b]);
+      x[9 + k] = (float)(e / emax);
+    }
+  }
+}
+
+__global__ void screen_mask_kernel(size_t n, const float* __restrict__ y, float thr, uint8_t* __restrict__ skip,
+                                   unsigned long long* __restrict__ nskip) {
+  unsigned long long c = 0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint8_t s = y[i] < thr ? 1 : 0;
+    skip[i] = s;
+    c += s;
+  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(nskip, c);
+}
+
 // FP32 copy of the eigenvector table (the split kernel's contractions)
 __global__ void u32_kernel(const double2* __restrict__ U, float2* __restrict__ U32, size_t n) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -910,7 +968,7 @@ size_t fp64_smem(int nq1, int nb, int nr3) { return wide_fp64_smem(nq1, nb, nr3)
 int split_kp(int nr3) { return ((2 * nr3 + kAKC - 1) / kAKC) * kAKC; }
 int split_mtiles(int nb) { return split_nt(nb); }
 size_t split_smem(int nb, int Kp) {
-  size_t o[7];
+  size_t o[8];
   return split_offsets(nb, Kp, o) + 1024;   // + alignment slack of the dynamic base
 }
 size_t split_img_bytes(int nb, int Kp) { return (size_t)nb * split_nt(nb) * (Kp / kAKC) * kAStage; }
@@ -990,6 +1048,21 @@ cudaError_t launch_convert(int nb, int nr3, int Kp, int q2_count, const double2*
 
 cudaError_t launch_u32(const double2* U, float2* U32, size_t n, cudaStream_t st) {
   u32_kernel<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 64), 256, 0, st>>>(U, U32, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pair_features(int nq, int nb, int n0, int n1, int n2, const double* E, double emax, int q2_first,
+                                 int q2_count, float* X, cudaStream_t st) {
+  const size_t n = (size_t)q2_count * nq;
+  pair_features_kernel<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 64), 256, 0, st>>>(
+      nq, nb, n0, n1, n2, E, emax, q2_first, q2_count, X);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_screen_mask(size_t n, const float* y, float log10_threshold, uint8_t* skip,
+                               unsigned long long* nskip, cudaStream_t st) {
+  screen_mask_kernel<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 64), 256, 0, st>>>(n, y, log10_threshold,
+                                                                                         skip, nskip);
   return cudaGetLastError();
 }
 

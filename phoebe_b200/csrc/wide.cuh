@@ -24,6 +24,9 @@ struct Args {
   double* lw;                 // (nq, nb, nT) partial linewidths (FP64 atomics)
   unsigned* counter;          // work queue, zero at launch
   int* status;
+  // screening: skip[(q2 - skip_base) * nq + q1] != 0 drops the vertex (q1, q2), or null
+  const uint8_t* skip;
+  int skip_base;
   // split path
   const uint8_t* img;         // A-operand tiles [j][b2][mt][kc], hi then lo
   const float2* U32;          // (nq, nb, nb) FP32 eigenvectors
@@ -55,6 +58,13 @@ cudaError_t launch_convert(int nb, int nr3, int Kp, int q2_count, const double2*
                            const unsigned* dmax, cudaStream_t st);
 // U32 = (float2) U, n complex entries
 cudaError_t launch_u32(const double2* U, float2* U32, size_t n, cudaStream_t st);
+// screening: features X ((q2 - q2_first) * nq + q1, 12) of the (q1, q2) pairs of a q2 range
+constexpr int kPairFeatures = 12;
+cudaError_t launch_pair_features(int nq, int nb, int n0, int n1, int n2, const double* E, double emax, int q2_first,
+                                 int q2_count, float* X, cudaStream_t st);
+// skip[i] = y[i] < log10_threshold
+cudaError_t launch_screen_mask(size_t n, const float* y, float log10_threshold, uint8_t* skip,
+                               unsigned long long* nskip, cudaStream_t st);
 // flags[r3 * nr2 + r2] = 1 for the non-zero blocks of D3w (nr3, nr2, nb^3)
 cudaError_t launch_nonzero_blocks(int nb, int nr3, int nr2, const double* D3w, int* flags, cudaStream_t st);
 

@@ -17,6 +17,14 @@ Triplet convention: the builder evaluates only the "+" vertex and lets each
 (q1, -q2) (same q3 = q1 + q2, time reversal), so the contribution of a triplet
 is |V+|^2 (symmetrised over degenerate blocks) times the sum of those rate
 factors, at the first temperature.
+
+Pair-level screening (the screened builder, phx_ph_linewidths_screened): the
+same network shape with 12 pair inputs (pair_features) predicts, for a vertex
+(q1, q2) -- one "triplet" in the benchmark's unit of work -- log10 of the
+largest fraction it adds to the linewidth of any mode of q1
+(pair_targets); the builder drops the vertices predicted below a threshold
+and evaluates the rest exactly.  Training pairs come from the exact builder
+itself, one q2 at a time (pair_contributions).
 """
 import ctypes
 
@@ -234,3 +242,50 @@ def relative_targets(c, A):
     """log10 of the contribution relative to the linewidth A (nq1, nb) of its mode."""
     r = c / np.where(A > 0, A, np.inf)[None, :, :, None, None]
     return np.log10(np.maximum(r, FLOOR)).astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# pair-level screening (the screened builder)
+# ---------------------------------------------------------------------------
+
+def pair_features(mesh, E, q2_list):
+    """Features (len(q2_list), nq1, 12) of the vertices (q1, q2): fractional
+    coordinates of q1, q2 and q3 = q1 + q2, and the lowest phonon energy at
+    each over the largest of the mesh (as the builder's pair_features_kernel,
+    in FP32)."""
+    n0, n1, n2 = mesh
+    nq = E.shape[0]
+    idx = np.arange(nq)
+    ix, iy, iz = idx % n0, (idx // n0) % n1, idx // (n0 * n1)
+    frac = np.stack([ix / n0, iy / n1, iz / n2], 1).astype(np.float32)
+    emin = (E.min(axis=1) / np.abs(E).max()).astype(np.float32)
+    out = np.zeros((len(q2_list), nq, NIN), dtype=np.float32)
+    for k, iq2 in enumerate(q2_list):
+        jx, jy, jz = iq2 % n0, (iq2 // n0) % n1, iq2 // (n0 * n1)
+        iq3 = ((iz + jz) % n2) * n0 * n1 + ((iy + jy) % n1) * n0 + (ix + jx) % n0
+        out[k, :, 0:3] = frac
+        out[k, :, 3:6] = frac[iq2]
+        out[k, :, 6:9] = frac[iq3]
+        out[k, :, 9] = emin
+        out[k, :, 10] = emin[iq2]
+        out[k, :, 11] = emin[iq3]
+    return out
+
+
+def pair_contributions(sm, q2_list, temperature_index=0):
+    """Exact contributions u (len(q2_list), nq1, nb) of each vertex (q1, q2) to the
+    linewidths of q1 (A_out units, one temperature), from the builder sm
+    (core.PhScatteringMatrix) run on one q2 at a time without finalisation."""
+    nq, nb = sm.bands.nq, sm.bands.nb
+    out = np.zeros((len(q2_list), nq, nb))
+    for k, iq2 in enumerate(q2_list):
+        A = sm.setup(int(iq2), int(iq2) + 1, finalize=False)
+        out[k] = A[temperature_index].reshape(nq, nb)
+    return out
+
+
+def pair_targets(u, A):
+    """log10 of the largest fraction max_b1 u(q1, q2, b1) / A(q1, b1) of a vertex,
+    with A (nq1, nb) the unscreened, unaveraged linewidths (A_out units)."""
+    r = u / np.where(A > 0, A, np.inf)[None, :, :]
+    return np.log10(np.maximum(r.max(axis=2), FLOOR)).astype(np.float32)

@@ -297,8 +297,10 @@ def random_fc3(crystal, num_pairs, seed, amp_ev=3.0, decay_ang=4.0,
     ridx = {v: i for i, v in enumerate(Rvecs)}
     nr = len(Rvecs)
     D3 = np.zeros((nb, nb, nb, nr, nr))
+    cols = np.empty(num_pairs, dtype=np.int64)
     for p, i in pidx.items():
-        D3[:, :, :, ridx[p[1]], ridx[p[0]]] = B[i]
+        cols[i] = ridx[p[1]] * nr + ridx[p[0]]
+    D3.reshape(nb ** 3, nr * nr)[:, cols] = B.reshape(num_pairs, nb ** 3).T
     Rcart = np.array([A @ np.array(v, dtype=np.float64) for v in Rvecs])
     w = np.ones((nr, nat, nat))
     return FC3(D3, Rcart.copy(), Rcart.copy(), w, w.copy(), num_pairs, it + 1, res)
@@ -399,6 +401,21 @@ def perovskite_workload(mesh=(24, 24, 24), num_pairs=1500, fc_grid=(7, 7, 7), sm
 def config2(mesh=(24, 24, 24)):
     """5-atom perovskite, 24^3 mesh, per-q1 q2 window (use q2_window on its bands)."""
     return perovskite_workload(mesh)
+
+
+def twelve_atom_workload(mesh=(16, 16, 16), num_pairs=4000, smearing="adaptive", temperatures_k=(300.0,)):
+    """The learned-screening cell: 12 atoms (36 branches), masses uniform in
+    20-80 amu, spring FC2 on a 2x2x2 grid, num_pairs FC3 pairs (seed of config 4)."""
+    cr = twelve_atom_crystal(SEED_BASE + 4)
+    fc2 = twelve_atom_fc2(cr)
+    fc3 = random_fc3(cr, num_pairs, SEED_BASE + 4)
+    return Workload("twelve-atom-%dx%dx%d" % tuple(mesh), cr, fc2, fc3, tuple(mesh),
+                    tuple(temperatures_k), smearing, 0.3 / C.ryToTHz)
+
+
+def config4(mesh=(16, 16, 16)):
+    """12-atom cell, 36 branches, 4000 FC3 pairs, 16^3 mesh."""
+    return twelve_atom_workload(mesh)
 
 
 def q2_window(E, mesh, seed=SEED_BASE + 2, keep_min=0.2, keep_max=1.0):

@@ -89,3 +89,55 @@ def test_screening_gain_at_bounded_error(ctx):
     net.close()
     v3.close()
     h0.close()
+
+
+def test_screened_builder(ctx, diamond):
+    """phx_ph_linewidths_screened: with no vertex dropped it reproduces the exact
+    builder; a network trained on the exact vertex contributions drops vertices
+    at a threshold calibrated on half of the q2 points, within 1e-3 on every
+    linewidth; dropping everything leaves only zeros."""
+    from phoebe_b200.core import Interaction3Ph, PhononH0, PhScatteringMatrix
+    cr = diamond["crystal"]
+    mesh = (8, 8, 8)
+    h0 = PhononH0(ctx, cr, diamond["fc2"])
+    bands = h0.populate(mesh, withVelocities=True)
+    E = bands.get(velocities=False)[0]
+    v3 = Interaction3Ph(ctx, cr, diamond["fc3"], precision="split_fp16")
+    T = np.array([C.kelvin_to_ry(300.0)])
+    sm = PhScatteringMatrix(v3, bands, T, "adaptive")
+    nq, nb = bands.nq, bands.nb
+    A = sm.setup()
+    net = screening.ScreeningMLP(ctx, seed=3)
+    A_none = sm.setup_screened(net, -np.inf)
+    assert sm.stats.pairs_screened_out == 0
+    ok = (E.reshape(-1) >= C.phExcludeCutoff)[None, :]
+    big = ok & (np.abs(A) > 1e-8 * np.abs(A).max())
+    assert (np.abs(A_none - A)[big] / np.abs(A)[big]).max() < 1e-5
+    A_all = sm.setup_screened(net, np.inf)
+    assert sm.stats.pairs_screened_out == nq * nq
+    assert np.all(A_all == 0.0)
+    # train on the vertices of every other q2 point, from the exact builder
+    q2s = np.arange(0, nq, 2)
+    u = screening.pair_contributions(sm, q2s)
+    A0 = A[0].reshape(nq, nb)
+    X = screening.pair_features(mesh, E, q2s).reshape(-1, 12)
+    y = screening.pair_targets(u, A0).reshape(-1)
+    net.train(X, y, epochs=10, batch=1024, lr=1e-3)
+    pred = net.infer(X).reshape(len(q2s), nq)
+    frac = u / np.where(A0 > 0, A0, np.inf)[None]
+    thr = None
+    for cand in np.arange(-3.0, -12.01, -0.25):
+        if (np.where((pred < cand)[:, :, None], frac, 0.0).sum(axis=0) * 2.0).max() <= 5e-4:
+            thr = float(cand)
+            break
+    assert thr is not None
+    A_scr = sm.setup_screened(net, thr)
+    dropped = sm.stats.pairs_screened_out
+    err = (np.abs(A_scr - A)[big] / np.abs(A)[big]).max()
+    print("screened builder: threshold 1e%.2f, %d of %d vertices dropped, max linewidth error %.2e"
+          % (thr, dropped, nq * nq, err))
+    assert err <= 1e-3
+    net.close()
+    v3.close()
+    bands.close()
+    h0.close()

@@ -10,11 +10,18 @@
 //     V- = sum T- e1(a,b1) conj(e2(b,b2)) conj(e3-(c,b3));  output |V|^2
 // This is the drop-in call-by-call path (one q2, a batch of q1).  The fused
 // builder in builder.cu restructures the same arithmetic for whole meshes.
+// With a split precision set on the object (phx_v3_set_precision), the R3
+// transform of the whole q1 batch runs as one tensor-core GEMM (tcgemm.cuh,
+// FP16 or BF16 hi/lo operands, FP32 accumulation) and the contractions with
+// the eigenvectors stay in FP64.
 #include <algorithm>
 #include <cmath>
 
+#include <cstring>
+
 #include "cplx.cuh"
 #include "phx_internal.h"
+#include "tcgemm.cuh"
 
 namespace {
 
@@ -56,6 +63,8 @@ __global__ void cache_d3_kernel(int nb, int nat, int nr2, int nr3, const double*
 // One block per q1: stage T+- (nb^3 complex each) in shared memory, then
 // contract with e1, e2, e3 and write |V|^2.  Shared memory limits this
 // call-by-call path to nb <= 15; wider cells use the fused builder.
+// Tg (split precision): T+- of every q1 from the tensor-core GEMM, FP32,
+// row iq = [(+, abc, re/im) | (-, abc, re/im)]; null: the FP64 R3 sum here.
 __global__ void couplings_kernel(int nb, int nat, int nr3, const double2* __restrict__ plus,
                                  const double2* __restrict__ mins, const double* __restrict__ R3,
                                  const double* __restrict__ w3, const double* __restrict__ q1s,
@@ -64,7 +73,8 @@ __global__ void couplings_kernel(int nb, int nat, int nr3, const double2* __rest
                                  const double2* __restrict__ ev3p, const int* __restrict__ nb3ps,
                                  const double2* __restrict__ ev3m, const int* __restrict__ nb3ms,
                                  const long* __restrict__ offP, const long* __restrict__ offM,
-                                 double* __restrict__ outP, double* __restrict__ outM) {
+                                 double* __restrict__ outP, double* __restrict__ outM,
+                                 const float* __restrict__ Tg) {
   extern __shared__ double2 sm[];
   const int iq = blockIdx.x;
   const int n3 = nb * nb * nb;
@@ -74,13 +84,20 @@ __global__ void couplings_kernel(int nb, int nat, int nr3, const double2* __rest
   double2* xP = ph + nr3;              // (nb1, nb, nb) scratch
   double2* xM = xP + n3;
   const double* q1 = q1s + 3 * iq;
-  for (int r = threadIdx.x; r < nr3; r += blockDim.x) {
+  if (Tg) {
+    const float* tg = Tg + (size_t)iq * 4 * n3;
+    for (int abc = threadIdx.x; abc < n3; abc += blockDim.x) {
+      tP[abc] = cmk((double)tg[2 * abc], (double)tg[2 * abc + 1]);
+      tM[abc] = cmk((double)tg[2 * (n3 + abc)], (double)tg[2 * (n3 + abc) + 1]);
+    }
+  }
+  for (int r = threadIdx.x; r < nr3 && !Tg; r += blockDim.x) {
     double sn, cs;
     sincos(-(q1[0] * R3[3 * r] + q1[1] * R3[3 * r + 1] + q1[2] * R3[3 * r + 2]), &sn, &cs);
     ph[r] = cmk(cs, sn);
   }
   __syncthreads();
-  for (int abc = threadIdx.x; abc < n3; abc += blockDim.x) {
+  for (int abc = threadIdx.x; abc < n3 && !Tg; abc += blockDim.x) {
     const int a3 = abc % nb, a1 = abc / (nb * nb);
     const int at1 = a1 / 3, at3 = a3 / 3;
     double2 sp = cmk(0, 0), sq = cmk(0, 0);
@@ -137,6 +154,45 @@ __global__ void couplings_kernel(int nb, int nat, int nr3, const double2* __rest
     double2 s = cmk(0, 0);
     for (int a3 = 0; a3 < nb; ++a3) cfmac(s, tM[b12 * nb + a3], e3m[a3 * nb + b3]);
     oM[idx] = s.x * s.x + s.y * s.y;
+  }
+}
+
+// Split path of getCouplingsSquared: operands of the R3 transform as one GEMM
+//   T(q1; s, abc) = sum_r3 D3s(abc, r3) w3(r3, a, c) e^{-i q1.R3},  s = +, -
+// on [Re | Im] extended K = 2 nr3: A row q1 = [cos | sin] of -q1.R3; B row
+// (s, abc, re) = [Dr | -Di], row (s, abc, im) = [Di | Dr] of D = D3s w3.
+__global__ void couplings_b_kernel(int nb, int nat, int nr3, const double2* __restrict__ plus,
+                                   const double2* __restrict__ mins, const double* __restrict__ w3,
+                                   float* __restrict__ B, unsigned* __restrict__ bmax) {
+  const size_t n3 = (size_t)nb * nb * nb, rows = 4 * n3, K = 2 * (size_t)nr3;
+  float m = 0.f;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows * K; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t row = i / K;
+    const int k = (int)(i % K), r = k < nr3 ? k : k - nr3;
+    const int ri = (int)(row & 1);
+    const size_t sa = row >> 1, abc = sa % n3;
+    const int a3 = (int)(abc % nb), a1 = (int)(abc / ((size_t)nb * nb));
+    const double2 d = (sa < n3 ? plus : mins)[abc * nr3 + r];
+    const double ww = w3[((size_t)r * nat + a1 / 3) * nat + a3 / 3];
+    double v;
+    if (ri == 0) v = k < nr3 ? d.x * ww : -d.y * ww;
+    else v = k < nr3 ? d.y * ww : d.x * ww;
+    B[i] = (float)v;
+    m = fmaxf(m, fabsf((float)v));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(bmax, __float_as_uint(m));
+}
+
+__global__ void couplings_a_kernel(int nq1, int nr3, const double* __restrict__ q1s, const double* __restrict__ R3,
+                                   float* __restrict__ A) {
+  const size_t K = 2 * (size_t)nr3;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)nq1 * K; i += (size_t)gridDim.x * blockDim.x) {
+    const int q = (int)(i / K), k = (int)(i % K), r = k < nr3 ? k : k - nr3;
+    const double* q1 = q1s + 3 * q;
+    double sn, cs;
+    sincos(-(q1[0] * R3[3 * r] + q1[1] * R3[3 * r + 1] + q1[2] * R3[3 * r + 2]), &sn, &cs);
+    A[i] = (float)(k < nr3 ? cs : sn);
   }
 }
 
@@ -333,15 +389,63 @@ extern "C" int phx_v3_couplings_sq(phx_v3* v, int nq1, const double* q1s, const 
     if (e == cudaSuccess) e = cudaMemcpyAsync(dofM, offM.data(), sizeof(long) * (nq1 + 1), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && smem > 48 * 1024)
       e = cudaFuncSetAttribute(couplings_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // split precision: T+- of the whole batch from one tensor-core GEMM
+    const bool split = v->precision != PHX_PREC_FP64;
+    const bool f16 = v->precision == PHX_PREC_SPLIT_FP16;
+    const int K = 2 * v->nr3, N = (int)(4 * n3);
+    float *dA = nullptr, *dB = nullptr, *dT = nullptr;
+    unsigned* dmx = nullptr;
+    if (e == cudaSuccess && split) {
+      if (rc == PHX_OK) rc = dmalloc(ctx, &dA, (size_t)nq1 * K);
+      if (rc == PHX_OK) rc = dmalloc(ctx, &dB, (size_t)N * K);
+      if (rc == PHX_OK) rc = dmalloc(ctx, &dT, (size_t)nq1 * N);
+      if (rc == PHX_OK) rc = dmalloc(ctx, &dmx, 1);
+      if (rc != PHX_OK) e = cudaErrorMemoryAllocation;
+      unsigned mx = 0;
+      if (e == cudaSuccess) e = cudaMemsetAsync(dmx, 0, sizeof(unsigned), st);
+      if (e == cudaSuccess) {
+        couplings_b_kernel<<<std::min<size_t>(((size_t)N * K + 255) / 256, (size_t)ctx->num_sms * 16), 256, 0, st>>>(
+            nb, v->nat, v->nr3, reinterpret_cast<const double2*>(v->d_plus),
+            reinterpret_cast<const double2*>(v->d_mins), v->d_w3, dB, dmx);
+        couplings_a_kernel<<<std::min<size_t>(((size_t)nq1 * K + 255) / 256, (size_t)ctx->num_sms * 16), 256, 0, st>>>(
+            nq1, v->nr3, dq, v->d_R3, dA);
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess) e = cudaMemcpyAsync(&mx, dmx, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      // FP16 hi/lo: B scaled by a power of 2 so that its largest entry lies in [0.5, 1]
+      float bscale = 1.f;
+      float bm = 0.f;
+      std::memcpy(&bm, &mx, sizeof(bm));
+      if (f16 && bm > 0.f) {
+        int ex;
+        std::frexp(bm, &ex);
+        bscale = std::ldexp(1.f, -ex);
+      }
+      if (e == cudaSuccess)
+        e = f16 ? tcgemm::launch<false, true, false, true>(nq1, N, K, dA, K, dB, K, dT, N, 0, bscale, ctx->d_status, st)
+                : tcgemm::launch<false, true, false, false>(nq1, N, K, dA, K, dB, K, dT, N, 0, 1.f, ctx->d_status, st);
+    }
     if (e == cudaSuccess) {
       couplings_kernel<<<nq1, 256, smem, st>>>(
           nb, v->nat, v->nr3, reinterpret_cast<const double2*>(v->d_plus),
           reinterpret_cast<const double2*>(v->d_mins), v->d_R3, v->d_w3, dq,
           reinterpret_cast<const double2*>(de1), dn1, reinterpret_cast<const double2*>(de2), nb2,
           reinterpret_cast<const double2*>(de3p), dn3p, reinterpret_cast<const double2*>(de3m),
-          dn3m, dofP, dofM, doP, doM);
+          dn3m, dofP, dofM, doP, doM, split ? dT : nullptr);
       e = cudaGetLastError();
     }
+    int kst = 0;
+    if (e == cudaSuccess && split) e = cudaMemcpyAsync(&kst, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && split) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess && kst) {
+      cudaMemset(ctx->d_status, 0, sizeof(int));
+      e = cudaErrorLaunchFailure;
+    }
+    phx_dev_free(ctx, dA);
+    phx_dev_free(ctx, dB);
+    phx_dev_free(ctx, dT);
+    phx_dev_free(ctx, dmx);
     if (e == cudaSuccess) e = cudaMemcpyAsync(outP, doP, sizeof(double) * offP[nq1], cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(outM, doM, sizeof(double) * offM[nq1], cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -116,6 +116,7 @@ __device__ void wide_contract(const Tile& t, int q0, int nq1, int nb, const C* _
     for (int i = 0; i < RT; ++i)
 #pragma unroll
       for (int k = 0; k < RT; ++k) acc[i][k] = czero<C>();
+#pragma unroll 2
     for (int a = 0; a < nb; ++a) {
       C ev[RT], tv[RT];
 #pragma unroll
@@ -147,6 +148,7 @@ __device__ void wide_contract(const Tile& t, int q0, int nq1, int nb, const C* _
     for (int i = 0; i < RT; ++i)
 #pragma unroll
       for (int k = 0; k < RT; ++k) acc[i][k] = czero<C>();
+#pragma unroll 2
     for (int c = 0; c < nb; ++c) {
       C xv[RT], ev[RT];
 #pragma unroll
@@ -533,7 +535,15 @@ constexpr int kN = 2 * kWideQ1;                         // MMA N
 constexpr int kItemSlots = 4;
 
 __host__ __device__ inline int split_nt(int nb) { return (nb * nb + 127) / 128; }
-__host__ __device__ inline int split_qp(int nb) { return nb > 24 ? 2 : kWideQ1; }
+__host__ __device__ inline size_t split_offsets_qp(int nb, int Kp, int qp, size_t* o);
+// q1 planes contracted per pass: all 8 when shared memory allows (one pass,
+// the most work units per barrier), else 4, else 2
+__host__ __device__ inline int split_qp(int nb, int Kp) {
+  size_t o[8];
+  for (int qp = kWideQ1; qp > 2; qp /= 2)
+    if (split_offsets_qp(nb, Kp, qp, o) + 1024 <= 227 * 1024) return qp;
+  return 2;
+}
 __host__ __device__ inline uint32_t split_tmem_cols(int nb) {
   const uint32_t need = 2u * split_nt(nb) * kN;
   uint32_t c = 32;
@@ -546,8 +556,8 @@ struct SplitSmem {
   uint8_t* B;        // [2][hi, lo] x kN rows x Kp
   float2* T;         // [kWideQ1][nb][nb]
   float2* X;         // [qp][nb][ldx]
-  float2* E1s;       // [qp][nb][nb] e1 of the planes of a pass
-  float2* E3s;       // [qp][nb][nb] e3 of the planes of a pass
+  float2* E1s;       // shared copies of e1 / e3 (not used: read through L1)
+  float2* E3s;
   char* tile;
   uint64_t* bars;
   int* items;        // [kItemSlots]
@@ -555,20 +565,23 @@ struct SplitSmem {
   uint32_t* tslot;
   volatile int* abort_flag;
 };
-__host__ __device__ inline size_t split_offsets(int nb, int Kp, size_t* o) {
+__host__ __device__ inline size_t split_offsets_qp(int nb, int Kp, int qp, size_t* o) {
   const size_t nbb = (size_t)nb * nb;
   size_t x = 0;
   o[0] = x; x += (size_t)kAStages * kAStage;                       // A ring (1024-aligned start)
   o[1] = x; x += 2 * (size_t)kN * Kp * 2 * 2;                      // B: 2 buffers x hi/lo
   o[2] = x; x += sizeof(float2) * kWideQ1 * nbb;                   // T
-  o[3] = x; x += sizeof(float2) * split_qp(nb) * nb * wide_ldx(nb); // X
-  o[7] = x; x += sizeof(float2) * split_qp(nb) * nbb * 2;          // E1s, E3s
+  o[3] = x; x += sizeof(float2) * qp * nb * wide_ldx(nb);           // X
+  o[7] = x;                                                        // (no shared copies of e1, e3)
   x = (x + 15) & ~size_t(15);
   o[4] = x; x += wide_tile_bytes(kWideQ1, nb);
   x = (x + 7) & ~size_t(7);
   o[5] = x; x += sizeof(uint64_t) * 32;                            // barriers
   o[6] = x; x += sizeof(int) * (kItemSlots + 4 + 4);               // items, ctl, tslot, abort
   return x;
+}
+__host__ __device__ inline size_t split_offsets(int nb, int Kp, size_t* o) {
+  return split_offsets_qp(nb, Kp, split_qp(nb, Kp), o);
 }
 __device__ inline SplitSmem carve_split(uint8_t* base, int nb, int Kp) {
   size_t o[8];
@@ -578,8 +591,8 @@ __device__ inline SplitSmem carve_split(uint8_t* base, int nb, int Kp) {
   s.B = base + o[1];
   s.T = reinterpret_cast<float2*>(base + o[2]);
   s.X = reinterpret_cast<float2*>(base + o[3]);
-  s.E1s = reinterpret_cast<float2*>(base + o[7]);
-  s.E3s = s.E1s + (size_t)split_qp(nb) * nb * nb;
+  s.E1s = nullptr;
+  s.E3s = nullptr;
   s.tile = reinterpret_cast<char*>(base + o[4]);
   s.bars = reinterpret_cast<uint64_t*>(base + o[5]);
   s.items = reinterpret_cast<int*>(base + o[6]);
@@ -782,7 +795,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) wide_split_kernel(WideArgs P
     const Tile t = carve_tile(S.tile, kWideQ1, nb);
     const int qd = warp & 3, half = warp >> 2;
     const uint32_t bBytes = (uint32_t)kN * Kp * 2;
-    const int qp = split_qp(nb);
+    const int qp = split_qp(nb, Kp);
     const double sc = P.fp16 ? (double)wide_fp16_scale(P.dmax) : 1.0;
     const double wscale = 1.0 / (sc * sc);
     int s = 0;
@@ -845,17 +858,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1) wide_split_kernel(WideArgs P
         tc::tc_fence_before();
         asm volatile("bar.sync 1, %0;" ::"r"(nth) : "memory");
         if (tid == 0) tc::mbar_arrive(&tfree[buf]);
-        for (int q0 = 0; q0 < kWideQ1; q0 += qp) {
-          // e1 and e3 of the pass's planes into shared memory (FP32)
-          for (int e = tid; e < qp * nbb; e += nth) {
-            const int q = q0 + e / nbb, x = e % nbb;
-            const int q1 = max(t.q1s[q], 0);
-            S.E1s[e] = P.U32[(size_t)q1 * nbb + x];
-            S.E3s[e] = P.U32[(size_t)t.q3s[q] * nbb + x];
-          }
-          asm volatile("bar.sync 1, %0;" ::"r"(nth) : "memory");
-          wide_contract<float, float2, RT>(t, q0, qp, nb, P.U32, S.E1s, S.E3s, S.T, S.X, wide_ldx(nb), tid, nth, 1);
-        }
+        for (int q0 = 0; q0 < kWideQ1; q0 += qp)
+          wide_contract<float, float2, RT>(t, q0, qp, nb, P.U32, nullptr, nullptr, S.T, S.X, wide_ldx(nb), tid, nth, 1);
         wide_rates<float>(t, M, kWideQ1, b2, iq2, iq2m, reinterpret_cast<const float*>(S.T), wscale, tid, nth);
         asm volatile("bar.sync 1, %0;" ::"r"(nth) : "memory");
       }

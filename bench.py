@@ -692,6 +692,7 @@ def run_perovskite(args):
             ms16.append(sm.stats.ms_total)
             pairs16.append(int(per_q2[q0:q0 + args.q2_slice].sum()))
     rate16 = float(np.sum(pairs16) / (np.sum(ms16) / 1000.0))
+    tile = {"register_tile": int(sm.stats.tile_rt), "q1_planes_per_pass": int(sm.stats.tile_qp)}
     line = {"metric": "windowed (q1,q2) pairs/s, 15 branches, 24^3 mesh, per-q1 q2 window",
             "value": rate, "unit": "pairs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
@@ -703,6 +704,7 @@ def run_perovskite(args):
             "bands_s_13824_points": bands_s,
             "projected_full_run_s": total / rate,
             "split_path": {"precision": prec, "value": rate16, "unit": "pairs/s", "ms_per_step": float(np.mean(ms16)),
+                           "tile_shape": tile,
                            "speedup_over_fp64": rate16 / rate, "projected_full_run_s": total / rate16},
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
@@ -744,6 +746,8 @@ def run_twelve(args):
     ms_step = float(np.mean(ms))
     pairs_step = nq * args.q2_slice
     rate = pairs_step / (ms_step / 1000.0)
+    tile = {"register_tile": int(sm.stats.tile_rt), "q1_planes_per_pass": int(sm.stats.tile_qp),
+            "q1_per_item": 8, "ctas": int(sm.stats.plan_slots), "q2_per_chunk": int(sm.stats.plan_chunk)}
     # FP64 on the same slices (the first two timed ones)
     v3.setPrecision("fp64")
     ms64, rel = [], []
@@ -772,6 +776,7 @@ def run_twelve(args):
                                    % (nr3, args.q2_slice, nq), "fc3_generation_s": gen_s},
             "bands_s_4096_points": bands_s,
             "projected_full_run_s": nq * nq / rate,
+            "tile_shape": tile,
             "fp64_path": {"value": rate64, "unit": "pairs/s", "ms_per_step": float(np.mean(ms64)),
                           "split_speedup": rate / rate64, "projected_full_run_s": nq * nq / rate64,
                           "split_partial_linewidth_rel_err_max": max(rel)},

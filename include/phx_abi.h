@@ -183,6 +183,9 @@ typedef struct phx_lw_stats {
   int edge_overflow_chunks;
   /* phx_ph_linewidths_screened: vertices (q1, q2) the network dropped */
   long long pairs_screened_out;
+  /* many-branch split builder: the tile shape in use (register tile of the
+   * contractions, q1 planes per pass), tuned per problem shape; 0 elsewhere */
+  int tile_rt, tile_qp;
 } phx_lw_stats;
 
 /* Whole PhScatteringMatrix::builder, switchCase 2 (linewidths), on the GPU:

@@ -46,7 +46,8 @@ class LwStats(ctypes.Structure):
                 ("pair_launches", ctypes.c_int), ("ms_pair", ctypes.c_double),
                 ("plan_chunk", ctypes.c_int), ("plan_slots", ctypes.c_int), ("graph", ctypes.c_int),
                 ("edge_events_peak", ctypes.c_longlong), ("edge_events_cap", ctypes.c_longlong),
-                ("edge_overflow_chunks", ctypes.c_int), ("pairs_screened_out", ctypes.c_longlong)]
+                ("edge_overflow_chunks", ctypes.c_int), ("pairs_screened_out", ctypes.c_longlong),
+                ("tile_rt", ctypes.c_int), ("tile_qp", ctypes.c_int)]
 
 
 class ElParams(ctypes.Structure):

@@ -2283,7 +2283,7 @@ int run_builder_wide(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Ao
   const int Kp = wide::split_kp(nr3);
   int nq1 = wide::kQ1;
   if (split) {
-    PHX_ARG(ctx, wide::split_smem(nb, Kp) <= 227 * 1024,
+    PHX_ARG(ctx, wide::split_smem(nb, Kp, 2) > 0,
             "phx_ph_linewidths: too many branches or R3 vectors for the split path");
   } else {
     nq1 = wide::fp64_q1(nb, nr3);
@@ -2377,7 +2377,63 @@ int run_builder_wide(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Ao
   A.dmax = dmax;
   A.skip = skip;
   A.skip_base = q2b;
+  A.rt = nb > 24 ? 4 : 2;
+  A.qp = wide::split_default_qp(nb, Kp);
   const int grid = ctx->num_sms * wide::blocks_per_sm(nb, nr3, split);
+  // split path: the tile shape (register tile, q1 planes per contraction pass)
+  // tuned once per problem shape on one chunk (PHX_TUNE=0: the defaults)
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const PlanKey pk{20 + fp16, nb, nq, nr3, nr2, nT, dev};
+  BuilderPlan shape{A.rt, A.qp};   // (chunk, slots) fields hold (rt, qp) here
+  const int tune_q2 = std::min(chunk, 64);   // q2 of the timed chunk (every q1)
+  if (split && !skip && !env_off("PHX_TUNE") && q2e - q2b >= 2 * tune_q2 && !find_plan(pk, &shape)) {
+    bose_kernel<<<std::min(1024, (nq * nb * nT + 255) / 256), 256, 0, st>>>(nq, nb, nT, b->d_E, temps, bose);
+    if (fp16) PHX_CUDA(ctx, cudaMemsetAsync(dmax, 0, sizeof(unsigned), st));
+    PHX_CUDA(ctx, wide::launch_fold(nb, nr2, nr3, v->d_D3w, v->d_r2_ofs, v->d_r2_list, v->r2_max_list, v->d_R2,
+                                    v->d_R3, b->d_q, reinterpret_cast<const double2*>(b->d_U), q2b, tune_q2, Dp,
+                                    fp16 ? dmax : nullptr, st));
+    PHX_CUDA(ctx, wide::launch_convert(nb, nr3, Kp, tune_q2, Dp, img, fp16, dmax, st));
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    PHX_CUDA(ctx, cudaEventCreate(&t0));
+    PHX_CUDA(ctx, cudaEventCreate(&t1));
+    double best = 1e300;
+    int rc = PHX_OK;
+    for (int rt : {2, 4})
+      for (int qp : {8, 4, 2}) {
+        if (!wide::split_smem(nb, Kp, qp)) continue;
+        wide::Args Ac = A;
+        Ac.rt = rt;
+        Ac.qp = qp;
+        Ac.q2_first = q2b;
+        Ac.q2_count = tune_q2;
+        Ac.counter = counters;
+        cudaMemsetAsync(counters, 0, sizeof(unsigned), st);
+        cudaEventRecord(t0, st);
+        cudaError_t e = wide::launch_split(Ac, grid, st);
+        cudaEventRecord(t1, st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+        if (e != cudaSuccess) {
+          phx_set_error(ctx, PHX_ERR_CUDA, std::string("builder autotuner: ") + cudaGetErrorString(e));
+          rc = PHX_ERR_CUDA;
+          break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t0, t1);
+        if (ms < best) {
+          best = ms;
+          shape = BuilderPlan{rt, qp};
+        }
+      }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rc != PHX_OK) return rc;
+    store_plan(pk, shape);
+  }
+  if (split) {
+    A.rt = shape.chunk;
+    A.qp = shape.slots;
+  }
   long long pairs = 0;
   for (int c0 = q2b; c0 < q2e; c0 += chunk) pairs += (long long)nq * std::min(chunk, q2e - c0);
   auto work = [&](phx_builder_graph& g) -> int {
@@ -2431,7 +2487,7 @@ int run_builder_wide(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Ao
       (uint64_t)p->smearing, bits(p->sigma), (uint64_t)p->finalize, (uint64_t)chunk, (uint64_t)windowed, bits(base),
       bits(Aout_d), bits(b->d_E), bits(b->d_U), bits(b->d_vg), bits(b->d_q), bits(b->d_U32), bits(v->d_D3w),
       bits(v->d_R2), bits(v->d_R3), bits(ctx->d_status), bits(giso), bits(p->boundary_length), (uint64_t)grid,
-      bits(skip)};
+      bits(skip), (uint64_t)A.rt, (uint64_t)A.qp};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   PHX_CUDA(ctx, cudaEventCreate(&ev0));
   PHX_CUDA(ctx, cudaEventCreate(&ev1));
@@ -2476,6 +2532,8 @@ int run_builder_wide(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Ao
     stats->plan_chunk = chunk;
     stats->plan_slots = grid;
     stats->graph = graph_state;
+    stats->tile_rt = split ? A.rt : 0;
+    stats->tile_qp = split ? A.qp : 0;
     cudaGetLastError();
   }
   phx_builder_graph_free(eager);

@@ -583,9 +583,9 @@ __host__ __device__ inline size_t split_offsets_qp(int nb, int Kp, int qp, size_
 __host__ __device__ inline size_t split_offsets(int nb, int Kp, size_t* o) {
   return split_offsets_qp(nb, Kp, split_qp(nb, Kp), o);
 }
-__device__ inline SplitSmem carve_split(uint8_t* base, int nb, int Kp) {
+__device__ inline SplitSmem carve_split(uint8_t* base, int nb, int Kp, int qp) {
   size_t o[8];
-  split_offsets(nb, Kp, o);
+  split_offsets_qp(nb, Kp, qp, o);
   SplitSmem s;
   s.A = base + o[0];
   s.B = base + o[1];
@@ -656,7 +656,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) wide_split_kernel(WideArgs P
   const MeshArgs& M = P.m;
   extern __shared__ __align__(1024) uint8_t smem[];
   const int nb = M.nb, nbb = nb * nb, nr3 = P.nr3, Kp = P.Kp, nkc = Kp / kAKC, mt_n = P.mtiles;
-  const SplitSmem S = carve_split(smem, nb, Kp);
+  const SplitSmem S = carve_split(smem, nb, Kp, P.qp);
   uint64_t* full = S.bars;                 // [kAStages] A stage loaded
   uint64_t* empty = full + kAStages;       // [kAStages] A stage consumed
   uint64_t* tfull = empty + kAStages;      // [2] TMEM buffer written by the MMAs
@@ -795,7 +795,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) wide_split_kernel(WideArgs P
     const Tile t = carve_tile(S.tile, kWideQ1, nb);
     const int qd = warp & 3, half = warp >> 2;
     const uint32_t bBytes = (uint32_t)kN * Kp * 2;
-    const int qp = split_qp(nb, Kp);
+    const int qp = P.qp;
     const double sc = P.fp16 ? (double)wide_fp16_scale(P.dmax) : 1.0;
     const double wscale = 1.0 / (sc * sc);
     int s = 0;
@@ -971,16 +971,18 @@ int fp64_q1(int nb, int nr3) {
 size_t fp64_smem(int nq1, int nb, int nr3) { return wide_fp64_smem(nq1, nb, nr3); }
 int split_kp(int nr3) { return ((2 * nr3 + kAKC - 1) / kAKC) * kAKC; }
 int split_mtiles(int nb) { return split_nt(nb); }
-size_t split_smem(int nb, int Kp) {
+size_t split_smem(int nb, int Kp, int qp) {
   size_t o[8];
-  return split_offsets(nb, Kp, o) + 1024;   // + alignment slack of the dynamic base
+  const size_t b = split_offsets_qp(nb, Kp, qp, o) + 1024;   // + alignment slack of the dynamic base
+  return b <= 227 * 1024 ? b : 0;
 }
+int split_default_qp(int nb, int Kp) { return split_qp(nb, Kp); }
 size_t split_img_bytes(int nb, int Kp) { return (size_t)nb * split_nt(nb) * (Kp / kAKC) * kAStage; }
 
 cudaError_t set_attributes(int nb, int nr3, bool split) {
   const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
   if (split) {
-    const int sm = (int)split_smem(nb, split_kp(nr3));
+    const int sm = (int)split_smem(nb, split_kp(nr3), split_qp(nb, split_kp(nr3)));
     cudaError_t e = cudaFuncSetAttribute(wide_split_kernel<4>, a, sm);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(wide_split_kernel<2>, a, sm);
     return e;
@@ -996,12 +998,7 @@ cudaError_t set_attributes(int nb, int nr3, bool split) {
 
 int blocks_per_sm(int nb, int nr3, bool split) {
   int n = 0;
-  if (split) {
-    const int sm = (int)split_smem(nb, split_kp(nr3));
-    if (nb > 24) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wide_split_kernel<4>, kSplitThreads, sm);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wide_split_kernel<2>, kSplitThreads, sm);
-    return std::max(1, std::min(n, 1));   // one TMEM allocation per SM keeps the buffers whole
-  }
+  if (split) return 1;   // one CTA (and one TMEM allocation) per SM keeps the buffers whole
   const int q = fp64_q1(nb, nr3);
   const int sm = (int)wide_fp64_smem(q, nb, nr3);
   if (q == 8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wide_fp64_kernel<8, 2>, kWideThreads, sm);
@@ -1020,8 +1017,9 @@ cudaError_t launch_fp64(const Args& A, int grid, cudaStream_t st) {
 }
 
 cudaError_t launch_split(const Args& A, int grid, cudaStream_t st) {
-  const size_t sm = split_smem(A.m.nb, A.Kp);
-  if (A.m.nb > 24) wide_split_kernel<4><<<grid, kSplitThreads, sm, st>>>(A);
+  const size_t sm = split_smem(A.m.nb, A.Kp, A.qp);
+  if (!sm) return cudaErrorInvalidValue;
+  if (A.rt == 4) wide_split_kernel<4><<<grid, kSplitThreads, sm, st>>>(A);
   else wide_split_kernel<2><<<grid, kSplitThreads, sm, st>>>(A);
   return cudaGetLastError();
 }

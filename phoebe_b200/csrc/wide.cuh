@@ -32,13 +32,16 @@ struct Args {
   const float2* U32;          // (nq, nb, nb) FP32 eigenvectors
   int Kp, mtiles, fp16;
   const unsigned* dmax;
+  int rt, qp;                 // split kernel tile shape: register tile (2 or 4), q1 planes per contraction pass
 };
 
 // FP64 kernel: q1 per item for this nb and nr3 (0: too large), and its shared memory
 int fp64_q1(int nb, int nr3);
 size_t fp64_smem(int nq1, int nb, int nr3);
-// split kernel: shared memory, and the bytes of one q2 of the A-operand image
-size_t split_smem(int nb, int Kp);
+// split kernel: shared memory for qp q1 planes per contraction pass (0 if it
+// does not fit), the default tile shape, and the bytes of one q2 of the image
+size_t split_smem(int nb, int Kp, int qp);
+int split_default_qp(int nb, int Kp);
 size_t split_img_bytes(int nb, int Kp);
 int split_kp(int nr3);
 int split_mtiles(int nb);
@@ -46,7 +49,7 @@ int split_mtiles(int nb);
 // persistent pair kernel over the items (q2 of the chunk) x (q1 tiles); grid = CTAs
 cudaError_t launch_fp64(const Args& A, int grid, cudaStream_t st);
 cudaError_t launch_split(const Args& A, int grid, cudaStream_t st);
-cudaError_t set_attributes(int nb, int nr3, bool split);
+cudaError_t set_attributes(int nb, int nr3, bool split);   // for every tile shape
 int blocks_per_sm(int nb, int nr3, bool split);
 // R2 fold of a chunk of q2 (sparse over the non-zero (r3, r2) blocks)
 size_t fold_smem(int nb, int max_list);

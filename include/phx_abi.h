@@ -132,7 +132,10 @@ int phx_v3_cache_d3(phx_v3* v3, const double* q2);
  * ev1 (nq1,nb,nb), ev2 (nb,nb), ev3p/ev3m (nq1,nb,nb) complex, of which the
  * first nb1s[i] / nb2 / nb3ps[i] / nb3ms[i] columns are used.  Outputs are
  * ragged and concatenated: block i of outP holds (nb1s[i], nb2, nb3ps[i])
- * row-major at offset sum_{j<i} nb1s[j]*nb2*nb3ps[j] (likewise outM). */
+ * row-major at offset sum_{j<i} nb1s[j]*nb2*nb3ps[j] (likewise outM).
+ * The precision of v3 applies: with a split precision the R3 transform of
+ * the batch is one tensor-core GEMM (|V|^2 within 2e-6 (FP16) / 2e-5 (BF16)
+ * of the batch's largest); nb <= 15 (one shared-memory block per q1). */
 int phx_v3_couplings_sq(phx_v3* v3, int nq1, const double* q1s, const double* ev1,
                         const int* nb1s, const double* ev2, int nb2, const double* ev3p,
                         const int* nb3ps, const double* ev3m, const int* nb3ms, double* outP,
@@ -192,9 +195,11 @@ typedef struct phx_lw_stats {
  * symmetrizeCoupling, cutoffs, Gaussian/adaptive deltas, Bose factors,
  * accumulation, degeneracy averaging (src/bte/ph_scattering.cpp:60-935;
  * src/bte/scattering.cpp:1168-1318).  A_out (nT, nq*nb) host, the reference's
- * internalDiagonal (linewidth * n(n+1)).  stats may be NULL.  nb = 6 runs on
- * the fused register-tiled kernels (FP64 or split precision); any nb <= 16, or
- * a q2 window, runs on the shared-memory FP64 kernel. */
+ * internalDiagonal (linewidth * n(n+1)).  stats may be NULL.  nb = 6 without
+ * a q2 window runs on the fused kernels (FP64 or split precision); FP64 up to
+ * nb = 16 or with a window on the shared-memory kernel; the split precisions
+ * otherwise, and FP64 beyond 16 branches, on the many-branch builder (nb <= 48,
+ * tcgen05 R3 transform, persistent work queue, tile shape tuned per problem). */
 int phx_ph_linewidths(phx_v3* v3, phx_bands* bands, const phx_lw_params* params,
                       double* A_out, phx_lw_stats* stats);
 /* Same with a device output buffer (nT*nq*nb doubles). */

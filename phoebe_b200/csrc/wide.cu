@@ -518,14 +518,16 @@ __global__ void nonzero_blocks_kernel(int nb3, int nblocks, const double* __rest
 // hi*hi + hi*lo + lo*hi with FP32 accumulation in TMEM, one M tile per 128 rows
 // of the nb^2 (a, c); two TMEM buffers, so the MMAs of the next b2 overlap
 // the epilogue of this one.
-// Warps: 0-7 epilogue (drain TMEM to the T slab, stages 2 and 3 in FP32,
-// rates in FP64), 8 producer (work queue, bulk copies of the A tiles), 9 MMA.
+// Warps: 0-15 epilogue (drain TMEM to the T slab, stages 2 and 3 in FP32,
+// rates in FP64), 16 producer (work queue, bulk copies of the A tiles), 17 MMA.
 // Control decisions of the epilogue (waits, items) are taken by its thread 0
 // and broadcast through a named barrier, so its warps never diverge on them.
+// 16 epilogue warps (4 per scheduler) hide the latency of the contractions'
+// shared and L1 loads; the register budget is 112 per thread.
 // Every wait is bounded; on timeout the kernel records a status bit and all
 // roles leave their loops.
 // ---------------------------------------------------------------------------
-constexpr int kSplitEpiWarps = 8;
+constexpr int kSplitEpiWarps = 16;
 constexpr int kSplitThreads = (kSplitEpiWarps + 2) * 32;
 constexpr int kAKC = 16;                                // K per A stage (one MMA K-step)
 constexpr int kAStages = 2;
@@ -793,7 +795,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) wide_split_kernel(WideArgs P
     // ---------------- epilogue (8 warps, named barrier 1) ----------------
     const int nth = kSplitEpiWarps * 32;
     const Tile t = carve_tile(S.tile, kWideQ1, nb);
-    const int qd = warp & 3, half = warp >> 2;
+    const int qd = warp & 3, grp = warp >> 2;   // TMEM lane quarter; group of M tiles drained
     const uint32_t bBytes = (uint32_t)kN * Kp * 2;
     const int qp = P.qp;
     const double sc = P.fp16 ? (double)wide_fp16_scale(P.dmax) : 1.0;
@@ -843,7 +845,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) wide_split_kernel(WideArgs P
         if (!epi_wait(&tfull[buf], (s >> 1) & 1, S, P, 1 << 17, tid)) { ok = false; break; }
         tc::tc_fence_after();
         // drain: TMEM lane = row (a, c) of an M tile, column 2q + re/im
-        for (int mt = half; mt < mt_n; mt += 2) {
+        for (int mt = grp; mt < mt_n; mt += kSplitEpiWarps / 4) {
           float v[kN];
           const uint32_t ta = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)buf * bufcols + (uint32_t)mt * kN;
           tc::tmem_ld8(ta, v);

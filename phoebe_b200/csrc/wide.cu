@@ -90,6 +90,125 @@ struct Tile {
   double* acc;  // [nq1][nb][kMaxT]
 };
 
+// symmetrizeCoupling (scattering.cpp:1209-1318) of the W planes q0 .. q0+nq1-1
+// of one b2 (W over T): average over the blocks of b3 (rows), then of b1
+// (columns); b2 enters the rates.  Starts and ends with a barrier.
+template <class R>
+__device__ void wide_symmetrize(const Tile& t, int q0, int nq1, int nb, void* Tv, int tid, int nthreads, int bar_id) {
+  const int nbb = nb * nb;
+  R* W = reinterpret_cast<R*>(Tv);
+  asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
+  for (int u = tid; u < nq1 * nb; u += nthreads) {
+    const int q = q0 + u / nb, b1 = u % nb;
+    if (t.q1s[q] < 0 || !t.inw[q]) continue;
+    R* w = W + (size_t)q * nbb + (size_t)b1 * nb;
+    const int* g = t.g3s + q * nb;
+    for (int s0 = 0; s0 < nb;) {
+      const int s1 = wide_block_end(g, nb, s0);
+      if (s1 - s0 > 1) {
+        R sum = 0;
+        for (int k = s0; k < s1; ++k) sum += w[k];
+        for (int k = s0; k < s1; ++k) w[k] = sum / (R)(s1 - s0);
+      }
+      s0 = s1;
+    }
+  }
+  asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
+  for (int u = tid; u < nq1 * nb; u += nthreads) {
+    const int q = q0 + u / nb, b3 = u % nb;
+    if (t.q1s[q] < 0 || !t.inw[q]) continue;
+    R* w = W + (size_t)q * nbb + b3;
+    const int* g = t.g1s + q * nb;
+    for (int s0 = 0; s0 < nb;) {
+      const int s1 = wide_block_end(g, nb, s0);
+      if (s1 - s0 > 1) {
+        R sum = 0;
+        for (int k = s0; k < s1; ++k) sum += w[(size_t)k * nb];
+        for (int k = s0; k < s1; ++k) w[(size_t)k * nb] = sum / (R)(s1 - s0);
+      }
+      s0 = s1;
+    }
+  }
+  asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
+}
+
+// wide_contract's FP32 4 x 4 tiles when nb is a multiple of 4: no bounds
+// checks, and the four consecutive complex values of a tile row (e1, T, e3)
+// move as two 16-byte accesses, a row of W as one.
+__device__ __forceinline__ float4 ld4(const float2* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ float4 ldg4(const float2* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ void wide_contract_f4(const Tile& t, int q0, int nq1, int nb, const float2* __restrict__ U, float2* T,
+                                 float2* X, int ldx, int tid, int nthreads, int bar_id) {
+  const int nt = nb / 4, per_q = nt * nt, nbb = nb * nb;
+  for (int u = tid; u < nq1 * per_q; u += nthreads) {
+    const int q = q0 + u / per_q, r = u % per_q, b10 = (r / nt) * 4, c0 = (r % nt) * 4;
+    const int q1 = t.q1s[q];
+    if (q1 < 0 || !t.inw[q]) continue;
+    const float2* e1 = U + (size_t)q1 * nbb + b10;
+    const float2* Tq = T + (size_t)q * nbb + c0;
+    float2 acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[i][k] = make_float2(0.f, 0.f);
+#pragma unroll 2
+    for (int a = 0; a < nb; ++a) {
+      const float4 e01 = ldg4(e1 + a * nb), e23 = ldg4(e1 + a * nb + 2);
+      const float4 t01 = ld4(Tq + a * nb), t23 = ld4(Tq + a * nb + 2);
+      const float2 ev[4] = {make_float2(e01.x, e01.y), make_float2(e01.z, e01.w), make_float2(e23.x, e23.y),
+                            make_float2(e23.z, e23.w)};
+      const float2 tv[4] = {make_float2(t01.x, t01.y), make_float2(t01.z, t01.w), make_float2(t23.x, t23.y),
+                            make_float2(t23.z, t23.w)};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) cfmaf(acc[i][k], ev[i], tv[k]);
+    }
+    float2* Xq = X + (size_t)(q - q0) * nb * ldx + c0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) Xq[(b10 + i) * ldx + k] = acc[i][k];
+  }
+  asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
+  float* W = reinterpret_cast<float*>(T);
+  for (int u = tid; u < nq1 * per_q; u += nthreads) {
+    const int q = q0 + u / per_q, r = u % per_q, b10 = (r / nt) * 4, b30 = (r % nt) * 4;
+    if (t.q1s[q] < 0 || !t.inw[q]) continue;
+    const float2* e3 = U + (size_t)t.q3s[q] * nbb + b30;
+    const float2* Xq = X + (size_t)(q - q0) * nb * ldx + (size_t)b10 * ldx;
+    float2 acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[i][k] = make_float2(0.f, 0.f);
+#pragma unroll 2
+    for (int c = 0; c < nb; ++c) {
+      float2 xv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) xv[i] = Xq[i * ldx + c];
+      const float4 e01 = ldg4(e3 + c * nb), e23 = ldg4(e3 + c * nb + 2);
+      const float2 ev[4] = {make_float2(e01.x, e01.y), make_float2(e01.z, e01.w), make_float2(e23.x, e23.y),
+                            make_float2(e23.z, e23.w)};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) cfmacf(acc[i][k], xv[i], ev[k]);
+    }
+    float* Wq = W + (size_t)q * nbb + b30;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      float4 w;
+      w.x = acc[i][0].x * acc[i][0].x + acc[i][0].y * acc[i][0].y;
+      w.y = acc[i][1].x * acc[i][1].x + acc[i][1].y * acc[i][1].y;
+      w.z = acc[i][2].x * acc[i][2].x + acc[i][2].y * acc[i][2].y;
+      w.w = acc[i][3].x * acc[i][3].x + acc[i][3].y * acc[i][3].y;
+      *reinterpret_cast<float4*>(Wq + (b10 + i) * nb) = w;
+    }
+  }
+  wide_symmetrize<float>(t, q0, nq1, nb, T, tid, nthreads, bar_id);
+}
+
 // Stages 2 and 3 for one b2 of every q1 of the item, on CUDA cores: T (a, c)
 // -> X (b1, c) -> W (b1, b3) = |V|^2, W written over T (as R).  Register
 // tiles of RT x RT outputs per thread.
@@ -104,6 +223,13 @@ template <class R, class C, int RT>
 __device__ void wide_contract(const Tile& t, int q0, int nq1, int nb, const C* __restrict__ U, const C* E1s,
                               const C* E3s, C* T, C* X, int ldx, int tid, int nthreads, int bar_id) {
   const int nt = (nb + RT - 1) / RT, per_q = nt * nt, nbb = nb * nb;
+  if constexpr (RT == 4 && sizeof(C) == 8) {
+    if ((nb & 3) == 0 && !E1s) {
+      wide_contract_f4(t, q0, nq1, nb, reinterpret_cast<const float2*>(U), reinterpret_cast<float2*>(T),
+                       reinterpret_cast<float2*>(X), ldx, tid, nthreads, bar_id);
+      return;
+    }
+  }
   // stage 2: X[q][b1][c] = sum_a e1(a, b1) T[q][a][c]
   for (int u = tid; u < nq1 * per_q; u += nthreads) {
     const int q = q0 + u / per_q, r = u % per_q, b10 = (r / nt) * RT, c0 = (r % nt) * RT;
@@ -167,41 +293,7 @@ __device__ void wide_contract(const Tile& t, int q0, int nq1, int nb, const C* _
       for (int k = 0; k < RT; ++k)
         if (b10 + i < nb && b30 + k < nb) Wq[(b10 + i) * nb + b30 + k] = acc[i][k].x * acc[i][k].x + acc[i][k].y * acc[i][k].y;
   }
-  asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
-  // symmetrizeCoupling (scattering.cpp:1209-1318) of this b2 plane: average
-  // over the blocks of b3 (rows), then of b1 (columns); b2 enters the rates
-  for (int u = tid; u < nq1 * nb; u += nthreads) {
-    const int q = q0 + u / nb, b1 = u % nb;
-    if (t.q1s[q] < 0 || !t.inw[q]) continue;
-    R* w = W + (size_t)q * nbb + (size_t)b1 * nb;
-    const int* g = t.g3s + q * nb;
-    for (int s0 = 0; s0 < nb;) {
-      const int s1 = wide_block_end(g, nb, s0);
-      if (s1 - s0 > 1) {
-        R sum = 0;
-        for (int k = s0; k < s1; ++k) sum += w[k];
-        for (int k = s0; k < s1; ++k) w[k] = sum / (R)(s1 - s0);
-      }
-      s0 = s1;
-    }
-  }
-  asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
-  for (int u = tid; u < nq1 * nb; u += nthreads) {
-    const int q = q0 + u / nb, b3 = u % nb;
-    if (t.q1s[q] < 0 || !t.inw[q]) continue;
-    R* w = W + (size_t)q * nbb + b3;
-    const int* g = t.g1s + q * nb;
-    for (int s0 = 0; s0 < nb;) {
-      const int s1 = wide_block_end(g, nb, s0);
-      if (s1 - s0 > 1) {
-        R sum = 0;
-        for (int k = s0; k < s1; ++k) sum += w[(size_t)k * nb];
-        for (int k = s0; k < s1; ++k) w[(size_t)k * nb] = sum / (R)(s1 - s0);
-      }
-      s0 = s1;
-    }
-  }
-  asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
+  wide_symmetrize<R>(t, q0, nq1, nb, T, tid, nthreads, bar_id);
 }
 
 // Rates of the b2 plane (ph_scattering.cpp:338-380, 466-518), FP64, with the

@@ -1015,7 +1015,7 @@ size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 // split-precision path (split.cu)
 int phx_split_kp(int nr3);
 size_t phx_split_bimg_bytes(int chunk, int nr3);
-size_t phx_split_smem_bytes(int nr3);
+size_t phx_split_smem_bytes(int nr3, int nT);
 int phx_split_set_attributes(phx_ctx* ctx, int nr3, int nT);
 int phx_split_prepare_bands(phx_ctx* ctx, phx_bands* b);
 size_t phx_split_rec_bytes(int nq);
@@ -1393,7 +1393,7 @@ int run_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* Aout_d,
   void* edges = base + sz_dp + sz_part + sz_bose + sz_T + sz_img + sz_rec + sz_iso + sz_max;
   if (split) {
     PHX_ARG(ctx, NB == 6, "split-precision path supports nb = 6");
-    PHX_ARG(ctx, phx_split_smem_bytes(nr3) <= 227 * 1024, "too many R3 vectors for the split path");
+    PHX_ARG(ctx, phx_split_smem_bytes(nr3, nT) <= 227 * 1024, "too many R3 vectors for the split path");
     PHX_TRY(phx_split_prepare_bands(ctx, b));
     if (b->emax < 0.0) {
       // largest energy of the mesh (margin of the split path's FP32 windows), once per band structure
@@ -1918,7 +1918,7 @@ int run_matrix_builder(phx_v3* v, phx_bands* b, const phx_lw_params* p, double* 
   unsigned* edge_over = dmax + 3;   // the matrix modes fail on an overflow
   void* edges = sbase + sz_img + sz_rec + sz_max;
   if (split) {
-    PHX_ARG(ctx, phx_split_smem_bytes(nr3) <= 227 * 1024, "too many R3 vectors for the split path");
+    PHX_ARG(ctx, phx_split_smem_bytes(nr3, nT) <= 227 * 1024, "too many R3 vectors for the split path");
     PHX_TRY(phx_split_prepare_bands(ctx, b));
     if (b->emax < 0.0) {
       std::vector<double> Eh((size_t)nq * NB);

@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(kThreads, 1) el_gemm_kernel(GemmArgs P) {
         float v[16];
         tc::tmem_ld8(base + c0, v);
         tc::tmem_ld8(base + c0 + 8, v + 8);
-        tc::tmem_wait_ld();
+        tc::tmem_wait_ld<16>(v);
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           const int x = x0 + c0 / 2 + i;
@@ -469,7 +469,7 @@ __global__ void __launch_bounds__(kThreads, 1) el_g1_gemm_kernel(G1Args P) {
         float v[kG1N];
 #pragma unroll
         for (int i = 0; i < kG1N; i += 8) tc::tmem_ld8(tmem + lanes + buf * kG1N + i, v + i);
-        tc::tmem_wait_ld();
+        tc::tmem_wait_ld<kG1N>(v);
         tc::tc_fence_before();
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&acce[buf]);

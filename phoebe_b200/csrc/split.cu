@@ -65,10 +65,17 @@ constexpr int kRecChunks = 37;
 constexpr int kChBand = 18;
 constexpr int kChGp = 36;
 constexpr int kU2Chunks = kRecChunks - kChBand;   // band blocks + blocks word
-constexpr int kQueue = 64;                        // live-triplet queue entries per warp
-// FP32 rate accumulators of a quarter: one row of 6 b1 x kMaxT per q1, padded
-// to an odd stride so that the rows of a warp fall in distinct banks
-constexpr int kAccRow = 6 * kMaxT + 1;
+// Sizes that depend on the number of temperatures NT:
+//  * kAccRow: FP32 rate accumulators of a quarter, one row of 6 b1 x NT per
+//    q1, padded to an odd stride so that the rows of a warp fall in distinct
+//    banks;
+//  * kQueue: live-triplet queue entries per warp (a push round adds at most
+//    32 to fewer than 32 queued).
+template <int NT>
+struct Pcfg {
+  static constexpr int kAccRow = 6 * NT + 1;
+  static constexpr int kQueue = 64;
+};
 
 struct TcArgs {
   MeshArgs m;
@@ -332,15 +339,16 @@ __device__ bool beyond_two_sigma(double de, const uint4* a, const uint4* b) {
 // difference, with the reference's cut-offs (delta_function.cpp:65-96).  The
 // cut-off |E| > 2 sigma is discontinuous; `near` is set when the FP32
 // comparison is within 1e-5 of it, and the caller then re-decides in FP64.
+// Evaluated without branches (the exponential always, then selects), so the
+// lanes of a warp stay together whatever their triplets.
 __device__ __forceinline__ float delta_ad(const Sig& g, double de, bool& near) {
-  if (g.vz && de == 0.0) return 1.f;
-  if (g.s == 0.f) return 0.f;
   const float e = (float)de;
   const float two_s = 2.f * g.s;
-  near = fabsf(fabsf(e) - two_s) <= two_s * 1e-5f;
-  if (fabsf(e) > two_s) return 0.f;
+  near = g.s != 0.f && fabsf(fabsf(e) - two_s) <= two_s * 1e-5f;
   const float x = e * g.inv;
-  return __expf(-x * x) * g.inv * (float)(1.0 / (phxc::sqrtPi * phxc::erf2));
+  float d = __expf(-x * x) * g.inv * (float)(1.0 / (phxc::sqrtPi * phxc::erf2));
+  d = (g.s == 0.f || fabsf(e) > two_s) ? 0.f : d;
+  return (g.vz && de == 0.0) ? 1.f : d;
 }
 __device__ __forceinline__ float delta_ga(float inv, double de) {
   const float x = (float)de * inv;
@@ -491,17 +499,18 @@ struct Smem {
   float2* E1v;         // e1 [36][128]
   double* En1;         // [6][128]
   float* iE1;          // [6][128]
-  float* N1;           // [kMaxT*6][128]
+  float* N1;           // [NT*6][128]
   uint4* rec;          // staged q3 records [kRecChunks][128]
   uint4* u2;           // [4 quarters][2: q2, -q2][kU2Chunks]
   unsigned long long* need;  // [6 b2][128] bit b1*6+b3
   uint2* queue;        // [12 warps][kQueue] live triplets awaiting their rates
-  float* acc;          // [4 quarters][32 rows][kAccRow: 6 b1 x kMaxT + pad] rates of the current q2
+  float* acc;          // [4 quarters][32 rows][kAccRow: 6 b1 x NT + pad] rates of the current q2
   uint64_t* bars;
 };
 
 __host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
+template <int NT>
 __host__ __device__ inline size_t smem_layout(int Kp, size_t* off) {
   size_t o = 0;
   const size_t aPart = (size_t)kM * Kp * 2;
@@ -510,19 +519,20 @@ __host__ __device__ inline size_t smem_layout(int Kp, size_t* off) {
   off[2] = o; o += align16(36 * kM * sizeof(float2));          // e1
   off[3] = o; o += align16(6 * kM * sizeof(double));           // E1
   off[4] = o; o += align16(6 * kM * sizeof(float));            // 1/E1
-  off[5] = o; o += align16(kMaxT * 6 * kM * sizeof(float));    // N1
+  off[5] = o; o += align16(NT * 6 * kM * sizeof(float));       // N1
   off[6] = o; o += align16((size_t)kRecChunks * kM * 16);      // staged records
   off[7] = o; o += align16(4 * 2 * kU2Chunks * 16);            // q2 bands
   off[8] = o; o += align16(6 * kM * sizeof(unsigned long long));  // masks
-  off[9] = o; o += align16(kEpiWarps * kQueue * sizeof(uint2));   // queues
-  off[10] = o; o += align16(4 * 32 * kAccRow * sizeof(float));  // q2 accumulators
+  off[9] = o; o += align16(kEpiWarps * Pcfg<NT>::kQueue * sizeof(uint2));   // queues
+  off[10] = o; o += align16(4 * 32 * Pcfg<NT>::kAccRow * sizeof(float));  // q2 accumulators
   off[11] = o; o += align16(32 * sizeof(uint64_t));            // barriers, tmem slot, flag
   return o;
 }
 
+template <int NT>
 __device__ __forceinline__ Smem carve(uint8_t* base, int Kp) {
   size_t off[12];
-  smem_layout(Kp, off);
+  smem_layout<NT>(Kp, off);
   Smem s;
   s.aPart = (uint32_t)kM * Kp * 2;
   s.A = base + off[0];
@@ -542,84 +552,57 @@ __device__ __forceinline__ Smem carve(uint8_t* base, int Kp) {
 
 // Rate of one queued live triplet, added to the FP32 accumulator of its row
 // and b1.  Kept out of line: the kernel's loop calls it from two places (a
-// full queue, the end of a q2), and one copy of its code instead of two keeps
-// the hot loop within the instruction cache (14% faster than inlined).  Entry: x = |V|^2 / n1, y = lane of the q1 row | b1 << 5 | b2 << 8 |
-// b3 << 11 | degenerate flag << 14.  Flagged entries average the rate factors
-// over the degenerate blocks of b2 and b3 (one band each otherwise).
+// full queue, the end of a q2), and one copy of its code keeps the hot loop
+// within the instruction cache.  Entry: x = weight |V|^2 / (n1 n2 n3),
+// y = lane of the q1 row | b1 << 5 | b2 << 8 | b3 << 11, where b2 and b3 are
+// single bands (degenerate blocks were expanded when the entry was queued).
 template <int NT, bool MAT, int SM>
 __device__ __noinline__ void rate_entry(uint2 e, int qd, const double* En1, const float* iE1s,
-                                           const float* N1, const uint4* rec, const uint4* u2,
-                                           unsigned gp2, int /*smearing: SM*/, float ginv, float pre,
-                                           float* qacc, const TcArgs& P, int iq2) {
+                                        const float* N1, const uint4* rec, const uint4* u2, float ginv,
+                                        float pre, float* qacc, const TcArgs& P, int iq2) {
   constexpr int smearing = SM;   // each smearing has its own instantiation
   const float wn = __uint_as_float(e.x);
   const int r = e.y & 31, b1 = (e.y >> 5) & 7, b2 = (e.y >> 8) & 7, b3 = (e.y >> 11) & 7;
   const int mm = qd * 32 + r;
-  const uint4* srow = rec + mm;
-  unsigned bm2 = 1u << b2, bm3 = 1u << b3;
-  if ((e.y >> 14) & 1) {
-    bm2 = blk_mask(gp2, b2);
-    bm3 = blk_mask(srow[kChGp * kM].x, b3);
-  }
   const double E1 = En1[b1 * kM + mm];
   const float iE1 = iE1s[b1 * kM + mm];
   float n1v[NT];
 #pragma unroll
   for (int t = 0; t < NT; ++t) n1v[t] = N1[(t * 6 + b1) * kM + mm];
-  float g[NT];
-#pragma unroll
-  for (int t = 0; t < NT; ++t) g[t] = 0.f;
-  unsigned anynear = 0u;
-  constexpr bool matm = MAT;   // matrix modes: their own instantiation
-  const double mscale = (double)(wn / (float)(__popc(bm2) * __popc(bm3)));
-  for (unsigned m2 = bm2; m2; m2 &= m2 - 1) {
-    const int c2 = __ffs(m2) - 1;
-    const Band x2 = load_band<NT>(u2 + 3 * c2, 1);
-    const Band x2m = load_band<NT>(u2 + kU2Chunks + 3 * c2, 1);
-    float gpl[NT], gmi[NT];   // matrix modes: the "+" and "-" sums of this c2
-#pragma unroll
-    for (int t = 0; t < NT; ++t) gpl[t] = gmi[t] = 0.f;
-    for (unsigned m3 = bm3; m3; m3 &= m3 - 1) {
-      const int c3 = __ffs(m3) - 1;
-      const Band x3 = load_band<NT>(srow + (kChBand + 3 * c3) * kM, kM);
-      Sig gp, gm;
-      if (smearing == PHX_SMEAR_ADAPTIVE) {
-        gp = sigma_ad(x2.P, x3.P, x2.vf, x3.vf);
-        gm = sigma_ad(x2m.P, x3.P, x2m.vf, x3.vf);
-      }
-      float f[NT];
-      unsigned near = 0u;
-      if constexpr (matm) {
-#pragma unroll
-        for (int t = 0; t < NT; ++t) f[t] = 0.f;
-        if (x3.E >= phxc::phEnergyCutoff) {
-          float dp, d1, d2, fpv[NT], fmv[NT];
-          deltas3(smearing, ginv, E1, x2, x2m, x3, gp, gm, dp, d1, d2, near);
-          rate_combine2<NT>(pre, iE1, n1v, x2, x2m, x3, dp, d1, d2, fpv, fmv);
-#pragma unroll
-          for (int t = 0; t < NT; ++t) {
-            gpl[t] += fpv[t];
-            gmi[t] += fmv[t];
-            f[t] = fpv[t] + fmv[t];
-          }
-        }
-      } else {
-        rate_f<NT>(smearing, ginv, pre, E1, iE1, n1v, x2, x2m, x3, gp, gm, f, near);
-      }
-#pragma unroll
-      for (int t = 0; t < NT; ++t) g[t] += f[t];
-      anynear |= near;
-    }
-    if constexpr (matm) add_matrix<NT>(P, P.q1_order[blockIdx.x * kM + mm], b1, iq2, c2, mscale, gpl, gmi);
+  const Band x2 = load_band<NT>(u2 + 3 * b2, 1);
+  const Band x2m = load_band<NT>(u2 + kU2Chunks + 3 * b2, 1);
+  const Band x3 = load_band<NT>(rec + mm + (kChBand + 3 * b3) * kM, kM);
+  Sig gp, gm;
+  if (smearing == PHX_SMEAR_ADAPTIVE) {
+    gp = sigma_ad(x2.P, x3.P, x2.vf, x3.vf);
+    gm = sigma_ad(x2m.P, x3.P, x2m.vf, x3.vf);
   }
-  if (anynear) {
+  float f[NT];
+  unsigned near = 0u;
+  if constexpr (MAT) {
+    // matrix modes: the "+" rates go to column (q2, b2), the "-" ones to (-q2, b2)
+    float fpv[NT], fmv[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) fpv[t] = fmv[t] = 0.f;
+    if (x3.E >= phxc::phEnergyCutoff) {
+      float dp, d1, d2;
+      deltas3(smearing, ginv, E1, x2, x2m, x3, gp, gm, dp, d1, d2, near);
+      rate_combine2<NT>(pre, iE1, n1v, x2, x2m, x3, dp, d1, d2, fpv, fmv);
+    }
+#pragma unroll
+    for (int t = 0; t < NT; ++t) f[t] = fpv[t] + fmv[t];
+    add_matrix<NT>(P, P.q1_order[blockIdx.x * kM + mm], b1, iq2, b2, (double)wn, fpv, fmv);
+  } else {
+    rate_f<NT>(smearing, ginv, pre, E1, iE1, n1v, x2, x2m, x3, gp, gm, f, near);
+  }
+  if (near) {
     // a cut-off decision too close for FP32: edge_fix_kernel re-decides the entry in FP64
     const unsigned i = atomicAdd(P.edge_count, 1u);
     if (i < P.edge_cap) P.edges[i] = EdgeEvent{(blockIdx.x << 12) | (blockIdx.y << 7) | (unsigned)mm, iq2, e};
   }
-  const float scale = wn / (float)(__popc(bm2) * __popc(bm3));
+  constexpr int AR = Pcfg<NT>::kAccRow;
 #pragma unroll
-  for (int t = 0; t < NT; ++t) atomicAdd(&qacc[r * kAccRow + b1 * kMaxT + t], scale * g[t]);
+  for (int t = 0; t < NT; ++t) atomicAdd(&qacc[r * AR + b1 * NT + t], wn * f[t]);
 }
 
 template <int NT, bool MAT, int SM>
@@ -627,7 +610,7 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
   const MeshArgs& M = P.m;
   extern __shared__ __align__(1024) uint8_t smem[];
   const int Kp = P.Kp, nkc = Kp / kKC;
-  const Smem S = carve(smem, Kp);
+  const Smem S = carve<NT>(smem, Kp);
   uint64_t* full = S.bars;                // [kStages]
   uint64_t* empty = full + kStages;       // [kStages]
   uint64_t* accf = empty + kStages;       // [kParts] MMA of a part done
@@ -697,7 +680,7 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
     S.En1[e] = x.E;
     S.iE1[e] = x.iE;
 #pragma unroll
-    for (int t = 0; t < kMaxT; ++t) S.N1[(t * 6 + b) * kM + mm] = x.N[t];
+    for (int t = 0; t < NT; ++t) S.N1[(t * 6 + b) * kM + mm] = x.N[t];
   }
   tc::fence_proxy_async_smem();
   tc::tc_fence_before();
@@ -790,12 +773,13 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
     for (int t = 0; t < NT; ++t) acc0[t] = acc1[t] = 0.0;
     uint4* u2 = S.u2 + qd * 2 * kU2Chunks;
     const uint4* srow = S.rec + m;
-    uint2* queue = S.queue + warp * kQueue;
-    float* qacc = S.acc + qd * 32 * kAccRow;
+    constexpr int AR = Pcfg<NT>::kAccRow;
+    uint2* queue = S.queue + warp * Pcfg<NT>::kQueue;
+    float* qacc = S.acc + qd * 32 * AR;
 #pragma unroll
-    for (int t = 0; t < kMaxT; ++t) {
-      qacc[lane * kAccRow + k * kMaxT + t] = 0.f;
-      qacc[lane * kAccRow + (k + 3) * kMaxT + t] = 0.f;
+    for (int t = 0; t < NT; ++t) {
+      qacc[lane * AR + k * NT + t] = 0.f;
+      qacc[lane * AR + (k + 3) * NT + t] = 0.f;
     }
     int qn = 0;  // queued live triplets (warp-uniform)
     const unsigned lanemask_lt = (1u << lane) - 1u;
@@ -804,10 +788,10 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
     auto flush = [&]() {
 #pragma unroll
       for (int t = 0; t < NT; ++t) {
-        acc0[t] += (double)qacc[lane * kAccRow + k * kMaxT + t];
-        acc1[t] += (double)qacc[lane * kAccRow + (k + 3) * kMaxT + t];
-        qacc[lane * kAccRow + k * kMaxT + t] = 0.f;
-        qacc[lane * kAccRow + (k + 3) * kMaxT + t] = 0.f;
+        acc0[t] += (double)qacc[lane * AR + k * NT + t];
+        acc1[t] += (double)qacc[lane * AR + (k + 3) * NT + t];
+        qacc[lane * AR + k * NT + t] = 0.f;
+        qacc[lane * AR + (k + 3) * NT + t] = 0.f;
       }
     };
     bool failed = false;
@@ -910,7 +894,7 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
               tc::tmem_ld4(col0 + a * 12 + 20, t + 20);
               const float2 e0 = S.E1v[(a * 6 + row) * kM + m];
               const float2 e1 = S.E1v[((a + 1) * 6 + row) * kM + m];
-              tc::tmem_wait_ld();
+              tc::tmem_wait_ld<24>(t);
 #pragma unroll
               for (int c = 0; c < 6; ++c) {
                 cfmaf(Y[c], e0, make_float2(t[2 * c], t[2 * c + 1]));
@@ -930,24 +914,41 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
                 cfmacf(v, Y[c], make_float2(__uint_as_float(e.x), __uint_as_float(e.y)));
               }
               const float w = fmaf(v.x, v.x, v.y * v.y);
-              // queue the live triplets of the owned b1 (block-averaged when degenerate)
-              const bool blk23 = (bm2 != (1u << b2)) || (deg3 && blk_mask(gp3, b3) != (1u << b3));
-              const unsigned meta =
-                  (unsigned)lane | ((unsigned)b2 << 8) | ((unsigned)b3 << 11) | (blk23 ? (1u << 14) : 0u);
-#pragma unroll
-              for (int o = 0; o < 2; ++o) {
-                const unsigned no = o ? nO1 : nO0, bmo = o ? bmO1 : bmO0;
-                const bool live = ((no >> b3) & 1u) && ((bmo >> row) & 1u);
-                const unsigned bal = __ballot_sync(FULL, live);
-                if (!bal) continue;
-                if (live)
+              // Queue the live triplets of the owned b1.  A degenerate b2 or b3
+              // averages the rate factors over its block: the entry is queued
+              // once per (c2, c3) of the two blocks with weight 1/(n1 n2 n3), so
+              // that every queued entry costs one rate evaluation and the lanes
+              // of a batch never wait for a degenerate neighbour.
+              const unsigned bm3 = deg3 ? blk_mask(gp3, b3) : (1u << b3);
+              const bool l0 = ((nO0 >> b3) & 1u) && ((bmO0 >> row) & 1u);
+              const bool l1 = ((nO1 >> b3) & 1u) && ((bmO1 >> row) & 1u);
+              unsigned orem = (l0 ? 1u : 0u) | (l1 ? 2u : 0u);
+              unsigned m2 = bm2, m3 = bm3;
+              const int n23 = __popc(bm2) * __popc(bm3);
+              unsigned bal;
+              while ((bal = __ballot_sync(FULL, orem != 0u)) != 0u) {
+                if (orem) {
+                  const int o = __ffs(orem) - 1;
+                  const int nd = __popc(o ? bmO1 : bmO0) * n23;
+                  const float ws = nd == 1 ? w : w / (float)nd;
                   queue[qn + __popc(bal & lanemask_lt)] =
-                      make_uint2(__float_as_uint(w / (float)__popc(bmo)), meta | ((unsigned)(r0 + 3 * o) << 5));
+                      make_uint2(__float_as_uint(ws), (unsigned)lane | ((unsigned)(r0 + 3 * o) << 5) |
+                                                          ((unsigned)(__ffs(m2) - 1) << 8) |
+                                                          ((unsigned)(__ffs(m3) - 1) << 11));
+                  m3 &= m3 - 1;
+                  if (!m3) {
+                    m3 = bm3;
+                    m2 &= m2 - 1;
+                    if (!m2) {
+                      m2 = bm2;
+                      orem &= orem - 1;
+                    }
+                  }
+                }
                 qn += __popc(bal);
                 if (qn >= 32) {
                   __syncwarp();
-                  rate_entry<NT, MAT, SM>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc, P,
-                                 iq2);
+                  rate_entry<NT, MAT, SM>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, ginv, pre, qacc, P, iq2);
                   const uint2 rest = lane + 32 < qn ? queue[lane + 32] : make_uint2(0u, 0u);
                   __syncwarp();
                   if (lane + 32 < qn) queue[lane] = rest;
@@ -966,7 +967,7 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
       if (qn) {
         __syncwarp();
         if (lane < qn)
-          rate_entry<NT, MAT, SM>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, gp2, smearing, ginv, pre, qacc, P, iq2);
+          rate_entry<NT, MAT, SM>(queue[lane], qd, S.En1, S.iE1, S.N1, S.rec, u2, ginv, pre, qacc, P, iq2);
         qn = 0;
       }
       __syncwarp();
@@ -1059,7 +1060,7 @@ __global__ void __launch_bounds__(128, 1) diag_gemm_kernel(int N, int Kp, const 
     for (int c0 = 0; c0 < N; c0 += 8) {
       float v[8];
       tc::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + c0, v);
-      tc::tmem_wait_ld();
+      tc::tmem_wait_ld<8>(v);
       for (int i = 0; i < 8; ++i) C[(size_t)tid * N + c0 + i] = v[i];
     }
   }
@@ -1071,14 +1072,15 @@ __global__ void __launch_bounds__(128, 1) diag_gemm_kernel(int N, int Kp, const 
   }
 }
 
+template <int NT>
 size_t pair_tc_smem(int Kp) {
   size_t off[12];
-  return smem_layout(Kp, off) + 1024;
+  return smem_layout<NT>(Kp, off) + 1024;
 }
 
 template <int NT>
 int launch_pair(phx_ctx* ctx, const TcArgs& A, int tiles, int slots) {
-  const size_t smem = pair_tc_smem(A.Kp);   // attribute set by phx_split_set_attributes
+  const size_t smem = pair_tc_smem<NT>(A.Kp);   // attribute set by phx_split_set_attributes
   constexpr int ad = PHX_SMEAR_ADAPTIVE, ga = PHX_SMEAR_GAUSSIAN;
   const bool adaptive = A.m.smearing == PHX_SMEAR_ADAPTIVE;
   const dim3 grid(tiles, slots);
@@ -1316,7 +1318,15 @@ int phx_split_pair_chunk(phx_ctx* ctx, const pairc::MeshArgs& M, const phx_v3* v
   return PHX_OK;
 }
 
-size_t phx_split_smem_bytes(int nr3) { return pair_tc_smem(phx_split_kp(nr3)); }
+size_t phx_split_smem_bytes(int nr3, int nT) {
+  const int Kp = phx_split_kp(nr3);
+  switch (nT) {
+    case 1: return pair_tc_smem<1>(Kp);
+    case 2: return pair_tc_smem<2>(Kp);
+    case 3: return pair_tc_smem<3>(Kp);
+    default: return pair_tc_smem<4>(Kp);
+  }
+}
 
 // capacity of the near-cut-off event list of one pair launch (a smaller one
 // may be set for tests: a launch with more events is re-run in pieces), and
@@ -1348,7 +1358,7 @@ int set_pair_attributes(phx_ctx* ctx, int smem) {
 // Dynamic shared-memory limit of the pair kernel for nT temperatures; called
 // before any launch (and outside graph capture).
 int phx_split_set_attributes(phx_ctx* ctx, int nr3, int nT) {
-  const int smem = (int)pair_tc_smem(phx_split_kp(nr3));
+  const int smem = (int)phx_split_smem_bytes(nr3, nT);
   switch (nT) {
     case 1: PHX_TRY(set_pair_attributes<1>(ctx, smem)); break;
     case 2: PHX_TRY(set_pair_attributes<2>(ctx, smem)); break;

@@ -151,7 +151,17 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
       : "memory");
 }
 
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// tcgen05.ld writes its destination registers asynchronously: they may be
+// read only after tcgen05.wait::ld.  The compiler sees no dependency between
+// the wait and those registers, so the wait also redefines the N loaded
+// values through empty asm statements ordered after it: no use of a loaded
+// value can then be scheduled above the wait.
+template <int N>
+__device__ __forceinline__ void tmem_wait_ld(float* v) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < N; ++i) asm volatile("" : "+f"(v[i]));
+}
 
 // 32 lanes x 32 bit, 8 consecutive columns per thread
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {

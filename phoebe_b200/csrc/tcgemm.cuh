@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(int M, int N, int K, const
       for (int c0 = 0; c0 < kTN; c0 += 8) {
         float v[8];
         tc::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + c0, v);
-        tc::tmem_wait_ld();
+        tc::tmem_wait_ld<8>(v);
 #pragma unroll
         for (int i = 0; i < 8; ++i) acc[c0 + i] += v[i];
       }

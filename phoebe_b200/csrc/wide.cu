@@ -942,7 +942,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) wide_split_kernel(WideArgs P
           const uint32_t ta = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)buf * bufcols + (uint32_t)mt * kN;
           tc::tmem_ld8(ta, v);
           tc::tmem_ld8(ta + 8, v + 8);
-          tc::tmem_wait_ld();
+          tc::tmem_wait_ld<16>(v);
           const int row = mt * 128 + qd * 32 + lane;
           if (row < nbb) {
 #pragma unroll

@@ -57,7 +57,8 @@ constexpr uint32_t kStageBytes = 2 * kPartBytes;  // hi + lo: 9216 B
 constexpr uint32_t kBSbo = (kKC / 8) * 128;       // 256 B between 8-row groups
 
 // Per-point record, 37 chunks of 16 bytes:
-//   chunks 0-17   e[a*6+b] (FP32 complex), two per chunk
+//   chunks 0-17   e(a, b) (FP32 complex) band-major: element b*6+a, two per
+//                 chunk, so band b's six components are chunks 3b .. 3b+2
 //   chunks 18+3b  band b: words 0-1 E (FP64), 2-4 P = qT.v (FP32), 5 1/E,
 //                 6-9 Bose factors of up to 4 temperatures, 10-11 unused
 //   chunk 36      word 0: degenerate blocks of the 6 bands (3 bits each)
@@ -178,9 +179,10 @@ __global__ void pack_records_kernel(MeshArgs M, uint4* __restrict__ rec) {
   uint32_t w[kRecChunks * 4];
 #pragma unroll 1
   for (int el = 0; el < 36; ++el) {
-    const double2 u = M.U[(size_t)q * 36 + el];
-    w[2 * el] = __float_as_uint((float)u.x);
-    w[2 * el + 1] = __float_as_uint((float)u.y);
+    const double2 u = M.U[(size_t)q * 36 + el];   // e(a, b), el = a*6 + b
+    const int t = (el % 6) * 6 + el / 6;
+    w[2 * t] = __float_as_uint((float)u.x);
+    w[2 * t + 1] = __float_as_uint((float)u.y);
   }
   double e[6];
 #pragma unroll 1
@@ -670,8 +672,8 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
   for (int e = tid; e < 36 * kM; e += kThreads) {
     const int el = e / kM, mm = e % kM;
     const int q = P.q1_order[min(tile0 + mm, nq - 1)];
-    const uint2 v = reinterpret_cast<const uint2*>(P.rec + (size_t)q * kRecChunks)[el];
-    S.E1v[e] = make_float2(__uint_as_float(v.x), __uint_as_float(v.y));
+    const uint2 v = reinterpret_cast<const uint2*>(P.rec + (size_t)q * kRecChunks)[(el % 6) * 6 + el / 6];
+    S.E1v[e] = make_float2(__uint_as_float(v.x), __uint_as_float(v.y));   // e1(a, b) at el = a*6 + b
   }
   for (int e = tid; e < 6 * kM; e += kThreads) {
     const int b = e / kM, mm = e % kM;
@@ -880,10 +882,12 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
           while (UR) {
             const int row = __ffs(UR) - 1;
             UR &= UR - 1;
-            // Y(c) = sum_a e1(a, row) X(a, c)
-            float2 Y[6];
+            // Y(c) = sum_a e1(a, row) X(a, c), with packed FP32 pairs:
+            // R(c) = sum_a Re e1 (Re X, Im X), I(c) = sum_a Im e1 (Re X, Im X),
+            // Y = (R.x - I.y, R.y + I.x)
+            float2 Y[6], Yi[6];
 #pragma unroll
-            for (int c = 0; c < 6; ++c) Y[c] = make_float2(0.f, 0.f);
+            for (int c = 0; c < 6; ++c) Y[c] = Yi[c] = make_float2(0.f, 0.f);
             // two rows a of X per TMEM wait
 #pragma unroll
             for (int a = 0; a < 6; a += 2) {
@@ -895,25 +899,46 @@ __global__ void __launch_bounds__(kThreads, 1) pair_tc_kernel(TcArgs P) {
               const float2 e0 = S.E1v[(a * 6 + row) * kM + m];
               const float2 e1 = S.E1v[((a + 1) * 6 + row) * kM + m];
               tc::tmem_wait_ld<24>(t);
+              const float2 e0r = make_float2(e0.x, e0.x), e0i = make_float2(e0.y, e0.y);
+              const float2 e1r = make_float2(e1.x, e1.x), e1i = make_float2(e1.y, e1.y);
 #pragma unroll
               for (int c = 0; c < 6; ++c) {
-                cfmaf(Y[c], e0, make_float2(t[2 * c], t[2 * c + 1]));
-                cfmaf(Y[c], e1, make_float2(t[12 + 2 * c], t[12 + 2 * c + 1]));
+                const float2 x0 = make_float2(t[2 * c], t[2 * c + 1]);
+                const float2 x1 = make_float2(t[12 + 2 * c], t[12 + 2 * c + 1]);
+                Y[c] = __ffma2_rn(e0r, x0, Y[c]);
+                Yi[c] = __ffma2_rn(e0i, x0, Yi[c]);
+                Y[c] = __ffma2_rn(e1r, x1, Y[c]);
+                Yi[c] = __ffma2_rn(e1i, x1, Yi[c]);
               }
+            }
+            // Y(c) as broadcast pairs (Re Y, Re Y) and (Im Y, Im Y) for the e3 contraction
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+              const float yr = Y[c].x - Yi[c].y, yi = Y[c].y + Yi[c].x;
+              Y[c] = make_float2(yr, yr);
+              Yi[c] = make_float2(yi, yi);
             }
             const unsigned cols = (((bmO0 >> row) & 1u) ? nO0 : 0u) | (((bmO1 >> row) & 1u) ? nO1 : 0u);
             unsigned UC = __reduce_or_sync(FULL, cols);
             while (UC) {
               const int b3 = __ffs(UC) - 1;
               UC &= UC - 1;
-              // V = sum_c Y(c) conj(e3(c, b3)), W = |V|^2
-              float2 v = make_float2(0.f, 0.f);
+              // V = sum_c Y(c) conj(e3(c, b3)), W = |V|^2; e3(., b3) is record chunks
+              // 3 b3 .. 3 b3 + 2 (two components each).  Packed pairs:
+              // A = sum Re Y (Re e, Im e), B = sum Im Y (Re e, Im e), V = (A.x + B.y, B.x - A.y)
+              float2 va = make_float2(0.f, 0.f), vb = make_float2(0.f, 0.f);
 #pragma unroll
-              for (int c = 0; c < 6; ++c) {
-                const uint2 e = reinterpret_cast<const uint2*>(srow + ((c * 6 + b3) >> 1) * kM)[(c * 6 + b3) & 1];
-                cfmacf(v, Y[c], make_float2(__uint_as_float(e.x), __uint_as_float(e.y)));
+              for (int j = 0; j < 3; ++j) {
+                const uint4 e = srow[(3 * b3 + j) * kM];
+                const float2 ea = make_float2(__uint_as_float(e.x), __uint_as_float(e.y));
+                const float2 eb = make_float2(__uint_as_float(e.z), __uint_as_float(e.w));
+                va = __ffma2_rn(Y[2 * j], ea, va);
+                vb = __ffma2_rn(Yi[2 * j], ea, vb);
+                va = __ffma2_rn(Y[2 * j + 1], eb, va);
+                vb = __ffma2_rn(Yi[2 * j + 1], eb, vb);
               }
-              const float w = fmaf(v.x, v.x, v.y * v.y);
+              const float vx = va.x + vb.y, vy = vb.x - va.y;
+              const float w = fmaf(vx, vx, vy * vy);
               // Queue the live triplets of the owned b1.  A degenerate b2 or b3
               // averages the rate factors over its block: the entry is queued
               // once per (c2, c3) of the two blocks with weight 1/(n1 n2 n3), so

@@ -604,13 +604,13 @@ def run_relaxons(args):
     scattering of 3e4 Bohr): a2Omega in device memory, the eigensolve of the ns x ns matrix
     (cuSOLVER, in place; all eigenpairs, or the smallest --num-relaxons), then the relaxon
     conductivity.  One pass (the eigensolve destroys the
-    matrix); each stage is a synchronous library call, timed by the host clock around it."""
-    import torch
+    matrix); each stage is a synchronous library call, timed by the host clock around it.  The
+    process does not load PyTorch: beyond the single-GPU eigensolvers' size the library opens
+    cuSOLVER's multi-GPU solver, which needs the toolkit's own cuBLAS."""
     from phoebe_b200 import constants as C
     from phoebe_b200 import lattice, solvers
     from phoebe_b200.core import Context, Interaction3Ph, PhononH0, PhScatteringMatrix
     cr, fc2, fc3, mesh = workload(args.mesh)
-    torch.cuda.set_device(0)
     ctx = Context(0)
     h0 = PhononH0(ctx, cr, fc2)
     bands = h0.populate(mesh, withVelocities=True)

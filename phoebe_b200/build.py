@@ -55,7 +55,7 @@ def build(verbose=False, ptxas_verbose=False):
             if verbose or ptxas_verbose:
                 print(out)
     if _needs(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcuda", "-lcusolver", "-ccbin", "/usr/bin/g++"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcuda", "-lcusolver", "-ldl", "-ccbin", "/usr/bin/g++"]
         run(cmd)
     return LIB
 

@@ -15,6 +15,10 @@
 // case) has its own instantiation, whose 3 accumulators leave room for 8
 // loads in flight per thread; more vectors go 4 per pass.
 #include <cusolverDn.h>
+#include <cusolverMg.h>
+#include <dlfcn.h>
+
+#include <type_traits>
 
 #include <algorithm>
 #include <cstdlib>
@@ -255,6 +259,84 @@ __global__ void __launch_bounds__(256) relaxon_project_kernel(int ns, long long 
   }
 }
 
+// A(c, r) = A(r, c) for r < c: the upper triangle copied onto the lower one
+// (32 x 32 tiles of the upper triangle, one block each)
+__global__ void mirror_upper_kernel(int ns, long long ld, double* __restrict__ A) {
+  const int ti = blockIdx.y, tj = blockIdx.x;
+  if (ti > tj) return;
+  __shared__ double a[32][33];
+  const int r0 = ti * 32, c0 = tj * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int r = r0 + threadIdx.x, c = c0 + k;   // a[k][x] = A(r0 + x, c0 + k)
+    a[k][threadIdx.x] = (r < ns && c < ns) ? A[(size_t)c * ld + r] : 0.0;
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    // A(c0 + x, r0 + k) = A(r0 + k, c0 + x) = a[x][k], strictly below the diagonal
+    const int r = c0 + threadIdx.x, c = r0 + k;
+    if (r < ns && c < r) A[(size_t)c * ld + r] = a[threadIdx.x][k];
+  }
+}
+
+// cuSOLVER's multi-GPU library, opened on first use rather than linked: it
+// needs a cuBLAS at least as new as the toolkit's, and a process that loaded
+// an older cuBLAS first (a PyTorch wheel's) cannot load it.  Then only the
+// eigensolves that need it fail, with the loader's message.
+struct MgApi {
+  decltype(&cusolverMgCreate) create = nullptr;
+  decltype(&cusolverMgDestroy) destroy = nullptr;
+  decltype(&cusolverMgDeviceSelect) device_select = nullptr;
+  decltype(&cusolverMgCreateDeviceGrid) create_grid = nullptr;
+  decltype(&cusolverMgDestroyGrid) destroy_grid = nullptr;
+  decltype(&cusolverMgCreateMatrixDesc) create_desc = nullptr;
+  decltype(&cusolverMgDestroyMatrixDesc) destroy_desc = nullptr;
+  decltype(&cusolverMgSyevd_bufferSize) syevd_buffer = nullptr;
+  decltype(&cusolverMgSyevd) syevd = nullptr;
+  std::string error;
+};
+const MgApi& mg_api() {
+  static const MgApi api = [] {
+    MgApi a;
+    void* lib = dlopen("libcusolverMg.so.11", RTLD_NOW | RTLD_LOCAL);
+    if (!lib) {
+      const char* e = dlerror();
+      a.error = e ? e : "dlopen failed";
+      return a;
+    }
+    auto get = [&](auto& f, const char* name) {
+      f = reinterpret_cast<std::remove_reference_t<decltype(f)>>(dlsym(lib, name));
+      if (!f && a.error.empty()) a.error = std::string("missing ") + name;
+    };
+    get(a.create, "cusolverMgCreate");
+    get(a.destroy, "cusolverMgDestroy");
+    get(a.device_select, "cusolverMgDeviceSelect");
+    get(a.create_grid, "cusolverMgCreateDeviceGrid");
+    get(a.destroy_grid, "cusolverMgDestroyGrid");
+    get(a.create_desc, "cusolverMgCreateMatrixDesc");
+    get(a.destroy_desc, "cusolverMgDestroyMatrixDesc");
+    get(a.syevd_buffer, "cusolverMgSyevd_bufferSize");
+    get(a.syevd, "cusolverMgSyevd");
+    return a;
+  }();
+  return api;
+}
+
+// cuSOLVER multi-GPU objects of one eigensolve, released on every path
+struct MgScratch {
+  const MgApi& api;
+  cusolverMgHandle_t h = nullptr;
+  cudaLibMgGrid_t grid = nullptr;
+  cudaLibMgMatrixDesc_t desc = nullptr;
+  void* dwork = nullptr;
+  explicit MgScratch(const MgApi& a) : api(a) {}
+  ~MgScratch() {
+    cudaFree(dwork);
+    if (desc) api.destroy_desc(desc);
+    if (grid) api.destroy_grid(grid);
+    if (h) api.destroy(h);
+  }
+};
+
 // cuSOLVER objects and buffers of one eigensolve, released on every path
 struct EigScratch {
   cusolverDnHandle_t h = nullptr;
@@ -428,6 +510,62 @@ extern "C" int phx_smatrix_a2omega(phx_smatrix* m) {
   return PHX_OK;
 }
 
+// All eigenpairs through cuSOLVER's multi-GPU solver on a grid of this one
+// device (the reference's distributed pdsyevd, scattering.cpp:816-910): its
+// 64-bit workspace takes matrices that the single-GPU solvers refuse at their
+// workspace query (48 000 states).  It reads the lower triangle, so the upper
+// one (the reference's uplo = 'U') is first mirrored onto it.  Column blocks of
+// a power of two up to 256 that divides ns (else one block): on one device the
+// distributed matrix is then exactly the ns x ns column-major array.
+// Eigenvalues ascending into w, eigenvectors over the matrix.
+int eig_mg(phx_smatrix* m, std::vector<double>& w, int* info) {
+  phx_ctx* ctx = m->ctx;
+  const int ns = m->ns;
+  cudaStream_t st = ctx->stream;
+  if (!mg_api().error.empty()) {
+    phx_set_error(ctx, PHX_ERR_CUDA, "phx_smatrix_diagonalize: cuSOLVER's multi-GPU solver, needed for " +
+                                         std::to_string(ns) + " states, could not be loaded: " + mg_api().error);
+    return PHX_ERR_CUDA;
+  }
+  const int t = (ns + 31) / 32;
+  mirror_upper_kernel<<<dim3(t, t), dim3(32, 8), 0, st>>>(ns, ns, m->d_A);
+  PHX_CUDA(ctx, cudaGetLastError());
+  PHX_CUDA(ctx, cudaStreamSynchronize(st));
+  auto mg = [&](cusolverStatus_t s, const char* what) {
+    if (s == CUSOLVER_STATUS_SUCCESS) return PHX_OK;
+    phx_set_error(ctx, PHX_ERR_CUDA, std::string("phx_smatrix_diagonalize: ") + what + " failed (cusolver status " +
+                                         std::to_string((int)s) + ")");
+    return PHX_ERR_CUDA;
+  };
+  int cb = ns;
+  for (int b = 256; b >= 32; b /= 2)
+    if (ns % b == 0) {
+      cb = b;
+      break;
+    }
+  const MgApi& api = mg_api();
+  MgScratch z(api);
+  int dev = ctx->device;
+  PHX_TRY(mg(api.create(&z.h), "cusolverMgCreate"));
+  PHX_TRY(mg(api.device_select(z.h, 1, &dev), "cusolverMgDeviceSelect"));
+  PHX_TRY(mg(api.create_grid(&z.grid, 1, 1, &dev, CUDALIBMG_GRID_MAPPING_COL_MAJOR), "cusolverMgCreateDeviceGrid"));
+  PHX_TRY(mg(api.create_desc(&z.desc, ns, ns, ns, cb, CUDA_R_64F, z.grid), "cusolverMgCreateMatrixDesc"));
+  void* arrA[1] = {m->d_A};
+  w.assign(ns, 0.0);
+  int64_t lwork = 0;
+  PHX_TRY(mg(api.syevd_buffer(z.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, ns, arrA, 1, 1, z.desc, w.data(),
+                              CUDA_R_64F, CUDA_R_64F, &lwork),
+             "cusolverMgSyevd_bufferSize"));
+  PHX_CUDA(ctx, cudaMalloc(&z.dwork, sizeof(double) * (size_t)std::max<int64_t>(lwork, 1)));
+  void* arrW[1] = {z.dwork};
+  PHX_TRY(mg(api.syevd(z.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, ns, arrA, 1, 1, z.desc, w.data(),
+                       CUDA_R_64F, CUDA_R_64F, arrW, lwork, info),
+             "cusolverMgSyevd"));
+  PHX_CUDA(ctx, cudaSetDevice(ctx->device));
+  PHX_CUDA(ctx, cudaDeviceSynchronize());
+  return PHX_OK;
+}
+
 extern "C" int phx_smatrix_diagonalize(phx_smatrix* m, int num_eigenvalues, double* eigenvalues, int* num_found) {
   PHX_ARG(nullptr, m && eigenvalues && num_found, "phx_smatrix_diagonalize: bad arguments");
   phx_ctx* ctx = m->ctx;
@@ -459,15 +597,37 @@ extern "C" int phx_smatrix_diagonalize(phx_smatrix* m, int num_eigenvalues, doub
   double vl = -1.0, vu = 0.0;
   int64_t meig = ns;
   size_t dws = 0, hws = 0;
-  if (some)
-    PHX_TRY(solver(cusolverDnXsyevdx_bufferSize(z.h, z.prm, jobz, CUSOLVER_EIG_RANGE_I, uplo, ns, CUDA_R_64F, m->d_A,
-                                                ns, &vl, &vu, 1, num_eigenvalues, &meig, CUDA_R_64F, m->d_W,
-                                                CUDA_R_64F, &dws, &hws),
-                   "cusolverDnXsyevdx_bufferSize"));
-  else
-    PHX_TRY(solver(cusolverDnXsyevd_bufferSize(z.h, z.prm, jobz, uplo, ns, CUDA_R_64F, m->d_A, ns, CUDA_R_64F, m->d_W,
-                                               CUDA_R_64F, &dws, &hws),
-                   "cusolverDnXsyevd_bufferSize"));
+  const char* force_mg = std::getenv("PHX_EIG_MG");
+  cusolverStatus_t qs = CUSOLVER_STATUS_INVALID_VALUE;
+  if (!(force_mg && force_mg[0] == '1')) {
+    if (some)
+      qs = cusolverDnXsyevdx_bufferSize(z.h, z.prm, jobz, CUSOLVER_EIG_RANGE_I, uplo, ns, CUDA_R_64F, m->d_A, ns, &vl,
+                                        &vu, 1, num_eigenvalues, &meig, CUDA_R_64F, m->d_W, CUDA_R_64F, &dws, &hws);
+    else
+      qs = cusolverDnXsyevd_bufferSize(z.h, z.prm, jobz, uplo, ns, CUDA_R_64F, m->d_A, ns, CUDA_R_64F, m->d_W,
+                                       CUDA_R_64F, &dws, &hws);
+  }
+  if (qs == CUSOLVER_STATUS_INVALID_VALUE) {
+    // refused at the workspace query (or PHX_EIG_MG=1): all eigenpairs by the
+    // multi-GPU solver on this device, the smallest num_eigenvalues kept
+    std::vector<double> w;
+    int info = 0;
+    const int rc = eig_mg(m, w, &info);
+    m->num_eig = 0;   // the matrix is overwritten from here on, whatever the outcome
+    if (rc != PHX_OK) return rc;
+    if (info != 0) {
+      phx_set_error(ctx, info > 0 ? PHX_ERR_NOCONV : PHX_ERR_ARG,
+                    "phx_smatrix_diagonalize: eigensolver info = " + std::to_string(info));
+      return info > 0 ? PHX_ERR_NOCONV : PHX_ERR_ARG;
+    }
+    const int k = some ? num_eigenvalues : ns;
+    PHX_CUDA(ctx, cudaMemcpy(m->d_W, w.data(), sizeof(double) * ns, cudaMemcpyHostToDevice));
+    std::memcpy(eigenvalues, w.data(), sizeof(double) * k);
+    m->num_eig = k;
+    *num_found = k;
+    return PHX_OK;
+  }
+  PHX_TRY(solver(qs, some ? "cusolverDnXsyevdx_bufferSize" : "cusolverDnXsyevd_bufferSize"));
   PHX_CUDA(ctx, cudaMalloc(&z.dwork, std::max<size_t>(dws, 8)));
   PHX_CUDA(ctx, cudaMalloc(&z.dinfo, sizeof(int)));
   z.hwork = std::malloc(std::max<size_t>(hws, 8));

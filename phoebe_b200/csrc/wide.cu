@@ -51,7 +51,6 @@ namespace {
 using wide::kMaxNb;
 constexpr int kWideQ1 = wide::kQ1;
 constexpr int kWideThreads = 256;     // FP64 kernel; split-path epilogue warps x 32
-constexpr int kRateSegs = 4;          // b3 segments per (q1, b1) in the rate loop
 using WideArgs = wide::Args;
 
 // forward-scan degenerate blocks (scattering.cpp:1223,1257,1291): gs[b] = first band of b's block
@@ -87,17 +86,23 @@ struct Tile {
   int* g1s;     // [nq1][nb] blocks of q1
   int* g3s;     // [nq1][nb] blocks of q3
   int* g2s;     // [nb] blocks of q2
+  int* dg;      // [nq1] q1 or q3 has a degenerate block (else symmetrizeCoupling changes nothing)
   double* acc;  // [nq1][nb][kMaxT]
 };
 
 // symmetrizeCoupling (scattering.cpp:1209-1318) of the W planes q0 .. q0+nq1-1
 // of one b2 (W over T): average over the blocks of b3 (rows), then of b1
-// (columns); b2 enters the rates.  Starts and ends with a barrier.
+// (columns); b2 enters the rates.  Starts and ends with a barrier; when no
+// plane's q1 or q3 has a degenerate block the averages change nothing and
+// only the ending barrier is taken.
 template <class R>
 __device__ void wide_symmetrize(const Tile& t, int q0, int nq1, int nb, void* Tv, int tid, int nthreads, int bar_id) {
   const int nbb = nb * nb;
   R* W = reinterpret_cast<R*>(Tv);
+  int any_dg = 0;
+  for (int q = q0; q < q0 + nq1; ++q) any_dg |= t.dg[q];
   asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
+  if (!any_dg) return;
   for (int u = tid; u < nq1 * nb; u += nthreads) {
     const int q = q0 + u / nb, b1 = u % nb;
     if (t.q1s[q] < 0 || !t.inw[q]) continue;
@@ -298,88 +303,106 @@ __device__ void wide_contract(const Tile& t, int q0, int nq1, int nb, const C* _
 
 // Rates of the b2 plane (ph_scattering.cpp:338-380, 466-518), FP64, with the
 // rate factors averaged over the degenerate block of b2: "+" of (q1, q2) and
-// "-" of (q1, -q2).  Units (segment of b3, q1, b1); one shared-memory atomic
-// per unit and temperature.  W scaled by wscale (split FP16 operands).
+// "-" of (q1, -q2).  The (q1, b1, b3) cells of the item are split into equal
+// contiguous ranges, one per thread, so that no thread has more than its
+// share; a thread adds its sums of a (q1, b1) row with one shared-memory
+// atomic per temperature when it leaves the row.  W scaled by wscale (split
+// FP16 operands).
 template <class R>
 __device__ void wide_rates(const Tile& t, const MeshArgs& M, int nq1, int b2, int iq2, int iq2m, const R* W,
                            double wscale, int tid, int nthreads) {
   const int nb = M.nb, nbb = nb * nb, nT = M.nT, nq = M.nq;
-  const int seg = (nb + kRateSegs - 1) / kRateSegs;
   const int* g2 = t.g2s;
   const int s0 = g2[b2], s1 = wide_block_end(g2, nb, s0);
   const double inv2 = 1.0 / (double)(s1 - s0);
-  for (int u = tid; u < kRateSegs * nq1 * nb; u += nthreads) {
-    const int sg = u / (nq1 * nb), rest = u % (nq1 * nb), q = rest / nb, b1 = rest % nb;
-    const int q1 = t.q1s[q];
-    if (q1 < 0 || !t.inw[q]) continue;
-    const double en1 = M.E[(size_t)q1 * nb + b1];
-    if (en1 < phxc::phExcludeCutoff || en1 < phxc::phEnergyCutoff) continue;
-    const int iq3 = t.q3s[q];
-    double r[kMaxT];
+  const int cells = nq1 * nbb, per = (cells + nthreads - 1) / nthreads;
+  const int cb = min(cells, tid * per), ce = min(cells, cb + per);
+  int row = -1, q = 0, b1 = 0, q1 = -1, iq3 = 0;
+  double en1 = 0.0;
+  bool live_row = false;
+  double r[kMaxT];
 #pragma unroll
-    for (int c = 0; c < kMaxT; ++c) r[c] = 0.0;
-    const int b3b = sg * seg, b3e = min(nb, b3b + seg);
-    for (int b3 = b3b; b3 < b3e; ++b3) {
-      const double w = (double)W[(size_t)q * nbb + (size_t)b1 * nb + b3] * wscale;
-      if (w == 0.0) continue;
-      const double en3 = M.E[(size_t)iq3 * nb + b3];
-      if (en3 < phxc::phEnergyCutoff) continue;
-      for (int c2 = s0; c2 < s1; ++c2) {
-        const double en2 = M.E[(size_t)iq2 * nb + c2];
-        const double en2m = M.E[(size_t)iq2m * nb + c2];
-        const bool ok2 = (t.inw[q] & 1) && en2 >= phxc::phExcludeCutoff && en2 >= phxc::phEnergyCutoff;
-        const bool ok2m = (t.inw[q] & 2) && en2m >= phxc::phExcludeCutoff && en2m >= phxc::phEnergyCutoff;
-        if (!ok2 && !ok2m) continue;
-        double sp = M.sigma, sm = M.sigma;
-        bool vzp = false, vzm = false;
-        if (M.smearing == PHX_SMEAR_ADAPTIVE) {
-          const double* v3 = M.vg + ((size_t)iq3 * nb + b3) * 3;
-          const double* v2 = M.vg + ((size_t)iq2 * nb + c2) * 3;
-          const double* v2m = M.vg + ((size_t)iq2m * nb + c2) * 3;
-          const double dp0 = v2[0] - v3[0], dp1 = v2[1] - v3[1], dp2 = v2[2] - v3[2];
-          const double dm0 = v2m[0] - v3[0], dm1 = v2m[1] - v3[1], dm2 = v2m[2] - v3[2];
-          vzp = (dp0 * dp0 + dp1 * dp1 + dp2 * dp2) == 0.0;
-          vzm = (dm0 * dm0 + dm1 * dm1 + dm2 * dm2) == 0.0;
-          sp = floor_sigma(adaptive_sigma(M.qT, dp0, dp1, dp2));
-          sm = floor_sigma(adaptive_sigma(M.qT, dm0, dm1, dm2));
+  for (int c = 0; c < kMaxT; ++c) r[c] = 0.0;
+  auto flush = [&]() {
+#pragma unroll
+    for (int c = 0; c < kMaxT; ++c) {
+      if (c < nT && r[c] != 0.0) atomicAdd(&t.acc[(q * nb + b1) * kMaxT + c], r[c]);
+      r[c] = 0.0;
+    }
+  };
+  for (int cell = cb; cell < ce; ++cell) {
+    if (cell / nb != row) {
+      if (row >= 0) flush();
+      row = cell / nb;
+      q = row / nb;
+      b1 = row % nb;
+      q1 = t.q1s[q];
+      live_row = q1 >= 0 && t.inw[q];
+      if (live_row) {
+        en1 = M.E[(size_t)q1 * nb + b1];
+        live_row = !(en1 < phxc::phExcludeCutoff || en1 < phxc::phEnergyCutoff);
+        iq3 = t.q3s[q];
+      }
+    }
+    if (!live_row) continue;
+    const int b3 = cell % nb;
+    const double w = (double)W[(size_t)q * nbb + (size_t)b1 * nb + b3] * wscale;
+    if (w == 0.0) continue;
+    const double en3 = M.E[(size_t)iq3 * nb + b3];
+    if (en3 < phxc::phEnergyCutoff) continue;
+    for (int c2 = s0; c2 < s1; ++c2) {
+      const double en2 = M.E[(size_t)iq2 * nb + c2];
+      const double en2m = M.E[(size_t)iq2m * nb + c2];
+      const bool ok2 = (t.inw[q] & 1) && en2 >= phxc::phExcludeCutoff && en2 >= phxc::phEnergyCutoff;
+      const bool ok2m = (t.inw[q] & 2) && en2m >= phxc::phExcludeCutoff && en2m >= phxc::phEnergyCutoff;
+      if (!ok2 && !ok2m) continue;
+      double sp = M.sigma, sm = M.sigma;
+      bool vzp = false, vzm = false;
+      if (M.smearing == PHX_SMEAR_ADAPTIVE) {
+        const double* v3 = M.vg + ((size_t)iq3 * nb + b3) * 3;
+        const double* v2 = M.vg + ((size_t)iq2 * nb + c2) * 3;
+        const double* v2m = M.vg + ((size_t)iq2m * nb + c2) * 3;
+        const double dp0 = v2[0] - v3[0], dp1 = v2[1] - v3[1], dp2 = v2[2] - v3[2];
+        const double dm0 = v2m[0] - v3[0], dm1 = v2m[1] - v3[1], dm2 = v2m[2] - v3[2];
+        vzp = (dp0 * dp0 + dp1 * dp1 + dp2 * dp2) == 0.0;
+        vzm = (dm0 * dm0 + dm1 * dm1 + dm2 * dm2) == 0.0;
+        sp = floor_sigma(adaptive_sigma(M.qT, dp0, dp1, dp2));
+        sm = floor_sigma(adaptive_sigma(M.qT, dm0, dm1, dm2));
+      }
+      if (ok2) {
+        const double dlt = delta_fn(M.smearing, sp, en1 + en2 - en3, vzp);
+        if (dlt > 0.0) {
+          const double f = phxc::pi * 0.25 * w * dlt * M.norm / (en1 * en2 * en3) * inv2;
+#pragma unroll
+          for (int c = 0; c < kMaxT; ++c)
+            if (c < nT) {
+              const double n1 = M.bose[((size_t)c * nq + q1) * nb + b1];
+              const double n2 = M.bose[((size_t)c * nq + iq2) * nb + c2];
+              const double n3 = M.bose[((size_t)c * nq + iq3) * nb + b3];
+              r[c] += 0.5 * (f * n1 * n2 * (n3 + 1.0));
+            }
         }
-        if (ok2) {
-          const double dlt = delta_fn(M.smearing, sp, en1 + en2 - en3, vzp);
-          if (dlt > 0.0) {
-            const double f = phxc::pi * 0.25 * w * dlt * M.norm / (en1 * en2 * en3) * inv2;
+      }
+      if (ok2m) {
+        double d1 = delta_fn(M.smearing, sm, en1 + en3 - en2m, vzm);
+        double d2 = delta_fn(M.smearing, sm, en2m + en3 - en1, vzm);
+        if (d1 > 0.0 || d2 > 0.0) {
+          d1 = fmax(d1, 0.0);
+          d2 = fmax(d2, 0.0);
+          const double f = phxc::pi * 0.25 * w * M.norm / (en1 * en2m * en3) * inv2;
 #pragma unroll
-            for (int c = 0; c < kMaxT; ++c)
-              if (c < nT) {
-                const double n1 = M.bose[((size_t)c * nq + q1) * nb + b1];
-                const double n2 = M.bose[((size_t)c * nq + iq2) * nb + c2];
-                const double n3 = M.bose[((size_t)c * nq + iq3) * nb + b3];
-                r[c] += 0.5 * (f * n1 * n2 * (n3 + 1.0));
-              }
-          }
-        }
-        if (ok2m) {
-          double d1 = delta_fn(M.smearing, sm, en1 + en3 - en2m, vzm);
-          double d2 = delta_fn(M.smearing, sm, en2m + en3 - en1, vzm);
-          if (d1 > 0.0 || d2 > 0.0) {
-            d1 = fmax(d1, 0.0);
-            d2 = fmax(d2, 0.0);
-            const double f = phxc::pi * 0.25 * w * M.norm / (en1 * en2m * en3) * inv2;
-#pragma unroll
-            for (int c = 0; c < kMaxT; ++c)
-              if (c < nT) {
-                const double n1 = M.bose[((size_t)c * nq + q1) * nb + b1];
-                const double n2m = M.bose[((size_t)c * nq + iq2m) * nb + c2];
-                const double n3 = M.bose[((size_t)c * nq + iq3) * nb + b3];
-                r[c] += 0.5 * (f * n3 * n1 * (n2m + 1.0) * d1 + f * n2m * n3 * (n1 + 1.0) * d2);
-              }
-          }
+          for (int c = 0; c < kMaxT; ++c)
+            if (c < nT) {
+              const double n1 = M.bose[((size_t)c * nq + q1) * nb + b1];
+              const double n2m = M.bose[((size_t)c * nq + iq2m) * nb + c2];
+              const double n3 = M.bose[((size_t)c * nq + iq3) * nb + b3];
+              r[c] += 0.5 * (f * n3 * n1 * (n2m + 1.0) * d1 + f * n2m * n3 * (n1 + 1.0) * d2);
+            }
         }
       }
     }
-#pragma unroll
-    for (int c = 0; c < kMaxT; ++c)
-      if (c < nT && r[c] != 0.0) atomicAdd(&t.acc[(q * nb + b1) * kMaxT + c], r[c]);
   }
+  if (row >= 0) flush();
 }
 
 // Loads the tile of the current item: q1, q3, window flags, blocks; returns
@@ -399,19 +422,26 @@ __device__ bool wide_load_tile(const Tile& t, const WideArgs& P, int tile, int i
     t.q1s[tid] = q1;
     t.inw[tid] = f;
     t.q3s[tid] = mesh_add(max(q1, 0), iq2, M.n0, M.n1, M.n2);
+    t.dg[tid] = 0;
   }
+  // zeroed before the early return too: the split kernel flushes every item
+  for (int i = tid; i < nq1 * nb * kMaxT; i += nthreads) t.acc[i] = 0.0;
   asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
   int any = 0;
   for (int q = 0; q < nq1; ++q) any |= t.inw[q];
   if (!any) return false;
   if (tid < nq1) {
     const int q1 = max(t.q1s[tid], 0);
-    wide_blocks(M.E + (size_t)q1 * nb, nb, t.g1s + tid * nb);
-    wide_blocks(M.E + (size_t)t.q3s[tid] * nb, nb, t.g3s + tid * nb);
+    int* g1 = t.g1s + tid * nb;
+    int* g3 = t.g3s + tid * nb;
+    wide_blocks(M.E + (size_t)q1 * nb, nb, g1);
+    wide_blocks(M.E + (size_t)t.q3s[tid] * nb, nb, g3);
+    int d = 0;
+    for (int b = 0; b < nb; ++b) d |= (g1[b] != b) | (g3[b] != b);
+    t.dg[tid] = d;
   } else if (tid == nq1) {
     wide_blocks(M.E + (size_t)iq2 * nb, nb, t.g2s);
   }
-  for (int i = tid; i < nq1 * nb * kMaxT; i += nthreads) t.acc[i] = 0.0;
   asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
   return true;
 }
@@ -427,7 +457,7 @@ __device__ void wide_flush(const Tile& t, const WideArgs& P, int tid, int nthrea
 }
 
 __host__ __device__ inline size_t wide_tile_bytes(int nq1, int nb) {
-  return sizeof(double) * (size_t)nq1 * nb * kMaxT + sizeof(int) * ((size_t)3 * nq1 + 2 * (size_t)nq1 * nb + nb);
+  return sizeof(double) * (size_t)nq1 * nb * kMaxT + sizeof(int) * ((size_t)4 * nq1 + 2 * (size_t)nq1 * nb + nb);
 }
 __device__ inline Tile carve_tile(char* p, int nq1, int nb) {
   Tile t;
@@ -438,6 +468,7 @@ __device__ inline Tile carve_tile(char* p, int nq1, int nb) {
   t.g1s = t.inw + nq1;
   t.g3s = t.g1s + nq1 * nb;
   t.g2s = t.g3s + nq1 * nb;
+  t.dg = t.g2s + nb;
   return t;
 }
 

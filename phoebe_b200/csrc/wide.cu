@@ -72,6 +72,39 @@ __device__ __forceinline__ void cfma_t(double2& acc, double2 a, double2 b) { cfm
 __device__ __forceinline__ void cfma_t(float2& acc, float2 a, float2 b) { cfmaf(acc, a, b); }
 __device__ __forceinline__ void cfmac_t(double2& acc, double2 a, double2 b) { cfmac(acc, a, b); }
 __device__ __forceinline__ void cfmac_t(float2& acc, float2 a, float2 b) { cfmacf(acc, a, b); }
+
+// 4 x 4 FP32 register tiles on packed FMAs: acc[i][k] += a[i] b[k]
+// (cmac_tile4) and acc[i][k] += a[i] conj(b[k]) (cmacc_tile4), each complex
+// product as (Re p, Re p) q + (Im p, Im p) q' with q' = i q or -i q, so that
+// the products keep the order of cfmaf / cfmacf (same results).
+__device__ __forceinline__ void cmac_tile4(float2 (&acc)[4][4], const float2 (&a)[4], const float2 (&b)[4]) {
+  float2 bn[4];   // i b
+#pragma unroll
+  for (int k = 0; k < 4; ++k) bn[k] = make_float2(-b[k].y, b[k].x);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float2 r = make_float2(a[i].x, a[i].x), m = make_float2(a[i].y, a[i].y);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      acc[i][k] = __ffma2_rn(r, b[k], acc[i][k]);
+      acc[i][k] = __ffma2_rn(m, bn[k], acc[i][k]);
+    }
+  }
+}
+__device__ __forceinline__ void cmacc_tile4(float2 (&acc)[4][4], const float2 (&a)[4], const float2 (&b)[4]) {
+  float2 as[4];   // -i a
+#pragma unroll
+  for (int i = 0; i < 4; ++i) as[i] = make_float2(a[i].y, -a[i].x);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float2 r = make_float2(b[k].x, b[k].x), m = make_float2(b[k].y, b[k].y);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      acc[i][k] = __ffma2_rn(r, a[i], acc[i][k]);
+      acc[i][k] = __ffma2_rn(m, as[i], acc[i][k]);
+    }
+  }
+}
 template <class C> __device__ __forceinline__ C czero();
 template <> __device__ __forceinline__ double2 czero<double2>() { return make_double2(0.0, 0.0); }
 template <> __device__ __forceinline__ float2 czero<float2>() { return make_float2(0.f, 0.f); }
@@ -164,10 +197,7 @@ __device__ void wide_contract_f4(const Tile& t, int q0, int nq1, int nb, const f
                             make_float2(e23.z, e23.w)};
       const float2 tv[4] = {make_float2(t01.x, t01.y), make_float2(t01.z, t01.w), make_float2(t23.x, t23.y),
                             make_float2(t23.z, t23.w)};
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int k = 0; k < 4; ++k) cfmaf(acc[i][k], ev[i], tv[k]);
+      cmac_tile4(acc, ev, tv);
     }
     float2* Xq = X + (size_t)(q - q0) * nb * ldx + c0;
 #pragma unroll
@@ -195,10 +225,7 @@ __device__ void wide_contract_f4(const Tile& t, int q0, int nq1, int nb, const f
       const float4 e01 = ldg4(e3 + c * nb), e23 = ldg4(e3 + c * nb + 2);
       const float2 ev[4] = {make_float2(e01.x, e01.y), make_float2(e01.z, e01.w), make_float2(e23.x, e23.y),
                             make_float2(e23.z, e23.w)};
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int k = 0; k < 4; ++k) cfmacf(acc[i][k], xv[i], ev[k]);
+      cmacc_tile4(acc, xv, ev);
     }
     float* Wq = W + (size_t)q * nbb + b30;
 #pragma unroll
@@ -301,110 +328,113 @@ __device__ void wide_contract(const Tile& t, int q0, int nq1, int nb, const C* _
   wide_symmetrize<R>(t, q0, nq1, nb, T, tid, nthreads, bar_id);
 }
 
+// Segments of b3 per (q1, b1) row in the rate loop: the count that minimises
+// the work of the busiest thread, (rounds of units over the threads) x
+// (cells per segment + one cell's worth for the unit's set-up and atomics),
+// the smallest such count on ties.  Each thread runs whole segments, so the
+// lanes of a warp stay in step.  nb = 36, 8 planes, 512 threads: 3 segments
+// of 12 cells (4 segments: 3 rounds of 9); nb = 15: 4 segments, one round.
+__device__ inline int wide_rate_segments(int nq1, int nb, int nthreads) {
+  const int rows = nq1 * nb;
+  int best = 1, best_cost = 1 << 30;
+  for (int sg = 1; sg <= nb; ++sg) {
+    const int cost = ((sg * rows + nthreads - 1) / nthreads) * ((nb + sg - 1) / sg + 1);
+    if (cost < best_cost) {
+      best_cost = cost;
+      best = sg;
+    }
+  }
+  return best;
+}
+
 // Rates of the b2 plane (ph_scattering.cpp:338-380, 466-518), FP64, with the
 // rate factors averaged over the degenerate block of b2: "+" of (q1, q2) and
-// "-" of (q1, -q2).  The (q1, b1, b3) cells of the item are split into equal
-// contiguous ranges, one per thread, so that no thread has more than its
-// share; a thread adds its sums of a (q1, b1) row with one shared-memory
-// atomic per temperature when it leaves the row.  W scaled by wscale (split
-// FP16 operands).
+// "-" of (q1, -q2).  Units (segment of b3, q1, b1), segs segments per row
+// (wide_rate_segments); one shared-memory atomic per unit and temperature.
+// W scaled by wscale (split FP16 operands).
 template <class R>
 __device__ void wide_rates(const Tile& t, const MeshArgs& M, int nq1, int b2, int iq2, int iq2m, const R* W,
-                           double wscale, int tid, int nthreads) {
+                           double wscale, int segs, int tid, int nthreads) {
   const int nb = M.nb, nbb = nb * nb, nT = M.nT, nq = M.nq;
+  const int seg = (nb + segs - 1) / segs;
   const int* g2 = t.g2s;
   const int s0 = g2[b2], s1 = wide_block_end(g2, nb, s0);
   const double inv2 = 1.0 / (double)(s1 - s0);
-  const int cells = nq1 * nbb, per = (cells + nthreads - 1) / nthreads;
-  const int cb = min(cells, tid * per), ce = min(cells, cb + per);
-  int row = -1, q = 0, b1 = 0, q1 = -1, iq3 = 0;
-  double en1 = 0.0;
-  bool live_row = false;
-  double r[kMaxT];
+  for (int u = tid; u < segs * nq1 * nb; u += nthreads) {
+    const int sg = u / (nq1 * nb), rest = u % (nq1 * nb), q = rest / nb, b1 = rest % nb;
+    const int q1 = t.q1s[q];
+    if (q1 < 0 || !t.inw[q]) continue;
+    const double en1 = M.E[(size_t)q1 * nb + b1];
+    if (en1 < phxc::phExcludeCutoff || en1 < phxc::phEnergyCutoff) continue;
+    const int iq3 = t.q3s[q];
+    double r[kMaxT];
 #pragma unroll
-  for (int c = 0; c < kMaxT; ++c) r[c] = 0.0;
-  auto flush = [&]() {
+    for (int c = 0; c < kMaxT; ++c) r[c] = 0.0;
+    const int b3b = sg * seg, b3e = min(nb, b3b + seg);
+    for (int b3 = b3b; b3 < b3e; ++b3) {
+      const double w = (double)W[(size_t)q * nbb + (size_t)b1 * nb + b3] * wscale;
+      if (w == 0.0) continue;
+      const double en3 = M.E[(size_t)iq3 * nb + b3];
+      if (en3 < phxc::phEnergyCutoff) continue;
+      for (int c2 = s0; c2 < s1; ++c2) {
+        const double en2 = M.E[(size_t)iq2 * nb + c2];
+        const double en2m = M.E[(size_t)iq2m * nb + c2];
+        const bool ok2 = (t.inw[q] & 1) && en2 >= phxc::phExcludeCutoff && en2 >= phxc::phEnergyCutoff;
+        const bool ok2m = (t.inw[q] & 2) && en2m >= phxc::phExcludeCutoff && en2m >= phxc::phEnergyCutoff;
+        if (!ok2 && !ok2m) continue;
+        double sp = M.sigma, sm = M.sigma;
+        bool vzp = false, vzm = false;
+        if (M.smearing == PHX_SMEAR_ADAPTIVE) {
+          const double* v3 = M.vg + ((size_t)iq3 * nb + b3) * 3;
+          const double* v2 = M.vg + ((size_t)iq2 * nb + c2) * 3;
+          const double* v2m = M.vg + ((size_t)iq2m * nb + c2) * 3;
+          const double dp0 = v2[0] - v3[0], dp1 = v2[1] - v3[1], dp2 = v2[2] - v3[2];
+          const double dm0 = v2m[0] - v3[0], dm1 = v2m[1] - v3[1], dm2 = v2m[2] - v3[2];
+          vzp = (dp0 * dp0 + dp1 * dp1 + dp2 * dp2) == 0.0;
+          vzm = (dm0 * dm0 + dm1 * dm1 + dm2 * dm2) == 0.0;
+          sp = floor_sigma(adaptive_sigma(M.qT, dp0, dp1, dp2));
+          sm = floor_sigma(adaptive_sigma(M.qT, dm0, dm1, dm2));
+        }
+        if (ok2) {
+          const double dlt = delta_fn(M.smearing, sp, en1 + en2 - en3, vzp);
+          if (dlt > 0.0) {
+            const double f = phxc::pi * 0.25 * w * dlt * M.norm / (en1 * en2 * en3) * inv2;
 #pragma unroll
-    for (int c = 0; c < kMaxT; ++c) {
+            for (int c = 0; c < kMaxT; ++c)
+              if (c < nT) {
+                const double n1 = M.bose[((size_t)c * nq + q1) * nb + b1];
+                const double n2 = M.bose[((size_t)c * nq + iq2) * nb + c2];
+                const double n3 = M.bose[((size_t)c * nq + iq3) * nb + b3];
+                r[c] += 0.5 * (f * n1 * n2 * (n3 + 1.0));
+              }
+          }
+        }
+        if (ok2m) {
+          double d1 = delta_fn(M.smearing, sm, en1 + en3 - en2m, vzm);
+          double d2 = delta_fn(M.smearing, sm, en2m + en3 - en1, vzm);
+          if (d1 > 0.0 || d2 > 0.0) {
+            d1 = fmax(d1, 0.0);
+            d2 = fmax(d2, 0.0);
+            const double f = phxc::pi * 0.25 * w * M.norm / (en1 * en2m * en3) * inv2;
+#pragma unroll
+            for (int c = 0; c < kMaxT; ++c)
+              if (c < nT) {
+                const double n1 = M.bose[((size_t)c * nq + q1) * nb + b1];
+                const double n2m = M.bose[((size_t)c * nq + iq2m) * nb + c2];
+                const double n3 = M.bose[((size_t)c * nq + iq3) * nb + b3];
+                r[c] += 0.5 * (f * n3 * n1 * (n2m + 1.0) * d1 + f * n2m * n3 * (n1 + 1.0) * d2);
+              }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < kMaxT; ++c)
       if (c < nT && r[c] != 0.0) atomicAdd(&t.acc[(q * nb + b1) * kMaxT + c], r[c]);
-      r[c] = 0.0;
-    }
-  };
-  for (int cell = cb; cell < ce; ++cell) {
-    if (cell / nb != row) {
-      if (row >= 0) flush();
-      row = cell / nb;
-      q = row / nb;
-      b1 = row % nb;
-      q1 = t.q1s[q];
-      live_row = q1 >= 0 && t.inw[q];
-      if (live_row) {
-        en1 = M.E[(size_t)q1 * nb + b1];
-        live_row = !(en1 < phxc::phExcludeCutoff || en1 < phxc::phEnergyCutoff);
-        iq3 = t.q3s[q];
-      }
-    }
-    if (!live_row) continue;
-    const int b3 = cell % nb;
-    const double w = (double)W[(size_t)q * nbb + (size_t)b1 * nb + b3] * wscale;
-    if (w == 0.0) continue;
-    const double en3 = M.E[(size_t)iq3 * nb + b3];
-    if (en3 < phxc::phEnergyCutoff) continue;
-    for (int c2 = s0; c2 < s1; ++c2) {
-      const double en2 = M.E[(size_t)iq2 * nb + c2];
-      const double en2m = M.E[(size_t)iq2m * nb + c2];
-      const bool ok2 = (t.inw[q] & 1) && en2 >= phxc::phExcludeCutoff && en2 >= phxc::phEnergyCutoff;
-      const bool ok2m = (t.inw[q] & 2) && en2m >= phxc::phExcludeCutoff && en2m >= phxc::phEnergyCutoff;
-      if (!ok2 && !ok2m) continue;
-      double sp = M.sigma, sm = M.sigma;
-      bool vzp = false, vzm = false;
-      if (M.smearing == PHX_SMEAR_ADAPTIVE) {
-        const double* v3 = M.vg + ((size_t)iq3 * nb + b3) * 3;
-        const double* v2 = M.vg + ((size_t)iq2 * nb + c2) * 3;
-        const double* v2m = M.vg + ((size_t)iq2m * nb + c2) * 3;
-        const double dp0 = v2[0] - v3[0], dp1 = v2[1] - v3[1], dp2 = v2[2] - v3[2];
-        const double dm0 = v2m[0] - v3[0], dm1 = v2m[1] - v3[1], dm2 = v2m[2] - v3[2];
-        vzp = (dp0 * dp0 + dp1 * dp1 + dp2 * dp2) == 0.0;
-        vzm = (dm0 * dm0 + dm1 * dm1 + dm2 * dm2) == 0.0;
-        sp = floor_sigma(adaptive_sigma(M.qT, dp0, dp1, dp2));
-        sm = floor_sigma(adaptive_sigma(M.qT, dm0, dm1, dm2));
-      }
-      if (ok2) {
-        const double dlt = delta_fn(M.smearing, sp, en1 + en2 - en3, vzp);
-        if (dlt > 0.0) {
-          const double f = phxc::pi * 0.25 * w * dlt * M.norm / (en1 * en2 * en3) * inv2;
-#pragma unroll
-          for (int c = 0; c < kMaxT; ++c)
-            if (c < nT) {
-              const double n1 = M.bose[((size_t)c * nq + q1) * nb + b1];
-              const double n2 = M.bose[((size_t)c * nq + iq2) * nb + c2];
-              const double n3 = M.bose[((size_t)c * nq + iq3) * nb + b3];
-              r[c] += 0.5 * (f * n1 * n2 * (n3 + 1.0));
-            }
-        }
-      }
-      if (ok2m) {
-        double d1 = delta_fn(M.smearing, sm, en1 + en3 - en2m, vzm);
-        double d2 = delta_fn(M.smearing, sm, en2m + en3 - en1, vzm);
-        if (d1 > 0.0 || d2 > 0.0) {
-          d1 = fmax(d1, 0.0);
-          d2 = fmax(d2, 0.0);
-          const double f = phxc::pi * 0.25 * w * M.norm / (en1 * en2m * en3) * inv2;
-#pragma unroll
-          for (int c = 0; c < kMaxT; ++c)
-            if (c < nT) {
-              const double n1 = M.bose[((size_t)c * nq + q1) * nb + b1];
-              const double n2m = M.bose[((size_t)c * nq + iq2m) * nb + c2];
-              const double n3 = M.bose[((size_t)c * nq + iq3) * nb + b3];
-              r[c] += 0.5 * (f * n3 * n1 * (n2m + 1.0) * d1 + f * n2m * n3 * (n1 + 1.0) * d2);
-            }
-        }
-      }
-    }
   }
-  if (row >= 0) flush();
 }
 
+// Loads the tile of the current item: q1, q3, window flags, blocks; returns
 // Loads the tile of the current item: q1, q3, window flags, blocks; returns
 // (block-uniform, after a barrier) whether any q1 of the tile pairs with q2 or -q2.
 __device__ bool wide_load_tile(const Tile& t, const WideArgs& P, int tile, int iq2, int iq2m, int tid,
@@ -497,6 +527,7 @@ __global__ void __launch_bounds__(kWideThreads) wide_fp64_kernel(WideArgs P) {
   int* item_s = reinterpret_cast<int*>(reinterpret_cast<char*>(Xend) + wide_tile_bytes(NQ1, nb));
   const int tid = threadIdx.x;
   const unsigned total = (unsigned)P.q2_count * P.ntiles;
+  const int segs = wide_rate_segments(NQ1, nb, kWideThreads);
   for (;;) {
     if (tid == 0) *item_s = (int)atomicAdd(P.counter, 1u);
     __syncthreads();
@@ -534,7 +565,8 @@ __global__ void __launch_bounds__(kWideThreads) wide_fp64_kernel(WideArgs P) {
       __syncthreads();
       wide_contract<double, double2, RT>(t, 0, NQ1, nb, M.U, nullptr, nullptr, T, X, wide_ldx(nb), tid, kWideThreads,
                                          1);
-      wide_rates<double>(t, M, NQ1, b2, iq2, iq2m, reinterpret_cast<const double*>(T), 1.0, tid, kWideThreads);
+      wide_rates<double>(t, M, NQ1, b2, iq2, iq2m, reinterpret_cast<const double*>(T), 1.0, segs, tid,
+                         kWideThreads);
       __syncthreads();
     }
     wide_flush(t, P, tid, kWideThreads);
@@ -923,6 +955,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) wide_split_kernel(WideArgs P
     const int qp = P.qp;
     const double sc = P.fp16 ? (double)wide_fp16_scale(P.dmax) : 1.0;
     const double wscale = 1.0 / (sc * sc);
+    const int segs = wide_rate_segments(kWideQ1, nb, nth);
     int s = 0;
     for (int n = 0;; ++n) {
       const int slot = n % kItemSlots;
@@ -985,7 +1018,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) wide_split_kernel(WideArgs P
         if (tid == 0) tc::mbar_arrive(&tfree[buf]);
         for (int q0 = 0; q0 < kWideQ1; q0 += qp)
           wide_contract<float, float2, RT>(t, q0, qp, nb, P.U32, nullptr, nullptr, S.T, S.X, wide_ldx(nb), tid, nth, 1);
-        wide_rates<float>(t, M, kWideQ1, b2, iq2, iq2m, reinterpret_cast<const float*>(S.T), wscale, tid, nth);
+        wide_rates<float>(t, M, kWideQ1, b2, iq2, iq2m, reinterpret_cast<const float*>(S.T), wscale, segs, tid, nth);
         asm volatile("bar.sync 1, %0;" ::"r"(nth) : "memory");
       }
       if (!ok) break;

@@ -73,33 +73,35 @@ __device__ __forceinline__ void cfma_t(float2& acc, float2 a, float2 b) { cfmaf(
 __device__ __forceinline__ void cfmac_t(double2& acc, double2 a, double2 b) { cfmac(acc, a, b); }
 __device__ __forceinline__ void cfmac_t(float2& acc, float2 a, float2 b) { cfmacf(acc, a, b); }
 
-// 4 x 4 FP32 register tiles on packed FMAs: acc[i][k] += a[i] b[k]
-// (cmac_tile4) and acc[i][k] += a[i] conj(b[k]) (cmacc_tile4), each complex
-// product as (Re p, Re p) q + (Im p, Im p) q' with q' = i q or -i q, so that
-// the products keep the order of cfmaf / cfmacf (same results).
-__device__ __forceinline__ void cmac_tile4(float2 (&acc)[4][4], const float2 (&a)[4], const float2 (&b)[4]) {
-  float2 bn[4];   // i b
+// FP32 register tiles on packed FMAs: acc[i][k] += a[i] b[k] (cmac_tile) and
+// acc[i][k] += a[i] conj(b[k]) (cmacc_tile), each complex product as
+// (Re p, Re p) q + (Im p, Im p) q' with q' = i q or -i q, so that the products
+// keep the order of cfmaf / cfmacf (same results).
+template <int TI>
+__device__ __forceinline__ void cmac_tile(float2 (&acc)[TI][TI], const float2 (&a)[TI], const float2 (&b)[TI]) {
+  float2 bn[TI];   // i b
 #pragma unroll
-  for (int k = 0; k < 4; ++k) bn[k] = make_float2(-b[k].y, b[k].x);
+  for (int k = 0; k < TI; ++k) bn[k] = make_float2(-b[k].y, b[k].x);
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < TI; ++i) {
     const float2 r = make_float2(a[i].x, a[i].x), m = make_float2(a[i].y, a[i].y);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < TI; ++k) {
       acc[i][k] = __ffma2_rn(r, b[k], acc[i][k]);
       acc[i][k] = __ffma2_rn(m, bn[k], acc[i][k]);
     }
   }
 }
-__device__ __forceinline__ void cmacc_tile4(float2 (&acc)[4][4], const float2 (&a)[4], const float2 (&b)[4]) {
-  float2 as[4];   // -i a
+template <int TI>
+__device__ __forceinline__ void cmacc_tile(float2 (&acc)[TI][TI], const float2 (&a)[TI], const float2 (&b)[TI]) {
+  float2 as[TI];   // -i a
 #pragma unroll
-  for (int i = 0; i < 4; ++i) as[i] = make_float2(a[i].y, -a[i].x);
+  for (int i = 0; i < TI; ++i) as[i] = make_float2(a[i].y, -a[i].x);
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < TI; ++k) {
     const float2 r = make_float2(b[k].x, b[k].x), m = make_float2(b[k].y, b[k].y);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < TI; ++i) {
       acc[i][k] = __ffma2_rn(r, a[i], acc[i][k]);
       acc[i][k] = __ffma2_rn(m, as[i], acc[i][k]);
     }
@@ -175,68 +177,106 @@ __device__ void wide_symmetrize(const Tile& t, int q0, int nq1, int nb, void* Tv
 // move as two 16-byte accesses, a row of W as one.
 __device__ __forceinline__ float4 ld4(const float2* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ float4 ldg4(const float2* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+// TI complex values from a 16-byte aligned address, through L1 (G) or shared memory
+template <int TI, bool G>
+__device__ __forceinline__ void ldc(float2 (&v)[TI], const float2* p) {
+#pragma unroll
+  for (int j = 0; j < TI; j += 2) {
+    const float4 x = G ? ldg4(p + j) : ld4(p + j);
+    v[j] = make_float2(x.x, x.y);
+    v[j + 1] = make_float2(x.z, x.w);
+  }
+}
+// stage-2 tile: X(b10 + i, c0 + k) = sum_a e1(a, b10 + i) T(a, c0 + k); e1 = U + q1 nbb + b10,
+// Tq = T plane + c0, Xq = X plane + b10 ldx + c0
+template <int TI>
+__device__ __forceinline__ void f4_x_tile(const float2* __restrict__ e1, const float2* Tq, float2* Xq, int nb,
+                                          int ldx) {
+  float2 acc[TI][TI];
+#pragma unroll
+  for (int i = 0; i < TI; ++i)
+#pragma unroll
+    for (int k = 0; k < TI; ++k) acc[i][k] = make_float2(0.f, 0.f);
+#pragma unroll 2
+  for (int a = 0; a < nb; ++a) {
+    float2 ev[TI], tv[TI];
+    ldc<TI, true>(ev, e1 + a * nb);
+    ldc<TI, false>(tv, Tq + a * nb);
+    cmac_tile<TI>(acc, ev, tv);
+  }
+#pragma unroll
+  for (int i = 0; i < TI; ++i)
+#pragma unroll
+    for (int k = 0; k < TI; ++k) Xq[i * ldx + k] = acc[i][k];
+}
+// stage-3 tile: W(b10 + i, b30 + k) = |sum_c X(b10 + i, c) conj(e3(c, b30 + k))|^2; e3 = U + q3 nbb
+// + b30, Xq = X plane + b10 ldx, Wq = W plane + b10 nb + b30
+template <int TI>
+__device__ __forceinline__ void f4_w_tile(const float2* __restrict__ e3, const float2* Xq, float* Wq, int nb,
+                                          int ldx) {
+  float2 acc[TI][TI];
+#pragma unroll
+  for (int i = 0; i < TI; ++i)
+#pragma unroll
+    for (int k = 0; k < TI; ++k) acc[i][k] = make_float2(0.f, 0.f);
+#pragma unroll 2
+  for (int c = 0; c < nb; ++c) {
+    float2 xv[TI], ev[TI];
+#pragma unroll
+    for (int i = 0; i < TI; ++i) xv[i] = Xq[i * ldx + c];
+    ldc<TI, true>(ev, e3 + c * nb);
+    cmacc_tile<TI>(acc, xv, ev);
+  }
+#pragma unroll
+  for (int i = 0; i < TI; ++i) {
+    float w[TI];
+#pragma unroll
+    for (int k = 0; k < TI; ++k) w[k] = acc[i][k].x * acc[i][k].x + acc[i][k].y * acc[i][k].y;
+    if constexpr (TI == 4)
+      *reinterpret_cast<float4*>(Wq + i * nb) = make_float4(w[0], w[1], w[2], w[3]);
+    else
+      *reinterpret_cast<float2*>(Wq + i * nb) = make_float2(w[0], w[1]);
+  }
+}
+// Units of both stages: the 4 x 4 tiles of the planes, whole in full rounds
+// over the threads; the tiles of a last, partial round are cut into four 2 x 2
+// tiles, so that no thread has a second 4 x 4 tile while others idle (nb = 36,
+// 8 planes, 512 threads: 648 tiles, at most 24 outputs a thread instead of 32).
+__device__ __forceinline__ int f4_whole_tiles(int units, int nthreads) {
+  return units >= nthreads ? units - units % nthreads : units;
+}
 __device__ void wide_contract_f4(const Tile& t, int q0, int nq1, int nb, const float2* __restrict__ U, float2* T,
                                  float2* X, int ldx, int tid, int nthreads, int bar_id) {
   const int nt = nb / 4, per_q = nt * nt, nbb = nb * nb;
-  for (int u = tid; u < nq1 * per_q; u += nthreads) {
-    const int q = q0 + u / per_q, r = u % per_q, b10 = (r / nt) * 4, c0 = (r % nt) * 4;
+  const int units = nq1 * per_q, whole = f4_whole_tiles(units, nthreads), subs = 4 * (units - whole);
+  for (int v = tid; v < whole + subs; v += nthreads) {
+    const int u = v < whole ? v : whole + (v - whole) / 4, sub = v < whole ? 0 : (v - whole) % 4;
+    const int q = q0 + u / per_q, r = u % per_q;
+    const int b10 = (r / nt) * 4 + (sub >> 1) * 2, c0 = (r % nt) * 4 + (sub & 1) * 2;
     const int q1 = t.q1s[q];
     if (q1 < 0 || !t.inw[q]) continue;
     const float2* e1 = U + (size_t)q1 * nbb + b10;
     const float2* Tq = T + (size_t)q * nbb + c0;
-    float2 acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int k = 0; k < 4; ++k) acc[i][k] = make_float2(0.f, 0.f);
-#pragma unroll 2
-    for (int a = 0; a < nb; ++a) {
-      const float4 e01 = ldg4(e1 + a * nb), e23 = ldg4(e1 + a * nb + 2);
-      const float4 t01 = ld4(Tq + a * nb), t23 = ld4(Tq + a * nb + 2);
-      const float2 ev[4] = {make_float2(e01.x, e01.y), make_float2(e01.z, e01.w), make_float2(e23.x, e23.y),
-                            make_float2(e23.z, e23.w)};
-      const float2 tv[4] = {make_float2(t01.x, t01.y), make_float2(t01.z, t01.w), make_float2(t23.x, t23.y),
-                            make_float2(t23.z, t23.w)};
-      cmac_tile4(acc, ev, tv);
-    }
-    float2* Xq = X + (size_t)(q - q0) * nb * ldx + c0;
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int k = 0; k < 4; ++k) Xq[(b10 + i) * ldx + k] = acc[i][k];
+    float2* Xq = X + (size_t)(q - q0) * nb * ldx + (size_t)b10 * ldx + c0;
+    if (v < whole)
+      f4_x_tile<4>(e1, Tq, Xq, nb, ldx);
+    else
+      f4_x_tile<2>(e1, Tq, Xq, nb, ldx);
   }
   asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
   float* W = reinterpret_cast<float*>(T);
-  for (int u = tid; u < nq1 * per_q; u += nthreads) {
-    const int q = q0 + u / per_q, r = u % per_q, b10 = (r / nt) * 4, b30 = (r % nt) * 4;
+  for (int v = tid; v < whole + subs; v += nthreads) {
+    const int u = v < whole ? v : whole + (v - whole) / 4, sub = v < whole ? 0 : (v - whole) % 4;
+    const int q = q0 + u / per_q, r = u % per_q;
+    const int b10 = (r / nt) * 4 + (sub >> 1) * 2, b30 = (r % nt) * 4 + (sub & 1) * 2;
     if (t.q1s[q] < 0 || !t.inw[q]) continue;
     const float2* e3 = U + (size_t)t.q3s[q] * nbb + b30;
     const float2* Xq = X + (size_t)(q - q0) * nb * ldx + (size_t)b10 * ldx;
-    float2 acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int k = 0; k < 4; ++k) acc[i][k] = make_float2(0.f, 0.f);
-#pragma unroll 2
-    for (int c = 0; c < nb; ++c) {
-      float2 xv[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) xv[i] = Xq[i * ldx + c];
-      const float4 e01 = ldg4(e3 + c * nb), e23 = ldg4(e3 + c * nb + 2);
-      const float2 ev[4] = {make_float2(e01.x, e01.y), make_float2(e01.z, e01.w), make_float2(e23.x, e23.y),
-                            make_float2(e23.z, e23.w)};
-      cmacc_tile4(acc, xv, ev);
-    }
-    float* Wq = W + (size_t)q * nbb + b30;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      float4 w;
-      w.x = acc[i][0].x * acc[i][0].x + acc[i][0].y * acc[i][0].y;
-      w.y = acc[i][1].x * acc[i][1].x + acc[i][1].y * acc[i][1].y;
-      w.z = acc[i][2].x * acc[i][2].x + acc[i][2].y * acc[i][2].y;
-      w.w = acc[i][3].x * acc[i][3].x + acc[i][3].y * acc[i][3].y;
-      *reinterpret_cast<float4*>(Wq + (b10 + i) * nb) = w;
-    }
+    float* Wq = W + (size_t)q * nbb + (size_t)b10 * nb + b30;
+    if (v < whole)
+      f4_w_tile<4>(e3, Xq, Wq, nb, ldx);
+    else
+      f4_w_tile<2>(e3, Xq, Wq, nb, ldx);
   }
   wide_symmetrize<float>(t, q0, nq1, nb, T, tid, nthreads, bar_id);
 }

@@ -110,8 +110,6 @@ __device__ __forceinline__ void cmacc_tile(float2 (&acc)[TI][TI], const float2 (
 template <class C> __device__ __forceinline__ C czero();
 template <> __device__ __forceinline__ double2 czero<double2>() { return make_double2(0.0, 0.0); }
 template <> __device__ __forceinline__ float2 czero<float2>() { return make_float2(0.f, 0.f); }
-__device__ __forceinline__ double2 ld_eig(const double2* U, size_t i) { return __ldg(U + i); }
-__device__ __forceinline__ float2 ld_eig(const float2* U, size_t i) { return __ldg(U + i); }
 
 // Per-item state of the tile in shared memory (both kernels).
 struct Tile {
@@ -387,19 +385,64 @@ __device__ inline int wide_rate_segments(int nq1, int nb, int nthreads) {
   return best;
 }
 
+// Adaptive delta (delta_function.cpp:65-96) from a tabulated width: sigma,
+// its reciprocal and whether the velocity difference is exactly zero.
+// exp(-x^2) / (sqrt(pi) sigma erf(2)) with x = e / sigma as products.
+__device__ __forceinline__ double delta_tab(double sigma, double inv, bool vz, double e) {
+  if (vz && e == 0.0) return 1.0;
+  if (sigma == 0.0) return 0.0;
+  if (fabs(e) > 2.0 * sigma) return 0.0;
+  const double x = e * inv;   // |x| <= 2 past the cut-off
+  return exp(-x * x) * inv * (1.0 / (phxc::sqrtPi * phxc::erf2));
+}
+
 // Rates of the b2 plane (ph_scattering.cpp:338-380, 466-518), FP64, with the
 // rate factors averaged over the degenerate block of b2: "+" of (q1, q2) and
 // "-" of (q1, -q2).  Units (segment of b3, q1, b1), segs segments per row
 // (wide_rate_segments); one shared-memory atomic per unit and temperature.
 // W scaled by wscale (split FP16 operands).
+//   With adaptive smearing the widths of the pairs (q3 b3, q2 c2) and
+// (q3 b3, -q2 c2), which every b1 of a plane shares, are tabulated first in
+// `sig` (sig_bytes of shared memory that is free during this phase: the X
+// slab), as (sigma, 1/sigma) with the zero-velocity flag in the sign bit of
+// sigma; a block of b2 too large for the table computes them per cell.
+// Called by all nthreads threads of named barrier bar_id.
 template <class R>
 __device__ void wide_rates(const Tile& t, const MeshArgs& M, int nq1, int b2, int iq2, int iq2m, const R* W,
-                           double wscale, int segs, int tid, int nthreads) {
+                           double wscale, int segs, double* sig, size_t sig_bytes, int tid, int nthreads,
+                           int bar_id) {
   const int nb = M.nb, nbb = nb * nb, nT = M.nT, nq = M.nq;
   const int seg = (nb + segs - 1) / segs;
   const int* g2 = t.g2s;
-  const int s0 = g2[b2], s1 = wide_block_end(g2, nb, s0);
-  const double inv2 = 1.0 / (double)(s1 - s0);
+  const int s0 = g2[b2], s1 = wide_block_end(g2, nb, s0), nblk = s1 - s0;
+  const double inv2 = 1.0 / (double)nblk;
+  const bool adaptive = M.smearing == PHX_SMEAR_ADAPTIVE;
+  const bool tab = adaptive && sizeof(double) * 4 * (size_t)nq1 * nb * nblk <= sig_bytes;
+  auto widths = [&](int iq3, int b3, int c2, double& sp, bool& vzp, double& sm, bool& vzm) {
+    const double* v3 = M.vg + ((size_t)iq3 * nb + b3) * 3;
+    const double* v2 = M.vg + ((size_t)iq2 * nb + c2) * 3;
+    const double* v2m = M.vg + ((size_t)iq2m * nb + c2) * 3;
+    const double dp0 = v2[0] - v3[0], dp1 = v2[1] - v3[1], dp2 = v2[2] - v3[2];
+    const double dm0 = v2m[0] - v3[0], dm1 = v2m[1] - v3[1], dm2 = v2m[2] - v3[2];
+    vzp = (dp0 * dp0 + dp1 * dp1 + dp2 * dp2) == 0.0;
+    vzm = (dm0 * dm0 + dm1 * dm1 + dm2 * dm2) == 0.0;
+    sp = floor_sigma(adaptive_sigma(M.qT, dp0, dp1, dp2));
+    sm = floor_sigma(adaptive_sigma(M.qT, dm0, dm1, dm2));
+  };
+  if (tab) {
+    for (int e = tid; e < nq1 * nb * nblk; e += nthreads) {
+      const int q = e / (nb * nblk), b3 = (e / nblk) % nb, c2 = s0 + e % nblk;
+      if (t.q1s[q] < 0 || !t.inw[q]) continue;
+      double sp, sm;
+      bool vzp, vzm;
+      widths(t.q3s[q], b3, c2, sp, vzp, sm, vzm);
+      sig[4 * e] = vzp ? -0.0 : sp;   // zero width when the velocities agree
+      sig[4 * e + 1] = sp > 0.0 ? 1.0 / sp : 0.0;
+      sig[4 * e + 2] = vzm ? -0.0 : sm;
+      sig[4 * e + 3] = sm > 0.0 ? 1.0 / sm : 0.0;
+    }
+    asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
+  }
   for (int u = tid; u < segs * nq1 * nb; u += nthreads) {
     const int sg = u / (nq1 * nb), rest = u % (nq1 * nb), q = rest / nb, b1 = rest % nb;
     const int q1 = t.q1s[q];
@@ -416,55 +459,55 @@ __device__ void wide_rates(const Tile& t, const MeshArgs& M, int nq1, int b2, in
       if (w == 0.0) continue;
       const double en3 = M.E[(size_t)iq3 * nb + b3];
       if (en3 < phxc::phEnergyCutoff) continue;
+      const double* sg4 = sig + (size_t)(q * nb + b3) * nblk * 4;
       for (int c2 = s0; c2 < s1; ++c2) {
         const double en2 = M.E[(size_t)iq2 * nb + c2];
         const double en2m = M.E[(size_t)iq2m * nb + c2];
         const bool ok2 = (t.inw[q] & 1) && en2 >= phxc::phExcludeCutoff && en2 >= phxc::phEnergyCutoff;
         const bool ok2m = (t.inw[q] & 2) && en2m >= phxc::phExcludeCutoff && en2m >= phxc::phEnergyCutoff;
         if (!ok2 && !ok2m) continue;
-        double sp = M.sigma, sm = M.sigma;
-        bool vzp = false, vzm = false;
-        if (M.smearing == PHX_SMEAR_ADAPTIVE) {
-          const double* v3 = M.vg + ((size_t)iq3 * nb + b3) * 3;
-          const double* v2 = M.vg + ((size_t)iq2 * nb + c2) * 3;
-          const double* v2m = M.vg + ((size_t)iq2m * nb + c2) * 3;
-          const double dp0 = v2[0] - v3[0], dp1 = v2[1] - v3[1], dp2 = v2[2] - v3[2];
-          const double dm0 = v2m[0] - v3[0], dm1 = v2m[1] - v3[1], dm2 = v2m[2] - v3[2];
-          vzp = (dp0 * dp0 + dp1 * dp1 + dp2 * dp2) == 0.0;
-          vzm = (dm0 * dm0 + dm1 * dm1 + dm2 * dm2) == 0.0;
-          sp = floor_sigma(adaptive_sigma(M.qT, dp0, dp1, dp2));
-          sm = floor_sigma(adaptive_sigma(M.qT, dm0, dm1, dm2));
-        }
-        if (ok2) {
-          const double dlt = delta_fn(M.smearing, sp, en1 + en2 - en3, vzp);
-          if (dlt > 0.0) {
-            const double f = phxc::pi * 0.25 * w * dlt * M.norm / (en1 * en2 * en3) * inv2;
-#pragma unroll
-            for (int c = 0; c < kMaxT; ++c)
-              if (c < nT) {
-                const double n1 = M.bose[((size_t)c * nq + q1) * nb + b1];
-                const double n2 = M.bose[((size_t)c * nq + iq2) * nb + c2];
-                const double n3 = M.bose[((size_t)c * nq + iq3) * nb + b3];
-                r[c] += 0.5 * (f * n1 * n2 * (n3 + 1.0));
-              }
+        double dlt = 0.0, d1 = 0.0, d2 = 0.0;
+        if (tab) {
+          const double* e4 = sg4 + (c2 - s0) * 4;
+          const double sp = e4[0], ip = e4[1], sm = e4[2], im = e4[3];
+          if (ok2) dlt = delta_tab(fabs(sp), ip, signbit(sp), en1 + en2 - en3);
+          if (ok2m) {
+            d1 = delta_tab(fabs(sm), im, signbit(sm), en1 + en3 - en2m);
+            d2 = delta_tab(fabs(sm), im, signbit(sm), en2m + en3 - en1);
+          }
+        } else {
+          double sp = M.sigma, sm = M.sigma;
+          bool vzp = false, vzm = false;
+          if (adaptive) widths(iq3, b3, c2, sp, vzp, sm, vzm);
+          if (ok2) dlt = delta_fn(M.smearing, sp, en1 + en2 - en3, vzp);
+          if (ok2m) {
+            d1 = delta_fn(M.smearing, sm, en1 + en3 - en2m, vzm);
+            d2 = delta_fn(M.smearing, sm, en2m + en3 - en1, vzm);
           }
         }
-        if (ok2m) {
-          double d1 = delta_fn(M.smearing, sm, en1 + en3 - en2m, vzm);
-          double d2 = delta_fn(M.smearing, sm, en2m + en3 - en1, vzm);
-          if (d1 > 0.0 || d2 > 0.0) {
-            d1 = fmax(d1, 0.0);
-            d2 = fmax(d2, 0.0);
-            const double f = phxc::pi * 0.25 * w * M.norm / (en1 * en2m * en3) * inv2;
+        if (ok2 && dlt > 0.0) {
+          const double f = phxc::pi * 0.25 * w * dlt * M.norm / (en1 * en2 * en3) * inv2;
 #pragma unroll
-            for (int c = 0; c < kMaxT; ++c)
-              if (c < nT) {
-                const double n1 = M.bose[((size_t)c * nq + q1) * nb + b1];
-                const double n2m = M.bose[((size_t)c * nq + iq2m) * nb + c2];
-                const double n3 = M.bose[((size_t)c * nq + iq3) * nb + b3];
-                r[c] += 0.5 * (f * n3 * n1 * (n2m + 1.0) * d1 + f * n2m * n3 * (n1 + 1.0) * d2);
-              }
-          }
+          for (int c = 0; c < kMaxT; ++c)
+            if (c < nT) {
+              const double n1 = M.bose[((size_t)c * nq + q1) * nb + b1];
+              const double n2 = M.bose[((size_t)c * nq + iq2) * nb + c2];
+              const double n3 = M.bose[((size_t)c * nq + iq3) * nb + b3];
+              r[c] += 0.5 * (f * n1 * n2 * (n3 + 1.0));
+            }
+        }
+        if (ok2m && (d1 > 0.0 || d2 > 0.0)) {
+          d1 = fmax(d1, 0.0);
+          d2 = fmax(d2, 0.0);
+          const double f = phxc::pi * 0.25 * w * M.norm / (en1 * en2m * en3) * inv2;
+#pragma unroll
+          for (int c = 0; c < kMaxT; ++c)
+            if (c < nT) {
+              const double n1 = M.bose[((size_t)c * nq + q1) * nb + b1];
+              const double n2m = M.bose[((size_t)c * nq + iq2m) * nb + c2];
+              const double n3 = M.bose[((size_t)c * nq + iq3) * nb + b3];
+              r[c] += 0.5 * (f * n3 * n1 * (n2m + 1.0) * d1 + f * n2m * n3 * (n1 + 1.0) * d2);
+            }
         }
       }
     }
@@ -474,7 +517,6 @@ __device__ void wide_rates(const Tile& t, const MeshArgs& M, int nq1, int b2, in
   }
 }
 
-// Loads the tile of the current item: q1, q3, window flags, blocks; returns
 // Loads the tile of the current item: q1, q3, window flags, blocks; returns
 // (block-uniform, after a barrier) whether any q1 of the tile pairs with q2 or -q2.
 __device__ bool wide_load_tile(const Tile& t, const WideArgs& P, int tile, int iq2, int iq2m, int tid,
@@ -605,8 +647,9 @@ __global__ void __launch_bounds__(kWideThreads) wide_fp64_kernel(WideArgs P) {
       __syncthreads();
       wide_contract<double, double2, RT>(t, 0, NQ1, nb, M.U, nullptr, nullptr, T, X, wide_ldx(nb), tid, kWideThreads,
                                          1);
-      wide_rates<double>(t, M, NQ1, b2, iq2, iq2m, reinterpret_cast<const double*>(T), 1.0, segs, tid,
-                         kWideThreads);
+      wide_rates<double>(t, M, NQ1, b2, iq2, iq2m, reinterpret_cast<const double*>(T), 1.0, segs,
+                         reinterpret_cast<double*>(X), sizeof(double2) * (size_t)NQ1 * nb * wide_ldx(nb), tid,
+                         kWideThreads, 0);
       __syncthreads();
     }
     wide_flush(t, P, tid, kWideThreads);
@@ -776,9 +819,6 @@ __host__ __device__ inline size_t split_offsets_qp(int nb, int Kp, int qp, size_
   o[5] = x; x += sizeof(uint64_t) * 32;                            // barriers
   o[6] = x; x += sizeof(int) * (kItemSlots + 4 + 4);               // items, ctl, tslot, abort
   return x;
-}
-__host__ __device__ inline size_t split_offsets(int nb, int Kp, size_t* o) {
-  return split_offsets_qp(nb, Kp, split_qp(nb, Kp), o);
 }
 __device__ inline SplitSmem carve_split(uint8_t* base, int nb, int Kp, int qp) {
   size_t o[8];
@@ -1058,7 +1098,9 @@ __global__ void __launch_bounds__(kSplitThreads, 1) wide_split_kernel(WideArgs P
         if (tid == 0) tc::mbar_arrive(&tfree[buf]);
         for (int q0 = 0; q0 < kWideQ1; q0 += qp)
           wide_contract<float, float2, RT>(t, q0, qp, nb, P.U32, nullptr, nullptr, S.T, S.X, wide_ldx(nb), tid, nth, 1);
-        wide_rates<float>(t, M, kWideQ1, b2, iq2, iq2m, reinterpret_cast<const float*>(S.T), wscale, segs, tid, nth);
+        wide_rates<float>(t, M, kWideQ1, b2, iq2, iq2m, reinterpret_cast<const float*>(S.T), wscale, segs,
+                          reinterpret_cast<double*>(S.X), sizeof(float2) * (size_t)qp * nb * wide_ldx(nb), tid, nth,
+                          1);
         asm volatile("bar.sync 1, %0;" ::"r"(nth) : "memory");
       }
       if (!ok) break;

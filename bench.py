@@ -39,7 +39,7 @@ FP64_PEAK_TFLOPS = 37.0
 # mesh, q2 per launch, slots) of the launch plan; None where not captured
 PAIR_TRAFFIC_BYTES = {("split_bf16", 20, 448, 7): 87476992 + 5594112,
                       ("split_bf16", 20, 1792, 28): 337188096 + 29478400,
-                      ("split_fp16", 20, 1792, 28): 339723264 + 160762368,
+                      ("split_fp16", 20, 1792, 28): 339046144 + 134754304,
                       ("split_bf16", 16, 448, 7): 85.2e6}
 
 

@@ -360,22 +360,24 @@ __device__ __forceinline__ ElWidth el_width(const ElArgs& A, const double v[3]) 
   return w;
 }
 
+
+// Delta of the reference (delta_function.cpp:65-96) from a tabulated width:
+// w.x the floored sigma with the zero-velocity flag in its sign bit, w.y its
+// reciprocal (adaptive), or the fixed Gaussian width's reciprocal ginv; the
+// quotients e / sigma and 1 / (sqrt(pi) sigma erf(2)) become products.
 template <int SM>
-__device__ __forceinline__ double el_delta(const ElArgs& A, double e, const ElWidth& w) {
+__device__ __forceinline__ double el_delta_tab(double ginv, double e, double2 w) {
   if constexpr (SM == PHX_SMEAR_GAUSSIAN) {
-    const double x = e / A.sigma;
+    const double x = e * ginv;
     if (x > 6.0) return 0.0;
-    return 1.0 / A.sigma / phxc::sqrtPi * exp(-x * x);
+    return ginv * (1.0 / phxc::sqrtPi) * exp(-x * x);
   }
-  // delta_function.cpp:65-96
-  if (w.vzero && e == 0.0) return 1.0;
-  double sg = w.sg;
+  const double sg = fabs(w.x);
+  if (signbit(w.x) && e == 0.0) return 1.0;
   if (sg == 0.0) return 0.0;
-  if (sg < phxc::adaptiveCutoff) sg = phxc::adaptiveCutoff;
   if (fabs(e) > 2.0 * sg) return 0.0;
-  const double x = e / sg;
-  if (x > 6.0) return 0.0;
-  return exp(-x * x) / phxc::sqrtPi / sg / phxc::erf2;
+  const double x = e * w.y;   // |x| <= 2 past the cut-off
+  return exp(-x * x) * w.y * (1.0 / (phxc::sqrtPi * phxc::erf2));
 }
 
 // G3IN: g3 from the tensor-core GEMM (split path); SM: the smearing.  Each
@@ -480,7 +482,8 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
     }
     s.n3[(q * kMaxPh + nu) * pairc::kMaxT + t] = n;
   }
-  // adaptive widths of the (b1, b2) pairs (delta_function.cpp:65-88)
+  // adaptive widths of the (b1, b2) pairs (delta_function.cpp:65-88), floored,
+  // as (sigma, 1/sigma) with the zero-velocity flag in the sign bit of sigma
   for (int x = tid; x < (SM == PHX_SMEAR_ADAPTIVE ? kQT * kMaxW * kMaxW : 0); x += NT) {
     const int b2 = x % kMaxW, b1 = (x / kMaxW) % kMaxW, q = x / (kMaxW * kMaxW);
     double2 wv = make_double2(0.0, 0.0);
@@ -490,7 +493,9 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
       for (int c = 0; c < 3; ++c)
         v[c] = A.vk[((size_t)ik1 * nw + lo1 + b1) * 3 + c] - A.vk[((size_t)ik2 * nw + A.lo[ik2] + b2) * 3 + c];
       const ElWidth w = el_width(A, v);
-      wv = make_double2(w.sg, w.vzero ? 1.0 : 0.0);
+      double sg = w.sg;
+      if (sg != 0.0 && sg < phxc::adaptiveCutoff) sg = phxc::adaptiveCutoff;
+      wv = make_double2(w.vzero ? -0.0 : sg, sg > 0.0 ? 1.0 / sg : 0.0);
     }
     s.wd[x] = wv;
   }
@@ -503,6 +508,7 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
   // thread adds its own
   const int per_b1 = kQT * kMaxW * nph;
   const bool warp_sums = per_b1 % 32 == 0;
+  const double ginv = SM == PHX_SMEAR_GAUSSIAN ? 1.0 / A.sigma : 0.0;
   for (int x = tid; x < nb1 * per_b1; x += NT) {
     const int nu = x % nph, b2 = (x / nph) % kMaxW, q = (x / (nph * kMaxW)) % kQT, b1 = x / per_b1;
     double r[pairc::kMaxT];
@@ -511,18 +517,17 @@ __global__ void __launch_bounds__(kPairThreads) el_pair_kernel(ElArgs A) {
     const double en3 = s.E3[q * nph + nu];
     if (s.info[4 * q] && b2 < s.info[4 * q + 1] && en3 >= phxc::elPhononCutoff) {
       const double en1 = E1[b1], en2 = s.E2[q * kMaxW + b2];
-      const double2 wv = s.wd[(q * kMaxW + b1) * kMaxW + b2];
-      const ElWidth w{wv.x, wv.y != 0.0};
-      const double d1 = el_delta<SM>(A, en1 - en2 + en3, w);
-      const double d2 = el_delta<SM>(A, en1 - en2 - en3, w);
+      const double2 wv = SM == PHX_SMEAR_ADAPTIVE ? s.wd[(q * kMaxW + b1) * kMaxW + b2] : make_double2(0.0, 0.0);
+      const double d1 = el_delta_tab<SM>(ginv, en1 - en2 + en3, wv);
+      const double d2 = el_delta_tab<SM>(ginv, en1 - en2 - en3, wv);
       if (d1 > 0.0 || d2 > 0.0) {
-        const double c = s.cs[((q * kMaxW + b1) * kMaxW + b2) * nph + nu];
+        const double c = s.cs[((q * kMaxW + b1) * kMaxW + b2) * nph + nu] * A.norm * phxc::pi / en3;
 #pragma unroll
         for (int t = 0; t < pairc::kMaxT; ++t) {
           if (t < A.nT) {
             const double fermi2 = s.f2[(q * kMaxW + b2) * pairc::kMaxT + t];
             const double bose3 = s.n3[(q * kMaxPh + nu) * pairc::kMaxT + t];
-            r[t] = c * ((fermi2 + bose3) * d1 + (1.0 - fermi2 + bose3) * d2) * A.norm / en3 * phxc::pi;
+            r[t] = c * ((fermi2 + bose3) * d1 + (1.0 - fermi2 + bose3) * d2);
           }
         }
       }

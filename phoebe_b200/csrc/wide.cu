@@ -387,13 +387,17 @@ __device__ inline int wide_rate_segments(int nq1, int nb, int nthreads) {
 
 // Adaptive delta (delta_function.cpp:65-96) from a tabulated width: sigma,
 // its reciprocal and whether the velocity difference is exactly zero.
-// exp(-x^2) / (sqrt(pi) sigma erf(2)) with x = e / sigma as products.
+// exp(-x^2) / (sqrt(pi) sigma erf(2)) with x = e / sigma as products.  The
+// cut-off decisions stay FP64; F32EXP evaluates the Gaussian itself in FP32
+// (relative error ~1e-7, for the split path, whose |V|^2 carries ~1e-6).
+template <bool F32EXP>
 __device__ __forceinline__ double delta_tab(double sigma, double inv, bool vz, double e) {
   if (vz && e == 0.0) return 1.0;
   if (sigma == 0.0) return 0.0;
   if (fabs(e) > 2.0 * sigma) return 0.0;
   const double x = e * inv;   // |x| <= 2 past the cut-off
-  return exp(-x * x) * inv * (1.0 / (phxc::sqrtPi * phxc::erf2));
+  const double g = F32EXP ? (double)expf((float)(-x * x)) : exp(-x * x);
+  return g * inv * (1.0 / (phxc::sqrtPi * phxc::erf2));
 }
 
 // Rates of the b2 plane (ph_scattering.cpp:338-380, 466-518), FP64, with the
@@ -470,10 +474,10 @@ __device__ void wide_rates(const Tile& t, const MeshArgs& M, int nq1, int b2, in
         if (tab) {
           const double* e4 = sg4 + (c2 - s0) * 4;
           const double sp = e4[0], ip = e4[1], sm = e4[2], im = e4[3];
-          if (ok2) dlt = delta_tab(fabs(sp), ip, signbit(sp), en1 + en2 - en3);
+          if (ok2) dlt = delta_tab<sizeof(R) == 4>(fabs(sp), ip, signbit(sp), en1 + en2 - en3);
           if (ok2m) {
-            d1 = delta_tab(fabs(sm), im, signbit(sm), en1 + en3 - en2m);
-            d2 = delta_tab(fabs(sm), im, signbit(sm), en2m + en3 - en1);
+            d1 = delta_tab<sizeof(R) == 4>(fabs(sm), im, signbit(sm), en1 + en3 - en2m);
+            d2 = delta_tab<sizeof(R) == 4>(fabs(sm), im, signbit(sm), en2m + en3 - en1);
           }
         } else {
           double sp = M.sigma, sm = M.sigma;

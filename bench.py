@@ -211,8 +211,18 @@ def cpu_baseline(cr, fc2, fc3, mesh, budget_s, q2_hint=None):
                  "sample_wall_s": t1 + dt}, **host_cpu())
 
 
+def headline_config(n, nr3, precision, world):
+    """The `config` of the headline line (n^3 mesh); the reference arm prints the same."""
+    nq = n ** 3
+    return {"workload": "diamond %dx%dx%d (%d q, %ge6 pairs), 400 FC3 pairs "
+                        "(nr3=%d), adaptive smearing, T=100/300/600 K" % (n, n, n, nq, nq * nq / 1e6, nr3),
+            "precision": precision, "l2": "flushed between steps (256 MB write)",
+            "parallelism": "q2-sliced x%d" % world}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     cr, fc2, fc3, mesh = workload(args.mesh)
@@ -232,8 +242,9 @@ def run_reference(args):
             "ms_per_step": 1000.0 * nq * nq / v, "projected_from_sample": True,
             "sample_wall_s_per_step": b["sample_wall_s"], "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "diamond 20x20x20, 400 FC3 pairs, adaptive smearing, "
-                                   "100/300/600 K (CPU sample per step)"},
+            # the workload of the GPU arm's line; what this arm ran of it per step is
+            # cpu_baseline.sample (a q2 sample of the same FP64 builder, on the host)
+            "config": headline_config(args.mesh, fc3.D3.shape[3], args.precision, world),
             "cpu_baseline": dict(b, value=v),
             "e2e": {"value": v, "unit": "triplets/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -457,10 +468,7 @@ def run_ours(args):
                "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else
                ("bf16x3->f32" if args.precision == "split_bf16" else "fp16x3->f32"),
                "data": "synthetic",
-               "config": {"workload": "diamond 20x20x20 (8000 q, 64e6 pairs), 400 FC3 pairs "
-                                      "(nr3=%d), adaptive smearing, T=100/300/600 K" % nr3,
-                          "precision": args.precision, "l2": "flushed between steps (256 MB write)",
-                          "parallelism": "q2-sliced x%d" % world},
+               "config": headline_config(args.mesh, nr3, args.precision, world),
                "linewidths_per_s": nq * nb * nT / (ms_step / 1000.0),
                "branch_triplets_per_s": value * 2 * nb ** 3,
                "wall_s_timed": wall,
